@@ -1,0 +1,79 @@
+/*
+ * pmf_b200.h -- flat C ABI of the B200 PreMixFEM solver library
+ * (libpremixfem_b200.so).  Plain pointers and sizes only; every function
+ * returns 0 on success or a PETSc-style error code (62 bad argument, 73 wrong
+ * state, 56 unsupported, 71 zero pivot, 76 CUDA/library failure) and leaves a
+ * message for pmf_last_error().
+ *
+ * Arrays are float64, natural order with x fastest (cell id
+ * (ez*N + ey)*M + ex), the DMDA ordering the reference uses.  "on_device"
+ * selects whether array arguments are device (CUDA) or host pointers.
+ *
+ * This ABI is what a foreign-function binding of the reference's solve path
+ * would call (see INTEGRATION.md for the ctypes binding); the PETSc-style
+ * drop-in header PreMixFEM_3D.h is implemented on top of it.  Mapping to the
+ * reference interface (src/PreMixFEM_3D.h of Laphet/PreMixFEM):
+ *   pmf_create        <- PC_init            (src/PreMixFEM_3D.h:47, src/PreMixFEM_3D.c:1650-1741)
+ *   pmf_set_kappa     <- caller fills PCCtx.kappa[3] (src/PreMixFEM_3D.h:34; src/Expe_scal.c:11-42)
+ *   pmf_set_dirichlet <- (extension: Dirichlet faces; the reference is pure Neumann)
+ *   pmf_apply_A       <- MatMult of the matrix built by PC_create_A (src/PreMixFEM_3D.h:55, .c:1757-1824)
+ *   pmf_setup         <- PC_setup / _PC_setup (src/PreMixFEM_3D.h:53, .c:1392-1427, 1826-1838)
+ *   pmf_pc_apply      <- PC_apply_vec       (src/PreMixFEM_3D.h:57, .c:1840-1936)
+ *   pmf_solve         <- KSPSolve with KSPCG + the PCSHELL above (src/Expe_scal.c:100-119)
+ *   pmf_get_stages    <- PCCtx.t_stages / PC_print_stat (src/PreMixFEM_3D.h:42, .c:1954-1999)
+ *   pmf_get_eigen_*   <- PCCtx.eigen_{min,max,num}_lv{1,2} (src/PreMixFEM_3D.h:40-41)
+ *   pmf_destroy       <- PC_final / PC_final_default (src/PreMixFEM_3D.h:63-65, .c:2001-2046)
+ */
+#ifndef PMF_B200_H
+#define PMF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pmf_solver pmf_solver;
+
+/* Options use the reference's PETSc option names: -sd, -en_lv1, -en_lv2,
+ * -eb_lv1, -eb_lv2, -si_lv1, -si_lv2, -eg_op, -use_W_cycle, -no_shift_A_cc,
+ * -ksp_rtol, -ksp_max_it; B200 extensions: -pmf_sd sx,sy,sz (subdomains per
+ * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
+ * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it. */
+int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out);
+int pmf_destroy(pmf_solver* s);
+
+int pmf_set_kappa(pmf_solver* s, const double* kx, const double* ky, const double* kz, int on_device);
+/* face: 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+ */
+int pmf_set_dirichlet(pmf_solver* s, int face, double value);
+int pmf_setup(pmf_solver* s);
+
+/* rhs = source + Dirichlet boundary contributions (needs pmf_setup). */
+int pmf_rhs(pmf_solver* s, const double* source, double* rhs, int on_device);
+int pmf_apply_A(pmf_solver* s, const double* x, double* y, int on_device);
+int pmf_pc_apply(pmf_solver* s, const double* x, double* y, int on_device);
+/* reason: 1 converged, 2 max_it, 3 indefinite, 4 nan/inf */
+int pmf_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason);
+
+/* info[0..11] = ncell_lo32, nsub, nrank, subdomains_per_rank, kmax, nr, en_lv2, n3,
+ *               max_cells, max_lines, precision, is_setup */
+int pmf_get_info(pmf_solver* s, int info[12]);
+int pmf_get_eigen_lv1(pmf_solver* s, double* evals, int* ks, int* iters, int* status);
+int pmf_get_eigen_lv2(pmf_solver* s, double* evals, int* ks, int* iters);
+/* subdomain boxes: 6 ints per subdomain (x0, nx, y0, ny, z0, nz) and its rank */
+int pmf_get_subdomains(pmf_solver* s, int* boxes, int* ranks);
+/* basis Phi, ncell * kmax values (cell-major), converted to float64 */
+int pmf_get_phi(pmf_solver* s, double* out);
+/* Galerkin blocks, nsub * 7 * kmax * kmax (diagonal, x-, x+, y-, y+, z-, z+) */
+int pmf_get_coarse_blocks(pmf_solver* s, double* out);
+/* t[10]: su_lv1, su_lv2_1, su_lv2_2, su_lv3_1, su_lv3_2, av_lv1, av_lv2, av_lv3, su, av (seconds) */
+int pmf_get_stages(pmf_solver* s, double t[10]);
+/* last setup and solve time measured with CUDA events on the solver stream (ms) */
+int pmf_get_timing(pmf_solver* s, double* setup_ms, double* solve_ms);
+
+const char* pmf_last_error(void);
+int pmf_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,209 @@
+// Flat C ABI (include/pmf_b200.h) over pmf::Solver.
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "../../include/pmf_b200.h"
+#include "solver.h"
+
+struct pmf_solver {
+  pmf::Solver* s;
+};
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  fprintf(stderr, "[premixfem_b200] error %d: %s\n", code, msg.c_str());
+  return code;
+}
+static int wrap(pmf_solver* h, int code) {
+  if (code) return fail(code, h->s->err);
+  return 0;
+}
+
+#define PMF_CHECK_HANDLE(h)                                        \
+  do {                                                             \
+    if (!(h) || !(h)->s) return fail(62, "null solver handle");    \
+  } while (0)
+
+extern "C" {
+
+int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out) {
+  if (!dom || !mesh || !out) return fail(62, "null argument to pmf_create");
+  // PC_init argument checks (src/PreMixFEM_3D.c:1653-1654)
+  if (!(dom[0] > 0.0 && dom[1] > 0.0 && dom[2] > 0.0)) return fail(62, "Errors in dom(L, W, H)");
+  if (!(mesh[0] > 0 && mesh[1] > 0 && mesh[2] > 0)) return fail(62, "Errors in mesh(M, N, P)");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(76, "no CUDA device available");
+  pmf::OptionDB db;
+  db.parse(options ? options : "");
+  pmf::Options o;
+  std::string err;
+  if (int e = pmf::options_from_db(db, &o, &err)) return fail(e, err);
+  try {
+    pmf_solver* h = new pmf_solver;
+    h->s = new pmf::Solver(dom, mesh, o);
+    *out = h;
+  } catch (const std::exception& ex) {
+    return fail(76, ex.what());
+  }
+  return 0;
+}
+
+int pmf_destroy(pmf_solver* h) {
+  if (!h) return 0;
+  delete h->s;
+  delete h;
+  return 0;
+}
+
+int pmf_set_kappa(pmf_solver* h, const double* kx, const double* ky, const double* kz, int on_device) {
+  PMF_CHECK_HANDLE(h);
+  if (!kx) return fail(62, "kappa[0] is null");
+  return wrap(h, h->s->set_kappa(kx, ky, kz, on_device != 0));
+}
+
+int pmf_set_dirichlet(pmf_solver* h, int face, double value) {
+  PMF_CHECK_HANDLE(h);
+  return wrap(h, h->s->set_dirichlet(face, value));
+}
+
+int pmf_setup(pmf_solver* h) {
+  PMF_CHECK_HANDLE(h);
+  return wrap(h, h->s->setup());
+}
+
+int pmf_rhs(pmf_solver* h, const double* source, double* rhs, int on_device) {
+  PMF_CHECK_HANDLE(h);
+  if (!source || !rhs) return fail(62, "null vector");
+  return wrap(h, h->s->rhs(source, rhs, on_device != 0));
+}
+
+int pmf_apply_A(pmf_solver* h, const double* x, double* y, int on_device) {
+  PMF_CHECK_HANDLE(h);
+  if (!x || !y) return fail(62, "null vector");
+  return wrap(h, h->s->apply_A(x, y, on_device != 0));
+}
+
+int pmf_pc_apply(pmf_solver* h, const double* x, double* y, int on_device) {
+  PMF_CHECK_HANDLE(h);
+  if (!x || !y) return fail(62, "null vector");
+  return wrap(h, h->s->pc_apply(x, y, on_device != 0));
+}
+
+int pmf_solve(pmf_solver* h, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason) {
+  PMF_CHECK_HANDLE(h);
+  if (!b || !x) return fail(62, "null vector");
+  return wrap(h, h->s->solve(b, x, on_device != 0, its, rnorm, reason));
+}
+
+int pmf_get_info(pmf_solver* h, int info[12]) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  info[0] = (int)s.g.ncell;
+  info[1] = s.nsub;
+  info[2] = s.nrank;
+  info[3] = s.spr;
+  info[4] = s.kmax;
+  info[5] = s.nr;
+  info[6] = s.en2;
+  info[7] = s.n3;
+  info[8] = s.max_cells;
+  info[9] = s.max_lines;
+  info[10] = s.opt.precision;
+  info[11] = s.is_setup ? 1 : 0;
+  return 0;
+}
+
+int pmf_get_eigen_lv1(pmf_solver* h, double* evals, int* ks, int* iters, int* status) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (!s.is_setup) return fail(73, "setup not done");
+  if (evals) memcpy(evals, s.eig1.data(), sizeof(double) * s.eig1.size());
+  if (ks) memcpy(ks, s.ks.data(), sizeof(int) * s.ks.size());
+  if (iters) memcpy(iters, s.eig_iters.data(), sizeof(int) * s.eig_iters.size());
+  if (status) memcpy(status, s.eig_status.data(), sizeof(int) * s.eig_status.size());
+  return 0;
+}
+
+int pmf_get_eigen_lv2(pmf_solver* h, double* evals, int* ks, int* iters) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (!s.is_setup) return fail(73, "setup not done");
+  if (evals) memcpy(evals, s.eig3.data(), sizeof(double) * s.eig3.size());
+  if (ks) memcpy(ks, s.ks3.data(), sizeof(int) * s.ks3.size());
+  if (iters) memcpy(iters, s.l3_iters.data(), sizeof(int) * s.l3_iters.size());
+  return 0;
+}
+
+int pmf_get_subdomains(pmf_solver* h, int* boxes, int* ranks) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (s.subs.empty()) return fail(73, "partition not built (set kappa first)");
+  for (int i = 0; i < s.nsub; ++i) {
+    const pmf::SubInfo& S = s.subs[i];
+    if (boxes) {
+      int* b = boxes + 6 * i;
+      b[0] = S.x0;
+      b[1] = S.nx;
+      b[2] = S.y0;
+      b[3] = S.ny;
+      b[4] = S.z0;
+      b[5] = S.nz;
+    }
+    if (ranks) ranks[i] = S.rank;
+  }
+  return 0;
+}
+
+int pmf_get_phi(pmf_solver* h, double* out) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (!s.is_setup) return fail(73, "setup not done");
+  const size_t n = (size_t)s.g.ncell * s.kmax;
+  if (s.opt.precision == 1) {
+    double* tmp = nullptr;
+    if (cudaMalloc(&tmp, n * 8) != cudaSuccess) return fail(76, "cudaMalloc");
+    pmf::launch_to_f64((const float*)s.phi, tmp, (long long)n, s.st);
+    cudaMemcpyAsync(out, tmp, n * 8, cudaMemcpyDeviceToHost, s.st);
+    cudaStreamSynchronize(s.st);
+    cudaFree(tmp);
+  } else {
+    cudaMemcpyAsync(out, s.phi, n * 8, cudaMemcpyDeviceToHost, s.st);
+    cudaStreamSynchronize(s.st);
+  }
+  return 0;
+}
+
+int pmf_get_coarse_blocks(pmf_solver* h, double* out) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (!s.is_setup) return fail(73, "setup not done");
+  cudaMemcpy(out, s.blk, sizeof(double) * s.nsub * 7 * s.kmax * s.kmax, cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+int pmf_get_stages(pmf_solver* h, double t[10]) {
+  PMF_CHECK_HANDLE(h);
+  for (int i = 0; i < 10; ++i) t[i] = h->s->t_stages[i];
+  return 0;
+}
+
+int pmf_get_timing(pmf_solver* h, double* setup_ms, double* solve_ms) {
+  PMF_CHECK_HANDLE(h);
+  if (setup_ms) *setup_ms = h->s->last_setup_ms;
+  if (solve_ms) *solve_ms = h->s->last_solve_ms;
+  return 0;
+}
+
+const char* pmf_last_error(void) { return g_last_error.c_str(); }
+
+int pmf_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+}  // extern "C"

@@ -1,0 +1,518 @@
+// Coarse-space kernels (FP64): level-2 Galerkin assembly, batched dense SPD
+// inverses, the level-3 eigenproblem and the small coarse products used by the
+// cycle executor.
+#include <algorithm>
+
+#include "pmf_dense.cuh"
+#include "pmf_kernels.h"
+
+namespace pmf {
+
+// ---------------------------------------------------------------------------
+// out = base - A2 v with A2 = Phi^T A Phi stored as 7 kmax x kmax blocks per
+// subdomain row (diagonal + six face neighbours).
+__global__ void k_a2_mult(const SubInfo* subs, int nsub, int kmax, const double* blk, const double* v,
+                          const double* base, double* out, const int* done) {
+  if (done && *done) return;
+  const long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (row >= (long long)nsub * kmax) return;
+  const int s = (int)(row / kmax), i = (int)(row % kmax);
+  const SubInfo& S = subs[s];
+  double acc = 0.0;
+  for (int b = 0; b < 7; ++b) {
+    const int nb = b == 0 ? s : S.nb[b - 1];
+    if (nb < 0) continue;
+    const double* B = blk + (((long long)s * 7 + b) * kmax + i) * kmax;
+    const double* vv = v + (long long)nb * kmax;
+    for (int j = 0; j < kmax; ++j) acc += B[j] * vv[j];
+  }
+  out[row] = (base ? base[row] : 0.0) - acc;
+}
+void launch_a2_mult(const SubInfo* subs, int nsub, int kmax, const double* blk, const double* v, const double* base,
+                    double* out, const int* done, cudaStream_t st) {
+  long long n = (long long)nsub * kmax;
+  k_a2_mult<<<(int)((n + 255) / 256), 256, 0, st>>>(subs, nsub, kmax, blk, v, base, out, done);
+}
+
+// Batched dense GEMV, one warp per row.
+__global__ void k_block_gemv(int nrank, int nr, const double* inv, const double* in, double* out, int accumulate,
+                             const int* done) {
+  if (done && *done) return;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= (long long)nrank * nr) return;
+  const long long r = row / nr;
+  const double* A = inv + row * nr;
+  const double* x = in + r * nr;
+  double acc = 0.0;
+  for (int j = lane; j < nr; j += 32) acc += A[j] * x[j];
+  acc = warp_sum(acc);
+  if (lane == 0) out[row] = accumulate ? out[row] + acc : acc;
+}
+void launch_block_gemv(int nrank, int nr, const double* inv, const double* in, double* out, int accumulate,
+                       const int* done, cudaStream_t st) {
+  long long threads = (long long)nrank * nr * 32;
+  k_block_gemv<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, inv, in, out, accumulate, done);
+}
+
+// d[r][j] = sum_i V[r][i][j] c[r][i]  (Psi^T r = V^T Phi^T r, per rank)
+__global__ void k_lv3_restrict(int nrank, int nr, int en2, const double* V, const double* c, double* d,
+                               const int* done) {
+  if (done && *done) return;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= (long long)nrank * en2) return;
+  const long long r = row / en2;
+  const int j = (int)(row % en2);
+  const double* Vr = V + r * nr * en2;
+  const double* cr = c + r * nr;
+  double acc = 0.0;
+  for (int i = lane; i < nr; i += 32) acc += Vr[(long long)i * en2 + j] * cr[i];
+  acc = warp_sum(acc);
+  if (lane == 0) d[row] = acc;
+}
+void launch_lv3_restrict(int nrank, int nr, int en2, const double* V, const double* c, double* d, const int* done,
+                         cudaStream_t st) {
+  long long threads = (long long)nrank * en2 * 32;
+  k_lv3_restrict<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, c, d, done);
+}
+
+// dz[r][i] = sum_j V[r][i][j] w[r][j]
+__global__ void k_lv3_prolong(int nrank, int nr, int en2, const double* V, const double* w, double* dz,
+                              const int* done) {
+  if (done && *done) return;
+  const long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (row >= (long long)nrank * nr) return;
+  const long long r = row / nr;
+  const double* Vi = V + row * en2;
+  const double* wr = w + r * en2;
+  double acc = 0.0;
+  for (int j = 0; j < en2; ++j) acc += Vi[j] * wr[j];
+  dz[row] = acc;
+}
+void launch_lv3_prolong(int nrank, int nr, int en2, const double* V, const double* w, double* dz, const int* done,
+                        cudaStream_t st) {
+  long long n = (long long)nrank * nr;
+  k_lv3_prolong<<<(int)((n + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, w, dz, done);
+}
+
+__global__ void k_axpy(long long n, double a, const double* x, double* y, const int* done) {
+  if (done && *done) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+__global__ void k_copy(long long n, const double* x, double* y, const int* done) {
+  if (done && *done) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+void launch_axpy(long long n, double a, const double* x, double* y, const int* done, cudaStream_t st) {
+  k_axpy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, a, x, y, done);
+}
+void launch_copy(long long n, const double* x, double* y, const int* done, cudaStream_t st) {
+  k_copy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, x, y, done);
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin blocks of Phi^T A Phi (_PC_setup_lv2_J, src/PreMixFEM_3D.c:756-890).
+// Warp i of the CTA for subdomain s computes row i of:
+//   blk[s][0]   = Phi_s^T A_s Phi_s, A_s the principal submatrix of A on s
+//                 (interior faces in difference form, globally interior
+//                 boundary faces and Dirichlet terms on the diagonal);
+//   blk[s][1+f] = -sum_{face f} t phi_s,i(c) phi_nb,j(c')  (neighbour coupling);
+//   gface[s][f] =  sum_{face f} t phi_s,i(c) phi_s,j(c)    (boundary-face part of
+//                 the diagonal block, removed again for rank-Neumann matrices).
+template <typename T, int KM>
+__global__ void k_galerkin(Grid g, const SubInfo* subs, int kmax, const double* tx, const double* ty,
+                           const double* tz, const double* diag, const T* phi, double* blk, double* gface) {
+  const int s = blockIdx.x;
+  const SubInfo S = subs[s];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (wid >= kmax) return;
+  const int i = wid;
+  const int nx = S.nx, ny = S.ny, nz = S.nz, ncells = nx * ny * nz;
+  double acc[KM];
+#pragma unroll
+  for (int j = 0; j < KM; ++j) acc[j] = 0.0;
+  for (int cl = lane; cl < ncells; cl += 32) {
+    const int ii = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
+    const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + ii);
+    const double pi = (double)phi[cg * kmax + i];
+    if (pi == 0.0) continue;
+    const double dg = diag[cg];
+    const double t_xm = ii > 0 ? tx[cg] : 0.0, t_xp = ii < nx - 1 ? tx[cg + 1] : 0.0;
+    const double t_ym = jj > 0 ? ty[cg] : 0.0, t_yp = jj < ny - 1 ? ty[cg + g.M] : 0.0;
+    const double t_zm = kk > 0 ? tz[cg] : 0.0, t_zp = kk < nz - 1 ? tz[cg + g.MN] : 0.0;
+#pragma unroll
+    for (int j = 0; j < KM; ++j) {
+      if (j >= kmax) break;
+      double a = dg * (double)phi[cg * kmax + j];
+      if (ii > 0) a -= t_xm * (double)phi[(cg - 1) * kmax + j];
+      if (ii < nx - 1) a -= t_xp * (double)phi[(cg + 1) * kmax + j];
+      if (jj > 0) a -= t_ym * (double)phi[(cg - g.M) * kmax + j];
+      if (jj < ny - 1) a -= t_yp * (double)phi[(cg + g.M) * kmax + j];
+      if (kk > 0) a -= t_zm * (double)phi[(cg - g.MN) * kmax + j];
+      if (kk < nz - 1) a -= t_zp * (double)phi[(cg + g.MN) * kmax + j];
+      acc[j] += pi * a;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < KM; ++j) {
+    if (j >= kmax) break;
+    const double v = warp_sum(acc[j]);
+    if (lane == 0) blk[(((long long)s * 7 + 0) * kmax + i) * kmax + j] = v;
+  }
+  // faces x-, x+, y-, y+, z-, z+
+  for (int f = 0; f < 6; ++f) {
+    const int axis = f >> 1, hi = f & 1;
+    bool exists;
+    int na, nb;  // face extents
+    if (axis == 0) {
+      exists = hi ? (S.x0 + nx < g.M) : (S.x0 > 0);
+      na = ny;
+      nb = nz;
+    } else if (axis == 1) {
+      exists = hi ? (S.y0 + ny < g.N) : (S.y0 > 0);
+      na = nx;
+      nb = nz;
+    } else {
+      exists = hi ? (S.z0 + nz < g.P) : (S.z0 > 0);
+      na = nx;
+      nb = ny;
+    }
+    double ag[KM], ac[KM];
+#pragma unroll
+    for (int j = 0; j < KM; ++j) ag[j] = ac[j] = 0.0;
+    if (exists) {
+      for (int idx = lane; idx < na * nb; idx += 32) {
+        const int a = idx % na, b = idx / na;
+        int ii, jj, kk;
+        if (axis == 0) {
+          ii = hi ? nx - 1 : 0;
+          jj = a;
+          kk = b;
+        } else if (axis == 1) {
+          ii = a;
+          jj = hi ? ny - 1 : 0;
+          kk = b;
+        } else {
+          ii = a;
+          jj = b;
+          kk = hi ? nz - 1 : 0;
+        }
+        const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + ii);
+        const long long off = axis == 0 ? 1 : (axis == 1 ? g.M : g.MN);
+        const long long cn = hi ? cg + off : cg - off;
+        const double* tt = axis == 0 ? tx : (axis == 1 ? ty : tz);
+        const double t = hi ? tt[cn] : tt[cg];
+        const double pi = (double)phi[cg * kmax + i];
+#pragma unroll
+        for (int j = 0; j < KM; ++j) {
+          if (j >= kmax) break;
+          ag[j] += t * pi * (double)phi[cg * kmax + j];
+          ac[j] -= t * pi * (double)phi[cn * kmax + j];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KM; ++j) {
+      if (j >= kmax) break;
+      const double vg = warp_sum(ag[j]);
+      const double vc = warp_sum(ac[j]);
+      if (lane == 0) {
+        gface[(((long long)s * 6 + f) * kmax + i) * kmax + j] = vg;
+        blk[(((long long)s * 7 + 1 + f) * kmax + i) * kmax + j] = vc;
+      }
+    }
+  }
+}
+
+template <typename T>
+void launch_galerkin(const Grid& g, const SubInfo* subs, int nsub, int kmax, const double* tx, const double* ty,
+                     const double* tz, const double* diag, const T* phi, double* blk, double* gface,
+                     cudaStream_t st) {
+  const int threads = 32 * kmax;
+  if (kmax <= 4)
+    k_galerkin<T, 4><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+  else if (kmax <= 8)
+    k_galerkin<T, 8><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+  else
+    k_galerkin<T, 16><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+}
+template void launch_galerkin<float>(const Grid&, const SubInfo*, int, int, const double*, const double*,
+                                     const double*, const double*, const float*, double*, double*, cudaStream_t);
+template void launch_galerkin<double>(const Grid&, const SubInfo*, int, int, const double*, const double*,
+                                      const double*, const double*, const double*, double*, double*, cudaStream_t);
+
+// Dense per-rank coarse matrices.  mode 0: the rank's principal block of
+// Phi^T A Phi (level-2 matrix of _PC_setup_lv2_J); mode 1: the rank-Neumann
+// matrix of _PC_setup_lv3_eigen (:938-1076), i.e. without the boundary-face
+// terms of faces that leave the rank.  Padded dofs (j >= k_s) are identity.
+__global__ void k_assemble_dense(const SubInfo* subs, int nrank, int spr, int kmax, const double* blk,
+                                 const double* gface, int mode, double* dense) {
+  const long long nr = (long long)spr * kmax;
+  const long long total = (long long)nrank * nr * nr;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / (nr * nr));
+    const long long rem = e % (nr * nr);
+    const int row = (int)(rem / nr), col = (int)(rem % nr);
+    const int a = row / kmax, i = row % kmax, b = col / kmax, j = col % kmax;
+    const int s = r * spr + a, s2 = r * spr + b;
+    const SubInfo& S = subs[s];
+    double v = 0.0;
+    if (i >= S.k || j >= subs[s2].k) {
+      v = (row == col) ? 1.0 : 0.0;
+    } else if (a == b) {
+      v = blk[(((long long)s * 7) * kmax + i) * kmax + j];
+      if (mode == 1)
+        for (int f = 0; f < 6; ++f)
+          if (S.nb[f] >= 0 && subs[S.nb[f]].rank != r) v -= gface[(((long long)s * 6 + f) * kmax + i) * kmax + j];
+    } else {
+      for (int f = 0; f < 6; ++f)
+        if (S.nb[f] == s2) v = blk[(((long long)s * 7 + 1 + f) * kmax + i) * kmax + j];
+    }
+    dense[e] = v;
+  }
+}
+void launch_assemble_dense(const SubInfo* subs, int nsub, int nrank, int spr, int kmax, const double* blk,
+                           const double* gface, int mode, double* dense, cudaStream_t st) {
+  (void)nsub;
+  long long total = (long long)nrank * spr * kmax * spr * kmax;
+  int nb = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+  k_assemble_dense<<<nb, 256, 0, st>>>(subs, nrank, spr, kmax, blk, gface, mode, dense);
+}
+
+// In-place Gauss-Jordan inverse of SPD matrices (one CTA per matrix).
+// Pivots <= tol * max diag are null directions: that row/column is dropped
+// (zero in the result), which equals inverting the matrix with the index
+// removed -- the same treatment as the semidefinite Cholesky of the oracle.
+__global__ void k_spd_inverse(int n, double* a_all, double tol, int* nnull) {
+  double* a = a_all + (long long)blockIdx.x * n * n;
+  extern __shared__ double sh[];
+  double* colk = sh;
+  double* rowk = sh + n;
+  __shared__ double red[32];
+  __shared__ int nul;
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(a[(long long)i * n + i]));
+  // block max via shared reduction
+  {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[wid] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+      for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) m = fmax(m, red[w]);
+      red[0] = m;
+      nul = 0;
+    }
+    __syncthreads();
+  }
+  const double scale = red[0] > 0 ? red[0] : 1.0;
+  const long long nn = (long long)n * n;
+  for (int k = 0; k < n; ++k) {
+    const double piv = a[(long long)k * n + k];
+    const bool isnull = !(piv > tol * scale);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      colk[i] = a[(long long)i * n + k];
+      rowk[i] = isnull ? 0.0 : (i == k ? 1.0 : a[(long long)k * n + i]) / piv;
+    }
+    __syncthreads();
+    if (isnull) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a[(long long)k * n + i] = 0.0;
+        a[(long long)i * n + k] = 0.0;
+      }
+      if (threadIdx.x == 0) nul += 1;
+    } else {
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e % n);
+        if (i == k)
+          a[e] = rowk[j];
+        else
+          a[e] = (j == k ? 0.0 : a[e]) - colk[i] * rowk[j];
+      }
+    }
+    __syncthreads();
+  }
+  for (long long e = threadIdx.x; e < nn; e += blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    if (i < j) {
+      const double v = 0.5 * (a[e] + a[(long long)j * n + i]);
+      a[e] = v;
+      a[(long long)j * n + i] = v;
+    }
+  }
+  if (threadIdx.x == 0 && nnull) atomicAdd(nnull, nul);
+}
+void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
+  const int smem = 2 * n * sizeof(double);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull);
+}
+
+// ---------------------------------------------------------------------------
+// Level-3 HEP (_PC_setup_lv3_eigen, :1086-1115): smallest en2 eigenpairs of
+// each rank's dense rank-Neumann matrix.  SLEPc's shift-and-invert Krylov-
+// Schur is replaced by block inverse subspace iteration with the precomputed
+// (A + mu I)^-1, SVQB orthonormalisation and a Rayleigh-Ritz step on A; the
+// eigenvectors come out orthonormal in the 2-norm as SLEPc returns them.
+// work: 3 * nr * p doubles per rank.
+#define PMF_L3_MAXP 32
+__global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all, const double* inv_all,
+                                     double* V_all, double* evals_all, int* iters, double tol, int max_it,
+                                     double* work_all) {
+  const int r = blockIdx.x;
+  const double* A = A_all + (long long)r * nr * nr;
+  const double* inv = inv_all + (long long)r * nr * nr;
+  double* X = work_all + (long long)r * 3 * nr * p;
+  double* Y = X + (long long)nr * p;
+  double* AY = Y + (long long)nr * p;
+  __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP],
+      C[PMF_L3_MAXP * PMF_L3_MAXP], dsc[PMF_L3_MAXP];
+  __shared__ int keep, conv;
+  __shared__ double anorm;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // scale of A: max |diag|
+  if (tid == 0) {
+    double m = 0.0;
+    for (int i = 0; i < nr; ++i) m = fmax(m, fabs(A[(long long)i * nr + i]));
+    anorm = m > 0 ? m : 1.0;
+  }
+  for (long long e = tid; e < (long long)nr * p; e += nt)
+    X[e] = hash_uniform(((unsigned long long)r << 40) ^ (unsigned long long)e);
+  __syncthreads();
+  int it = 0;
+  for (; it < max_it; ++it) {
+    // Y = inv X
+    for (long long e = tid; e < (long long)nr * p; e += nt) {
+      const int i = (int)(e / p), j = (int)(e % p);
+      const double* row = inv + (long long)i * nr;
+      double acc = 0.0;
+      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + j];
+      Y[e] = acc;
+    }
+    __syncthreads();
+    // SVQB: G = Y^T Y, D^-1/2 G D^-1/2 = U w U^T, X = Y D^-1/2 U w^-1/2 (kept columns)
+    for (int e = tid; e < p * p; e += nt) {
+      const int a = e / p, b = e % p;
+      double acc = 0.0;
+      for (int l = 0; l < nr; ++l) acc += Y[(long long)l * p + a] * Y[(long long)l * p + b];
+      G[a * PMF_L3_MAXP + b] = acc;
+    }
+    __syncthreads();
+    if (tid < p) dsc[tid] = 1.0 / sqrt(fmax(G[tid * PMF_L3_MAXP + tid], 1e-300));
+    __syncthreads();
+    for (int e = tid; e < p * p; e += nt) {
+      const int a = e / p, b = e % p;
+      G[a * PMF_L3_MAXP + b] *= dsc[a] * dsc[b];
+    }
+    __syncthreads();
+    if (tid < 32) warp_jacobi_eigh(G, U, w, p, PMF_L3_MAXP);
+    __syncthreads();
+    if (tid == 0) {
+      int kk = 0;
+      const double wmax = w[p - 1];
+      for (int c = p - 1; c >= 0; --c)
+        if (w[c] > 1e-12 * wmax) ++kk;
+      keep = kk;
+    }
+    __syncthreads();
+    const int q = keep;  // kept columns are the last q (largest w)
+    for (int e = tid; e < p * q; e += nt) {
+      const int a = e / q, c = e % q;
+      const int cc = p - q + c;
+      C[a * PMF_L3_MAXP + c] = dsc[a] * U[a * PMF_L3_MAXP + cc] / sqrt(w[cc]);
+    }
+    __syncthreads();
+    for (long long e = tid; e < (long long)nr * q; e += nt) {
+      const int i = (int)(e / q), c = (int)(e % q);
+      double acc = 0.0;
+      for (int a = 0; a < p; ++a) acc += Y[(long long)i * p + a] * C[a * PMF_L3_MAXP + c];
+      X[(long long)i * p + c] = acc;
+    }
+    __syncthreads();
+    // AY = A X (q columns), H = X^T A X
+    for (long long e = tid; e < (long long)nr * q; e += nt) {
+      const int i = (int)(e / q), c = (int)(e % q);
+      const double* row = A + (long long)i * nr;
+      double acc = 0.0;
+      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
+      AY[(long long)i * p + c] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < q * q; e += nt) {
+      const int a = e / q, b = e % q;
+      double acc = 0.0;
+      for (int l = 0; l < nr; ++l) acc += X[(long long)l * p + a] * AY[(long long)l * p + b];
+      G[a * PMF_L3_MAXP + b] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < q * q; e += nt) {  // symmetrise
+      const int a = e / q, b = e % q;
+      if (a < b) {
+        const double v = 0.5 * (G[a * PMF_L3_MAXP + b] + G[b * PMF_L3_MAXP + a]);
+        G[a * PMF_L3_MAXP + b] = v;
+        G[b * PMF_L3_MAXP + a] = v;
+      }
+    }
+    __syncthreads();
+    if (tid < 32) warp_jacobi_eigh(G, U, w, q, PMF_L3_MAXP);
+    __syncthreads();
+    // X <- X U (through Y as scratch)
+    for (long long e = tid; e < (long long)nr * q; e += nt) {
+      const int i = (int)(e / q), c = (int)(e % q);
+      double ax = 0.0;
+      for (int a = 0; a < q; ++a) ax += X[(long long)i * p + a] * U[a * PMF_L3_MAXP + c];
+      Y[(long long)i * p + c] = ax;
+    }
+    __syncthreads();
+    for (long long e = tid; e < (long long)nr * q; e += nt) {
+      const int i = (int)(e / q), c = (int)(e % q);
+      X[(long long)i * p + c] = Y[(long long)i * p + c];
+    }
+    __syncthreads();
+    // recompute AY for the Ritz vectors and the residuals of the wanted ones
+    for (long long e = tid; e < (long long)nr * q; e += nt) {
+      const int i = (int)(e / q), c = (int)(e % q);
+      const double* row = A + (long long)i * nr;
+      double acc = 0.0;
+      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
+      AY[(long long)i * p + c] = acc - w[c] * X[(long long)i * p + c];
+    }
+    __syncthreads();
+    if (tid == 0) conv = 1;
+    __syncthreads();
+    for (int c = tid; c < min(en2, q); c += nt) {
+      double rr = 0.0;
+      for (int l = 0; l < nr; ++l) rr += AY[(long long)l * p + c] * AY[(long long)l * p + c];
+      if (sqrt(rr) > tol * anorm) conv = 0;
+    }
+    if (q < en2 && tid == 0) conv = 0;
+    __syncthreads();
+    // pad dropped columns with fresh random directions for the next sweep
+    for (long long e = tid; e < (long long)nr * (p - q); e += nt) {
+      const int i = (int)(e / (p - q)), c = q + (int)(e % (p - q));
+      X[(long long)i * p + c] = hash_uniform(((unsigned long long)(r + 7) << 44) ^ ((unsigned long long)it << 32) ^
+                                             (unsigned long long)e);
+    }
+    __syncthreads();
+    if (conv) break;
+  }
+  double* V = V_all + (long long)r * nr * en2;
+  for (long long e = tid; e < (long long)nr * en2; e += nt) {
+    const int i = (int)(e / en2), j = (int)(e % en2);
+    V[e] = X[(long long)i * p + j];
+  }
+  if (tid < en2) evals_all[(long long)r * en2 + tid] = w[tid];
+  if (tid == 0) iters[r] = it + 1;
+}
+
+void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
+                               double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st) {
+  k_dense_smallest_eig<<<nrank, 512, 0, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work);
+}
+
+}  // namespace pmf

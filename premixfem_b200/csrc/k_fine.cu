@@ -1,0 +1,597 @@
+// Fine-grid kernels: operator assembly, stencil products, CG vector updates,
+// level-1 IC(0) block solves and the level-2 restriction / prolongation.
+#include <algorithm>
+
+#include "pmf_kernels.h"
+
+namespace pmf {
+
+int cell_blocks(long long n) {
+  long long b = (n + kCellThreads - 1) / kCellThreads;
+  const long long cap = 148LL * 16;
+  return (int)std::max(1LL, std::min(b, cap));
+}
+
+__device__ __forceinline__ void decode(long long c, const Grid& g, int& ex, int& ey, int& ez) {
+  ex = (int)(c % g.M);
+  long long t = c / g.M;
+  ey = (int)(t % g.N);
+  ez = (int)(t / g.N);
+}
+
+// ---------------------------------------------------------------------------
+// PC_create_A (src/PreMixFEM_3D.c:1757-1824): interior faces get
+// t = |f|^2/|K| * 2 / (1/k_L + 1/k_R), evaluated in the reference's order.
+// Dirichlet faces (extension) add t_b = |f|^2/|K| * 2 k_cell to the diagonal
+// and t_b * p_D to the right-hand side.
+__device__ __forceinline__ double hmean(double a, double b) { return 2.0 / (1.0 / a + 1.0 / b); }
+
+__global__ void k_assemble(AssembleArgs a, double* tx, double* ty, double* tz, double* diag, double* db,
+                           double* bval) {
+  const Grid g = a.g;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    int ex, ey, ez;
+    decode(c, g, ex, ey, ez);
+    const double txc = ex > 0 ? a.cx * hmean(a.kx[c - 1], a.kx[c]) : 0.0;
+    const double tyc = ey > 0 ? a.cy * hmean(a.ky[c - g.M], a.ky[c]) : 0.0;
+    const double tzc = ez > 0 ? a.cz * hmean(a.kz[c - g.MN], a.kz[c]) : 0.0;
+    const double txn = ex < g.M - 1 ? a.cx * hmean(a.kx[c], a.kx[c + 1]) : 0.0;
+    const double tyn = ey < g.N - 1 ? a.cy * hmean(a.ky[c], a.ky[c + g.M]) : 0.0;
+    const double tzn = ez < g.P - 1 ? a.cz * hmean(a.kz[c], a.kz[c + g.MN]) : 0.0;
+    double dbc = 0.0, bv = 0.0;
+    const bool on[6] = {ex == 0, ex == g.M - 1, ey == 0, ey == g.N - 1, ez == 0, ez == g.P - 1};
+    const double cf[6] = {a.cx, a.cx, a.cy, a.cy, a.cz, a.cz};
+    const double kk[6] = {a.kx[c], a.kx[c], a.ky[c], a.ky[c], a.kz[c], a.kz[c]};
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (a.dir_on[f] && on[f]) {
+        const double tb = cf[f] * (2.0 * kk[f]);
+        dbc += tb;
+        bv += tb * a.dir_val[f];
+      }
+    }
+    tx[c] = txc;
+    ty[c] = tyc;
+    tz[c] = tzc;
+    double d = txc + tyc;
+    d = d + tzc;
+    d = d + txn;
+    d = d + tyn;
+    d = d + tzn;
+    d = d + dbc;
+    diag[c] = d;
+    db[c] = dbc;
+    bval[c] = bv;
+  }
+}
+
+void launch_assemble(const AssembleArgs& a, double* tx, double* ty, double* tz, double* diag, double* db,
+                     double* bval, cudaStream_t st) {
+  k_assemble<<<cell_blocks(a.g.ncell), kCellThreads, 0, st>>>(a, tx, ty, tz, diag, db, bval);
+}
+
+__global__ void k_to_f32(const double* in, float* out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+__global__ void k_to_f64(const float* in, double* out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+void launch_to_f32(const double* in, float* out, long long n, cudaStream_t st) {
+  k_to_f32<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n);
+}
+void launch_to_f64(const float* in, double* out, long long n, cudaStream_t st) {
+  k_to_f64<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n);
+}
+
+// ---------------------------------------------------------------------------
+// 7-point stencil product A x, precision T.
+template <typename T>
+__device__ __forceinline__ T apply_A(const Grid& g, long long c, int ex, int ey, int ez, const T* tx, const T* ty,
+                                     const T* tz, const T* diag, const T* x) {
+  T v = diag[c] * x[c];
+  if (ex > 0) v -= tx[c] * x[c - 1];
+  if (ex < g.M - 1) v -= tx[c + 1] * x[c + 1];
+  if (ey > 0) v -= ty[c] * x[c - g.M];
+  if (ey < g.N - 1) v -= ty[c + g.M] * x[c + g.M];
+  if (ez > 0) v -= tz[c] * x[c - g.MN];
+  if (ez < g.P - 1) v -= tz[c + g.MN] * x[c + g.MN];
+  return v;
+}
+
+__global__ void k_spmv(Grid g, const double* tx, const double* ty, const double* tz, const double* diag,
+                       const double* x, double* y) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    int ex, ey, ez;
+    decode(c, g, ex, ey, ez);
+    y[c] = apply_A(g, c, ex, ey, ez, tx, ty, tz, diag, x);
+  }
+}
+
+void launch_spmv(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                 const double* x, double* y, cudaStream_t st) {
+  k_spmv<<<cell_blocks(g.ncell), kCellThreads, 0, st>>>(g, tx, ty, tz, diag, x, y);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: each block writes one partial; a single block
+// sums the partials in a fixed order.
+__device__ __forceinline__ double fixed_sum(const double* part, int n, double* scratch) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
+  return block_sum(v, scratch);
+}
+
+__global__ void k_dot(const double* a, const double* b, long long n, double* part) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v += a[i] * b[i];
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+__global__ void k_fin_sum(const double* part, int n, double* out) {
+  __shared__ double red[32];
+  double v = fixed_sum(part, n, red);
+  if (threadIdx.x == 0) *out = v;
+}
+void launch_dot(const double* a, const double* b, long long n, double* part, double* out, cudaStream_t st) {
+  int nb = cell_blocks(n);
+  k_dot<<<nb, kCellThreads, 0, st>>>(a, b, n, part);
+  k_fin_sum<<<1, 256, 0, st>>>(part, nb, out);
+}
+
+// --- KSPSolve_CG (PETSc src/ksp/ksp/impls/cg/cg.c) with the unpreconditioned norm ---
+__global__ void k_pcg_start(long long n, const double* b, double* x, double* r, double* part) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    x[i] = 0.0;
+    r[i] = bi;
+    v += bi * bi;
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+__global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double rtol, int max_it) {
+  __shared__ double red[32];
+  const double v = fixed_sum(part, nb, red);
+  if (threadIdx.x == 0) {
+    const double dp = sqrt(v);
+    s->dp = dp;
+    s->rnorm0 = dp;
+    s->ttol = fmax(rtol * dp, 1.0e-50);  // KSPConvergedDefault: max(rtol*rnorm0, abstol)
+    s->its = 0;
+    s->max_it = max_it;
+    s->first = 1;
+    s->beta = s->betaold = s->dpi = s->dpiold = s->alpha = 0.0;
+    s->done = (dp <= s->ttol) ? 1 : 0;
+  }
+}
+void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,
+                      int max_it, cudaStream_t st) {
+  int nb = cell_blocks(g.ncell);
+  k_pcg_start<<<nb, kCellThreads, 0, st>>>(g.ncell, b, x, r, part);
+  k_pcg_start_fin<<<1, 256, 0, st>>>(part, nb, s, rtol, max_it);
+}
+
+// beta = z.r (the dot is written per block by the preconditioner's last kernel
+// or by k_dot); a zero beta ends the loop (KSP_CONVERGED_ATOL).
+__global__ void k_pcg_beta_fin(const double* part, int nb, PcgState* s) {
+  __shared__ double red[32];
+  if (s->done) return;
+  const double v = fixed_sum(part, nb, red);
+  if (threadIdx.x == 0) {
+    s->beta = v;
+    if (v == 0.0) {
+      s->its += 1;
+      s->done = 1;
+    }
+  }
+}
+void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream_t st) {
+  k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nparts, s);
+}
+void launch_pcg_beta(const double* r, const double* z, long long n, double* part, PcgState* s, cudaStream_t st) {
+  int nb = cell_blocks(n);
+  k_dot<<<nb, kCellThreads, 0, st>>>(r, z, n, part);
+  k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nb, s);
+}
+
+// p <- z (first) or z + (beta/betaold) p; w <- A p; partial p.w.
+// In-place on p: the stencil reads p at neighbours, so p_new is formed from z
+// and the old p of each neighbour on the fly, and written to pout != pin.
+__global__ void k_pcg_iter_a(Grid g, const double* tx, const double* ty, const double* tz, const double* diag,
+                             const double* z, const double* pin, double* pout, double* w, double* part,
+                             const PcgState* s) {
+  __shared__ double red[32];
+  if (s->done) return;
+  const bool first = s->first != 0;
+  const double b = first ? 0.0 : s->beta / s->betaold;
+  double v = 0.0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    int ex, ey, ez;
+    decode(c, g, ex, ey, ez);
+#define PNEW(i) (first ? z[i] : z[i] + b * pin[i])
+    const double pc = PNEW(c);
+    double a = diag[c] * pc;
+    if (ex > 0) a -= tx[c] * PNEW(c - 1);
+    if (ex < g.M - 1) a -= tx[c + 1] * PNEW(c + 1);
+    if (ey > 0) a -= ty[c] * PNEW(c - g.M);
+    if (ey < g.N - 1) a -= ty[c + g.M] * PNEW(c + g.M);
+    if (ez > 0) a -= tz[c] * PNEW(c - g.MN);
+    if (ez < g.P - 1) a -= tz[c + g.MN] * PNEW(c + g.MN);
+#undef PNEW
+    pout[c] = pc;
+    w[c] = a;
+    v += pc * a;
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+__global__ void k_pcg_iter_a_fin(const double* part, int nb, PcgState* s) {
+  __shared__ double red[32];
+  if (s->done) return;
+  const double dpi = fixed_sum(part, nb, red);
+  if (threadIdx.x == 0) {
+    s->dpiold = s->dpi;
+    s->dpi = dpi;
+    s->betaold = s->beta;
+    const bool flip = !s->first && ((dpi > 0) != (s->dpiold > 0));
+    s->first = 0;
+    if (dpi == 0.0 || flip) {
+      s->its += 1;
+      s->done = 3;  // KSP_DIVERGED_INDEFINITE_MAT
+    } else {
+      s->alpha = s->beta / dpi;
+    }
+  }
+}
+void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                       const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
+                       cudaStream_t st) {
+  int nb = cell_blocks(g.ncell);
+  k_pcg_iter_a<<<nb, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s);
+  k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s);
+}
+
+// x += alpha p; r -= alpha w; partial r.r; then dp, its and the convergence test.
+__global__ void k_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
+                             const PcgState* s) {
+  __shared__ double red[32];
+  if (s->done) return;
+  const double a = s->alpha;
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * w[i];
+    r[i] = ri;
+    v += ri * ri;
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+__global__ void k_pcg_iter_b_fin(const double* part, int nb, PcgState* s) {
+  __shared__ double red[32];
+  if (s->done) return;
+  const double v = fixed_sum(part, nb, red);
+  if (threadIdx.x == 0) {
+    const double dp = sqrt(v);
+    s->dp = dp;
+    s->its += 1;
+    if (!(dp == dp) || isinf(dp))
+      s->done = 4;
+    else if (dp <= s->ttol)
+      s->done = 1;
+    else if (s->its >= s->max_it)
+      s->done = 2;
+  }
+}
+void launch_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
+                       PcgState* s, cudaStream_t st) {
+  int nb = cell_blocks(n);
+  k_pcg_iter_b<<<nb, kCellThreads, 0, st>>>(n, x, r, p, w, part, s);
+  k_pcg_iter_b_fin<<<1, 256, 0, st>>>(part, nb, s);
+}
+
+// ---------------------------------------------------------------------------
+// Level 1: IC(0) of each subdomain's principal submatrix (PCICC, natural
+// order, src/PreMixFEM_3D.c:200-215).  For the 7-point pattern the factor is
+// (D + L) D^-1 (D + L^T) with D_i = a_ii - sum_{lower nb j} a_ij^2 / D_j.
+//
+// Both the factorisation and the solves run as hyperplane wavefronts inside
+// one CTA per subdomain: thread (j, k) owns the x-line (., j, k) and handles
+// its cell i = d - j - k on plane d; neighbours on the previous plane are
+// read from shared memory after a barrier.
+struct SubGeom {
+  int x0, y0, z0, nx, ny, nz, nxny, ncells, nlines, nplanes;
+};
+__device__ __forceinline__ SubGeom sub_geom(const SubInfo& s) {
+  SubGeom q;
+  q.x0 = s.x0;
+  q.y0 = s.y0;
+  q.z0 = s.z0;
+  q.nx = s.nx;
+  q.ny = s.ny;
+  q.nz = s.nz;
+  q.nxny = s.nx * s.ny;
+  q.ncells = q.nxny * s.nz;
+  q.nlines = s.ny * s.nz;
+  q.nplanes = s.nx + s.ny + s.nz - 2;
+  return q;
+}
+
+__global__ void k_ic_factor(Grid g, const SubInfo* subs, const double* tx, const double* ty, const double* tz,
+                            const double* diag, double* inv_d, int* bad) {
+  extern __shared__ double Dsh[];
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  const int t = threadIdx.x;
+  const int j = t % q.ny, k = t / q.ny;
+  for (int d = 0; d < q.nplanes; ++d) {
+    const int i = d - j - k;
+    if (t < q.nlines && i >= 0 && i < q.nx) {
+      const int cl = (k * q.ny + j) * q.nx + i;
+      const long long cg = ((long long)(q.z0 + k) * g.N + (q.y0 + j)) * g.M + (q.x0 + i);
+      double s = 0.0;
+      if (k > 0) {
+        const double a = tz[cg];
+        s += a * a / Dsh[cl - q.nxny];
+      }
+      if (j > 0) {
+        const double a = ty[cg];
+        s += a * a / Dsh[cl - q.nx];
+      }
+      if (i > 0) {
+        const double a = tx[cg];
+        s += a * a / Dsh[cl - 1];
+      }
+      double D = diag[cg] - s;
+      if (!(D > 0.0)) {
+        atomicAdd(bad, 1);
+        D = diag[cg];
+      }
+      Dsh[cl] = D;
+      inv_d[cg] = 1.0 / D;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_lines, const double* tx,
+                      const double* ty, const double* tz, const double* diag, double* inv_d, int* bad,
+                      cudaStream_t st) {
+  // the caller guarantees ny*nz <= PMF_MAX_LINES and cells <= PMF_MAX_SUB_CELLS for every subdomain
+  int threads = std::max(32, ((max_lines + 31) / 32) * 32);
+  const int smem = PMF_MAX_SUB_CELLS * sizeof(double);
+  cudaFuncSetAttribute(k_ic_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k_ic_factor<<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, bad);
+}
+
+template <typename T>
+__device__ __forceinline__ void ic_sweeps(const Grid& g, const SubGeom& q, const T* tx, const T* ty, const T* tz,
+                                          const T* inv_d, T* u) {
+  const int t = threadIdx.x;
+  const int j = t % q.ny, k = t / q.ny;
+  const bool line = t < q.nlines;
+  const long long base = ((long long)(q.z0 + k) * g.N + (q.y0 + j)) * g.M + q.x0;
+  // forward: (D + L) w = r  ->  w_i = (r_i + sum t_ij w_j) / D_i
+  for (int d = 0; d < q.nplanes; ++d) {
+    const int i = d - j - k;
+    if (line && i >= 0 && i < q.nx) {
+      const int cl = (k * q.ny + j) * q.nx + i;
+      const long long cg = base + i;
+      T s = u[cl];
+      if (k > 0) s += tz[cg] * u[cl - q.nxny];
+      if (j > 0) s += ty[cg] * u[cl - q.nx];
+      if (i > 0) s += tx[cg] * u[cl - 1];
+      u[cl] = s * inv_d[cg];
+    }
+    __syncthreads();
+  }
+  // backward: (D + L^T) z = D w  ->  z_i = w_i + (sum_{upper j} t_ij z_j) / D_i
+  for (int d = q.nplanes - 1; d >= 0; --d) {
+    const int i = d - j - k;
+    if (line && i >= 0 && i < q.nx) {
+      const int cl = (k * q.ny + j) * q.nx + i;
+      const long long cg = base + i;
+      T s = (T)0;
+      if (i < q.nx - 1) s += tx[cg + 1] * u[cl + 1];
+      if (j < q.ny - 1) s += ty[cg + g.M] * u[cl + q.nx];
+      if (k < q.nz - 1) s += tz[cg + g.MN] * u[cl + q.nxny];
+      u[cl] = u[cl] + s * inv_d[cg];
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, bool HAS_Y, bool FINAL>
+__global__ void k_ic_apply(Grid g, const SubInfo* subs, const T* tx, const T* ty, const T* tz, const T* diag,
+                           const T* inv_d, const double* x, const T* yin, T* out_t, double* out_d, double* part,
+                           const int* done) {
+  if (done && *done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* red = reinterpret_cast<double*>(smem_raw);
+  T* u = reinterpret_cast<T*>(smem_raw + 32 * sizeof(double));
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  // right-hand side r = x - A y on the subdomain (y read across subdomain faces)
+  for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
+    const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
+    const int ex = q.x0 + i, ey = q.y0 + j, ez = q.z0 + k;
+    const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    T r = (T)x[cg];
+    if (HAS_Y) r -= apply_A(g, cg, ex, ey, ez, tx, ty, tz, diag, yin);
+    u[cl] = r;
+  }
+  __syncthreads();
+  ic_sweeps(g, q, tx, ty, tz, inv_d, u);
+  double dot = 0.0;
+  for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
+    const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
+    const long long cg = ((long long)(q.z0 + k) * g.N + (q.y0 + j)) * g.M + (q.x0 + i);
+    T o = u[cl];
+    if (HAS_Y) o += yin[cg];
+    if (FINAL) {
+      const double od = (double)o;
+      out_d[cg] = od;
+      dot += x[cg] * od;
+    } else {
+      out_t[cg] = o;
+    }
+  }
+  if (FINAL) {
+    dot = block_sum(dot, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = dot;
+  }
+}
+
+template <typename T>
+void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines, int max_cells, const T* tx,
+                     const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
+                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st) {
+  int threads = std::max(64, ((max_lines + 31) / 32) * 32);
+  size_t smem = 32 * sizeof(double) + (size_t)max_cells * sizeof(T);
+  const bool fin = out_d != nullptr;
+  static bool attr_set[2][2][2] = {};
+  bool& done_attr = attr_set[sizeof(T) == 8][yin != nullptr][fin];
+  if (!done_attr) {
+    const int lim = 32 * sizeof(double) + PMF_MAX_SUB_CELLS * sizeof(T);
+    if (yin) {
+      cudaFuncSetAttribute(k_ic_apply<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+      cudaFuncSetAttribute(k_ic_apply<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    } else {
+      cudaFuncSetAttribute(k_ic_apply<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+      cudaFuncSetAttribute(k_ic_apply<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    }
+    done_attr = true;
+  }
+  if (yin) {
+    if (fin)
+      k_ic_apply<T, true, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d,
+                                                             part, done);
+    else
+      k_ic_apply<T, true, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                              out_d, part, done);
+  } else {
+    if (fin)
+      k_ic_apply<T, false, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                              out_d, part, done);
+    else
+      k_ic_apply<T, false, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                               out_d, part, done);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Level-2 restriction c_s = Phi_s^T (x - A y)|_s  (VecMDot in
+// _PC_apply_vec_lv2, src/PreMixFEM_3D.c:1564) fused with the residual update
+// r = x - A y of PC_apply_vec (:1859-1926): the residual is never stored.
+template <typename T, int KM, bool HAS_Y>
+__global__ void k_resid_restrict(Grid g, const SubInfo* subs, int kmax, const T* tx, const T* ty, const T* tz,
+                                 const T* diag, const T* phi, const double* x, const T* y, double* c,
+                                 const int* done) {
+  if (done && *done) return;
+  __shared__ double red[KM][33];
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  double acc[KM];
+#pragma unroll
+  for (int j = 0; j < KM; ++j) acc[j] = 0.0;
+  for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
+    const int i = cl % q.nx, tt = cl / q.nx, jj = tt % q.ny, k = tt / q.ny;
+    const int ex = q.x0 + i, ey = q.y0 + jj, ez = q.z0 + k;
+    const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    T r = (T)x[cg];
+    if (HAS_Y) r -= apply_A(g, cg, ex, ey, ez, tx, ty, tz, diag, y);
+    const T* ph = phi + cg * kmax;
+#pragma unroll
+    for (int j = 0; j < KM; ++j)
+      if (j < kmax) acc[j] += (double)(ph[j] * r);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < KM; ++j) {
+    double v = warp_sum(acc[j]);
+    if (lane == 0) red[j][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kmax) {
+    double v = 0.0;
+    for (int w = 0; w < nw; ++w) v += red[threadIdx.x][w];
+    c[(long long)blockIdx.x * kmax + threadIdx.x] = v;
+  }
+}
+
+template <typename T, int KM>
+static void rr_dispatch(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
+                        const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
+                        const int* done, cudaStream_t st) {
+  if (y)
+    k_resid_restrict<T, KM, true><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done);
+  else
+    k_resid_restrict<T, KM, false><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done);
+}
+
+template <typename T>
+void launch_resid_restrict(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
+                           const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
+                           const int* done, cudaStream_t st) {
+  if (kmax <= 4)
+    rr_dispatch<T, 4>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+  else if (kmax <= 8)
+    rr_dispatch<T, 8>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+  else
+    rr_dispatch<T, 16>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+}
+
+// Prolongation y += Phi_s Z_s (VecMAXPY in _PC_apply_vec_lv2, :1578).
+template <typename T, int KM>
+__global__ void k_prolong(Grid g, const SubInfo* subs, int kmax, const T* phi, const double* Z, T* y,
+                          const int* done) {
+  if (done && *done) return;
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  T z[KM];
+#pragma unroll
+  for (int j = 0; j < KM; ++j) z[j] = j < kmax ? (T)Z[(long long)blockIdx.x * kmax + j] : (T)0;
+  for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
+    const int i = cl % q.nx, tt = cl / q.nx, jj = tt % q.ny, k = tt / q.ny;
+    const long long cg = ((long long)(q.z0 + k) * g.N + (q.y0 + jj)) * g.M + (q.x0 + i);
+    const T* ph = phi + cg * kmax;
+    T v = y[cg];
+#pragma unroll
+    for (int j = 0; j < KM; ++j)
+      if (j < kmax) v += ph[j] * z[j];
+    y[cg] = v;
+  }
+}
+
+template <typename T>
+void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* phi, const double* Z, T* y,
+                    const int* done, cudaStream_t st) {
+  if (kmax <= 4)
+    k_prolong<T, 4><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+  else if (kmax <= 8)
+    k_prolong<T, 8><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+  else
+    k_prolong<T, 16><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+}
+
+#define PMF_INST(T)                                                                                              \
+  template void launch_ic_apply<T>(const Grid&, const SubInfo*, int, int, int, const T*, const T*, const T*,      \
+                                   const T*, const T*, const double*, const T*, T*, double*, double*, const int*, \
+                                   cudaStream_t);                                                                \
+  template void launch_resid_restrict<T>(const Grid&, const SubInfo*, int, int, const T*, const T*, const T*,     \
+                                         const T*, const T*, const double*, const T*, double*, const int*,        \
+                                         cudaStream_t);                                                           \
+  template void launch_prolong<T>(const Grid&, const SubInfo*, int, int, const T*, const double*, T*, const int*, \
+                                  cudaStream_t);
+PMF_INST(float)
+PMF_INST(double)
+#undef PMF_INST
+
+}  // namespace pmf

@@ -1,0 +1,136 @@
+// Host-side launchers for the B200 PreMixFEM kernels (internal interface).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pmf_common.cuh"
+
+namespace pmf {
+
+// Scalars of the preconditioned CG loop, resident on the device so that an
+// iteration needs no host round trip (PETSc KSPSolve_CG recurrences).
+struct PcgState {
+  double dp, ttol, beta, betaold, dpi, dpiold, alpha, rnorm0;
+  int its, max_it, first, done;  // done: 0 running, 1 converged, 2 max_it, 3 indefinite, 4 nan
+};
+
+constexpr int kCellThreads = 256;
+int cell_blocks(long long n);  // grid size for grid-stride cell loops (fixed per n)
+
+// ---- operator ----------------------------------------------------------------
+struct AssembleArgs {
+  Grid g;
+  const double *kx, *ky, *kz;  // permeability per direction (device)
+  double cx, cy, cz;           // |face|^2/|cell| per direction
+  double dir_val[6];           // Dirichlet value per face (x-,x+,y-,y+,z-,z+)
+  int dir_on[6];
+};
+void launch_assemble(const AssembleArgs& a, double* tx, double* ty, double* tz, double* diag, double* db,
+                     double* bval, cudaStream_t st);
+void launch_to_f32(const double* in, float* out, long long n, cudaStream_t st);
+void launch_to_f64(const float* in, double* out, long long n, cudaStream_t st);
+
+// y = A x (FP64 operator).
+void launch_spmv(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                 const double* x, double* y, cudaStream_t st);
+
+// ---- PCG -----------------------------------------------------------------------
+void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,
+                      int max_it, cudaStream_t st);
+// beta = z.r from nparts per-block partials (written by the preconditioner's last kernel).
+void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream_t st);
+// same, computing the partials itself
+void launch_pcg_beta(const double* r, const double* z, long long n, double* part, PcgState* s, cudaStream_t st);
+void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                       const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
+                       cudaStream_t st);
+void launch_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
+                       PcgState* s, cudaStream_t st);
+void launch_dot(const double* a, const double* b, long long n, double* part, double* out, cudaStream_t st);
+
+// ---- level 1 (IC(0) block solves) -------------------------------------------
+void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_lines, const double* tx, const double* ty,
+                      const double* tz, const double* diag, double* inv_d, int* bad, cudaStream_t st);
+
+// out = yin + IC^-1 (x - A yin)   (yin may be null -> rhs = x).
+// T: precision of the sweep; x is FP64 (the CG residual) or T; out is T or
+// FP64 (final visit, with dot(x, out) per subdomain written to part).
+template <typename T>
+void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines, int max_cells, const T* tx,
+                     const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
+                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st);
+
+// c[s*kmax + j] = sum_{cells of s} phi[c*kmax + j] * (x - A y)[c]   (y may be null)
+template <typename T>
+void launch_resid_restrict(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
+                           const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
+                           const int* done, cudaStream_t st);
+
+// y[c] += sum_j phi[c*kmax + j] * Z[s*kmax + j]
+template <typename T>
+void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* phi, const double* Z, T* y,
+                    const int* done, cudaStream_t st);
+
+// ---- coarse (FP64) -------------------------------------------------------------
+// out = alpha*v_in_out_base - A2 * v   where A2 is block sparse: blk[s][b][kmax][kmax],
+// b = 0 diagonal, 1..6 couplings to nb[b-1].  If base is null the base term is 0.
+void launch_a2_mult(const SubInfo* subs, int nsub, int kmax, const double* blk, const double* v, const double* base,
+                    double* out, const int* done, cudaStream_t st);
+// out[r][i] = sum_j inv[r][i][j] * in[r][j] for nrank dense blocks of size nr (batched GEMV).
+void launch_block_gemv(int nrank, int nr, const double* inv, const double* in, double* out, int accumulate,
+                       const int* done, cudaStream_t st);
+// Level-3 restriction / prolongation with the per-rank eigenvector blocks V[r][nr][en2].
+void launch_lv3_restrict(int nrank, int nr, int en2, const double* V, const double* c, double* d, const int* done,
+                         cudaStream_t st);
+void launch_lv3_prolong(int nrank, int nr, int en2, const double* V, const double* w, double* dz, const int* done,
+                        cudaStream_t st);
+void launch_axpy(long long n, double a, const double* x, double* y, const int* done, cudaStream_t st);
+void launch_copy(long long n, const double* x, double* y, const int* done, cudaStream_t st);
+
+// ---- coarse setup ----------------------------------------------------------------
+template <typename T>
+void launch_galerkin(const Grid& g, const SubInfo* subs, int nsub, int kmax, const double* tx, const double* ty,
+                     const double* tz, const double* diag, const T* phi, double* blk, double* gface,
+                     cudaStream_t st);
+// dense per-rank matrices from the block-sparse coarse operator.
+// mode 0: principal block of Phi^T A Phi (level 2); mode 1: rank-Neumann (level 3 eigen)
+void launch_assemble_dense(const SubInfo* subs, int nsub, int nrank, int spr, int kmax, const double* blk,
+                           const double* gface, int mode, double* dense, cudaStream_t st);
+// In-place batched SPD inverse by Gauss-Jordan; pivots <= tol*max|diag| are null directions.
+void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st);
+
+// ---- eigen solvers -----------------------------------------------------------------
+struct LobpcgArgs {
+  Grid g;
+  const SubInfo* subs;
+  int nsub;
+  int k;      // eigenpairs wanted (en_lv1)
+  int m;      // block size (k + guard)
+  int kmax;   // phi stride
+  int eg_op;  // mass matrix variant
+  int max_it;
+  double tol;
+  double sigma_rel;  // IC(0) preconditioner shift, relative
+  unsigned long long seed;
+  const double *tx, *ty, *tz, *diag, *db;  // FP64 operator
+  const double *kx, *ky, *kz;              // permeability (for the MOD/MEAN mass)
+  double Hx, Hy, Hz, meas;
+  const double* xinit;  // optional initial block (per cell, m values), may be null
+  int dirichlet_mask;   // bit f set: face f (x-,x+,y-,y+,z-,z+) is a Dirichlet face
+  int ld;               // column stride of the work block vectors (set by the launcher)
+};
+// Work buffer size in bytes for the LOBPCG kernel, per concurrently processed subdomain.
+size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes);
+// One persistent CTA per block; each handles subdomains blockIdx.x, +nblocks, ...
+// ks[s] receives the adaptive eigen count (first j with lambda_j >= eb, else k).
+// Requires ny*nz <= 512 and cells <= PMF_MAX_SUB_CELLS, m <= 10.
+template <typename T>
+void launch_lobpcg(const LobpcgArgs& a, int nblocks, void* work, T* phi, double* evals, int* iters, int* status,
+                   int* ks, double eb, int max_cells, int max_lines, cudaStream_t st);
+
+// Level-3 eigenpairs: smallest en2 of dense symmetric A[r] (nr x nr), via subspace
+// iteration with the inverse of (A + mu I) (given as inv) and Rayleigh-Ritz.
+void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
+                               double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st);
+
+}  // namespace pmf

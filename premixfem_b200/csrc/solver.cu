@@ -1,0 +1,774 @@
+// Solver orchestration: setup stages (_PC_setup, src/PreMixFEM_3D.c:1392-1427),
+// the V/W-cycle executor (PC_apply_vec, :1840-1936) and the preconditioned CG
+// loop (PETSc KSPCG as driven by src/Expe_scal.c:100-119).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+
+#include "solver.h"
+
+namespace pmf {
+
+// ---------------------------------------------------------------------------
+// options
+void OptionDB::parse(const std::string& s) {
+  std::istringstream is(s);
+  std::vector<std::string> tok;
+  std::string t;
+  while (is >> t) tok.push_back(t);
+  for (size_t i = 0; i < tok.size(); ++i) {
+    if (tok[i].size() > 1 && tok[i][0] == '-' && !(tok[i][1] >= '0' && tok[i][1] <= '9') && tok[i][1] != '.') {
+      std::string v;
+      if (i + 1 < tok.size()) {
+        const std::string& n = tok[i + 1];
+        const bool is_opt = n.size() > 1 && n[0] == '-' && !(n[1] >= '0' && n[1] <= '9') && n[1] != '.';
+        if (!is_opt) {
+          v = n;
+          ++i;
+        }
+      }
+      kv[tok[i - (v.empty() ? 0 : 1)].substr(1)] = v;
+    }
+  }
+}
+bool OptionDB::get_int(const char* name, int* v) const {
+  auto it = kv.find(name);
+  if (it == kv.end() || it->second.empty()) return false;
+  *v = (int)strtol(it->second.c_str(), nullptr, 10);
+  return true;
+}
+bool OptionDB::get_real(const char* name, double* v) const {
+  auto it = kv.find(name);
+  if (it == kv.end() || it->second.empty()) return false;
+  *v = strtod(it->second.c_str(), nullptr);
+  return true;
+}
+bool OptionDB::get_ints(const char* name, int* v, int n) const {
+  auto it = kv.find(name);
+  if (it == kv.end() || it->second.empty()) return false;
+  std::string s = it->second;
+  for (auto& ch : s)
+    if (ch == ',') ch = ' ';
+  std::istringstream is(s);
+  int cnt = 0;
+  while (cnt < n && (is >> v[cnt])) ++cnt;
+  if (cnt == 1)
+    for (int i = 1; i < n; ++i) v[i] = v[0];
+  return cnt > 0;
+}
+
+// PC_init option semantics (src/PreMixFEM_3D.c:1662-1721).
+int options_from_db(const OptionDB& db, Options* o, std::string* err) {
+  int sd = 2;
+  const bool has_sd = db.get_int("sd", &sd);
+  if (has_sd && sd < 1) {
+    *err = "Error in sub_domains (-sd must be >= 1)";
+    return 62;  // PETSC_ERR_ARG_WRONG
+  }
+  if (sd == 1) sd = 2;  // :1718-1721
+  o->sd[0] = o->sd[1] = o->sd[2] = sd;
+  db.get_ints("pmf_sd", o->sd, 3);
+  db.get_ints("pmf_vranks", o->vranks, 3);
+  if (db.get_int("si_lv1", &o->si_lv1)) o->si_lv1 = std::max(1, o->si_lv1);
+  if (db.get_int("si_lv2", &o->si_lv2)) o->si_lv2 = std::max(1, o->si_lv2);
+  db.get_int("en_lv1", &o->en_lv1);
+  db.get_int("en_lv2", &o->en_lv2);
+  if (o->en_lv1 < 1 || o->en_lv2 < 1) {
+    *err = "Error in max_eigen_num (-en_lv1/-en_lv2 must be >= 1)";
+    return 62;
+  }
+  db.get_int("eg_op", &o->eg_op);
+  if (o->eg_op < 0 || o->eg_op > 2) {
+    *err = "Error in lv2_eigen_op (-eg_op must be 0, 1 or 2)";
+    return 62;
+  }
+  db.get_real("eb_lv1", &o->eb_lv1);
+  db.get_real("eb_lv2", &o->eb_lv2);
+  o->use_W_cycle = db.has("use_W_cycle");
+  o->no_shift_A_cc = db.has("no_shift_A_cc");
+  o->use_full_Cholesky_lv1 = db.has("use_full_Cholesky_lv1");
+  o->use_2level = db.has("use_2level");
+  db.get_real("ksp_rtol", &o->rtol);
+  db.get_int("ksp_max_it", &o->max_it);
+  std::string prec;
+  auto it = db.kv.find("pmf_precision");
+  if (it != db.kv.end()) {
+    if (it->second == "mixed" || it->second == "fp32")
+      o->precision = 1;
+    else if (it->second == "fp64" || it->second == "double")
+      o->precision = 0;
+    else {
+      *err = "Error in -pmf_precision (fp64 | mixed)";
+      return 62;
+    }
+  }
+  db.get_int("pmf_eig_max_it", &o->eig_max_it);
+  db.get_real("pmf_eig_tol", &o->eig_tol);
+  db.get_real("pmf_eig_sigma", &o->eig_sigma);
+  db.get_int("pmf_eig_guard", &o->eig_guard);
+  db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
+  if (o->use_full_Cholesky_lv1) {
+    *err = "-use_full_Cholesky_lv1 is not supported by this build (IC(0) only)";
+    return 56;  // PETSC_ERR_SUP
+  }
+  if (o->use_2level) {
+    *err = "-use_2level is not supported by this build (three-level cycle only)";
+    return 56;
+  }
+  return 0;
+}
+
+static void split(int n, int parts, std::vector<int>& start, std::vector<int>& len) {
+  start.assign(parts, 0);
+  len.assign(parts, 0);
+  for (int i = 0; i < parts; ++i) len[i] = n / parts + ((n % parts) > i ? 1 : 0);
+  for (int i = 1; i < parts; ++i) start[i] = start[i - 1] + len[i - 1];
+}
+
+// ---------------------------------------------------------------------------
+// small setup kernels
+__global__ void k_add_diag(int nb, int n, double* a, double mu_rel, int relative) {
+  const int b = blockIdx.x;
+  double* A = a + (long long)b * n * n;
+  __shared__ double mx;
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) m = fmax(m, fabs(A[(long long)i * n + i]));
+    mx = relative ? m * mu_rel : mu_rel;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) A[(long long)i * n + i] += mx;
+}
+
+// A3 = V^T (Phi^T A Phi) V block (r, r2): sum over subdomains s of rank r and the
+// block-sparse coupling to subdomains of rank r2.  Padded level-3 dofs are identity.
+__global__ void k_build_a3(const SubInfo* subs, int spr, int kmax, int en2, const double* blk, const double* V,
+                           const int* rank_nb, const int* ks3, double* A3, int n3, double nil) {
+  const int r = blockIdx.x / 7, q = blockIdx.x % 7;
+  const int r2 = q == 0 ? r : rank_nb[r * 6 + q - 1];
+  if (r2 < 0) return;
+  const int nr = spr * kmax;
+  for (int e = threadIdx.x; e < en2 * en2; e += blockDim.x) {
+    const int j = e / en2, j2 = e % en2;
+    double v = 0.0;
+    if (j < ks3[r] && j2 < ks3[r2]) {
+      for (int a = 0; a < spr; ++a) {
+        const int s = r * spr + a;
+        const SubInfo& S = subs[s];
+        for (int b = 0; b < 7; ++b) {
+          const int nb = b == 0 ? s : S.nb[b - 1];
+          if (nb < 0 || subs[nb].rank != r2) continue;
+          const int la = subs[nb].local;
+          const double* B = blk + ((long long)s * 7 + b) * kmax * kmax;
+          for (int i = 0; i < kmax; ++i) {
+            const double vi = V[((long long)r * nr + a * kmax + i) * en2 + j];
+            if (vi == 0.0) continue;
+            double t = 0.0;
+            for (int i2 = 0; i2 < kmax; ++i2) t += B[i * kmax + i2] * V[((long long)r2 * nr + la * kmax + i2) * en2 + j2];
+            v += vi * t;
+          }
+        }
+      }
+      if (q == 0 && j == j2) v += nil;
+    } else if (q == 0 && j == j2) {
+      v = 1.0;
+    }
+    A3[(long long)(r * en2 + j) * n3 + (r2 * en2 + j2)] = v;
+  }
+}
+
+__global__ void k_zero_v_cols(int nrank, int nr, int en2, double* V, const int* ks3) {
+  const long long n = (long long)nrank * nr * en2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / ((long long)nr * en2));
+    const int j = (int)(e % en2);
+    if (j >= ks3[r]) V[e] = 0.0;
+  }
+}
+
+__global__ void k_zero_d(double* a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+int Solver::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return 0;
+  err = std::string(what) + ": " + cudaGetErrorString(e);
+  return 76;  // PETSC_ERR_LIB
+}
+
+Solver::Solver(const double d[3], const int mesh[3], const Options& o) : opt(o) {
+  for (int i = 0; i < 3; ++i) dom[i] = d[i];
+  g.M = mesh[0];
+  g.N = mesh[1];
+  g.P = mesh[2];
+  g.MN = g.M * g.N;
+  g.ncell = (long long)g.M * g.N * g.P;
+  H[0] = dom[0] / (double)g.M;  // :1707-1709
+  H[1] = dom[1] / (double)g.N;
+  H[2] = dom[2] / (double)g.P;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaMallocHost(&h_state, sizeof(PcgState));
+}
+
+Solver::~Solver() {
+  if (st) cudaStreamSynchronize(st);
+  void* ptrs[] = {d_subs, kx,    ky,    kz,    tx,     ty,    tz,     diag,     db,       bval,    tx32,  ty32,
+                  tz32,   diag32, inv32, inv64, phi,    blk,   gface,  A2inv,    AN,       ANinv,   V3,    A3inv,
+                  d_eig1, d_eig3, d_ks,  d_iters, d_status, d_l3it, d_flag, d_rank_nb, eig_work, c,     dz,    Zacc,
+                  d3,     w3,     y0,    y1,    vb,     vx,    r,      z,        p0,       p1,      w,     part,
+                  state};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h_state) cudaFreeHost(h_state);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (st) cudaStreamDestroy(st);
+}
+
+int Solver::build_partition() {
+  const int px = opt.vranks[0], py = opt.vranks[1], pz = opt.vranks[2];
+  const int sx = opt.sd[0], sy = opt.sd[1], sz = opt.sd[2];
+  if (px < 1 || py < 1 || pz < 1 || sx < 1 || sy < 1 || sz < 1) {
+    err = "virtual rank grid and subdomain counts must be positive";
+    return 62;
+  }
+  rank_grid[0] = px;
+  rank_grid[1] = py;
+  rank_grid[2] = pz;
+  std::vector<int> rxs, rxl, rys, ryl, rzs, rzl;
+  split(g.M, px, rxs, rxl);
+  split(g.N, py, rys, ryl);
+  split(g.P, pz, rzs, rzl);
+  nrank = px * py * pz;
+  spr = sx * sy * sz;
+  nsub = nrank * spr;
+  subs.assign(nsub, SubInfo());
+  const int GX = px * sx, GY = py * sy, GZ = pz * sz;
+  std::vector<int> gmap((size_t)GX * GY * GZ, -1);
+  max_cells = 0;
+  max_lines = 0;
+  for (int kz = 0; kz < pz; ++kz)
+    for (int ky = 0; ky < py; ++ky)
+      for (int kx_ = 0; kx_ < px; ++kx_) {
+        const int rr = (kz * py + ky) * px + kx_;
+        std::vector<int> xs, xl, ys, yl, zs, zl;
+        split(rxl[kx_], sx, xs, xl);
+        split(ryl[ky], sy, ys, yl);
+        split(rzl[kz], sz, zs, zl);
+        for (int cz = 0; cz < sz; ++cz)
+          for (int cy = 0; cy < sy; ++cy)
+            for (int cx = 0; cx < sx; ++cx) {
+              const int loc = (cz * sy + cy) * sx + cx;
+              const int s = rr * spr + loc;
+              SubInfo& S = subs[s];
+              S.x0 = rxs[kx_] + xs[cx];
+              S.nx = xl[cx];
+              S.y0 = rys[ky] + ys[cy];
+              S.ny = yl[cy];
+              S.z0 = rzs[kz] + zs[cz];
+              S.nz = zl[cz];
+              S.rank = rr;
+              S.local = loc;
+              S.k = opt.en_lv1;
+              S.pad = 0;
+              if (S.nx < 1 || S.ny < 1 || S.nz < 1) {
+                err = "empty subdomain: too many subdomains or ranks for the mesh";
+                return 62;
+              }
+              const int gx = kx_ * sx + cx, gy = ky * sy + cy, gz = kz * sz + cz;
+              gmap[((size_t)gz * GY + gy) * GX + gx] = s;
+              max_cells = std::max(max_cells, S.nx * S.ny * S.nz);
+              max_lines = std::max(max_lines, S.ny * S.nz);
+            }
+      }
+  for (int s = 0; s < nsub; ++s) {
+    SubInfo& S = subs[s];
+    const int kx_ = (S.rank % px), ky = (S.rank / px) % py, kz = S.rank / (px * py);
+    const int cx = S.local % sx, cy = (S.local / sx) % sy, cz = S.local / (sx * sy);
+    const int gx = kx_ * sx + cx, gy = ky * sy + cy, gz = kz * sz + cz;
+    auto at = [&](int x, int y, int zz) -> int {
+      if (x < 0 || y < 0 || zz < 0 || x >= GX || y >= GY || zz >= GZ) return -1;
+      return gmap[((size_t)zz * GY + y) * GX + x];
+    };
+    S.nb[0] = at(gx - 1, gy, gz);
+    S.nb[1] = at(gx + 1, gy, gz);
+    S.nb[2] = at(gx, gy - 1, gz);
+    S.nb[3] = at(gx, gy + 1, gz);
+    S.nb[4] = at(gx, gy, gz - 1);
+    S.nb[5] = at(gx, gy, gz + 1);
+  }
+  if (max_cells > PMF_MAX_SUB_CELLS || max_lines > 512) {
+    err = "subdomain too large for the shared-memory sweeps (cells <= 8192, ny*nz <= 512)";
+    return 62;
+  }
+  kmax = opt.en_lv1;
+  if (kmax > 8 || opt.en_lv1 + opt.eig_guard > 10) {
+    err = "en_lv1 must be <= 8 (block size en_lv1 + guard <= 10)";
+    return 62;
+  }
+  if (kmax > max_cells) {
+    err = "en_lv1 larger than a subdomain";
+    return 62;
+  }
+  nr = spr * kmax;
+  en2 = std::min(opt.en_lv2, nr);
+  n3 = nrank * en2;
+  if (nr > 4096 || n3 > 8192) {
+    err = "coarse blocks too large (subdomains per rank * en_lv1 <= 4096, ranks * en_lv2 <= 8192)";
+    return 62;
+  }
+  return 0;
+}
+
+void Solver::alloc_fine() {
+  const size_t n = (size_t)g.ncell;
+  cudaMalloc(&tx, n * 8);
+  cudaMalloc(&ty, n * 8);
+  cudaMalloc(&tz, n * 8);
+  cudaMalloc(&diag, n * 8);
+  cudaMalloc(&db, n * 8);
+  cudaMalloc(&bval, n * 8);
+  cudaMalloc(&inv64, n * 8);
+  cudaMalloc(&vb, n * 8);
+  cudaMalloc(&vx, n * 8);
+  cudaMalloc(&r, n * 8);
+  cudaMalloc(&z, n * 8);
+  cudaMalloc(&p0, n * 8);
+  cudaMalloc(&p1, n * 8);
+  cudaMalloc(&w, n * 8);
+  const size_t pb = opt.precision == 1 ? 4 : 8;
+  cudaMalloc(&y0, n * pb);
+  cudaMalloc(&y1, n * pb);
+  cudaMalloc(&phi, n * kmax * pb);
+  if (opt.precision == 1) {
+    cudaMalloc(&tx32, n * 4);
+    cudaMalloc(&ty32, n * 4);
+    cudaMalloc(&tz32, n * 4);
+    cudaMalloc(&diag32, n * 4);
+    cudaMalloc(&inv32, n * 4);
+  }
+  const int nparts = std::max(cell_blocks(g.ncell), nsub) + 64;
+  cudaMalloc(&part, nparts * 8);
+  cudaMalloc(&state, sizeof(PcgState));
+}
+
+int Solver::set_kappa(const double* k0, const double* k1, const double* k2, bool on_device) {
+  if (int e = build_partition()) return e;
+  const size_t n = (size_t)g.ncell;
+  if (!kx) {
+    if (int e = check(cudaMalloc(&kx, n * 8), "cudaMalloc kappa")) return e;
+    cudaMalloc(&ky, n * 8);
+    cudaMalloc(&kz, n * 8);
+  }
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaMemcpyAsync(kx, k0, n * 8, kind, st);
+  cudaMemcpyAsync(ky, k1 ? k1 : k0, n * 8, kind, st);
+  cudaMemcpyAsync(kz, k2 ? k2 : k0, n * 8, kind, st);
+  return check(cudaStreamSynchronize(st), "set_kappa");
+}
+
+int Solver::set_dirichlet(int face, double value) {
+  if (face < 0 || face > 5) {
+    err = "Dirichlet face must be 0..5 (x-,x+,y-,y+,z-,z+)";
+    return 62;
+  }
+  dir_on_[face] = 1;
+  dir_val_[face] = value;
+  return 0;
+}
+
+std::vector<int> Solver::schedule() const {
+  std::vector<int> s;
+  for (int i = 0; i < opt.si_lv1; ++i) s.push_back(1);
+  for (int i = 0; i < opt.si_lv2; ++i) s.push_back(2);
+  s.push_back(3);
+  if (opt.use_W_cycle) {  // :1857-1894
+    for (int i = 0; i < opt.si_lv2; ++i) s.push_back(2);
+    s.push_back(3);
+  }
+  for (int i = 0; i < opt.si_lv2; ++i) s.push_back(2);
+  for (int i = 0; i < opt.si_lv1; ++i) s.push_back(1);
+  return s;
+}
+
+int Solver::setup() {
+  if (!kx) {
+    err = "kappa not set (PC_init contract: the caller constructs kappa before setup)";
+    return 73;  // PETSC_ERR_ARG_WRONGSTATE
+  }
+  cudaEvent_t e[8];
+  for (auto& x : e) cudaEventCreate(&x);
+  const bool mixed = opt.precision == 1;
+  if (!tx) alloc_fine();
+  if (!d_subs) cudaMalloc(&d_subs, sizeof(SubInfo) * nsub);
+  cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
+  cudaEventRecord(e[0], st);
+  // operator (PC_create_A) and level 1
+  AssembleArgs aa;
+  aa.g = g;
+  aa.kx = kx;
+  aa.ky = ky;
+  aa.kz = kz;
+  const double meas = H[0] * H[1] * H[2];
+  const double fyz = H[1] * H[2], fzx = H[2] * H[0], fxy = H[0] * H[1];
+  aa.cx = fyz * fyz / meas;
+  aa.cy = fzx * fzx / meas;
+  aa.cz = fxy * fxy / meas;
+  int dmask = 0;
+  for (int f = 0; f < 6; ++f) {
+    aa.dir_on[f] = dir_on_[f];
+    aa.dir_val[f] = dir_val_[f];
+    if (dir_on_[f]) dmask |= 1 << f;
+  }
+  launch_assemble(aa, tx, ty, tz, diag, db, bval, st);
+  if (!d_flag) cudaMalloc(&d_flag, 4 * sizeof(int));
+  cudaMemsetAsync(d_flag, 0, 4 * sizeof(int), st);
+  launch_ic_factor(g, d_subs, nsub, max_lines, tx, ty, tz, diag, inv64, d_flag, st);
+  if (mixed) {
+    launch_to_f32(tx, tx32, g.ncell, st);
+    launch_to_f32(ty, ty32, g.ncell, st);
+    launch_to_f32(tz, tz32, g.ncell, st);
+    launch_to_f32(diag, diag32, g.ncell, st);
+    launch_to_f32(inv64, inv32, g.ncell, st);
+  }
+  cudaEventRecord(e[1], st);
+  // level-2 local eigenproblems
+  if (!d_eig1) {
+    cudaMalloc(&d_eig1, sizeof(double) * nsub * opt.en_lv1);
+    cudaMalloc(&d_ks, sizeof(int) * nsub);
+    cudaMalloc(&d_iters, sizeof(int) * nsub);
+    cudaMalloc(&d_status, sizeof(int) * nsub);
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int eig_blocks = std::min(nsub, nsm);
+  LobpcgArgs la;
+  la.g = g;
+  la.subs = d_subs;
+  la.nsub = nsub;
+  la.k = opt.en_lv1;
+  la.m = opt.en_lv1 + opt.eig_guard;
+  la.kmax = kmax;
+  la.eg_op = opt.eg_op;
+  la.max_it = opt.eig_max_it;
+  la.tol = opt.eig_tol;
+  la.sigma_rel = opt.eig_sigma;
+  la.seed = opt.seed;
+  la.tx = tx;
+  la.ty = ty;
+  la.tz = tz;
+  la.diag = diag;
+  la.db = db;
+  la.kx = kx;
+  la.ky = ky;
+  la.kz = kz;
+  la.Hx = H[0];
+  la.Hy = H[1];
+  la.Hz = H[2];
+  la.meas = meas;
+  la.xinit = nullptr;
+  la.dirichlet_mask = dmask;
+  la.ld = 0;
+  const size_t need = ((lobpcg_work_bytes(max_cells, la.m, mixed ? 4 : 8) + 255) & ~(size_t)255) * eig_blocks;
+  if (eig_work_bytes < need) {
+    if (eig_work) cudaFree(eig_work);
+    if (int er = check(cudaMalloc(&eig_work, need), "cudaMalloc eigen work")) return er;
+    eig_work_bytes = need;
+  }
+  const double eb1 = opt.eb_lv1 < 0 ? 1.0e12 : opt.eb_lv1;  // 1/NIL
+  if (mixed)
+    launch_lobpcg<float>(la, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                         max_lines, st);
+  else
+    launch_lobpcg<double>(la, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                          max_lines, st);
+  cudaEventRecord(e[2], st);
+  if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;
+  ks.resize(nsub);
+  eig_iters.resize(nsub);
+  eig_status.resize(nsub);
+  eig1.resize((size_t)nsub * opt.en_lv1);
+  cudaMemcpy(ks.data(), d_ks, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+  cudaMemcpy(eig_iters.data(), d_iters, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+  cudaMemcpy(eig_status.data(), d_status, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+  cudaMemcpy(eig1.data(), d_eig1, sizeof(double) * eig1.size(), cudaMemcpyDeviceToHost);
+  int bad_pivots = 0;
+  cudaMemcpy(&bad_pivots, d_flag, sizeof(int), cudaMemcpyDeviceToHost);
+  if (bad_pivots) {
+    err = "non-positive IC(0) pivot in a level-1 factorisation";
+    return 71;  // PETSC_ERR_MAT_LU_ZRPVT
+  }
+  for (int s = 0; s < nsub; ++s) subs[s].k = ks[s];
+  cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
+  // level-2 Galerkin (Phi^T A Phi) and per-rank inverses
+  if (!blk) {
+    cudaMalloc(&blk, sizeof(double) * nsub * 7 * kmax * kmax);
+    cudaMalloc(&gface, sizeof(double) * nsub * 6 * kmax * kmax);
+    cudaMalloc(&A2inv, sizeof(double) * nrank * nr * nr);
+    cudaMalloc(&AN, sizeof(double) * nrank * nr * nr);
+    cudaMalloc(&ANinv, sizeof(double) * nrank * nr * nr);
+    cudaMalloc(&V3, sizeof(double) * nrank * nr * en2);
+    cudaMalloc(&d_eig3, sizeof(double) * nrank * en2);
+    cudaMalloc(&d_l3it, sizeof(int) * nrank);
+    cudaMalloc(&A3inv, sizeof(double) * n3 * n3);
+    cudaMalloc(&c, sizeof(double) * nsub * kmax);
+    cudaMalloc(&dz, sizeof(double) * nsub * kmax);
+    cudaMalloc(&Zacc, sizeof(double) * nsub * kmax);
+    cudaMalloc(&d3, sizeof(double) * n3);
+    cudaMalloc(&w3, sizeof(double) * n3);
+    cudaMalloc(&d_rank_nb, sizeof(int) * nrank * 6);
+  }
+  if (mixed)
+    launch_galerkin<float>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const float*)phi, blk, gface, st);
+  else
+    launch_galerkin<double>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const double*)phi, blk, gface, st);
+  launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 0, A2inv, st);
+  launch_spd_inverse(nrank, nr, A2inv, 1e-14, d_flag + 1, st);
+  cudaEventRecord(e[3], st);
+  // level 3: rank-Neumann HEP
+  launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 1, AN, st);
+  cudaMemcpyAsync(ANinv, AN, sizeof(double) * nrank * nr * nr, cudaMemcpyDeviceToDevice, st);
+  k_add_diag<<<nrank, 256, 0, st>>>(nrank, nr, ANinv, 1e-8, 1);
+  launch_spd_inverse(nrank, nr, ANinv, 1e-14, d_flag + 2, st);
+  const int p = std::min(nr, std::min(32, 2 * en2 + 4));
+  double* l3work = nullptr;
+  if (int er = check(cudaMalloc(&l3work, sizeof(double) * nrank * 3 * nr * p), "cudaMalloc l3 work")) return er;
+  launch_dense_smallest_eig(nrank, nr, en2, p, AN, ANinv, V3, d_eig3, d_l3it, opt.l3_tol, opt.l3_max_it, l3work, st);
+  if (int er = check(cudaStreamSynchronize(st), "level-3 eigensolve")) {
+    cudaFree(l3work);
+    return er;
+  }
+  cudaFree(l3work);
+  eig3.resize((size_t)nrank * en2);
+  l3_iters.resize(nrank);
+  cudaMemcpy(eig3.data(), d_eig3, sizeof(double) * eig3.size(), cudaMemcpyDeviceToHost);
+  cudaMemcpy(l3_iters.data(), d_l3it, sizeof(int) * nrank, cudaMemcpyDeviceToHost);
+  const double eb2 = opt.eb_lv2 < 0 ? 1.0e12 : opt.eb_lv2;
+  ks3.assign(nrank, en2);
+  for (int rr = 0; rr < nrank; ++rr)
+    for (int j = 0; j < en2; ++j)
+      if (eig3[(size_t)rr * en2 + j] >= eb2) {  // :1100-1115
+        ks3[rr] = j + 1;
+        break;
+      }
+  std::vector<int> rnb((size_t)nrank * 6, -1);
+  for (int rr = 0; rr < nrank; ++rr) {
+    const int px = rank_grid[0], py = rank_grid[1], pz = rank_grid[2];
+    const int rx = rr % px, ry = (rr / px) % py, rz = rr / (px * py);
+    auto at = [&](int x, int y, int zz) { return (x < 0 || y < 0 || zz < 0 || x >= px || y >= py || zz >= pz) ? -1 : (zz * py + y) * px + x; };
+    rnb[rr * 6 + 0] = at(rx - 1, ry, rz);
+    rnb[rr * 6 + 1] = at(rx + 1, ry, rz);
+    rnb[rr * 6 + 2] = at(rx, ry - 1, rz);
+    rnb[rr * 6 + 3] = at(rx, ry + 1, rz);
+    rnb[rr * 6 + 4] = at(rx, ry, rz - 1);
+    rnb[rr * 6 + 5] = at(rx, ry, rz + 1);
+  }
+  int* d_ks3 = nullptr;
+  cudaMalloc(&d_ks3, sizeof(int) * nrank);
+  cudaMemcpyAsync(d_ks3, ks3.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_rank_nb, rnb.data(), sizeof(int) * nrank * 6, cudaMemcpyHostToDevice, st);
+  k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3);
+  cudaEventRecord(e[4], st);
+  k_zero_d<<<256, 256, 0, st>>>(A3inv, (long long)n3 * n3);
+  k_build_a3<<<nrank * 7, 64, 0, st>>>(d_subs, spr, kmax, en2, blk, V3, d_rank_nb, d_ks3, A3inv, n3,
+                                       opt.no_shift_A_cc ? 0.0 : 1.0e-12);
+  launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
+  cudaEventRecord(e[5], st);
+  if (int er = check(cudaStreamSynchronize(st), "coarse setup")) return er;
+  cudaFree(d_ks3);
+  float ms[5];
+  for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], e[i], e[i + 1]);
+  t_stages[ST_SU_LV1] += ms[0] * 1e-3;
+  t_stages[ST_SU_LV2_1] += ms[1] * 1e-3;
+  t_stages[ST_SU_LV2_2] += ms[2] * 1e-3;
+  t_stages[ST_SU_LV3_1] += ms[3] * 1e-3;
+  t_stages[ST_SU_LV3_2] += ms[4] * 1e-3;
+  float tot;
+  cudaEventElapsedTime(&tot, e[0], e[5]);
+  t_stages[ST_SU] += tot * 1e-3;
+  last_setup_ms = tot;
+  for (auto& x : e) cudaEventDestroy(x);
+  is_setup = true;
+  return 0;
+}
+
+template <typename T>
+void Solver::apply_impl(const double* x, double* out, double* partial, const int* done) {
+  const bool f32 = sizeof(T) == 4;
+  const T* ttx = f32 ? (const T*)tx32 : (const T*)tx;
+  const T* tty = f32 ? (const T*)ty32 : (const T*)ty;
+  const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
+  const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
+  const T* tinv = f32 ? (const T*)inv32 : (const T*)inv64;
+  const T* tphi = (const T*)phi;
+  T* yb[2] = {(T*)y0, (T*)y1};
+  const std::vector<int> sch = schedule();
+  int cur = 0;
+  bool y_zero = true, z_pend = false, c_valid = false;
+  const long long ncoarse = (long long)nsub * kmax;
+  for (size_t idx = 0; idx < sch.size(); ++idx) {
+    const int v = sch[idx];
+    const bool last = idx + 1 == sch.size();
+    if (v == 1) {
+      if (z_pend) {
+        launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st);
+        z_pend = false;
+      }
+      const T* yin = y_zero ? nullptr : yb[cur];
+      if (last)
+        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, nullptr, out,
+                           partial, done, st);
+      else {
+        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, yb[1 - cur],
+                           nullptr, nullptr, done, st);
+        cur = 1 - cur;
+      }
+      y_zero = false;
+      c_valid = false;
+    } else {
+      if (!c_valid) {
+        if (z_pend) {
+          launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st);
+          z_pend = false;
+        }
+        launch_resid_restrict<T>(g, d_subs, nsub, kmax, ttx, tty, ttz, tdg, tphi, x, y_zero ? nullptr : yb[cur], c,
+                                 done, st);
+        c_valid = true;
+      }
+      if (v == 2) {
+        launch_block_gemv(nrank, nr, A2inv, c, dz, 0, done, st);
+      } else {
+        launch_lv3_restrict(nrank, nr, en2, V3, c, d3, done, st);
+        launch_block_gemv(1, n3, A3inv, d3, w3, 0, done, st);
+        launch_lv3_prolong(nrank, nr, en2, V3, w3, dz, done, st);
+      }
+      if (z_pend)
+        launch_axpy(ncoarse, 1.0, dz, Zacc, done, st);
+      else
+        launch_copy(ncoarse, dz, Zacc, done, st);
+      z_pend = true;
+      const bool next_coarse = !last && sch[idx + 1] != 1;
+      if (next_coarse)
+        launch_a2_mult(d_subs, nsub, kmax, blk, dz, c, c, done, st);
+      else
+        c_valid = false;
+    }
+  }
+}
+
+void Solver::apply(const double* x, double* out, double* partial, const int* done) {
+  if (opt.precision == 1)
+    apply_impl<float>(x, out, partial, done);
+  else
+    apply_impl<double>(x, out, partial, done);
+}
+
+int Solver::rhs(const double* source, double* out, bool on_device) {
+  if (!is_setup) {
+    err = "setup not done";
+    return 73;
+  }
+  const size_t n = (size_t)g.ncell;
+  cudaMemcpyAsync(vb, source, n * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+  launch_axpy(g.ncell, 1.0, bval, vb, nullptr, st);
+  cudaMemcpyAsync(out, vb, n * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
+  return check(cudaStreamSynchronize(st), "rhs");
+}
+
+int Solver::apply_A(const double* x_in, double* y_out, bool on_device) {
+  if (!tx) {
+    err = "operator not assembled";
+    return 73;
+  }
+  const size_t n = (size_t)g.ncell;
+  const double* xs = x_in;
+  double* ys = y_out;
+  if (!on_device) {
+    cudaMemcpyAsync(vx, x_in, n * 8, cudaMemcpyHostToDevice, st);
+    xs = vx;
+    ys = w;
+  }
+  launch_spmv(g, tx, ty, tz, diag, xs, ys, st);
+  if (!on_device) cudaMemcpyAsync(y_out, ys, n * 8, cudaMemcpyDeviceToHost, st);
+  return check(cudaStreamSynchronize(st), "apply_A");
+}
+
+int Solver::pc_apply(const double* x_in, double* y_out, bool on_device) {
+  if (!is_setup) {
+    err = "setup not done";
+    return 73;
+  }
+  const size_t n = (size_t)g.ncell;
+  const double* xs = x_in;
+  double* ys = y_out;
+  if (!on_device) {
+    cudaMemcpyAsync(vx, x_in, n * 8, cudaMemcpyHostToDevice, st);
+    xs = vx;
+    ys = z;
+  }
+  cudaEventRecord(ev0, st);
+  apply(xs, ys, part, nullptr);
+  cudaEventRecord(ev1, st);
+  if (!on_device) cudaMemcpyAsync(y_out, ys, n * 8, cudaMemcpyDeviceToHost, st);
+  int e = check(cudaStreamSynchronize(st), "PC_apply_vec");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  t_stages[ST_AV] += ms * 1e-3;
+  return e;
+}
+
+int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, double* rnorm, int* reason) {
+  if (!is_setup) {
+    err = "setup not done";
+    return 73;
+  }
+  const size_t n = (size_t)g.ncell;
+  const double* bs = b_in;
+  double* xs = x_out;
+  if (!on_device) {
+    cudaMemcpyAsync(vb, b_in, n * 8, cudaMemcpyHostToDevice, st);
+    bs = vb;
+    xs = vx;
+  }
+  cudaEventRecord(ev0, st);
+  launch_pcg_start(g, bs, xs, r, part, state, opt.rtol, opt.max_it, st);
+  const int* done = &state->done;
+  apply(r, z, part, done);
+  launch_pcg_beta_fin(part, nparts_apply(), state, st);
+  double* pin = p0;
+  double* pout = p1;
+  int guard = 0;
+  for (;;) {
+    for (int c_ = 0; c_ < std::max(1, opt.pcg_chunk); ++c_) {
+      launch_pcg_iter_a(g, tx, ty, tz, diag, z, pin, pout, w, part, state, st);
+      launch_pcg_iter_b(g.ncell, xs, r, pout, w, part, state, st);
+      apply(r, z, part, done);
+      launch_pcg_beta_fin(part, nparts_apply(), state, st);
+      std::swap(pin, pout);
+    }
+    cudaMemcpyAsync(h_state, state, sizeof(PcgState), cudaMemcpyDeviceToHost, st);
+    if (int e = check(cudaStreamSynchronize(st), "KSPSolve")) return e;
+    if (h_state->done) break;
+    if (++guard > opt.max_it + 8) break;
+  }
+  cudaEventRecord(ev1, st);
+  if (!on_device) cudaMemcpyAsync(x_out, xs, n * 8, cudaMemcpyDeviceToHost, st);
+  int e = check(cudaStreamSynchronize(st), "KSPSolve");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  last_solve_ms = ms;
+  last_its = h_state->its;
+  if (its) *its = h_state->its;
+  if (rnorm) *rnorm = h_state->dp;
+  if (reason) *reason = h_state->done;
+  return e;
+}
+
+}  // namespace pmf

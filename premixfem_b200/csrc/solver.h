@@ -1,0 +1,124 @@
+// Host-side solver object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "pmf_kernels.h"
+
+namespace pmf {
+
+// Preconditioner options; names follow PC_init (src/PreMixFEM_3D.c:1662-1705)
+// plus the B200 extensions (-pmf_*).
+struct Options {
+  int sd[3] = {2, 2, 2};
+  int vranks[3] = {1, 1, 1};
+  int en_lv1 = 4, en_lv2 = 4;
+  double eb_lv1 = -1.0, eb_lv2 = -1.0;
+  int si_lv1 = 1, si_lv2 = 1;
+  int eg_op = 0;
+  bool use_W_cycle = false, no_shift_A_cc = false, use_full_Cholesky_lv1 = false, use_2level = false;
+  int precision = 0;  // 0 plain FP64, 1 FP32 preconditioner inside FP64 PCG
+  double rtol = 1e-8;
+  int max_it = 10000;
+  int eig_max_it = 300;
+  double eig_tol = 1e-6;
+  double eig_sigma = 1e-2;
+  int eig_guard = 2;
+  int l3_max_it = 500;
+  double l3_tol = 1e-10;
+  unsigned long long seed = 20240611ull;
+  int pcg_chunk = 4;
+};
+
+// PETSc-style options database ("-name value" pairs); flags carry an empty value.
+struct OptionDB {
+  std::map<std::string, std::string> kv;
+  void parse(const std::string& s);
+  bool has(const char* name) const { return kv.count(name) > 0; }
+  bool get_int(const char* name, int* v) const;
+  bool get_real(const char* name, double* v) const;
+  bool get_ints(const char* name, int* v, int n) const;  // "a,b,c"
+};
+int options_from_db(const OptionDB& db, Options* o, std::string* err);
+
+enum Stage {
+  ST_SU_LV1 = 0,
+  ST_SU_LV2_1,
+  ST_SU_LV2_2,
+  ST_SU_LV3_1,
+  ST_SU_LV3_2,
+  ST_AV_LV1,
+  ST_AV_LV2,
+  ST_AV_LV3,
+  ST_SU,
+  ST_AV,
+  ST_COUNT
+};
+
+class Solver {
+ public:
+  Solver(const double dom[3], const int mesh[3], const Options& o);
+  ~Solver();
+
+  int set_kappa(const double* kx, const double* ky, const double* kz, bool on_device);
+  int set_dirichlet(int face, double value);
+  int setup();
+  int rhs(const double* source, double* out, bool on_device);
+  int apply_A(const double* x, double* y, bool on_device);
+  int pc_apply(const double* x, double* y, bool on_device);
+  int solve(const double* b, double* x, bool on_device, int* its, double* rnorm, int* reason);
+
+  // introspection for tests and stats
+  Grid g;
+  double dom[3], H[3];
+  Options opt;
+  cudaStream_t st = nullptr;
+  std::vector<SubInfo> subs;
+  int nsub = 0, nrank = 0, spr = 0, kmax = 0, max_cells = 0, max_lines = 0, nr = 0, en2 = 0, n3 = 0;
+  int rank_grid[3];
+  bool is_setup = false;
+  std::vector<double> eig1, eig3;  // per subdomain k values / per rank en2 values
+  std::vector<int> ks, ks3, eig_iters, eig_status, l3_iters;
+  double t_stages[ST_COUNT] = {0};
+  std::string err;
+
+  // device data
+  SubInfo* d_subs = nullptr;
+  double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  double *tx = nullptr, *ty = nullptr, *tz = nullptr, *diag = nullptr, *db = nullptr, *bval = nullptr;
+  float *tx32 = nullptr, *ty32 = nullptr, *tz32 = nullptr, *diag32 = nullptr, *inv32 = nullptr;
+  double* inv64 = nullptr;
+  void* phi = nullptr;
+  double *blk = nullptr, *gface = nullptr, *A2inv = nullptr, *AN = nullptr, *ANinv = nullptr, *V3 = nullptr,
+         *A3inv = nullptr, *d_eig1 = nullptr, *d_eig3 = nullptr;
+  int *d_ks = nullptr, *d_iters = nullptr, *d_status = nullptr, *d_l3it = nullptr, *d_flag = nullptr;
+  int* d_rank_nb = nullptr;
+  void* eig_work = nullptr;
+  size_t eig_work_bytes = 0;
+  double *c = nullptr, *dz = nullptr, *Zacc = nullptr, *d3 = nullptr, *w3 = nullptr;
+  void *y0 = nullptr, *y1 = nullptr;
+  double *vb = nullptr, *vx = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *w = nullptr,
+         *part = nullptr;
+  PcgState* state = nullptr;
+  PcgState* h_state = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  int check(cudaError_t e, const char* what);
+  int build_partition();
+  void alloc_fine();
+  template <typename T>
+  void apply_impl(const double* x, double* out, double* partial, const int* done);
+  void apply(const double* x, double* out, double* partial, const int* done);
+  std::vector<int> schedule() const;
+  int dir_on_[6] = {0, 0, 0, 0, 0, 0};
+  double dir_val_[6] = {0, 0, 0, 0, 0, 0};
+  double last_setup_ms = 0, last_solve_ms = 0;
+  int last_its = 0;
+  int nparts_apply() const { return nsub; }
+};
+
+}  // namespace pmf

@@ -1,0 +1,161 @@
+"""GPU parity: libpremixfem_b200.so (through the C ABI) against the CPU oracle.
+
+Tolerances (FP64 plain form unless stated):
+  * operator A x and the right-hand side: 1e-13 relative (same arithmetic);
+  * local (level-2) and level-3 eigenvalues: 1e-6 relative, with an absolute
+    floor of 1e-9 x the largest wanted eigenvalue for the zero (constant) modes;
+  * one preconditioner application: 1e-6 relative L2 (the eigenvectors are
+    converged to a 1e-6 residual, not to machine precision);
+  * PCG: iteration count within +-1 of the oracle, solution within 1e-8
+    relative L2 of an FP64 direct solve;
+  * mixed precision (FP32 preconditioner, FP64 PCG): iterations within +-1 of
+    the oracle, same 1e-8 solution bound.
+"""
+import numpy as np
+import pytest
+
+from oracle import pmf_oracle as O
+from premixfem_b200 import fields
+from premixfem_b200.solver import DarcySolver, options_string
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_opts(d):
+    o = O.Options()
+    for k, v in d.items():
+        if k == "pmf_vranks":
+            o.vranks = tuple(v)
+        elif k == "pmf_sd":
+            o.sd = tuple(v)
+        elif k == "pmf_precision":
+            continue
+        else:
+            setattr(o, k, v)
+    return o
+
+
+def _gpu(problem, d):
+    s = DarcySolver.from_problem(problem, options_string(d))
+    s.setup()
+    return s
+
+
+CASES = {
+    "grf16_sd2": (lambda: fields.unit_cube_grf(16, seed=1), {"sd": 2, "en_lv1": 4, "en_lv2": 4}),
+    "grf16_vr222": (lambda: fields.unit_cube_grf(16, seed=3),
+                    {"sd": 2, "pmf_vranks": (2, 2, 2), "en_lv1": 4, "en_lv2": 3}),
+    "ragged_vr": (lambda: fields.random_box((13, 11, 9), seed=7, sigma=2.0),
+                  {"pmf_sd": (2, 2, 1), "pmf_vranks": (2, 1, 3), "en_lv1": 3, "en_lv2": 2}),
+    "cross16_cr3": (lambda: dict(fields.cross(16, 3), dirichlet={"x-": 0.0}),
+                    {"sd": 2, "pmf_vranks": (1, 2, 2), "en_lv1": 4, "en_lv2": 4}),
+    "aniso_wcycle": (lambda: dict(fields.aniso_const(8, 8, 8), dirichlet={"z+": 1.0}),
+                     {"sd": 2, "en_lv1": 3, "en_lv2": 2, "use_W_cycle": True}),
+}
+
+
+@pytest.fixture(scope="module")
+def oracle_cache():
+    return {}
+
+
+def _oracle(name, cache):
+    if name not in cache:
+        mk, d = CASES[name]
+        prob = mk()
+        cache[name] = (prob, d, O.solve(prob, _oracle_opts(d)))
+    return cache[name]
+
+
+def test_operator_and_rhs(native):
+    prob = fields.random_box((11, 7, 5), seed=2, sigma=2.0, dirichlet={"x-": 1.0, "y+": 0.5})
+    op = O.Operator(prob)
+    s = DarcySolver.from_problem(prob, "-sd 2")
+    s.setup()
+    x = np.random.default_rng(0).standard_normal(op.n)
+    y = s.apply_A(x)
+    ref = op.A @ x
+    assert np.linalg.norm(y - ref) <= 1e-13 * np.linalg.norm(ref)
+    b = s.rhs(prob["source"].ravel())
+    np.testing.assert_allclose(b, op.rhs(), rtol=1e-14, atol=1e-14 * np.abs(op.rhs()).max())
+    s.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_local_and_level3_eigenvalues(native, name, oracle_cache):
+    prob, d, ref = _oracle(name, oracle_cache)
+    s = _gpu(prob, d)
+    ev, ks, iters, status = s.eigen_lv1()
+    pc = ref["pc"]
+    assert (status == 0).all(), f"LOBPCG did not converge on {np.nonzero(status)[0]}"
+    ref1 = np.stack(pc.eigvals_lv1)
+    scale = np.abs(ref1).max(axis=1, keepdims=True)
+    err = np.abs(ev - ref1) / np.maximum(np.abs(ref1), 1e-3 * scale)
+    assert err.max() <= 1e-6, f"max rel eigen error {err.max():.2e}"
+    ev3, ks3, _ = s.eigen_lv2()
+    ref3 = np.stack([w for w in pc.eigvals_lv2])
+    scale3 = np.abs(ref3).max(axis=1, keepdims=True)
+    err3 = np.abs(ev3 - ref3) / np.maximum(np.abs(ref3), 1e-3 * scale3)
+    assert err3.max() <= 1e-6, f"max rel level-3 eigen error {err3.max():.2e}"
+    s.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_pc_apply_matches_oracle(native, name, oracle_cache):
+    prob, d, ref = _oracle(name, oracle_cache)
+    s = _gpu(prob, d)
+    x = np.random.default_rng(11).standard_normal(ref["op"].n)
+    y = s.pc_apply(x)
+    yr = ref["pc"].apply(x)
+    rel = np.linalg.norm(y - yr) / np.linalg.norm(yr)
+    assert rel <= 1e-6, f"PC_apply_vec relative difference {rel:.2e}"
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_pcg_iterations_and_solution(native, name, precision, oracle_cache):
+    prob, d, ref = _oracle(name, oracle_cache)
+    s = _gpu(prob, dict(d, pmf_precision=precision))
+    op = ref["op"]
+    b = s.rhs(prob["source"].ravel())
+    x, its, rnorm, reason = s.solve(b)
+    assert reason == "converged"
+    assert abs(its - ref["its"]) <= 1, f"iterations {its} vs oracle {ref['its']}"
+    assert np.linalg.norm(b - op.A @ x) <= 1e-8 * np.linalg.norm(b) * (1 + 1e-6)
+    xd = O.direct_solve(op, ref["b"])
+    if not op.dir_faces:
+        x = x - x.mean()
+        xd = xd - xd.mean()
+    err = np.linalg.norm(x - xd) / np.linalg.norm(xd)
+    assert err <= 1e-8, f"solution error vs direct {err:.2e}"
+    s.close()
+
+
+def test_device_pointer_path_matches_host_path(native):
+    torch = pytest.importorskip("torch")
+    prob = fields.unit_cube_grf(16, seed=5)
+    s = DarcySolver.from_problem(prob, "-sd 2")
+    s.setup()
+    b = s.rhs(prob["source"].ravel())
+    xh, its_h, _, _ = s.solve(b)
+    bd = torch.from_numpy(b).cuda()
+    xd, its_d, _, _ = s.solve(bd)
+    assert its_h == its_d
+    np.testing.assert_array_equal(xd.cpu().numpy(), xh)
+    s.close()
+
+
+def test_bad_arguments_return_errors(native):
+    from premixfem_b200._native import PmfError
+    with pytest.raises(PmfError) as e:
+        DarcySolver((1, 1, 1), (0, 4, 4), "")
+    assert e.value.code == 62
+    with pytest.raises(PmfError) as e:
+        DarcySolver((1, 1, 1), (8, 8, 8), "-eg_op 7")
+    assert e.value.code == 62
+    s = DarcySolver((1, 1, 1), (8, 8, 8), "-sd 2")
+    with pytest.raises(PmfError) as e:
+        s.setup()  # kappa not set
+    assert e.value.code == 73
+    s.close()
