@@ -69,6 +69,9 @@ int pmf_get_stages(pmf_solver* s, double t[10]);
 /* last setup and solve time measured with CUDA events on the solver stream (ms) */
 int pmf_get_timing(pmf_solver* s, double* setup_ms, double* solve_ms);
 
+/* total number of CUDA kernels launched by this library in this process */
+unsigned long long pmf_launch_count(void);
+
 const char* pmf_last_error(void);
 int pmf_device_count(void);
 

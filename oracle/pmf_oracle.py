@@ -71,6 +71,7 @@ class Options:
     use_2level: bool = False
     rtol: float = 1.0e-8
     max_it: int = 10000
+    eig_method: str = "dense"  # "dense": scipy.linalg.eigh; "arpack": eigsh shift-and-invert (SLEPc-like)
 
     def normalized(self):
         o = Options(**self.__dict__)
@@ -464,11 +465,18 @@ class Preconditioner:
         self.eigvals_lv1 = []
         self.phi = []  # per subdomain (n_s, en_lv1) M-normalised eigenvectors
         for s in self.lay.subs:
-            An = self.op.neumann(s).toarray()
+            An = self.op.neumann(s)
+            An = An if o.eig_method == "arpack" else An.toarray()
             Md = self.op.mass_diag(s, o.eg_op)
             if k > An.shape[0]:
                 raise ValueError("en_lv1 larger than a subdomain")
-            w, V = sla.eigh(An, np.diag(Md), subset_by_index=[0, k - 1])
+            if o.eig_method == "arpack" and k < An.shape[0] - 1:
+                # SLEPc EPS with STSINVERT and target -NIL (:354-365): Lanczos on (A + NIL M)^-1 M
+                w, V = spla.eigsh(sp.csc_matrix(An), k=k, M=sp.diags(Md).tocsc(), sigma=-NIL, which="LM")
+                order = np.argsort(w)
+                w, V = w[order], V[:, order]
+            else:
+                w, V = sla.eigh(An, np.diag(Md), subset_by_index=[0, k - 1])
             self.eigvals_lv1.append(w)
             # adaptive count, :369-383
             num, vmax = k, w[k - 1]

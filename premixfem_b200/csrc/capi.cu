@@ -198,6 +198,8 @@ int pmf_get_timing(pmf_solver* h, double* setup_ms, double* solve_ms) {
   return 0;
 }
 
+unsigned long long pmf_launch_count(void) { return __atomic_load_n(&pmf::g_launches, __ATOMIC_RELAXED); }
+
 const char* pmf_last_error(void) { return g_last_error.c_str(); }
 
 int pmf_device_count(void) {

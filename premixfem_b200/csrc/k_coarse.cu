@@ -31,7 +31,7 @@ __global__ void k_a2_mult(const SubInfo* subs, int nsub, int kmax, const double*
 void launch_a2_mult(const SubInfo* subs, int nsub, int kmax, const double* blk, const double* v, const double* base,
                     double* out, const int* done, cudaStream_t st) {
   long long n = (long long)nsub * kmax;
-  k_a2_mult<<<(int)((n + 255) / 256), 256, 0, st>>>(subs, nsub, kmax, blk, v, base, out, done);
+  { note_launch(); k_a2_mult<<<(int)((n + 255) / 256), 256, 0, st>>>(subs, nsub, kmax, blk, v, base, out, done); }
 }
 
 // Batched dense GEMV, one warp per row.
@@ -52,7 +52,7 @@ __global__ void k_block_gemv(int nrank, int nr, const double* inv, const double*
 void launch_block_gemv(int nrank, int nr, const double* inv, const double* in, double* out, int accumulate,
                        const int* done, cudaStream_t st) {
   long long threads = (long long)nrank * nr * 32;
-  k_block_gemv<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, inv, in, out, accumulate, done);
+  { note_launch(); k_block_gemv<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, inv, in, out, accumulate, done); }
 }
 
 // d[r][j] = sum_i V[r][i][j] c[r][i]  (Psi^T r = V^T Phi^T r, per rank)
@@ -74,7 +74,7 @@ __global__ void k_lv3_restrict(int nrank, int nr, int en2, const double* V, cons
 void launch_lv3_restrict(int nrank, int nr, int en2, const double* V, const double* c, double* d, const int* done,
                          cudaStream_t st) {
   long long threads = (long long)nrank * en2 * 32;
-  k_lv3_restrict<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, c, d, done);
+  { note_launch(); k_lv3_restrict<<<(int)((threads + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, c, d, done); }
 }
 
 // dz[r][i] = sum_j V[r][i][j] w[r][j]
@@ -93,7 +93,7 @@ __global__ void k_lv3_prolong(int nrank, int nr, int en2, const double* V, const
 void launch_lv3_prolong(int nrank, int nr, int en2, const double* V, const double* w, double* dz, const int* done,
                         cudaStream_t st) {
   long long n = (long long)nrank * nr;
-  k_lv3_prolong<<<(int)((n + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, w, dz, done);
+  { note_launch(); k_lv3_prolong<<<(int)((n + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, w, dz, done); }
 }
 
 __global__ void k_axpy(long long n, double a, const double* x, double* y, const int* done) {
@@ -107,10 +107,10 @@ __global__ void k_copy(long long n, const double* x, double* y, const int* done)
     y[i] = x[i];
 }
 void launch_axpy(long long n, double a, const double* x, double* y, const int* done, cudaStream_t st) {
-  k_axpy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, a, x, y, done);
+  { note_launch(); k_axpy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, a, x, y, done); }
 }
 void launch_copy(long long n, const double* x, double* y, const int* done, cudaStream_t st) {
-  k_copy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, x, y, done);
+  { note_launch(); k_copy<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(n, x, y, done); }
 }
 
 // ---------------------------------------------------------------------------
@@ -233,11 +233,11 @@ void launch_galerkin(const Grid& g, const SubInfo* subs, int nsub, int kmax, con
                      cudaStream_t st) {
   const int threads = 32 * kmax;
   if (kmax <= 4)
-    k_galerkin<T, 4><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+    { note_launch(); k_galerkin<T, 4><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface); }
   else if (kmax <= 8)
-    k_galerkin<T, 8><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+    { note_launch(); k_galerkin<T, 8><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface); }
   else
-    k_galerkin<T, 16><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface);
+    { note_launch(); k_galerkin<T, 16><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, blk, gface); }
 }
 template void launch_galerkin<float>(const Grid&, const SubInfo*, int, int, const double*, const double*,
                                      const double*, const double*, const float*, double*, double*, cudaStream_t);
@@ -280,7 +280,7 @@ void launch_assemble_dense(const SubInfo* subs, int nsub, int nrank, int spr, in
   (void)nsub;
   long long total = (long long)nrank * spr * kmax * spr * kmax;
   int nb = (int)std::min<long long>((total + 255) / 256, 148 * 32);
-  k_assemble_dense<<<nb, 256, 0, st>>>(subs, nrank, spr, kmax, blk, gface, mode, dense);
+  { note_launch(); k_assemble_dense<<<nb, 256, 0, st>>>(subs, nrank, spr, kmax, blk, gface, mode, dense); }
 }
 
 // In-place Gauss-Jordan inverse of SPD matrices (one CTA per matrix).
@@ -350,7 +350,7 @@ __global__ void k_spd_inverse(int n, double* a_all, double tol, int* nnull) {
 void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
   const int smem = 2 * n * sizeof(double);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull);
+  { note_launch(); k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull); }
 }
 
 // ---------------------------------------------------------------------------
@@ -361,7 +361,7 @@ void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaSt
 // eigenvectors come out orthonormal in the 2-norm as SLEPc returns them.
 // work: 3 * nr * p doubles per rank.
 #define PMF_L3_MAXP 32
-__global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all, const double* inv_all,
+__global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int p, const double* A_all, const double* inv_all,
                                      double* V_all, double* evals_all, int* iters, double tol, int max_it,
                                      double* work_all) {
   const int r = blockIdx.x;
@@ -371,7 +371,7 @@ __global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all
   double* Y = X + (long long)nr * p;
   double* AY = Y + (long long)nr * p;
   __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP],
-      C[PMF_L3_MAXP * PMF_L3_MAXP], dsc[PMF_L3_MAXP];
+      C[PMF_L3_MAXP * PMF_L3_MAXP], dsc[PMF_L3_MAXP], jac[64];
   __shared__ int keep, conv;
   __shared__ double anorm;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -410,7 +410,7 @@ __global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all
       G[a * PMF_L3_MAXP + b] *= dsc[a] * dsc[b];
     }
     __syncthreads();
-    if (tid < 32) warp_jacobi_eigh(G, U, w, p, PMF_L3_MAXP);
+    if (tid < 32) warp_jacobi_eigh(G, U, w, p, PMF_L3_MAXP, jac);
     __syncthreads();
     if (tid == 0) {
       int kk = 0;
@@ -459,7 +459,7 @@ __global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all
       }
     }
     __syncthreads();
-    if (tid < 32) warp_jacobi_eigh(G, U, w, q, PMF_L3_MAXP);
+    if (tid < 32) warp_jacobi_eigh(G, U, w, q, PMF_L3_MAXP, jac);
     __syncthreads();
     // X <- X U (through Y as scratch)
     for (long long e = tid; e < (long long)nr * q; e += nt) {
@@ -512,7 +512,7 @@ __global__ void k_dense_smallest_eig(int nr, int en2, int p, const double* A_all
 
 void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
                                double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st) {
-  k_dense_smallest_eig<<<nrank, 512, 0, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work);
+  { note_launch(); k_dense_smallest_eig<<<nrank, 512, 0, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work); }
 }
 
 }  // namespace pmf

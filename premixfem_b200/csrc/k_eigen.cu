@@ -4,15 +4,17 @@
 // M_i the diagonal "mass" of the selected variant (MOD / MEAN / DIAG).
 //
 // SLEPc's shift-and-invert Krylov-Schur is replaced by a batched LOBPCG
-// (Knyazev 2001) in one persistent launch: each CTA owns a subdomain at a
-// time; its block vectors live in a private global work slab that stays in
-// L2.  The preconditioner is IC(0) of (A_i^N + sigma M_i) applied with the
-// same hyperplane wavefront as the level-1 solves; the basis [X W P] is
-// M-orthonormalised by SVQB (Stathopoulos & Wu 2002) and the Rayleigh-Ritz
-// projection is always formed and solved in FP64.  Vectors are stored in T
+// (Knyazev 2001) in one persistent launch: each CTA owns one subdomain at a
+// time and keeps its block vectors in a private global slab (L2-resident).
+// Preconditioner: IC(0) of (A_i^N + sigma M_i), applied as a hyperplane
+// wavefront with its coefficients and all active vectors held in shared
+// memory (FP32: it only shapes the search directions).  The basis
+// [X W P] is M-orthonormalised by SVQB (Stathopoulos & Wu 2002) and the
+// Rayleigh-Ritz projection is formed and solved in FP64.  Converged vectors
+// are soft-locked (their residuals leave the basis).  Vectors are stored in T
 // (float for the mixed-precision setup, double for the plain form); a final
-// FP64 Rayleigh-Ritz polish fixes the returned eigenvalues and the
-// M-normalisation (v^T M v = 1, the GHEP normalisation SLEPc returns).
+// FP64 Rayleigh-Ritz fixes the returned eigenvalues and the normalisation
+// v^T M v = 1 (the GHEP normalisation SLEPc returns).
 #include <algorithm>
 
 #include "pmf_dense.cuh"
@@ -20,28 +22,22 @@
 
 namespace pmf {
 
-#define LB_LD 32     // leading dimension of the small matrices
-#define LB_CH 32     // cell chunk of the Gram tiles
+#define LB_LD 32  // leading dimension of the small matrices
+#define LB_CH 32  // cell chunk of the Gram tiles
+#define LB_MM 10  // largest block size m (3m <= 32)
 #define LB_THREADS 256
 
-struct LbSmem {
-  double GM[LB_LD * LB_LD];
-  double GA[LB_LD * LB_LD];
-  double U[LB_LD * LB_LD];
-  double Q[LB_LD * LB_LD];
-  double H[LB_LD * LB_LD];
-  double V[LB_LD * LB_LD];
-  double Y[LB_LD * LB_LD];
-  double w[LB_LD], th[LB_LD], dsc[LB_LD], lam[LB_LD], res[LB_LD];
-  double stile[LB_LD * (LB_CH + 1)];
-  double ttile[LB_LD * (LB_CH + 1)];
-  double red[LB_LD * 33];
-  double scal[4];
-  int ival[4];
+struct __align__(16) LbSmall {
+  double w[32], th[32], dsc[32], lam[32], res[32], jac[64], scal[8];
+  int ival[8], act[32];
+};
+struct LbMats {
+  double GM[LB_LD * LB_LD], GA[LB_LD * LB_LD], U[LB_LD * LB_LD], Q[LB_LD * LB_LD], H[LB_LD * LB_LD],
+      V[LB_LD * LB_LD], Y[LB_LD * LB_LD];
+  double stile[LB_LD * (LB_CH + 1)], ttile[LB_LD * (LB_CH + 1)];
+  double red[32 * 33];
 };
 
-// Column stride of the block vectors: max_cells rounded up to 64 so every
-// column (and the FP64 polish buffer laid over W|P) starts 256-byte aligned.
 __host__ __device__ inline int lb_ld(int max_cells) { return (max_cells + 63) & ~63; }
 
 size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes) {
@@ -51,33 +47,68 @@ size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes) {
 
 __device__ __forceinline__ double avg_k(double a, double b) { return 2.0 / (1.0 / a + 1.0 / b); }
 
-// G[a][b] = sum_cl wgt[cl] * S[a][cl] * T[b][cl], a < na, b < nb; S, T column-major
-// with column stride nc.  All threads of the CTA must call it.
+// Column c of a segmented block [A0 (n0 cols) | A1 (n1 cols) | A2 (n2 cols)], stride ld.
+template <typename T>
+struct Seg3 {
+  const T* b[3];
+  int n[3];
+  int ld;
+  __device__ __forceinline__ const T* col(int c) const {
+    if (c < n[0]) return b[0] + (size_t)c * ld;
+    c -= n[0];
+    if (c < n[1]) return b[1] + (size_t)c * ld;
+    return b[2] + (size_t)(c - n[1]) * ld;
+  }
+  __device__ __forceinline__ int total() const { return n[0] + n[1] + n[2]; }
+};
+
+// G[a][b] = sum_cl wgt[cl] * S_a[cl] * T_b[cl] (a, b < 32), register-tiled 2x2 per thread.
+// Tiles of 32 cells are staged through shared memory; the next tile is loaded
+// into registers while the current one is multiplied (one tile of prefetch).
 template <typename TS, typename TT>
-__device__ void cta_gram(const TS* S, int na, const TT* Tm, int nb, const double* wgt, int ncells, int ld,
-                         double* G, LbSmem& sm) {
+__device__ void cta_gram(const Seg3<TS>& S, const Seg3<TT>& Tm, const double* wgt, int ncells, double* G,
+                         LbMats& mt) {
   const int t = threadIdx.x;
   const bool own = t < 256;
+  const int na = S.total(), nb = Tm.total();
   const int a0 = 2 * (t >> 4), b0 = 2 * (t & 15);
+  const int lc = t & 31, ab = (t >> 5) & 7;
+  const TS* sp[4];
+  const TT* tp[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int a = ab + 8 * r;
+    sp[r] = (own && a < na) ? S.col(a) : nullptr;
+    tp[r] = (own && a < nb) ? Tm.col(a) : nullptr;
+  }
+  double sv[4], tv[4];
+  auto load = [&](int c0) {
+    const int c = c0 + lc;
+    const bool in = c < ncells;
+    const double wv = (in && wgt) ? wgt[c] : 1.0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      sv[r] = (in && sp[r]) ? (double)sp[r][c] * wv : 0.0;
+      tv[r] = (in && tp[r]) ? (double)tp[r][c] : 0.0;
+    }
+  };
+  load(0);
   double acc00 = 0, acc01 = 0, acc10 = 0, acc11 = 0;
   for (int c0 = 0; c0 < ncells; c0 += LB_CH) {
-    const int ch = min(LB_CH, ncells - c0);
-    for (int e = t; e < LB_LD * LB_CH; e += blockDim.x) {
-      const int a = e / LB_CH, cl = e % LB_CH;
-      double sv = 0.0, tv = 0.0;
-      if (cl < ch) {
-        if (a < na) sv = (double)S[(long long)a * ld + c0 + cl] * (wgt ? wgt[c0 + cl] : 1.0);
-        if (a < nb) tv = (double)Tm[(long long)a * ld + c0 + cl];
+    if (own) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        mt.stile[(ab + 8 * r) * (LB_CH + 1) + lc] = sv[r];
+        mt.ttile[(ab + 8 * r) * (LB_CH + 1) + lc] = tv[r];
       }
-      sm.stile[a * (LB_CH + 1) + cl] = sv;
-      sm.ttile[a * (LB_CH + 1) + cl] = tv;
     }
     __syncthreads();
+    if (c0 + LB_CH < ncells) load(c0 + LB_CH);
     if (own && a0 < na && b0 < nb) {
 #pragma unroll 8
       for (int cl = 0; cl < LB_CH; ++cl) {
-        const double s0 = sm.stile[a0 * (LB_CH + 1) + cl], s1 = sm.stile[(a0 + 1) * (LB_CH + 1) + cl];
-        const double t0 = sm.ttile[b0 * (LB_CH + 1) + cl], t1 = sm.ttile[(b0 + 1) * (LB_CH + 1) + cl];
+        const double s0 = mt.stile[a0 * (LB_CH + 1) + cl], s1 = mt.stile[(a0 + 1) * (LB_CH + 1) + cl];
+        const double t0 = mt.ttile[b0 * (LB_CH + 1) + cl], t1 = mt.ttile[(b0 + 1) * (LB_CH + 1) + cl];
         acc00 += s0 * t0;
         acc01 += s0 * t1;
         acc10 += s1 * t0;
@@ -95,7 +126,7 @@ __device__ void cta_gram(const TS* S, int na, const TT* Tm, int nb, const double
   __syncthreads();
 }
 
-// C[n1 x n3] = A[n1 x n2] * B[n2 x n3] (small, ld LB_LD), optional transpose of A.
+// C[n1 x n3] = op(A)[n1 x n2] * B[n2 x n3] (small, ld LB_LD).
 __device__ void cta_small_gemm(const double* A, bool transA, const double* B, double* C, int n1, int n2, int n3) {
   for (int e = threadIdx.x; e < n1 * n3; e += blockDim.x) {
     const int i = e / n3, j = e % n3;
@@ -107,67 +138,126 @@ __device__ void cta_small_gemm(const double* A, bool transA, const double* B, do
 }
 
 // Rayleigh-Ritz on a basis with Gram matrices GM (M) and GA (A), size nS.
-// Produces Y (nS x m): coefficients of the m lowest Ritz vectors, M-orthonormal,
-// and their Ritz values in sm.lam.  Returns the kept rank q (>= m on success).
-__device__ int cta_rayleigh_ritz(LbSmem& sm, int nS, int m, double drop) {
-  // symmetrise the Grams
+// Produces Y (nS x m) holding the coefficients of the m lowest Ritz vectors
+// (M-orthonormal) and their Ritz values in sm.lam.  Returns the kept rank.
+//
+// The basis is first scaled to unit M-norm (D = diag(GM)^-1/2).  Normally the
+// scaled Gram is factored by Cholesky, L L^T = D GM D, and Q = D L^-T; if a
+// pivot falls below `drop` the basis is nearly dependent and SVQB takes over
+// (eigendecomposition of D GM D, directions with eigenvalue <= drop * max
+// dropped).  Then H = Q^T GA Q is diagonalised and Y = Q V[:, :m].
+__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop) {
   for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
     const int a = e / nS, b = e % nS;
     if (a < b) {
-      const double vm = 0.5 * (sm.GM[a * LB_LD + b] + sm.GM[b * LB_LD + a]);
-      sm.GM[a * LB_LD + b] = sm.GM[b * LB_LD + a] = vm;
-      const double va = 0.5 * (sm.GA[a * LB_LD + b] + sm.GA[b * LB_LD + a]);
-      sm.GA[a * LB_LD + b] = sm.GA[b * LB_LD + a] = va;
+      const double vm = 0.5 * (mt.GM[a * LB_LD + b] + mt.GM[b * LB_LD + a]);
+      mt.GM[a * LB_LD + b] = mt.GM[b * LB_LD + a] = vm;
+      const double va = 0.5 * (mt.GA[a * LB_LD + b] + mt.GA[b * LB_LD + a]);
+      mt.GA[a * LB_LD + b] = mt.GA[b * LB_LD + a] = va;
     }
   }
   __syncthreads();
-  if (threadIdx.x < nS) sm.dsc[threadIdx.x] = 1.0 / sqrt(fmax(sm.GM[threadIdx.x * LB_LD + threadIdx.x], 1e-300));
+  if (threadIdx.x == 0) {
+    double mx = 0.0;
+    for (int a = 0; a < nS; ++a) mx = fmax(mx, mt.GM[a * LB_LD + a]);
+    sm.scal[1] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < nS) {
+    const double gaa = mt.GM[threadIdx.x * LB_LD + threadIdx.x];
+    sm.dsc[threadIdx.x] = gaa > 1e-28 * sm.scal[1] ? 1.0 / sqrt(gaa) : 0.0;
+  }
   __syncthreads();
   for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
     const int a = e / nS, b = e % nS;
-    sm.H[a * LB_LD + b] = sm.GM[a * LB_LD + b] * sm.dsc[a] * sm.dsc[b];
+    const double v = mt.GM[a * LB_LD + b] * sm.dsc[a] * sm.dsc[b];
+    mt.H[a * LB_LD + b] = v;
+    mt.U[a * LB_LD + b] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 32) warp_jacobi_eigh(sm.H, sm.U, sm.w, nS, LB_LD);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int q = 0;
-    const double wmax = sm.w[nS - 1];
-    for (int c = 0; c < nS; ++c)
-      if (sm.w[c] > drop * wmax) ++q;
-    sm.ival[0] = q;
+  // Cholesky of the scaled Gram (warp 0, right-looking, lower factor in U)
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
+    int ok = 1;
+    for (int j = 0; j < nS; ++j) {
+      const double d = mt.U[j * LB_LD + j];
+      if (!(d > drop) || sm.dsc[j] == 0.0) {
+        ok = 0;
+        break;
+      }
+      const double ljj = sqrt(d);
+      __syncwarp();
+      if (l == 0) mt.U[j * LB_LD + j] = ljj;
+      if (l > j && l < nS) mt.U[l * LB_LD + j] /= ljj;
+      __syncwarp();
+      if (l > j && l < nS) {
+        const double lij = mt.U[l * LB_LD + j];
+        for (int kk = j + 1; kk <= l; ++kk) mt.U[l * LB_LD + kk] -= lij * mt.U[kk * LB_LD + j];
+      }
+      __syncwarp();
+    }
+    if (l == 0) sm.ival[4] = ok;
   }
   __syncthreads();
-  const int q = sm.ival[0];
-  // Q = D U_kept w^-1/2  (kept = last q columns)
-  for (int e = threadIdx.x; e < nS * q; e += blockDim.x) {
-    const int a = e / q, c = e % q, cc = nS - q + c;
-    sm.Q[a * LB_LD + c] = sm.dsc[a] * sm.U[a * LB_LD + cc] / sqrt(sm.w[cc]);
+  int q;
+  if (sm.ival[4]) {
+    // Q = D L^-T: lane c solves L x = e_c (forward substitution), Q[a][c] = D_a x[c -> row a]
+    if (threadIdx.x < nS) {
+      const int c = threadIdx.x;
+      for (int i = 0; i < nS; ++i) {
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int kk = c; kk < i; ++kk) s -= mt.U[i * LB_LD + kk] * mt.V[kk * LB_LD + c];
+        mt.V[i * LB_LD + c] = i < c ? 0.0 : s / mt.U[i * LB_LD + i];
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
+      const int a = e / nS, c = e % nS;
+      mt.Q[a * LB_LD + c] = sm.dsc[a] * mt.V[c * LB_LD + a];  // (L^-1)^T
+    }
+    __syncthreads();
+    q = nS;
+  } else {
+    if (threadIdx.x < 32) warp_jacobi_eigh(mt.H, mt.U, sm.w, nS, LB_LD, sm.jac);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int qq = 0;
+      const double wmax = sm.w[nS - 1];
+      for (int c = 0; c < nS; ++c)
+        if (sm.w[c] > drop * wmax && sm.w[c] > 0.0) ++qq;
+      sm.ival[0] = qq;
+    }
+    __syncthreads();
+    q = sm.ival[0];
+    for (int e = threadIdx.x; e < nS * q; e += blockDim.x) {
+      const int a = e / q, c = e % q, cc = nS - q + c;
+      mt.Q[a * LB_LD + c] = sm.dsc[a] * mt.U[a * LB_LD + cc] / sqrt(sm.w[cc]);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  // H = Q^T GA Q
-  cta_small_gemm(sm.GA, false, sm.Q, sm.V, nS, nS, q);  // V = GA Q
-  cta_small_gemm(sm.Q, true, sm.V, sm.H, q, nS, q);     // H = Q^T V
+  cta_small_gemm(mt.GA, false, mt.Q, mt.V, nS, nS, q);  // V = GA Q
+  cta_small_gemm(mt.Q, true, mt.V, mt.H, q, nS, q);     // H = Q^T GA Q
   for (int e = threadIdx.x; e < q * q; e += blockDim.x) {
     const int a = e / q, b = e % q;
     if (a < b) {
-      const double v = 0.5 * (sm.H[a * LB_LD + b] + sm.H[b * LB_LD + a]);
-      sm.H[a * LB_LD + b] = sm.H[b * LB_LD + a] = v;
+      const double v = 0.5 * (mt.H[a * LB_LD + b] + mt.H[b * LB_LD + a]);
+      mt.H[a * LB_LD + b] = mt.H[b * LB_LD + a] = v;
     }
   }
   __syncthreads();
-  if (threadIdx.x < 32) warp_jacobi_eigh(sm.H, sm.V, sm.th, q, LB_LD);
+  if (threadIdx.x < 32) warp_jacobi_eigh(mt.H, mt.V, sm.th, q, LB_LD, sm.jac);
   __syncthreads();
   const int mm = min(m, q);
-  cta_small_gemm(sm.Q, false, sm.V, sm.Y, nS, q, mm);  // Y = Q V[:, :m]
+  cta_small_gemm(mt.Q, false, mt.V, mt.Y, nS, q, mm);  // Y = Q V[:, :m]
   if (threadIdx.x < mm) sm.lam[threadIdx.x] = sm.th[threadIdx.x];
   __syncthreads();
   return q;
 }
 
-template <typename T>
+// out = A^N v on the subdomain (FP64 arithmetic, stored as TO).
+template <typename TI, typename TO>
 __device__ __forceinline__ void neumann_apply_col(const Grid& g, const SubInfo& S, const double* tx, const double* ty,
-                                                  const double* tz, const double* dN, const T* v, T* out,
+                                                  const double* tz, const double* dN, const TI* v, TO* out,
                                                   int ncells) {
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny;
   for (int cl = threadIdx.x; cl < ncells; cl += blockDim.x) {
@@ -180,20 +270,46 @@ __device__ __forceinline__ void neumann_apply_col(const Grid& g, const SubInfo& 
     if (j < ny - 1) a -= ty[cg + g.M] * (double)v[cl + nx];
     if (k > 0) a -= tz[cg] * (double)v[cl - nxny];
     if (k < nz - 1) a -= tz[cg + g.MN] * (double)v[cl + nxny];
-    out[cl] = (T)a;
+    out[cl] = (TO)a;
   }
 }
 
+// Phase timer for diagnostics: thread 0 accumulates clock64() deltas.
+struct PhaseClock {
+  long long* p;
+  long long t0;
+  __device__ void start() {
+    if (p && threadIdx.x == 0) t0 = clock64();
+  }
+  __device__ void lap(int ph) {
+    if (p && threadIdx.x == 0) {
+      const long long t1 = clock64();
+      p[ph] += t1 - t0;
+      t0 = t1;
+    }
+  }
+};
+
 template <typename T>
-__global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* work, size_t work_stride, T* phi,
-                                                 double* evals, int* iters, int* status, int* ks, double eb) {
+__global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned char* work, size_t work_stride, T* phi,
+                                                double* evals, int* iters, int* status, int* ks, double eb) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  LbSmem& sm = *reinterpret_cast<LbSmem*>(smraw);
-  double* u = reinterpret_cast<double*>(smraw + sizeof(LbSmem));
+  LbSmall& sm = *reinterpret_cast<LbSmall*>(smraw);
+  const int ldc = a.ldc;
+  float* ctx = reinterpret_cast<float*>(smraw + sizeof(LbSmall));
+  float* cty = ctx + ldc;
+  float* ctz = cty + ldc;
+  float* cinv = ctz + ldc;
+  unsigned char* uni = smraw + sizeof(LbSmall) + (size_t)16 * ldc;
+  LbMats& mt = *reinterpret_cast<LbMats*>(uni);
+  float* u = reinterpret_cast<float*>(uni);
+  double* Dtmp = reinterpret_cast<double*>(uni);
   const Grid g = a.g;
-  const int m = a.m, k = a.k;
+  const int m = a.m, k = a.k, mb = a.mb;
   unsigned char* wb = work + (size_t)blockIdx.x * work_stride;
   const int ld = a.ld;
+  PhaseClock pc{a.prof ? a.prof + (size_t)blockIdx.x * 8 : nullptr, 0};
+  pc.start();
 
   for (int s = blockIdx.x; s < a.nsub; s += gridDim.x) {
     const SubInfo S = a.subs[s];
@@ -206,9 +322,8 @@ __global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* wor
     T* AP = AW + (size_t)m * ld;
     double* Md = reinterpret_cast<double*>(AP + (size_t)m * ld);
     double* dN = Md + ld;
-    double* invD = dN + ld;
 
-    // ---- mass diagonal (src/PreMixFEM_3D.c:243-346) and Neumann diagonal
+    // ---- mass diagonal (src/PreMixFEM_3D.c:243-346), Neumann diagonal, sweep coefficients
     double ratio = 0.0;
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
       const int i = cl % nx, tt = cl / nx, j = tt % ny, kk = tt / ny;
@@ -236,64 +351,60 @@ __global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* wor
         if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / a.Hz / a.Hz;
         if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
         // Dirichlet extension: 2 t_b per boundary face
-        if (a.db[cg] != 0.0) {
-          if (a.dirichlet_mask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-          if (a.dirichlet_mask & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-          if (a.dirichlet_mask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-          if (a.dirichlet_mask & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-          if (a.dirichlet_mask & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-          if (a.dirichlet_mask & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-        }
+        if (a.dirichlet_mask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+        if (a.dirichlet_mask & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+        if (a.dirichlet_mask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+        if (a.dirichlet_mask & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+        if (a.dirichlet_mask & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
+        if (a.dirichlet_mask & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
         mv = mv * a.meas;
       }
       Md[cl] = mv;
       dN[cl] = dn;
+      ctx[cl] = i > 0 ? (float)a.tx[cg] : 0.0f;
+      cty[cl] = j > 0 ? (float)a.ty[cg] : 0.0f;
+      ctz[cl] = kk > 0 ? (float)a.tz[cg] : 0.0f;
       ratio = fmax(ratio, dn / mv);
     }
-    // block max of dN / M: a scale for the eigenvalues (>= lambda_max / 2)
-    {
-      for (int o = 16; o > 0; o >>= 1) ratio = fmax(ratio, __shfl_xor_sync(0xffffffffu, ratio, o));
-      if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = ratio;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double r = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sm.red[w]);
-        sm.scal[0] = r > 0 ? r : 1.0;
-      }
-      __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) ratio = fmax(ratio, __shfl_xor_sync(0xffffffffu, ratio, o));
+    if ((threadIdx.x & 31) == 0) mt.red[threadIdx.x >> 5] = ratio;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double r = 0.0;
+      for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) r = fmax(r, mt.red[wi]);
+      sm.scal[0] = r > 0 ? r : 1.0;
     }
+    __syncthreads();
     const double lscale = sm.scal[0];
     const double sigma = a.sigma_rel * lscale;
 
-    // ---- IC(0) pivots of A^N + sigma M (wavefront, natural order)
-    {
-      const int t = threadIdx.x, jj = t % ny, kk = t / ny;
-      const int nplanes = nx + ny + nz - 2;
-      for (int d = 0; d < nplanes; ++d) {
-        const int i = d - jj - kk;
-        if (t < ny * nz && i >= 0 && i < nx) {
-          const int cl = (kk * ny + jj) * nx + i;
-          const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + i);
-          double sacc = 0.0;
-          if (kk > 0) sacc += a.tz[cg] * a.tz[cg] / u[cl - nxny];
-          if (jj > 0) sacc += a.ty[cg] * a.ty[cg] / u[cl - nx];
-          if (i > 0) sacc += a.tx[cg] * a.tx[cg] / u[cl - 1];
-          double D = dN[cl] + sigma * Md[cl] - sacc;
-          if (!(D > 0.0)) D = dN[cl] + sigma * Md[cl];
-          u[cl] = D;
-          invD[cl] = 1.0 / D;
-        }
-        __syncthreads();
+    // ---- IC(0) pivots of A^N + sigma M (wavefront, natural order, FP64)
+    const int t = threadIdx.x, jj = t % ny, kk = t / ny;
+    const bool line = t < ny * nz;
+    const int nplanes = nx + ny + nz - 2;
+    for (int d = 0; d < nplanes; ++d) {
+      const int i = d - jj - kk;
+      if (line && i >= 0 && i < nx) {
+        const int cl = (kk * ny + jj) * nx + i;
+        double sacc = 0.0;
+        if (kk > 0) sacc += (double)ctz[cl] * (double)ctz[cl] / Dtmp[cl - nxny];
+        if (jj > 0) sacc += (double)cty[cl] * (double)cty[cl] / Dtmp[cl - nx];
+        if (i > 0) sacc += (double)ctx[cl] * (double)ctx[cl] / Dtmp[cl - 1];
+        double D = dN[cl] + sigma * Md[cl] - sacc;
+        if (!(D > 0.0)) D = dN[cl] + sigma * Md[cl];
+        Dtmp[cl] = D;
+        cinv[cl] = (float)(1.0 / D);
       }
+      __syncthreads();
     }
 
-    // ---- initial block
+    // ---- initial block, A X, first Rayleigh-Ritz
     for (int e = threadIdx.x; e < m * nc; e += blockDim.x) {
       const int j = e / nc, cl = e % nc;
       double v;
       if (a.xinit) {
-        const int i = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
-        const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + i);
+        const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+        const long long cg = ((long long)(S.z0 + kz_) * g.N + (S.y0 + jy)) * g.M + (S.x0 + i);
         v = a.xinit[cg * m + j];
       } else {
         v = hash_uniform(a.seed ^ ((unsigned long long)s << 32) ^ (unsigned long long)e);
@@ -301,80 +412,115 @@ __global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* wor
       X[(size_t)j * ld + cl] = (T)v;
     }
     __syncthreads();
-    for (int j = 0; j < m; ++j) neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
+    for (int j = 0; j < m; ++j)
+      neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
     __syncthreads();
     const double drop = sizeof(T) == 4 ? 1e-9 : 1e-13;
-    cta_gram(X, m, X, m, Md, nc, ld, sm.GM, sm);
-    cta_gram(X, m, AX, m, (const double*)nullptr, nc, ld, sm.GA, sm);
-    cta_rayleigh_ritz(sm, m, m, drop);
-    // X <- X Y, AX <- AX Y (per cell, in place)
+    {
+      Seg3<T> sx{{X, X, X}, {m, 0, 0}, ld};
+      Seg3<T> sax{{AX, AX, AX}, {m, 0, 0}, ld};
+      cta_gram(sx, sx, Md, nc, mt.GM, mt);
+      cta_gram(sx, sax, (const double*)nullptr, nc, mt.GA, mt);
+    }
+    cta_rayleigh_ritz(sm, mt, m, m, drop);
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-      double xr[LB_LD], ar[LB_LD];
-      for (int b = 0; b < m; ++b) {
-        xr[b] = (double)X[(size_t)b * ld + cl];
-        ar[b] = (double)AX[(size_t)b * ld + cl];
+      double xr[LB_MM], ar[LB_MM];
+#pragma unroll
+      for (int b = 0; b < LB_MM; ++b) {
+        xr[b] = b < m ? (double)X[(size_t)b * ld + cl] : 0.0;
+        ar[b] = b < m ? (double)AX[(size_t)b * ld + cl] : 0.0;
       }
-      for (int j = 0; j < m; ++j) {
-        double xn = 0.0, an = 0.0;
-        for (int b = 0; b < m; ++b) {
-          xn += xr[b] * sm.Y[b * LB_LD + j];
-          an += ar[b] * sm.Y[b * LB_LD + j];
+#pragma unroll
+      for (int j = 0; j < LB_MM; ++j)
+        if (j < m) {
+          double xn = 0.0, an = 0.0;
+#pragma unroll
+          for (int b = 0; b < LB_MM; ++b)
+            if (b < m) {
+              xn += xr[b] * mt.Y[b * LB_LD + j];
+              an += ar[b] * mt.Y[b * LB_LD + j];
+            }
+          X[(size_t)j * ld + cl] = (T)xn;
+          AX[(size_t)j * ld + cl] = (T)an;
         }
-        X[(size_t)j * ld + cl] = (T)xn;
-        AX[(size_t)j * ld + cl] = (T)an;
-      }
     }
     __syncthreads();
 
     bool hasP = false;
     int it = 0;
     bool conv = false;
+    pc.lap(0);
     for (; it < a.max_it; ++it) {
-      // residuals R = AX - M X Lambda (into W), ||R_j||_{M^-1}
-      double racc[LB_LD];
-      for (int j = 0; j < m; ++j) racc[j] = 0.0;
+      // ---- residuals R = AX - M X Lambda (into W) and ||R_j||_{M^-1}
+      double racc[LB_MM];
+#pragma unroll
+      for (int j = 0; j < LB_MM; ++j) racc[j] = 0.0;
       for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
         const double mv = Md[cl];
-        for (int j = 0; j < m; ++j) {
-          const double r = (double)AX[(size_t)j * ld + cl] - sm.lam[j] * mv * (double)X[(size_t)j * ld + cl];
-          W[(size_t)j * ld + cl] = (T)r;
-          racc[j] += r * r / mv;
+#pragma unroll
+        for (int j = 0; j < LB_MM; ++j)
+          if (j < m) {
+            const double r = (double)AX[(size_t)j * ld + cl] - sm.lam[j] * mv * (double)X[(size_t)j * ld + cl];
+            W[(size_t)j * ld + cl] = (T)r;
+            racc[j] += r * r / mv;
+          }
+      }
+#pragma unroll
+      for (int j = 0; j < LB_MM; ++j)
+        if (j < m) {
+          const double v = warp_sum(racc[j]);
+          if ((threadIdx.x & 31) == 0) mt.red[j * 33 + (threadIdx.x >> 5)] = v;
         }
-      }
-      for (int j = 0; j < m; ++j) {
-        const double v = warp_sum(racc[j]);
-        if ((threadIdx.x & 31) == 0) sm.red[j * 33 + (threadIdx.x >> 5)] = v;
-      }
       __syncthreads();
       if (threadIdx.x < m) {
         double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sm.red[threadIdx.x * 33 + w];
+        for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += mt.red[threadIdx.x * 33 + wi];
         sm.res[threadIdx.x] = sqrt(v) / lscale;
       }
       __syncthreads();
-      conv = true;
-      for (int j = 0; j < k; ++j)
-        if (!(sm.res[j] <= a.tol)) conv = false;
+      if (threadIdx.x == 0) {
+        int na = 0, cv = 1;
+        for (int j = 0; j < m; ++j) {
+          const bool done_j = sm.res[j] <= a.tol;
+          if (j < k && !done_j) cv = 0;
+          if (!done_j || j >= k) sm.act[na++] = j;  // soft locking of converged wanted vectors
+        }
+        sm.ival[2] = na;
+        sm.ival[3] = cv;
+      }
+      __syncthreads();
+      conv = sm.ival[3] != 0;
+      pc.lap(1);
       if (conv) break;
-      // W = T R: IC(0) solve of (A^N + sigma M) per column
-      for (int j = 0; j < m; ++j) {
-        T* Wj = W + (size_t)j * ld;
-        for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) u[cl] = (double)Wj[cl];
+      const int nact = sm.ival[2];
+      // compact the active residuals to the front of W (act[] is increasing)
+      for (int c = 0; c < nact; ++c) {
+        const int src = sm.act[c];
+        if (src != c)
+          for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) W[(size_t)c * ld + cl] = W[(size_t)src * ld + cl];
         __syncthreads();
-        const int t = threadIdx.x, jj = t % ny, kk = t / ny;
-        const bool line = t < ny * nz;
-        const long long base = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + S.x0;
-        const int nplanes = nx + ny + nz - 2;
+      }
+      // ---- W = T R: IC(0) sweeps, mb vectors per wavefront, FP32 in shared memory
+      for (int j0 = 0; j0 < nact; j0 += mb) {
+        const int nb = min(mb, nact - j0);
+        for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
+          const int b = e / nc, cl = e % nc;
+          u[b * ldc + cl] = (float)W[(size_t)(j0 + b) * ld + cl];
+        }
+        __syncthreads();
         for (int d = 0; d < nplanes; ++d) {
           const int i = d - jj - kk;
           if (line && i >= 0 && i < nx) {
             const int cl = (kk * ny + jj) * nx + i;
-            const long long cg = base + i;
-            double sacc = u[cl];
-            if (kk > 0) sacc += a.tz[cg] * u[cl - nxny];
-            if (jj > 0) sacc += a.ty[cg] * u[cl - nx];
-            if (i > 0) sacc += a.tx[cg] * u[cl - 1];
-            u[cl] = sacc * invD[cl];
+            const float cz_ = ctz[cl], cy_ = cty[cl], cx_ = ctx[cl], ci = cinv[cl];
+            for (int b = 0; b < nb; ++b) {
+              float* ub = u + b * ldc;
+              float sacc = ub[cl];
+              if (kk > 0) sacc += cz_ * ub[cl - nxny];
+              if (jj > 0) sacc += cy_ * ub[cl - nx];
+              if (i > 0) sacc += cx_ * ub[cl - 1];
+              ub[cl] = sacc * ci;
+            }
           }
           __syncthreads();
         }
@@ -382,79 +528,106 @@ __global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* wor
           const int i = d - jj - kk;
           if (line && i >= 0 && i < nx) {
             const int cl = (kk * ny + jj) * nx + i;
-            const long long cg = base + i;
-            double sacc = 0.0;
-            if (i < nx - 1) sacc += a.tx[cg + 1] * u[cl + 1];
-            if (jj < ny - 1) sacc += a.ty[cg + g.M] * u[cl + nx];
-            if (kk < nz - 1) sacc += a.tz[cg + g.MN] * u[cl + nxny];
-            u[cl] = u[cl] + sacc * invD[cl];
+            const float cxp = i < nx - 1 ? ctx[cl + 1] : 0.0f;
+            const float cyp = jj < ny - 1 ? cty[cl + nx] : 0.0f;
+            const float czp = kk < nz - 1 ? ctz[cl + nxny] : 0.0f;
+            const float ci = cinv[cl];
+            for (int b = 0; b < nb; ++b) {
+              float* ub = u + b * ldc;
+              float sacc = 0.0f;
+              if (i < nx - 1) sacc += cxp * ub[cl + 1];
+              if (jj < ny - 1) sacc += cyp * ub[cl + nx];
+              if (kk < nz - 1) sacc += czp * ub[cl + nxny];
+              ub[cl] = ub[cl] + sacc * ci;
+            }
           }
           __syncthreads();
         }
-        for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) Wj[cl] = (T)u[cl];
+        for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
+          const int b = e / nc, cl = e % nc;
+          W[(size_t)(j0 + b) * ld + cl] = (T)u[b * ldc + cl];
+        }
         __syncthreads();
       }
-      for (int j = 0; j < m; ++j)
+      pc.lap(2);
+      for (int j = 0; j < nact; ++j)
         neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, W + (size_t)j * ld, AW + (size_t)j * ld, nc);
       __syncthreads();
-      const int nS = hasP ? 3 * m : 2 * m;
-      cta_gram(X, nS, X, nS, Md, nc, ld, sm.GM, sm);
-      cta_gram(X, nS, AX, nS, (const double*)nullptr, nc, ld, sm.GA, sm);
-      const int q = cta_rayleigh_ritz(sm, nS, m, drop);
+      pc.lap(3);
+      const int np = hasP ? m : 0;
+      const int nS = m + nact + np;
+      {
+        Seg3<T> sS{{X, W, P}, {m, nact, np}, ld};
+        Seg3<T> sA{{AX, AW, AP}, {m, nact, np}, ld};
+        cta_gram(sS, sS, Md, nc, mt.GM, mt);
+        cta_gram(sS, sA, (const double*)nullptr, nc, mt.GA, mt);
+      }
+      pc.lap(4);
+      const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop);
+      pc.lap(5);
       if (q < m) {  // basis collapsed: restart without P
         hasP = false;
         continue;
       }
-      // X <- S Y, P <- [W P] Y_WP, same for AX / AP (per cell, in place)
+      // ---- X <- S Y, P <- [W P] Y_WP, same for AX / AP (per cell, in place)
       for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-        double xr[3 * 10];
-        for (int b = 0; b < nS; ++b) xr[b] = (double)X[(size_t)b * ld + cl];
-        for (int j = 0; j < m; ++j) {
-          double pn = 0.0;
-          for (int b = m; b < nS; ++b) pn += xr[b] * sm.Y[b * LB_LD + j];
-          double xn = pn;
-          for (int b = 0; b < m; ++b) xn += xr[b] * sm.Y[b * LB_LD + j];
-          X[(size_t)j * ld + cl] = (T)xn;
-          P[(size_t)j * ld + cl] = (T)pn;
-        }
-        for (int b = 0; b < nS; ++b) xr[b] = (double)AX[(size_t)b * ld + cl];
-        for (int j = 0; j < m; ++j) {
-          double pn = 0.0;
-          for (int b = m; b < nS; ++b) pn += xr[b] * sm.Y[b * LB_LD + j];
-          double xn = pn;
-          for (int b = 0; b < m; ++b) xn += xr[b] * sm.Y[b * LB_LD + j];
-          AX[(size_t)j * ld + cl] = (T)xn;
-          AP[(size_t)j * ld + cl] = (T)pn;
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {
+          T* B0 = pass ? AX : X;
+          T* B1 = pass ? AW : W;
+          T* B2 = pass ? AP : P;
+          double xr[3 * LB_MM];
+#pragma unroll
+          for (int b = 0; b < 3 * LB_MM; ++b) {
+            double v = 0.0;
+            if (b < m)
+              v = (double)B0[(size_t)b * ld + cl];
+            else if (b < m + nact)
+              v = (double)B1[(size_t)(b - m) * ld + cl];
+            else if (b < nS)
+              v = (double)B2[(size_t)(b - m - nact) * ld + cl];
+            xr[b] = v;
+          }
+#pragma unroll
+          for (int j = 0; j < LB_MM; ++j)
+            if (j < m) {
+              double pn = 0.0, xn = 0.0;
+#pragma unroll
+              for (int b = 0; b < 3 * LB_MM; ++b) {
+                if (b < m)
+                  xn += xr[b] * mt.Y[b * LB_LD + j];
+                else if (b < nS)
+                  pn += xr[b] * mt.Y[b * LB_LD + j];
+              }
+              B0[(size_t)j * ld + cl] = (T)(xn + pn);
+              B2[(size_t)j * ld + cl] = (T)pn;
+            }
         }
       }
       __syncthreads();
+      if (sizeof(T) == 4) {  // implicit A-image updates drift in float: recompute
+        for (int j = 0; j < m; ++j) {
+          neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
+          neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, P + (size_t)j * ld, AP + (size_t)j * ld, nc);
+        }
+        __syncthreads();
+      }
       hasP = true;
+      pc.lap(6);
     }
 
-    // ---- final FP64 Rayleigh-Ritz polish on X (A X recomputed in FP64 into the W/P slab)
+    // ---- final FP64 Rayleigh-Ritz on X (A X recomputed in FP64 over the W|P slab)
     double* AX64 = reinterpret_cast<double*>(W);
+    for (int j = 0; j < m; ++j)
+      neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX64 + (size_t)j * ld, nc);
+    __syncthreads();
     {
-      for (int j = 0; j < m; ++j) {
-        const T* v = X + (size_t)j * ld;
-        double* o = AX64 + (size_t)j * ld;
-        for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-          const int i = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
-          const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + i);
-          double av = dN[cl] * (double)v[cl];
-          if (i > 0) av -= a.tx[cg] * (double)v[cl - 1];
-          if (i < nx - 1) av -= a.tx[cg + 1] * (double)v[cl + 1];
-          if (jj > 0) av -= a.ty[cg] * (double)v[cl - nx];
-          if (jj < ny - 1) av -= a.ty[cg + g.M] * (double)v[cl + nx];
-          if (kk > 0) av -= a.tz[cg] * (double)v[cl - nxny];
-          if (kk < nz - 1) av -= a.tz[cg + g.MN] * (double)v[cl + nxny];
-          o[cl] = av;
-        }
-      }
-      __syncthreads();
-      cta_gram(X, m, X, m, Md, nc, ld, sm.GM, sm);
-      cta_gram(X, m, AX64, m, (const double*)nullptr, nc, ld, sm.GA, sm);
-      cta_rayleigh_ritz(sm, m, m, 1e-14);
+      Seg3<T> sx{{X, X, X}, {m, 0, 0}, ld};
+      Seg3<double> sax{{AX64, AX64, AX64}, {m, 0, 0}, ld};
+      cta_gram(sx, sx, Md, nc, mt.GM, mt);
+      cta_gram(sx, sax, (const double*)nullptr, nc, mt.GA, mt);
     }
+    cta_rayleigh_ritz(sm, mt, m, m, 1e-14);
     // adaptive count (:369-383) and output
     if (threadIdx.x == 0) {
       int num = k;
@@ -472,18 +645,23 @@ __global__ void __launch_bounds__(512) k_lobpcg(LobpcgArgs a, unsigned char* wor
     const int num = sm.ival[1];
     if (threadIdx.x < k) evals[(long long)s * k + threadIdx.x] = sm.lam[threadIdx.x];
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-      const int i = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
-      const long long cg = ((long long)(S.z0 + kk) * g.N + (S.y0 + jj)) * g.M + (S.x0 + i);
-      double xr[LB_LD];
-      for (int b = 0; b < m; ++b) xr[b] = (double)X[(size_t)b * ld + cl];
+      const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+      const long long cg = ((long long)(S.z0 + kz_) * g.N + (S.y0 + jy)) * g.M + (S.x0 + i);
+      double xr[LB_MM];
+#pragma unroll
+      for (int b = 0; b < LB_MM; ++b) xr[b] = b < m ? (double)X[(size_t)b * ld + cl] : 0.0;
       for (int j = 0; j < a.kmax; ++j) {
         double v = 0.0;
-        if (j < num)
-          for (int b = 0; b < m; ++b) v += xr[b] * sm.Y[b * LB_LD + j];
+        if (j < num) {
+#pragma unroll
+          for (int b = 0; b < LB_MM; ++b)
+            if (b < m) v += xr[b] * mt.Y[b * LB_LD + j];
+        }
         phi[cg * a.kmax + j] = (T)v;
       }
     }
     __syncthreads();
+    pc.lap(7);
   }
 }
 
@@ -492,11 +670,20 @@ void launch_lobpcg(const LobpcgArgs& a_in, int nblocks, void* work, T* phi, doub
                    int* ks, double eb, int max_cells, int max_lines, cudaStream_t st) {
   LobpcgArgs a = a_in;
   a.ld = lb_ld(max_cells);
-  const int threads = std::max(LB_THREADS, ((max_lines + 31) / 32) * 32);
-  const size_t smem = sizeof(LbSmem) + (size_t)max_cells * sizeof(double);
+  a.ldc = (max_cells + 3) & ~3;
+  const size_t fixed = sizeof(LbSmall) + (size_t)16 * a.ldc;
+  const size_t limit = 227 * 1024;
+  const size_t avail = limit > fixed ? limit - fixed : 0;
+  int mb = (int)std::min<size_t>(a.m, avail / ((size_t)4 * a.ldc));
+  if (mb < 1) mb = 1;
+  a.mb = mb;
+  const size_t uni = std::max(std::max(sizeof(LbMats), (size_t)mb * 4 * a.ldc), (size_t)8 * a.ldc);
+  const size_t smem = fixed + uni;
+  const int threads = LB_THREADS;  // one x-line per thread: callers guarantee ny*nz <= 256
+  (void)max_lines;
   cudaFuncSetAttribute(k_lobpcg<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const size_t stride = (lobpcg_work_bytes(max_cells, a.m, sizeof(T)) + 255) & ~(size_t)255;
-  k_lobpcg<T><<<nblocks, threads, smem, st>>>(a, (unsigned char*)work, stride, phi, evals, iters, status, ks, eb);
+  { note_launch(); k_lobpcg<T><<<nblocks, threads, smem, st>>>(a, (unsigned char*)work, stride, phi, evals, iters, status, ks, eb); }
 }
 template void launch_lobpcg<float>(const LobpcgArgs&, int, void*, float*, double*, int*, int*, int*, double, int, int,
                                    cudaStream_t);

@@ -68,7 +68,7 @@ __global__ void k_assemble(AssembleArgs a, double* tx, double* ty, double* tz, d
 
 void launch_assemble(const AssembleArgs& a, double* tx, double* ty, double* tz, double* diag, double* db,
                      double* bval, cudaStream_t st) {
-  k_assemble<<<cell_blocks(a.g.ncell), kCellThreads, 0, st>>>(a, tx, ty, tz, diag, db, bval);
+  { note_launch(); k_assemble<<<cell_blocks(a.g.ncell), kCellThreads, 0, st>>>(a, tx, ty, tz, diag, db, bval); }
 }
 
 __global__ void k_to_f32(const double* in, float* out, long long n) {
@@ -80,10 +80,10 @@ __global__ void k_to_f64(const float* in, double* out, long long n) {
     out[i] = (double)in[i];
 }
 void launch_to_f32(const double* in, float* out, long long n, cudaStream_t st) {
-  k_to_f32<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n);
+  { note_launch(); k_to_f32<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n); }
 }
 void launch_to_f64(const float* in, double* out, long long n, cudaStream_t st) {
-  k_to_f64<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n);
+  { note_launch(); k_to_f64<<<cell_blocks(n), kCellThreads, 0, st>>>(in, out, n); }
 }
 
 // ---------------------------------------------------------------------------
@@ -113,7 +113,7 @@ __global__ void k_spmv(Grid g, const double* tx, const double* ty, const double*
 
 void launch_spmv(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
                  const double* x, double* y, cudaStream_t st) {
-  k_spmv<<<cell_blocks(g.ncell), kCellThreads, 0, st>>>(g, tx, ty, tz, diag, x, y);
+  { note_launch(); k_spmv<<<cell_blocks(g.ncell), kCellThreads, 0, st>>>(g, tx, ty, tz, diag, x, y); }
 }
 
 // ---------------------------------------------------------------------------
@@ -140,8 +140,8 @@ __global__ void k_fin_sum(const double* part, int n, double* out) {
 }
 void launch_dot(const double* a, const double* b, long long n, double* part, double* out, cudaStream_t st) {
   int nb = cell_blocks(n);
-  k_dot<<<nb, kCellThreads, 0, st>>>(a, b, n, part);
-  k_fin_sum<<<1, 256, 0, st>>>(part, nb, out);
+  { note_launch(); k_dot<<<nb, kCellThreads, 0, st>>>(a, b, n, part); }
+  { note_launch(); k_fin_sum<<<1, 256, 0, st>>>(part, nb, out); }
 }
 
 // --- KSPSolve_CG (PETSc src/ksp/ksp/impls/cg/cg.c) with the unpreconditioned norm ---
@@ -176,8 +176,8 @@ __global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double 
 void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,
                       int max_it, cudaStream_t st) {
   int nb = cell_blocks(g.ncell);
-  k_pcg_start<<<nb, kCellThreads, 0, st>>>(g.ncell, b, x, r, part);
-  k_pcg_start_fin<<<1, 256, 0, st>>>(part, nb, s, rtol, max_it);
+  { note_launch(); k_pcg_start<<<nb, kCellThreads, 0, st>>>(g.ncell, b, x, r, part); }
+  { note_launch(); k_pcg_start_fin<<<1, 256, 0, st>>>(part, nb, s, rtol, max_it); }
 }
 
 // beta = z.r (the dot is written per block by the preconditioner's last kernel
@@ -195,12 +195,12 @@ __global__ void k_pcg_beta_fin(const double* part, int nb, PcgState* s) {
   }
 }
 void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream_t st) {
-  k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nparts, s);
+  { note_launch(); k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nparts, s); }
 }
 void launch_pcg_beta(const double* r, const double* z, long long n, double* part, PcgState* s, cudaStream_t st) {
   int nb = cell_blocks(n);
-  k_dot<<<nb, kCellThreads, 0, st>>>(r, z, n, part);
-  k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nb, s);
+  { note_launch(); k_dot<<<nb, kCellThreads, 0, st>>>(r, z, n, part); }
+  { note_launch(); k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nb, s); }
 }
 
 // p <- z (first) or z + (beta/betaold) p; w <- A p; partial p.w.
@@ -257,8 +257,8 @@ void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const 
                        const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
                        cudaStream_t st) {
   int nb = cell_blocks(g.ncell);
-  k_pcg_iter_a<<<nb, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s);
-  k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s);
+  { note_launch(); k_pcg_iter_a<<<nb, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s); }
+  { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s); }
 }
 
 // x += alpha p; r -= alpha w; partial r.r; then dp, its and the convergence test.
@@ -297,8 +297,8 @@ __global__ void k_pcg_iter_b_fin(const double* part, int nb, PcgState* s) {
 void launch_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
                        PcgState* s, cudaStream_t st) {
   int nb = cell_blocks(n);
-  k_pcg_iter_b<<<nb, kCellThreads, 0, st>>>(n, x, r, p, w, part, s);
-  k_pcg_iter_b_fin<<<1, 256, 0, st>>>(part, nb, s);
+  { note_launch(); k_pcg_iter_b<<<nb, kCellThreads, 0, st>>>(n, x, r, p, w, part, s); }
+  { note_launch(); k_pcg_iter_b_fin<<<1, 256, 0, st>>>(part, nb, s); }
 }
 
 // ---------------------------------------------------------------------------
@@ -371,7 +371,7 @@ void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_line
   int threads = std::max(32, ((max_lines + 31) / 32) * 32);
   const int smem = PMF_MAX_SUB_CELLS * sizeof(double);
   cudaFuncSetAttribute(k_ic_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k_ic_factor<<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, bad);
+  { note_launch(); k_ic_factor<<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, bad); }
 }
 
 template <typename T>
@@ -473,18 +473,18 @@ void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines
   }
   if (yin) {
     if (fin)
-      k_ic_apply<T, true, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d,
-                                                             part, done);
+      { note_launch(); k_ic_apply<T, true, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d,
+                                                             part, done); }
     else
-      k_ic_apply<T, true, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                              out_d, part, done);
+      { note_launch(); k_ic_apply<T, true, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                              out_d, part, done); }
   } else {
     if (fin)
-      k_ic_apply<T, false, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                              out_d, part, done);
+      { note_launch(); k_ic_apply<T, false, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                              out_d, part, done); }
     else
-      k_ic_apply<T, false, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                               out_d, part, done);
+      { note_launch(); k_ic_apply<T, false, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
+                                                               out_d, part, done); }
   }
 }
 
@@ -532,9 +532,9 @@ static void rr_dispatch(const Grid& g, const SubInfo* subs, int nsub, int kmax, 
                         const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
                         const int* done, cudaStream_t st) {
   if (y)
-    k_resid_restrict<T, KM, true><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done);
+    { note_launch(); k_resid_restrict<T, KM, true><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
   else
-    k_resid_restrict<T, KM, false><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done);
+    { note_launch(); k_resid_restrict<T, KM, false><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
 }
 
 template <typename T>
@@ -574,11 +574,11 @@ template <typename T>
 void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* phi, const double* Z, T* y,
                     const int* done, cudaStream_t st) {
   if (kmax <= 4)
-    k_prolong<T, 4><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+    { note_launch(); k_prolong<T, 4><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
   else if (kmax <= 8)
-    k_prolong<T, 8><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+    { note_launch(); k_prolong<T, 8><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
   else
-    k_prolong<T, 16><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done);
+    { note_launch(); k_prolong<T, 16><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
 }
 
 #define PMF_INST(T)                                                                                              \

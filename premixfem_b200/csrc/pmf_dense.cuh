@@ -1,92 +1,160 @@
 // Small dense symmetric eigensolver used inside the batched Rayleigh-Ritz
-// steps (local GHEP, level-3 HEP).  Cyclic Jacobi rotations (Jacobi's method
-// as given in Golub & Van Loan, "Matrix Computations", section 8.5) executed
-// by one warp on a matrix in shared memory, followed by an ascending sort.
+// steps (local GHEP, level-3 HEP): Jacobi's method with the parallel
+// round-robin ("chess tournament") ordering of Brent & Luk (1985), executed by
+// one warp on a matrix in shared memory, followed by an ascending sort.
 #pragma once
 
 #include "pmf_common.cuh"
 
 namespace pmf {
 
-// A: n x n symmetric, row-major with leading dimension lda (destroyed; on
-// return its diagonal holds the eigenvalues in the original order).
-// V: n x n eigenvector matrix (columns), lda.  w: n sorted eigenvalues; V is
-// permuted to match.  n <= 32.  Must be called by all 32 lanes of one warp.
-__device__ inline void warp_jacobi_eigh(double* A, double* V, double* w, int n, int lda, int max_sweeps = 30) {
+// A: n x n symmetric, row-major, leading dimension lda (destroyed).
+// V: n x n eigenvectors (columns).  w: n eigenvalues, ascending; V permuted
+// to match.  n <= 32.  scratch: unused (kept for call-site compatibility).
+// Must be called by all 32 lanes of one warp.
+//
+// Each round, lane k < n_even/2 computes the rotation of pair k; the
+// parameters reach every lane by warp shuffles, and each lane then rotates
+// its own column (row pass) and its own row (column pass) for all pairs with
+// the loads of a group of pairs issued before any dependent arithmetic.
+// Sweeps stop when every off-diagonal entry is below 1e-14 ||A||_F.
+__device__ inline void warp_jacobi_eigh(double* A, double* V, double* w, int n, int lda, double* scratch,
+                                        int max_sweeps = 20) {
+  (void)scratch;
   const int l = threadIdx.x & 31;
   for (int i = 0; i < n; ++i)
     if (l < n) V[i * lda + l] = (i == l) ? 1.0 : 0.0;
   __syncwarp();
-  double norm = 0.0;
+  const int ne = n + (n & 1);
+  const int half = ne >> 1;
+  double fro = 0.0;
   if (l < n)
-    for (int j = 0; j < n; ++j) norm += A[l * lda + j] * A[l * lda + j];
-  norm = warp_sum(norm);
-  const double tiny = 1e-300;
-  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
-    double off = 0.0;
+    for (int j = 0; j < n; ++j) fro += A[l * lda + j] * A[l * lda + j];
+  fro = sqrt(warp_sum(fro));
+  for (int sweep = 0; sweep < max_sweeps && n > 1; ++sweep) {
+    int bad = 0;
     if (l < n)
       for (int j = 0; j < n; ++j)
-        if (j != l) off += A[l * lda + j] * A[l * lda + j];
-    off = warp_sum(off);
-    if (off <= 1e-30 * norm || off < tiny) break;
-    for (int p = 0; p < n - 1; ++p) {
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = A[p * lda + q];
-        const double app = A[p * lda + p];
-        const double aqq = A[q * lda + q];
-        if (fabs(apq) <= 1e-18 * sqrt(fabs(app * aqq)) || fabs(apq) < tiny) continue;
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-        const double c = 1.0 / sqrt(t * t + 1.0);
-        const double s = t * c;
-        __syncwarp();
-        if (l < n) {  // columns p, q
-          const double akp = A[l * lda + p], akq = A[l * lda + q];
-          A[l * lda + p] = c * akp - s * akq;
-          A[l * lda + q] = s * akp + c * akq;
+        if (j != l && fabs(A[l * lda + j]) > 1e-14 * fro) bad = 1;
+    if (!__any_sync(0xffffffffu, bad)) break;
+    for (int round = 0; round < ne - 1; ++round) {
+      int p = 0, q = 0;
+      double c = 1.0, s = 0.0;
+      if (l < half) {
+        const int pa = l, pb = ne - 1 - l;
+        p = pa == 0 ? 0 : ((pa - 1 + round) % (ne - 1)) + 1;
+        q = ((pb - 1 + round) % (ne - 1)) + 1;
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
         }
-        __syncwarp();
-        if (l < n) {  // rows p, q
-          const double apk = A[p * lda + l], aqk = A[q * lda + l];
-          A[p * lda + l] = c * apk - s * aqk;
-          A[q * lda + l] = s * apk + c * aqk;
+        if (q < n) {
+          const double apq = A[p * lda + q];
+          const double app = A[p * lda + p];
+          const double aqq = A[q * lda + q];
+          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * sqrt(fabs(app * aqq))) {
+            // tan of the rotation angle from single-precision arithmetic: an
+            // approximate angle still shrinks a_pq, and (c, s) below are made
+            // exactly orthonormal in FP64 from whatever t is used.
+            const double theta = (aqq - app) * (0.5 / apq);
+            double t;
+            if (fabs(theta) < 1e18) {
+              const float th = (float)theta;
+              t = (double)(copysignf(1.0f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.0f))));
+            } else {
+              t = 0.5 / theta;
+            }
+            c = rsqrt(fma(t, t, 1.0));
+            s = t * c;
+          }
+        } else {
+          q = p;  // dummy partner: no rotation
         }
-        __syncwarp();
+      }
+      __syncwarp();
+      // row pass (J^T A): lane = column l; pairs in groups of 4
+      for (int k0 = 0; k0 < half; k0 += 4) {
+        int pk[4], qk[4];
+        double ck[4], sk[4], ap[4], aq[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int src = min(k0 + u, half - 1);
+          pk[u] = __shfl_sync(0xffffffffu, p, src);
+          qk[u] = __shfl_sync(0xffffffffu, q, src);
+          ck[u] = __shfl_sync(0xffffffffu, c, src);
+          sk[u] = __shfl_sync(0xffffffffu, s, src);
+          if (k0 + u >= half) sk[u] = 0.0;
+        }
         if (l < n) {
-          const double vkp = V[l * lda + p], vkq = V[l * lda + q];
-          V[l * lda + p] = c * vkp - s * vkq;
-          V[l * lda + q] = s * vkp + c * vkq;
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (sk[u] != 0.0) {
+              ap[u] = A[pk[u] * lda + l];
+              aq[u] = A[qk[u] * lda + l];
+            }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (sk[u] != 0.0) {
+              A[pk[u] * lda + l] = ck[u] * ap[u] - sk[u] * aq[u];
+              A[qk[u] * lda + l] = sk[u] * ap[u] + ck[u] * aq[u];
+            }
         }
-        __syncwarp();
       }
+      __syncwarp();
+      // column pass (A J, V J): lane = row l
+      for (int k0 = 0; k0 < half; k0 += 4) {
+        int pk[4], qk[4];
+        double ck[4], sk[4], ap[4], aq[4], vp[4], vq[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int src = min(k0 + u, half - 1);
+          pk[u] = __shfl_sync(0xffffffffu, p, src);
+          qk[u] = __shfl_sync(0xffffffffu, q, src);
+          ck[u] = __shfl_sync(0xffffffffu, c, src);
+          sk[u] = __shfl_sync(0xffffffffu, s, src);
+          if (k0 + u >= half) sk[u] = 0.0;
+        }
+        if (l < n) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (sk[u] != 0.0) {
+              ap[u] = A[l * lda + pk[u]];
+              aq[u] = A[l * lda + qk[u]];
+              vp[u] = V[l * lda + pk[u]];
+              vq[u] = V[l * lda + qk[u]];
+            }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (sk[u] != 0.0) {
+              A[l * lda + pk[u]] = ck[u] * ap[u] - sk[u] * aq[u];
+              A[l * lda + qk[u]] = sk[u] * ap[u] + ck[u] * aq[u];
+              V[l * lda + pk[u]] = ck[u] * vp[u] - sk[u] * vq[u];
+              V[l * lda + qk[u]] = sk[u] * vp[u] + ck[u] * vq[u];
+            }
+        }
+      }
+      __syncwarp();
     }
   }
-  // ascending selection sort of eigenvalues, permuting columns of V
-  if (l < n) w[l] = A[l * lda + l];
+  // ascending sort of eigenvalues (rank by counting), permuting columns of V
+  // through A, which is no longer needed once its diagonal has been read
+  const double d = l < n ? A[l * lda + l] : 0.0;
+  int rank = 0;
+  for (int j = 0; j < n; ++j) {
+    const double dj = __shfl_sync(0xffffffffu, d, j);
+    if (l < n && (dj < d || (dj == d && j < l))) ++rank;
+  }
+  if (l < n) w[rank] = d;
   __syncwarp();
-  for (int i = 0; i < n - 1; ++i) {
-    int best = i;
-    double bv = w[i];
-    for (int j = i + 1; j < n; ++j)
-      if (w[j] < bv) {
-        bv = w[j];
-        best = j;
-      }
-    __syncwarp();
-    if (best != i) {
-      if (l < n) {
-        const double a = V[l * lda + i];
-        V[l * lda + i] = V[l * lda + best];
-        V[l * lda + best] = a;
-      }
-      if (l == 0) {
-        const double a = w[i];
-        w[i] = w[best];
-        w[best] = a;
-      }
-    }
-    __syncwarp();
+  if (l < n)
+    for (int j = 0; j < n; ++j) A[l * lda + j] = V[l * lda + j];
+  __syncwarp();
+  for (int j = 0; j < n; ++j) {
+    const int rj = __shfl_sync(0xffffffffu, rank, j);
+    if (l < n) V[l * lda + rj] = A[l * lda + j];
   }
+  __syncwarp();
 }
 
 // Cheap deterministic pseudo-random number in [-1, 1) (splitmix64 finaliser).

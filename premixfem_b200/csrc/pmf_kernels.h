@@ -7,6 +7,10 @@
 
 namespace pmf {
 
+// Number of kernels this library has launched (reported by bench and tests).
+extern unsigned long long g_launches;
+inline void note_launch() { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+
 // Scalars of the preconditioned CG loop, resident on the device so that an
 // iteration needs no host round trip (PETSc KSPSolve_CG recurrences).
 struct PcgState {
@@ -118,12 +122,15 @@ struct LobpcgArgs {
   const double* xinit;  // optional initial block (per cell, m values), may be null
   int dirichlet_mask;   // bit f set: face f (x-,x+,y-,y+,z-,z+) is a Dirichlet face
   int ld;               // column stride of the work block vectors (set by the launcher)
+  int ldc;              // stride of the shared-memory sweep arrays (set by the launcher)
+  int mb;               // vectors per shared-memory sweep (set by the launcher)
+  long long* prof;      // optional: per-CTA clock64 totals of 8 phases (diagnostics), may be null
 };
 // Work buffer size in bytes for the LOBPCG kernel, per concurrently processed subdomain.
 size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes);
 // One persistent CTA per block; each handles subdomains blockIdx.x, +nblocks, ...
 // ks[s] receives the adaptive eigen count (first j with lambda_j >= eb, else k).
-// Requires ny*nz <= 512 and cells <= PMF_MAX_SUB_CELLS, m <= 10.
+// Requires ny*nz <= 256 and cells <= PMF_MAX_SUB_CELLS, m <= 10.
 template <typename T>
 void launch_lobpcg(const LobpcgArgs& a, int nblocks, void* work, T* phi, double* evals, int* iters, int* status,
                    int* ks, double eb, int max_cells, int max_lines, cudaStream_t st);

@@ -4,12 +4,15 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
 #include "solver.h"
 
 namespace pmf {
+
+unsigned long long g_launches = 0;
 
 // ---------------------------------------------------------------------------
 // options
@@ -303,8 +306,8 @@ int Solver::build_partition() {
     S.nb[4] = at(gx, gy, gz - 1);
     S.nb[5] = at(gx, gy, gz + 1);
   }
-  if (max_cells > PMF_MAX_SUB_CELLS || max_lines > 512) {
-    err = "subdomain too large for the shared-memory sweeps (cells <= 8192, ny*nz <= 512)";
+  if (max_cells > PMF_MAX_SUB_CELLS || max_lines > 256) {
+    err = "subdomain too large for the shared-memory sweeps (cells <= 8192, ny*nz <= 256)";
     return 62;
   }
   kmax = opt.en_lv1;
@@ -458,7 +461,7 @@ int Solver::setup() {
   la.kmax = kmax;
   la.eg_op = opt.eg_op;
   la.max_it = opt.eig_max_it;
-  la.tol = opt.eig_tol;
+  la.tol = opt.eig_tol > 0 ? opt.eig_tol : (mixed ? 1e-6 : 1e-8);
   la.sigma_rel = opt.eig_sigma;
   la.seed = opt.seed;
   la.tx = tx;
@@ -476,6 +479,14 @@ int Solver::setup() {
   la.xinit = nullptr;
   la.dirichlet_mask = dmask;
   la.ld = 0;
+  la.prof = nullptr;
+  long long* d_prof = nullptr;
+  const bool prof_eig = getenv("PMF_PROFILE_EIGEN") != nullptr;
+  if (prof_eig) {
+    cudaMalloc(&d_prof, sizeof(long long) * 8 * eig_blocks);
+    cudaMemsetAsync(d_prof, 0, sizeof(long long) * 8 * eig_blocks, st);
+    la.prof = d_prof;
+  }
   const size_t need = ((lobpcg_work_bytes(max_cells, la.m, mixed ? 4 : 8) + 255) & ~(size_t)255) * eig_blocks;
   if (eig_work_bytes < need) {
     if (eig_work) cudaFree(eig_work);
@@ -491,6 +502,24 @@ int Solver::setup() {
                           max_lines, st);
   cudaEventRecord(e[2], st);
   if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;
+  if (prof_eig) {  // diagnostics: cycles per LOBPCG phase, summed over CTAs
+    std::vector<long long> hp(8 * eig_blocks);
+    cudaMemcpy(hp.data(), d_prof, sizeof(long long) * hp.size(), cudaMemcpyDeviceToHost);
+    const char* names[8] = {"init", "residual", "precond", "stencil", "gram", "rayleigh_ritz", "update", "final"};
+    long long tot[8] = {0}, mx = 0;
+    for (int b = 0; b < eig_blocks; ++b) {
+      long long sb = 0;
+      for (int p = 0; p < 8; ++p) {
+        tot[p] += hp[b * 8 + p];
+        sb += hp[b * 8 + p];
+      }
+      mx = std::max(mx, sb);
+    }
+    fprintf(stderr, "[premixfem_b200] LOBPCG cycles per phase (sum over %d CTAs; slowest CTA %lld):", eig_blocks, mx);
+    for (int p = 0; p < 8; ++p) fprintf(stderr, " %s=%lld", names[p], tot[p]);
+    fprintf(stderr, "\n");
+    cudaFree(d_prof);
+  }
   ks.resize(nsub);
   eig_iters.resize(nsub);
   eig_status.resize(nsub);
@@ -535,7 +564,7 @@ int Solver::setup() {
   // level 3: rank-Neumann HEP
   launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 1, AN, st);
   cudaMemcpyAsync(ANinv, AN, sizeof(double) * nrank * nr * nr, cudaMemcpyDeviceToDevice, st);
-  k_add_diag<<<nrank, 256, 0, st>>>(nrank, nr, ANinv, 1e-8, 1);
+  { note_launch(); k_add_diag<<<nrank, 256, 0, st>>>(nrank, nr, ANinv, 1e-8, 1); }
   launch_spd_inverse(nrank, nr, ANinv, 1e-14, d_flag + 2, st);
   const int p = std::min(nr, std::min(32, 2 * en2 + 4));
   double* l3work = nullptr;
@@ -574,11 +603,11 @@ int Solver::setup() {
   cudaMalloc(&d_ks3, sizeof(int) * nrank);
   cudaMemcpyAsync(d_ks3, ks3.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_rank_nb, rnb.data(), sizeof(int) * nrank * 6, cudaMemcpyHostToDevice, st);
-  k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3);
+  { note_launch(); k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3); }
   cudaEventRecord(e[4], st);
-  k_zero_d<<<256, 256, 0, st>>>(A3inv, (long long)n3 * n3);
-  k_build_a3<<<nrank * 7, 64, 0, st>>>(d_subs, spr, kmax, en2, blk, V3, d_rank_nb, d_ks3, A3inv, n3,
-                                       opt.no_shift_A_cc ? 0.0 : 1.0e-12);
+  { note_launch(); k_zero_d<<<256, 256, 0, st>>>(A3inv, (long long)n3 * n3); }
+  { note_launch(); k_build_a3<<<nrank * 7, 64, 0, st>>>(d_subs, spr, kmax, en2, blk, V3, d_rank_nb, d_ks3, A3inv, n3,
+                                       opt.no_shift_A_cc ? 0.0 : 1.0e-12); }
   launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
   cudaEventRecord(e[5], st);
   if (int er = check(cudaStreamSynchronize(st), "coarse setup")) return er;

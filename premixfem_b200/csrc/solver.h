@@ -25,7 +25,7 @@ struct Options {
   double rtol = 1e-8;
   int max_it = 10000;
   int eig_max_it = 300;
-  double eig_tol = 1e-6;
+  double eig_tol = -1.0;  // < 0: 1e-8 for the FP64 setup, 1e-6 for the FP32 setup
   double eig_sigma = 1e-2;
   int eig_guard = 2;
   int l3_max_it = 500;
