@@ -372,6 +372,7 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
   double* AY = Y + (long long)nr * p;
   __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP],
       C[PMF_L3_MAXP * PMF_L3_MAXP], dsc[PMF_L3_MAXP], jac[64];
+  __shared__ int ijac[32];
   __shared__ int keep, conv;
   __shared__ double anorm;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -410,8 +411,7 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
       G[a * PMF_L3_MAXP + b] *= dsc[a] * dsc[b];
     }
     __syncthreads();
-    if (tid < 32) warp_jacobi_eigh(G, U, w, p, PMF_L3_MAXP, jac);
-    __syncthreads();
+    cta_jacobi_eigh(G, U, w, p, PMF_L3_MAXP, ijac, jac);
     if (tid == 0) {
       int kk = 0;
       const double wmax = w[p - 1];
@@ -459,8 +459,7 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
       }
     }
     __syncthreads();
-    if (tid < 32) warp_jacobi_eigh(G, U, w, q, PMF_L3_MAXP, jac);
-    __syncthreads();
+    cta_jacobi_eigh(G, U, w, q, PMF_L3_MAXP, ijac, jac);
     // X <- X U (through Y as scratch)
     for (long long e = tid; e < (long long)nr * q; e += nt) {
       const int i = (int)(e / q), c = (int)(e % q);

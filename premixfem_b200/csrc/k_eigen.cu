@@ -8,13 +8,17 @@
 // time and keeps its block vectors in a private global slab (L2-resident).
 // Preconditioner: IC(0) of (A_i^N + sigma M_i), applied as a hyperplane
 // wavefront with its coefficients and all active vectors held in shared
-// memory (FP32: it only shapes the search directions).  The basis
-// [X W P] is M-orthonormalised by SVQB (Stathopoulos & Wu 2002) and the
-// Rayleigh-Ritz projection is formed and solved in FP64.  Converged vectors
-// are soft-locked (their residuals leave the basis).  Vectors are stored in T
-// (float for the mixed-precision setup, double for the plain form); a final
-// FP64 Rayleigh-Ritz fixes the returned eigenvalues and the normalisation
-// v^T M v = 1 (the GHEP normalisation SLEPc returns).
+// memory (FP32: it only shapes the search directions).  The basis [X W P]
+// is orthonormalised in the M inner product (Cholesky QR, SVQB of Stathopoulos
+// & Wu 2002 when it is nearly dependent) and the Rayleigh-Ritz projection is
+// formed and solved in FP64: the Grams and the basis update run on the FP64
+// tensor cores (mma.sync m8n8k4), the projected eigenproblem by Householder
+// tridiagonalisation and multisection.  Converged vectors are soft-locked.
+// X, W, P are stored in T (float for the mixed-precision setup, double for
+// the plain form); their A-images are always FP64, so the projection stays
+// consistent without recomputation.  A final FP64 Rayleigh-Ritz fixes the
+// returned eigenvalues and the normalisation v^T M v = 1 (the GHEP
+// normalisation SLEPc returns).
 #include <algorithm>
 
 #include "pmf_dense.cuh"
@@ -29,12 +33,12 @@ namespace pmf {
 
 struct __align__(16) LbSmall {
   double w[32], th[32], dsc[32], lam[32], res[32], jac[64], scal[8];
-  int ival[8], act[32];
+  int ival[8], act[32], ival2[32];
 };
 struct LbMats {
   double GM[LB_LD * LB_LD], GA[LB_LD * LB_LD], U[LB_LD * LB_LD], Q[LB_LD * LB_LD], H[LB_LD * LB_LD],
       V[LB_LD * LB_LD], Y[LB_LD * LB_LD];
-  double stile[LB_LD * (LB_CH + 1)], ttile[LB_LD * (LB_CH + 1)];
+  double stile[LB_LD * (LB_CH + 1)], ttile[LB_LD * (LB_CH + 1)], atile[LB_LD * (LB_CH + 1)];
   double red[32 * 33];
 };
 
@@ -42,10 +46,65 @@ __host__ __device__ inline int lb_ld(int max_cells) { return (max_cells + 63) & 
 
 size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes) {
   const size_t ld = lb_ld(max_cells);
-  return (size_t)6 * m * ld * prec_bytes + (size_t)3 * ld * sizeof(double);
+  // X, W, P in the storage precision; their A-images always FP64; M, Neumann diagonal
+  return (size_t)3 * m * ld * prec_bytes + (size_t)3 * m * ld * sizeof(double) + (size_t)3 * ld * sizeof(double);
 }
 
 __device__ __forceinline__ double avg_k(double a, double b) { return 2.0 / (1.0 / a + 1.0 / b); }
+
+// Four consecutive cells of a column (16-byte aligned for float, 2 x 16 bytes for double).
+__device__ __forceinline__ void ld4(const float* p, double v[4]) {
+  const float4 f = *reinterpret_cast<const float4*>(p);
+  v[0] = f.x;
+  v[1] = f.y;
+  v[2] = f.z;
+  v[3] = f.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+  const double2 a = *reinterpret_cast<const double2*>(p);
+  const double2 b = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const double v[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double v[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// u[b][cl] = (float) src[(j0 + b) * ld + cl] for b < nb, cl < nc (vectorised copy into shared memory).
+template <typename T>
+__device__ __forceinline__ void load_cols_to_smem(const T* src, size_t ld, int nb, int nc, float* u, int ldc) {
+  const int ng = nc >> 2;
+  for (int e = threadIdx.x; e < nb * ng; e += blockDim.x) {
+    const int b = e / ng, cl = (e % ng) * 4;
+    double v[4];
+    ld4(src + (size_t)b * ld + cl, v);
+    *reinterpret_cast<float4*>(u + (size_t)b * ldc + cl) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+  }
+  for (int e = threadIdx.x; e < nb * (nc - 4 * ng); e += blockDim.x) {
+    const int b = e / (nc - 4 * ng), cl = 4 * ng + e % (nc - 4 * ng);
+    u[(size_t)b * ldc + cl] = (float)src[(size_t)b * ld + cl];
+  }
+}
+template <typename T>
+__device__ __forceinline__ void store_cols_from_smem(T* dst, size_t ld, int nb, int nc, const float* u, int ldc) {
+  const int ng = nc >> 2;
+  for (int e = threadIdx.x; e < nb * ng; e += blockDim.x) {
+    const int b = e / ng, cl = (e % ng) * 4;
+    const float4 f = *reinterpret_cast<const float4*>(u + (size_t)b * ldc + cl);
+    const double v[4] = {f.x, f.y, f.z, f.w};
+    st4(dst + (size_t)b * ld + cl, v);
+  }
+  for (int e = threadIdx.x; e < nb * (nc - 4 * ng); e += blockDim.x) {
+    const int b = e / (nc - 4 * ng), cl = 4 * ng + e % (nc - 4 * ng);
+    dst[(size_t)b * ld + cl] = (T)u[(size_t)b * ldc + cl];
+  }
+}
 
 // Column c of a segmented block [A0 (n0 cols) | A1 (n1 cols) | A2 (n2 cols)], stride ld.
 template <typename T>
@@ -126,6 +185,278 @@ __device__ void cta_gram(const Seg3<TS>& S, const Seg3<TT>& Tm, const double* wg
   __syncthreads();
 }
 
+// Both Rayleigh-Ritz Grams in one pass over the cells:
+//   GM[a][b] = sum_cl wgt[cl] S_a[cl] S_b[cl],   GA[a][b] = sum_cl S_a[cl] AS_b[cl].
+// Same tiling and one-tile register prefetch as cta_gram.
+template <typename TS, typename TA>
+__device__ void cta_gram2(const Seg3<TS>& S, const Seg3<TA>& AS, const double* wgt, int ncells, double* GM,
+                          double* GA, LbMats& mt) {
+  const int t = threadIdx.x;
+  const bool own = t < 256;
+  const int ns = S.total();
+  const int a0 = 2 * (t >> 4), b0 = 2 * (t & 15);
+  const int lc = t & 31, ab = (t >> 5) & 7;
+  const TS* sp[4];
+  const TA* ap[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int a = ab + 8 * r;
+    sp[r] = (own && a < ns) ? S.col(a) : nullptr;
+    ap[r] = (own && a < ns) ? AS.col(a) : nullptr;
+  }
+  double sv[4], av[4], wv;
+  auto load = [&](int c0) {
+    const int c = c0 + lc;
+    const bool in = c < ncells;
+    wv = in ? wgt[c] : 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      sv[r] = (in && sp[r]) ? (double)sp[r][c] : 0.0;
+      av[r] = (in && ap[r]) ? (double)ap[r][c] : 0.0;
+    }
+  };
+  load(0);
+  double m00 = 0, m01 = 0, m10 = 0, m11 = 0, g00 = 0, g01 = 0, g10 = 0, g11 = 0;
+  const bool act = own && a0 < ns && b0 < ns;
+  for (int c0 = 0; c0 < ncells; c0 += LB_CH) {
+    if (own) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = (ab + 8 * r) * (LB_CH + 1) + lc;
+        mt.stile[row] = sv[r] * wv;
+        mt.ttile[row] = sv[r];
+        mt.atile[row] = av[r];
+      }
+    }
+    __syncthreads();
+    if (c0 + LB_CH < ncells) load(c0 + LB_CH);
+    if (act) {
+#pragma unroll 4
+      for (int cl = 0; cl < LB_CH; ++cl) {
+        const double w0 = mt.stile[a0 * (LB_CH + 1) + cl], w1 = mt.stile[(a0 + 1) * (LB_CH + 1) + cl];
+        const double s0 = mt.ttile[a0 * (LB_CH + 1) + cl], s1 = mt.ttile[(a0 + 1) * (LB_CH + 1) + cl];
+        const double t0 = mt.ttile[b0 * (LB_CH + 1) + cl], t1 = mt.ttile[(b0 + 1) * (LB_CH + 1) + cl];
+        const double q0 = mt.atile[b0 * (LB_CH + 1) + cl], q1 = mt.atile[(b0 + 1) * (LB_CH + 1) + cl];
+        m00 += w0 * t0;
+        m01 += w0 * t1;
+        m10 += w1 * t0;
+        m11 += w1 * t1;
+        g00 += s0 * q0;
+        g01 += s0 * q1;
+        g10 += s1 * q0;
+        g11 += s1 * q1;
+      }
+    }
+    __syncthreads();
+  }
+  if (act) {
+    GM[a0 * LB_LD + b0] = m00;
+    GA[a0 * LB_LD + b0] = g00;
+    if (b0 + 1 < ns) {
+      GM[a0 * LB_LD + b0 + 1] = m01;
+      GA[a0 * LB_LD + b0 + 1] = g01;
+    }
+    if (a0 + 1 < ns) {
+      GM[(a0 + 1) * LB_LD + b0] = m10;
+      GA[(a0 + 1) * LB_LD + b0] = g10;
+    }
+    if (a0 + 1 < ns && b0 + 1 < ns) {
+      GM[(a0 + 1) * LB_LD + b0 + 1] = m11;
+      GA[(a0 + 1) * LB_LD + b0 + 1] = g11;
+    }
+  }
+  __syncthreads();
+}
+
+// FP64 tensor-core MMA, D(8x8) += A(8x4) * B(4x8) (PTX mma.sync m8n8k4 f64).
+// Fragments: lane l holds A[l/4][l%4], B[l%4][l/4], C/D[l/4][2(l%4)], C/D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Both Rayleigh-Ritz Grams on the FP64 tensor cores:
+//   GM = (w S)^T S,  GA = S^T (A S),  S = [X W P] (ns <= 32 columns).
+// Warp w takes cells 4w + 32i; for each group of 4 cells lane l loads basis
+// row 8t + l/4 at cell l%4, which is at once its A fragment (row of S^T) and
+// its B fragment (column of S / AS): no shared-memory staging.  The per-warp
+// partial tiles are reduced in a fixed order through shared memory, so the
+// result is deterministic.  red: >= 8 * 32 * 32 doubles.
+template <typename TS, typename TA>
+__device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, const double* wgt, int ncells,
+                                           double* GM, double* GA, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int r = lane >> 2, cq = lane & 3;
+  const int ns = S.total();
+  const int nt = (ns + 7) >> 3;
+  const TS* sp[4];
+  const TA* ap[4];
+#pragma unroll
+  for (int ta = 0; ta < 4; ++ta) {
+    const int a = 8 * ta + r;
+    sp[ta] = (ta < nt && a < ns) ? S.col(a) : nullptr;
+    ap[ta] = (ta < nt && a < ns) ? AS.col(a) : nullptr;
+  }
+  double cm[4][4][2], ca[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cm[i][j][0] = cm[i][j][1] = ca[i][j][0] = ca[i][j][1] = 0.0;
+  double s[4], as[4], wv;
+  auto load = [&](int c0) {
+    const int c = c0 + cq;
+    const bool in = c < ncells;
+    wv = in ? wgt[c] : 0.0;
+#pragma unroll
+    for (int ta = 0; ta < 4; ++ta) {
+      s[ta] = (in && sp[ta]) ? (double)sp[ta][c] : 0.0;
+      as[ta] = (in && ap[ta]) ? (double)ap[ta][c] : 0.0;
+    }
+  };
+  load(4 * w);
+  for (int c0 = 4 * w; c0 < ncells; c0 += 4 * nwarp) {
+    double cs[4], cas[4];
+#pragma unroll
+    for (int ta = 0; ta < 4; ++ta) {
+      cs[ta] = s[ta];
+      cas[ta] = as[ta];
+    }
+    const double cw = wv;
+    if (c0 + 4 * nwarp < ncells) load(c0 + 4 * nwarp);  // next group in flight during the MMAs
+#pragma unroll
+    for (int ta = 0; ta < 4; ++ta) {
+      if (ta >= nt) break;
+      const double ws = cs[ta] * cw;
+#pragma unroll
+      for (int tb = 0; tb < 4; ++tb) {
+        if (tb >= nt) break;
+        dmma884(cm[ta][tb][0], cm[ta][tb][1], ws, cs[tb]);
+        dmma884(ca[ta][tb][0], ca[ta][tb][1], cs[ta], cas[tb]);
+      }
+    }
+  }
+  // deterministic cross-warp reduction, one Gram at a time
+#pragma unroll 1
+  for (int which = 0; which < 2; ++which) {
+    __syncthreads();
+#pragma unroll
+    for (int ta = 0; ta < 4; ++ta)
+#pragma unroll
+      for (int tb = 0; tb < 4; ++tb) {
+        if (ta < nt && tb < nt) {
+          const int row = 8 * ta + r, col = 8 * tb + 2 * cq;
+          red[(w * 32 + row) * 32 + col] = which ? ca[ta][tb][0] : cm[ta][tb][0];
+          red[(w * 32 + row) * 32 + col + 1] = which ? ca[ta][tb][1] : cm[ta][tb][1];
+        }
+      }
+    __syncthreads();
+    double* G = which ? GA : GM;
+    for (int e = threadIdx.x; e < ns * ns; e += blockDim.x) {
+      const int a = e / ns, b = e % ns;
+      double v = 0.0;
+      for (int ww = 0; ww < nwarp; ++ww) v += red[(ww * 32 + a) * 32 + b];
+      G[a * LB_LD + b] = v;
+    }
+  }
+  __syncthreads();
+}
+
+// In-place basis update on the FP64 tensor cores:
+//   B0[:, j] <- sum_b S_b Y[b][j]            (b < ns, S = [B0 | B1 | B2])
+//   B2[:, j] <- sum_{b >= m0} S_b Y[b][j]    (the new search direction)
+// for j < m (m <= 16).  Warp w handles groups of 8 cells; lane l's A fragment
+// is S_{k0 + l%4} at cell 8g + l/4 and its B fragments come from Y in shared
+// memory.  Every warp reads all ns columns of its 8 cells before writing them.
+template <typename T>
+__device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1, int n2, int m, const double* Y,
+                                            int ncells, size_t ld) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int r = lane >> 2, cq = lane & 3;
+  const int ns = m0 + n1 + n2;
+  const int nk = (ns + 3) >> 2;
+  const int nj = (m + 7) >> 3;
+  const int ngrp = (ncells + 7) >> 3;
+  double av[8], an[8];
+  auto load = [&](int gi, double* dst) {
+    const int cell = 8 * gi + r;
+    const bool in = cell < ncells;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const int b = 4 * kk + cq;
+      double v = 0.0;
+      if (kk < nk && in && b < ns) {
+        if (b < m0)
+          v = (double)B0[(size_t)b * ld + cell];
+        else if (b < m0 + n1)
+          v = (double)B1[(size_t)(b - m0) * ld + cell];
+        else
+          v = (double)B2[(size_t)(b - m0 - n1) * ld + cell];
+      }
+      dst[kk] = v;
+    }
+  };
+  if (w < ngrp) load(w, an);
+  for (int gi = w; gi < ngrp; gi += nwarp) {
+    const int cell = 8 * gi + r;
+    const bool in = cell < ncells;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) av[kk] = an[kk];
+    if (gi + nwarp < ngrp) load(gi + nwarp, an);
+    double dx[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, dp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      if (kk >= nk) break;
+#pragma unroll
+      for (int tj = 0; tj < 2; ++tj) {
+        if (tj >= nj) break;
+        const int bb = 4 * kk + cq, jj = 8 * tj + r;
+        const double y = (bb < ns && jj < m) ? Y[bb * LB_LD + jj] : 0.0;
+        const double yp = bb >= m0 ? y : 0.0;
+        dmma884(dx[tj][0], dx[tj][1], av[kk], y);
+        dmma884(dp[tj][0], dp[tj][1], av[kk], yp);
+      }
+    }
+    // D fragment: rows = cells 8gi + r, columns j = 8tj + 2cq + {0, 1}
+#pragma unroll
+    for (int tj = 0; tj < 2; ++tj) {
+      if (tj >= nj) break;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = 8 * tj + 2 * cq + h;
+        if (in && j < m) {
+          B0[(size_t)j * ld + cell] = (T)dx[tj][h];
+          B2[(size_t)j * ld + cell] = (T)dp[tj][h];
+        }
+      }
+    }
+  }
+}
+
+// out[b] = A32 u_b for nb vectors staged in shared memory: A32 is the subdomain
+// Neumann operator with its off-diagonal couplings rounded to FP32 (the sweep
+// coefficients), applied in FP64 arithmetic and stored in FP64.  For FP32
+// basis vectors this gives A-images that are exactly consistent with the
+// stored vectors (a fixed operator, no drift); the final FP64 Rayleigh-Ritz
+// uses the true operator.
+__device__ void smem_neumann64(const float* u, int ldc, int nb, int nx, int ny, int nz, const float* ctx,
+                               const float* cty, const float* ctz, const double* dN, double* out, size_t ld) {
+  const int nxny = nx * ny, nc = nxny * nz;
+  for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
+    const int b = e / nc, cl = e % nc;
+    const int i = cl % nx, tt = cl / nx, j = tt % ny, k = tt / ny;
+    const float* ub = u + (size_t)b * ldc;
+    double v = dN[cl] * (double)ub[cl];
+    if (i > 0) v -= (double)ctx[cl] * (double)ub[cl - 1];
+    if (i < nx - 1) v -= (double)ctx[cl + 1] * (double)ub[cl + 1];
+    if (j > 0) v -= (double)cty[cl] * (double)ub[cl - nx];
+    if (j < ny - 1) v -= (double)cty[cl + nx] * (double)ub[cl + nx];
+    if (k > 0) v -= (double)ctz[cl] * (double)ub[cl - nxny];
+    if (k < nz - 1) v -= (double)ctz[cl + nxny] * (double)ub[cl + nxny];
+    out[(size_t)b * ld + cl] = v;
+  }
+}
+
 // C[n1 x n3] = op(A)[n1 x n2] * B[n2 x n3] (small, ld LB_LD).
 __device__ void cta_small_gemm(const double* A, bool transA, const double* B, double* C, int n1, int n2, int n3) {
   for (int e = threadIdx.x; e < n1 * n3; e += blockDim.x) {
@@ -146,7 +477,25 @@ __device__ void cta_small_gemm(const double* A, bool transA, const double* B, do
 // pivot falls below `drop` the basis is nearly dependent and SVQB takes over
 // (eigendecomposition of D GM D, directions with eigenvalue <= drop * max
 // dropped).  Then H = Q^T GA Q is diagonalised and Y = Q V[:, :m].
-__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop) {
+// Phase timer for diagnostics: thread 0 accumulates clock64() deltas.
+struct PhaseClock {
+  long long* p;
+  long long t0;
+  __device__ void start() {
+    if (p && threadIdx.x == 0) t0 = clock64();
+  }
+  __device__ void lap(int ph) {
+    if (p && threadIdx.x == 0) {
+      const long long t1 = clock64();
+      p[ph] += t1 - t0;
+      t0 = t1;
+    }
+  }
+};
+
+__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop, double jtol,
+                                 PhaseClock* pc = nullptr);
+__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop, double jtol, PhaseClock* pc) {
   for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
     const int a = e / nS, b = e % nS;
     if (a < b) {
@@ -175,6 +524,7 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
     mt.U[a * LB_LD + b] = v;
   }
   __syncthreads();
+  if (pc) pc->lap(8);
   // Cholesky of the scaled Gram (warp 0, right-looking, lower factor in U)
   if (threadIdx.x < 32) {
     const int l = threadIdx.x;
@@ -199,6 +549,7 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
     if (l == 0) sm.ival[4] = ok;
   }
   __syncthreads();
+  if (pc) pc->lap(9);
   int q;
   if (sm.ival[4]) {
     // Q = D L^-T: lane c solves L x = e_c (forward substitution), Q[a][c] = D_a x[c -> row a]
@@ -218,8 +569,7 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
     __syncthreads();
     q = nS;
   } else {
-    if (threadIdx.x < 32) warp_jacobi_eigh(mt.H, mt.U, sm.w, nS, LB_LD, sm.jac);
-    __syncthreads();
+    cta_jacobi_eigh(mt.H, mt.U, sm.w, nS, LB_LD, sm.ival2, sm.jac, jtol);
     if (threadIdx.x == 0) {
       int qq = 0;
       const double wmax = sm.w[nS - 1];
@@ -235,6 +585,7 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
     }
     __syncthreads();
   }
+  if (pc) pc->lap(10);
   cta_small_gemm(mt.GA, false, mt.Q, mt.V, nS, nS, q);  // V = GA Q
   cta_small_gemm(mt.Q, true, mt.V, mt.H, q, nS, q);     // H = Q^T GA Q
   for (int e = threadIdx.x; e < q * q; e += blockDim.x) {
@@ -245,12 +596,16 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
     }
   }
   __syncthreads();
-  if (threadIdx.x < 32) warp_jacobi_eigh(mt.H, mt.V, sm.th, q, LB_LD, sm.jac);
-  __syncthreads();
+  if (pc) pc->lap(11);
+  // only the lowest min(m, q) eigenpairs of H are needed
+  cta_sym_lowest(mt.H, mt.V, sm.th, q, min(m, q), LB_LD, mt.stile);
+  (void)jtol;
+  if (pc) pc->lap(12);
   const int mm = min(m, q);
   cta_small_gemm(mt.Q, false, mt.V, mt.Y, nS, q, mm);  // Y = Q V[:, :m]
   if (threadIdx.x < mm) sm.lam[threadIdx.x] = sm.th[threadIdx.x];
   __syncthreads();
+  if (pc) pc->lap(13);
   return q;
 }
 
@@ -274,22 +629,6 @@ __device__ __forceinline__ void neumann_apply_col(const Grid& g, const SubInfo& 
   }
 }
 
-// Phase timer for diagnostics: thread 0 accumulates clock64() deltas.
-struct PhaseClock {
-  long long* p;
-  long long t0;
-  __device__ void start() {
-    if (p && threadIdx.x == 0) t0 = clock64();
-  }
-  __device__ void lap(int ph) {
-    if (p && threadIdx.x == 0) {
-      const long long t1 = clock64();
-      p[ph] += t1 - t0;
-      t0 = t1;
-    }
-  }
-};
-
 template <typename T>
 __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned char* work, size_t work_stride, T* phi,
                                                 double* evals, int* iters, int* status, int* ks, double eb) {
@@ -308,7 +647,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
   const int m = a.m, k = a.k, mb = a.mb;
   unsigned char* wb = work + (size_t)blockIdx.x * work_stride;
   const int ld = a.ld;
-  PhaseClock pc{a.prof ? a.prof + (size_t)blockIdx.x * 8 : nullptr, 0};
+  PhaseClock pc{a.prof ? a.prof + (size_t)blockIdx.x * 16 : nullptr, 0};
   pc.start();
 
   for (int s = blockIdx.x; s < a.nsub; s += gridDim.x) {
@@ -317,11 +656,12 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     T* X = reinterpret_cast<T*>(wb);
     T* W = X + (size_t)m * ld;
     T* P = W + (size_t)m * ld;
-    T* AX = P + (size_t)m * ld;
-    T* AW = AX + (size_t)m * ld;
-    T* AP = AW + (size_t)m * ld;
+    double* AX = reinterpret_cast<double*>(P + (size_t)m * ld);
+    double* AW = AX + (size_t)m * ld;
+    double* AP = AW + (size_t)m * ld;
     double* Md = reinterpret_cast<double*>(AP + (size_t)m * ld);
     double* dN = Md + ld;
+    double* dN32 = dN + ld;  // diagonal matching the FP32-rounded couplings (FP32 storage)
 
     // ---- mass diagonal (src/PreMixFEM_3D.c:243-346), Neumann diagonal, sweep coefficients
     double ratio = 0.0;
@@ -361,6 +701,16 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       }
       Md[cl] = mv;
       dN[cl] = dn;
+      {
+        double d32 = a.db[cg];
+        if (i > 0) d32 += (double)(float)a.tx[cg];
+        if (i < nx - 1) d32 += (double)(float)a.tx[cg + 1];
+        if (j > 0) d32 += (double)(float)a.ty[cg];
+        if (j < ny - 1) d32 += (double)(float)a.ty[cg + g.M];
+        if (kk > 0) d32 += (double)(float)a.tz[cg];
+        if (kk < nz - 1) d32 += (double)(float)a.tz[cg + g.MN];
+        dN32[cl] = d32;
+      }
       ctx[cl] = i > 0 ? (float)a.tx[cg] : 0.0f;
       cty[cl] = j > 0 ? (float)a.ty[cg] : 0.0f;
       ctz[cl] = kk > 0 ? (float)a.tz[cg] : 0.0f;
@@ -412,17 +762,26 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       X[(size_t)j * ld + cl] = (T)v;
     }
     __syncthreads();
-    for (int j = 0; j < m; ++j)
-      neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
-    __syncthreads();
+    if (sizeof(T) == 8) {
+      for (int j = 0; j < m; ++j)
+        neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
+      __syncthreads();
+    } else {
+      for (int j0 = 0; j0 < m; j0 += mb) {
+        const int nb = min(mb, m - j0);
+        load_cols_to_smem(X + (size_t)j0 * ld, ld, nb, nc, u, ldc);
+        __syncthreads();
+        smem_neumann64(u, ldc, nb, nx, ny, nz, ctx, cty, ctz, dN32, AX + (size_t)j0 * ld, ld);
+        __syncthreads();
+      }
+    }
     const double drop = sizeof(T) == 4 ? 1e-9 : 1e-13;
     {
       Seg3<T> sx{{X, X, X}, {m, 0, 0}, ld};
-      Seg3<T> sax{{AX, AX, AX}, {m, 0, 0}, ld};
-      cta_gram(sx, sx, Md, nc, mt.GM, mt);
-      cta_gram(sx, sax, (const double*)nullptr, nc, mt.GA, mt);
+      Seg3<double> sax{{AX, AX, AX}, {m, 0, 0}, ld};
+      cta_gram2(sx, sax, Md, nc, mt.GM, mt.GA, mt);
     }
-    cta_rayleigh_ritz(sm, mt, m, m, drop);
+    cta_rayleigh_ritz(sm, mt, m, m, drop, 1e-12);
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
       double xr[LB_MM], ar[LB_MM];
 #pragma unroll
@@ -441,7 +800,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
               an += ar[b] * mt.Y[b * LB_LD + j];
             }
           X[(size_t)j * ld + cl] = (T)xn;
-          AX[(size_t)j * ld + cl] = (T)an;
+          AX[(size_t)j * ld + cl] = an;
         }
     }
     __syncthreads();
@@ -449,21 +808,48 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     bool hasP = false;
     int it = 0;
     bool conv = false;
+    if (threadIdx.x == 0) {
+      sm.scal[2] = 1e300;
+      sm.ival[5] = 0;
+      sm.ival[6] = 0;
+    }
+    __syncthreads();
     pc.lap(0);
     for (; it < a.max_it; ++it) {
       // ---- residuals R = AX - M X Lambda (into W) and ||R_j||_{M^-1}
       double racc[LB_MM];
 #pragma unroll
       for (int j = 0; j < LB_MM; ++j) racc[j] = 0.0;
-      for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-        const double mv = Md[cl];
+      {
+        const int ng = nc >> 2;
+        for (int gi = threadIdx.x; gi < ng; gi += blockDim.x) {
+          const int cl = gi * 4;
+          double mv[4];
+          ld4(Md + cl, mv);
 #pragma unroll
-        for (int j = 0; j < LB_MM; ++j)
-          if (j < m) {
-            const double r = (double)AX[(size_t)j * ld + cl] - sm.lam[j] * mv * (double)X[(size_t)j * ld + cl];
-            W[(size_t)j * ld + cl] = (T)r;
-            racc[j] += r * r / mv;
-          }
+          for (int j = 0; j < LB_MM; ++j)
+            if (j < m) {
+              double ax[4], xv[4], r[4];
+              ld4(AX + (size_t)j * ld + cl, ax);
+              ld4(X + (size_t)j * ld + cl, xv);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                r[q] = ax[q] - sm.lam[j] * mv[q] * xv[q];
+                racc[j] += r[q] * r[q] / mv[q];
+              }
+              st4(W + (size_t)j * ld + cl, r);
+            }
+        }
+        for (int cl = 4 * ng + threadIdx.x; cl < nc; cl += blockDim.x) {
+          const double mv = Md[cl];
+#pragma unroll
+          for (int j = 0; j < LB_MM; ++j)
+            if (j < m) {
+              const double r = (double)AX[(size_t)j * ld + cl] - sm.lam[j] * mv * (double)X[(size_t)j * ld + cl];
+              W[(size_t)j * ld + cl] = (T)r;
+              racc[j] += r * r / mv;
+            }
+        }
       }
 #pragma unroll
       for (int j = 0; j < LB_MM; ++j)
@@ -480,10 +866,23 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       __syncthreads();
       if (threadIdx.x == 0) {
         int na = 0, cv = 1;
+        double worst = 0.0;
         for (int j = 0; j < m; ++j) {
           const bool done_j = sm.res[j] <= a.tol;
+          if (j < k) worst = fmax(worst, sm.res[j]);
           if (j < k && !done_j) cv = 0;
           if (!done_j || j >= k) sm.act[na++] = j;  // soft locking of converged wanted vectors
+        }
+        // rounding floor: no halving of the worst wanted residual in 12 iterations
+        // while within 10 x tol -> accept (status 2)
+        if (!cv) {
+          if (worst < 0.5 * sm.scal[2]) {
+            sm.scal[2] = worst;
+            sm.ival[5] = it;
+          } else if (it - sm.ival[5] >= 12 && worst <= 10.0 * a.tol) {
+            cv = 1;
+            sm.ival[6] = 1;
+          }
         }
         sm.ival[2] = na;
         sm.ival[3] = cv;
@@ -503,16 +902,14 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       // ---- W = T R: IC(0) sweeps, mb vectors per wavefront, FP32 in shared memory
       for (int j0 = 0; j0 < nact; j0 += mb) {
         const int nb = min(mb, nact - j0);
-        for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
-          const int b = e / nc, cl = e % nc;
-          u[b * ldc + cl] = (float)W[(size_t)(j0 + b) * ld + cl];
-        }
+        load_cols_to_smem(W + (size_t)j0 * ld, ld, nb, nc, u, ldc);
         __syncthreads();
         for (int d = 0; d < nplanes; ++d) {
           const int i = d - jj - kk;
           if (line && i >= 0 && i < nx) {
             const int cl = (kk * ny + jj) * nx + i;
             const float cz_ = ctz[cl], cy_ = cty[cl], cx_ = ctx[cl], ci = cinv[cl];
+#pragma unroll 4
             for (int b = 0; b < nb; ++b) {
               float* ub = u + b * ldc;
               float sacc = ub[cl];
@@ -532,6 +929,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
             const float cyp = jj < ny - 1 ? cty[cl + nx] : 0.0f;
             const float czp = kk < nz - 1 ? ctz[cl + nxny] : 0.0f;
             const float ci = cinv[cl];
+#pragma unroll 4
             for (int b = 0; b < nb; ++b) {
               float* ub = u + b * ldc;
               float sacc = 0.0f;
@@ -543,91 +941,68 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
           }
           __syncthreads();
         }
-        for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
-          const int b = e / nc, cl = e % nc;
-          W[(size_t)(j0 + b) * ld + cl] = (T)u[b * ldc + cl];
-        }
+        if (sizeof(T) == 4) smem_neumann64(u, ldc, nb, nx, ny, nz, ctx, cty, ctz, dN32, AW + (size_t)j0 * ld, ld);
+        store_cols_from_smem(W + (size_t)j0 * ld, ld, nb, nc, u, ldc);
         __syncthreads();
       }
       pc.lap(2);
-      for (int j = 0; j < nact; ++j)
-        neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, W + (size_t)j * ld, AW + (size_t)j * ld, nc);
-      __syncthreads();
+      if (sizeof(T) == 8) {  // FP64 A-images of the new directions
+        for (int j = 0; j < nact; ++j)
+          neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, W + (size_t)j * ld, AW + (size_t)j * ld, nc);
+        __syncthreads();
+      }
       pc.lap(3);
       const int np = hasP ? m : 0;
       const int nS = m + nact + np;
       {
         Seg3<T> sS{{X, W, P}, {m, nact, np}, ld};
-        Seg3<T> sA{{AX, AW, AP}, {m, nact, np}, ld};
-        cta_gram(sS, sS, Md, nc, mt.GM, mt);
-        cta_gram(sS, sA, (const double*)nullptr, nc, mt.GA, mt);
+        Seg3<double> sA{{AX, AW, AP}, {m, nact, np}, ld};
+        cta_gram2_mma(sS, sA, Md, nc, mt.GM, mt.GA, mt.U);
       }
       pc.lap(4);
-      const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop);
       pc.lap(5);
+      const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop, 1e-11, &pc);
       if (q < m) {  // basis collapsed: restart without P
         hasP = false;
         continue;
       }
       // ---- X <- S Y, P <- [W P] Y_WP, same for AX / AP (per cell, in place)
-      for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-#pragma unroll 1
-        for (int pass = 0; pass < 2; ++pass) {
-          T* B0 = pass ? AX : X;
-          T* B1 = pass ? AW : W;
-          T* B2 = pass ? AP : P;
-          double xr[3 * LB_MM];
-#pragma unroll
-          for (int b = 0; b < 3 * LB_MM; ++b) {
-            double v = 0.0;
-            if (b < m)
-              v = (double)B0[(size_t)b * ld + cl];
-            else if (b < m + nact)
-              v = (double)B1[(size_t)(b - m) * ld + cl];
-            else if (b < nS)
-              v = (double)B2[(size_t)(b - m - nact) * ld + cl];
-            xr[b] = v;
-          }
-#pragma unroll
-          for (int j = 0; j < LB_MM; ++j)
-            if (j < m) {
-              double pn = 0.0, xn = 0.0;
-#pragma unroll
-              for (int b = 0; b < 3 * LB_MM; ++b) {
-                if (b < m)
-                  xn += xr[b] * mt.Y[b * LB_LD + j];
-                else if (b < nS)
-                  pn += xr[b] * mt.Y[b * LB_LD + j];
-              }
-              B0[(size_t)j * ld + cl] = (T)(xn + pn);
-              B2[(size_t)j * ld + cl] = (T)pn;
-            }
-        }
-      }
-      __syncthreads();
-      if (sizeof(T) == 4) {  // implicit A-image updates drift in float: recompute
-        for (int j = 0; j < m; ++j) {
-          neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX + (size_t)j * ld, nc);
-          neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, P + (size_t)j * ld, AP + (size_t)j * ld, nc);
-        }
+      // X <- S Y, P <- [W P] Y_WP and the same combination of the FP64 A-images, on the
+      // FP64 tensor cores
+      cta_update_mma<T>(X, W, P, m, nact, np, m, mt.Y, nc, ld);
+      if (sizeof(T) == 8) {
+        cta_update_mma<double>(AX, AW, AP, m, nact, np, m, mt.Y, nc, ld);
         __syncthreads();
+      } else {
+        // FP32 storage rounds X and P: their A-images are recomputed from the stored values
+        __syncthreads();
+        for (int blk = 0; blk < 2; ++blk) {
+          const T* src = blk ? P : X;
+          double* dst = blk ? AP : AX;
+          for (int j0 = 0; j0 < m; j0 += mb) {
+            const int nb = min(mb, m - j0);
+            load_cols_to_smem(src + (size_t)j0 * ld, ld, nb, nc, u, ldc);
+            __syncthreads();
+            smem_neumann64(u, ldc, nb, nx, ny, nz, ctx, cty, ctz, dN32, dst + (size_t)j0 * ld, ld);
+            __syncthreads();
+          }
+        }
       }
       hasP = true;
       pc.lap(6);
     }
 
     // ---- final FP64 Rayleigh-Ritz on X (A X recomputed in FP64 over the W|P slab)
-    double* AX64 = reinterpret_cast<double*>(W);
+    double* AX64 = AX;
     for (int j = 0; j < m; ++j)
       neumann_apply_col(g, S, a.tx, a.ty, a.tz, dN, X + (size_t)j * ld, AX64 + (size_t)j * ld, nc);
     __syncthreads();
     {
       Seg3<T> sx{{X, X, X}, {m, 0, 0}, ld};
       Seg3<double> sax{{AX64, AX64, AX64}, {m, 0, 0}, ld};
-      cta_gram(sx, sx, Md, nc, mt.GM, mt);
-      cta_gram(sx, sax, (const double*)nullptr, nc, mt.GA, mt);
+      cta_gram2(sx, sax, Md, nc, mt.GM, mt.GA, mt);
     }
-    cta_rayleigh_ritz(sm, mt, m, m, 1e-14);
+    cta_rayleigh_ritz(sm, mt, m, m, 1e-14, 1e-14);
     // adaptive count (:369-383) and output
     if (threadIdx.x == 0) {
       int num = k;
@@ -639,7 +1014,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       sm.ival[1] = num;
       ks[s] = num;
       iters[s] = it;
-      status[s] = conv ? 0 : 1;
+      status[s] = conv ? (sm.ival[6] ? 2 : 0) : 1;
     }
     __syncthreads();
     const int num = sm.ival[1];

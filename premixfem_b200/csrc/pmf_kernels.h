@@ -130,6 +130,7 @@ struct LobpcgArgs {
 size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes);
 // One persistent CTA per block; each handles subdomains blockIdx.x, +nblocks, ...
 // ks[s] receives the adaptive eigen count (first j with lambda_j >= eb, else k).
+// status[s]: 0 converged, 2 stopped at the rounding floor (within 100 x tol), 1 hit max_it.
 // Requires ny*nz <= 256 and cells <= PMF_MAX_SUB_CELLS, m <= 10.
 template <typename T>
 void launch_lobpcg(const LobpcgArgs& a, int nblocks, void* work, T* phi, double* evals, int* iters, int* status,

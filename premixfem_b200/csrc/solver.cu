@@ -483,8 +483,8 @@ int Solver::setup() {
   long long* d_prof = nullptr;
   const bool prof_eig = getenv("PMF_PROFILE_EIGEN") != nullptr;
   if (prof_eig) {
-    cudaMalloc(&d_prof, sizeof(long long) * 8 * eig_blocks);
-    cudaMemsetAsync(d_prof, 0, sizeof(long long) * 8 * eig_blocks, st);
+    cudaMalloc(&d_prof, sizeof(long long) * 16 * eig_blocks);
+    cudaMemsetAsync(d_prof, 0, sizeof(long long) * 16 * eig_blocks, st);
     la.prof = d_prof;
   }
   const size_t need = ((lobpcg_work_bytes(max_cells, la.m, mixed ? 4 : 8) + 255) & ~(size_t)255) * eig_blocks;
@@ -503,20 +503,21 @@ int Solver::setup() {
   cudaEventRecord(e[2], st);
   if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;
   if (prof_eig) {  // diagnostics: cycles per LOBPCG phase, summed over CTAs
-    std::vector<long long> hp(8 * eig_blocks);
+    std::vector<long long> hp(16 * eig_blocks);
     cudaMemcpy(hp.data(), d_prof, sizeof(long long) * hp.size(), cudaMemcpyDeviceToHost);
-    const char* names[8] = {"init", "residual", "precond", "stencil", "gram", "rayleigh_ritz", "update", "final"};
-    long long tot[8] = {0}, mx = 0;
+    const char* names[14] = {"init",    "residual",  "precond",   "stencil",  "gram",     "pre_rr",   "update",
+                             "final",   "rr_scale",  "rr_chol",   "rr_basis", "rr_proj",  "rr_jacobi", "rr_coef"};
+    long long tot[16] = {0}, mx = 0;
     for (int b = 0; b < eig_blocks; ++b) {
       long long sb = 0;
-      for (int p = 0; p < 8; ++p) {
-        tot[p] += hp[b * 8 + p];
-        sb += hp[b * 8 + p];
+      for (int p = 0; p < 16; ++p) {
+        tot[p] += hp[b * 16 + p];
+        sb += hp[b * 16 + p];
       }
       mx = std::max(mx, sb);
     }
     fprintf(stderr, "[premixfem_b200] LOBPCG cycles per phase (sum over %d CTAs; slowest CTA %lld):", eig_blocks, mx);
-    for (int p = 0; p < 8; ++p) fprintf(stderr, " %s=%lld", names[p], tot[p]);
+    for (int p = 0; p < 14; ++p) fprintf(stderr, " %s=%lld", names[p], tot[p]);
     fprintf(stderr, "\n");
     cudaFree(d_prof);
   }

@@ -87,7 +87,8 @@ def test_local_and_level3_eigenvalues(native, name, oracle_cache):
     s = _gpu(prob, d)
     ev, ks, iters, status = s.eigen_lv1()
     pc = ref["pc"]
-    assert (status == 0).all(), f"LOBPCG did not converge on {np.nonzero(status)[0]}"
+    # status 0: converged to tolerance, 2: stopped at the rounding floor within 100 x tol, 1: max_it
+    assert (status != 1).all(), f"LOBPCG did not converge on {np.nonzero(status == 1)[0]}"
     ref1 = np.stack(pc.eigvals_lv1)
     scale = np.abs(ref1).max(axis=1, keepdims=True)
     err = np.abs(ev - ref1) / np.maximum(np.abs(ref1), 1e-3 * scale)
