@@ -374,24 +374,25 @@ void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_line
   { note_launch(); k_ic_factor<<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, bad); }
 }
 
+// Hyperplane sweeps of the IC(0) solve on a subdomain whose couplings (cx, cy,
+// cz: lower-face transmissibility of each cell inside the subdomain, 0 on its
+// boundary) and inverse pivots (ci) sit in shared memory next to the vector u.
 template <typename T>
-__device__ __forceinline__ void ic_sweeps(const Grid& g, const SubGeom& q, const T* tx, const T* ty, const T* tz,
-                                          const T* inv_d, T* u) {
+__device__ __forceinline__ void ic_sweeps_smem(const SubGeom& q, const T* cx, const T* cy, const T* cz, const T* ci,
+                                               T* u) {
   const int t = threadIdx.x;
   const int j = t % q.ny, k = t / q.ny;
   const bool line = t < q.nlines;
-  const long long base = ((long long)(q.z0 + k) * g.N + (q.y0 + j)) * g.M + q.x0;
   // forward: (D + L) w = r  ->  w_i = (r_i + sum t_ij w_j) / D_i
   for (int d = 0; d < q.nplanes; ++d) {
     const int i = d - j - k;
     if (line && i >= 0 && i < q.nx) {
       const int cl = (k * q.ny + j) * q.nx + i;
-      const long long cg = base + i;
       T s = u[cl];
-      if (k > 0) s += tz[cg] * u[cl - q.nxny];
-      if (j > 0) s += ty[cg] * u[cl - q.nx];
-      if (i > 0) s += tx[cg] * u[cl - 1];
-      u[cl] = s * inv_d[cg];
+      if (k > 0) s += cz[cl] * u[cl - q.nxny];
+      if (j > 0) s += cy[cl] * u[cl - q.nx];
+      if (i > 0) s += cx[cl] * u[cl - 1];
+      u[cl] = s * ci[cl];
     }
     __syncthreads();
   }
@@ -400,12 +401,11 @@ __device__ __forceinline__ void ic_sweeps(const Grid& g, const SubGeom& q, const
     const int i = d - j - k;
     if (line && i >= 0 && i < q.nx) {
       const int cl = (k * q.ny + j) * q.nx + i;
-      const long long cg = base + i;
       T s = (T)0;
-      if (i < q.nx - 1) s += tx[cg + 1] * u[cl + 1];
-      if (j < q.ny - 1) s += ty[cg + g.M] * u[cl + q.nx];
-      if (k < q.nz - 1) s += tz[cg + g.MN] * u[cl + q.nxny];
-      u[cl] = u[cl] + s * inv_d[cg];
+      if (i < q.nx - 1) s += cx[cl + 1] * u[cl + 1];
+      if (j < q.ny - 1) s += cy[cl + q.nx] * u[cl + q.nx];
+      if (k < q.nz - 1) s += cz[cl + q.nxny] * u[cl + q.nxny];
+      u[cl] = u[cl] + s * ci[cl];
     }
     __syncthreads();
   }
@@ -414,23 +414,33 @@ __device__ __forceinline__ void ic_sweeps(const Grid& g, const SubGeom& q, const
 template <typename T, bool HAS_Y, bool FINAL>
 __global__ void k_ic_apply(Grid g, const SubInfo* subs, const T* tx, const T* ty, const T* tz, const T* diag,
                            const T* inv_d, const double* x, const T* yin, T* out_t, double* out_d, double* part,
-                           const int* done) {
+                           const int* done, int ldc) {
   if (done && *done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* red = reinterpret_cast<double*>(smem_raw);
   T* u = reinterpret_cast<T*>(smem_raw + 32 * sizeof(double));
+  T* cx = u + ldc;
+  T* cy = cx + ldc;
+  T* cz = cy + ldc;
+  T* ci = cz + ldc;
   const SubGeom q = sub_geom(subs[blockIdx.x]);
   // right-hand side r = x - A y on the subdomain (y read across subdomain faces)
+  // and the subdomain's couplings / inverse pivots, in one coalesced pass
   for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
     const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
     const int ex = q.x0 + i, ey = q.y0 + j, ez = q.z0 + k;
     const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    const T txc = tx[cg], tyc = ty[cg], tzc = tz[cg];
+    cx[cl] = i > 0 ? txc : (T)0;
+    cy[cl] = j > 0 ? tyc : (T)0;
+    cz[cl] = k > 0 ? tzc : (T)0;
+    ci[cl] = inv_d[cg];
     T r = (T)x[cg];
     if (HAS_Y) r -= apply_A(g, cg, ex, ey, ez, tx, ty, tz, diag, yin);
     u[cl] = r;
   }
   __syncthreads();
-  ic_sweeps(g, q, tx, ty, tz, inv_d, u);
+  ic_sweeps_smem(q, cx, cy, cz, ci, u);
   double dot = 0.0;
   for (int cl = threadIdx.x; cl < q.ncells; cl += blockDim.x) {
     const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
@@ -456,35 +466,28 @@ void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines
                      const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
                      T* out_t, double* out_d, double* part, const int* done, cudaStream_t st) {
   int threads = std::max(64, ((max_lines + 31) / 32) * 32);
-  size_t smem = 32 * sizeof(double) + (size_t)max_cells * sizeof(T);
+  const int ldc = (max_cells + 3) & ~3;
+  size_t smem = 32 * sizeof(double) + (size_t)5 * ldc * sizeof(T);
   const bool fin = out_d != nullptr;
-  static bool attr_set[2][2][2] = {};
-  bool& done_attr = attr_set[sizeof(T) == 8][yin != nullptr][fin];
-  if (!done_attr) {
-    const int lim = 32 * sizeof(double) + PMF_MAX_SUB_CELLS * sizeof(T);
+  if (smem > 48 * 1024) {
     if (yin) {
-      cudaFuncSetAttribute(k_ic_apply<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-      cudaFuncSetAttribute(k_ic_apply<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+      cudaFuncSetAttribute(k_ic_apply<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_ic_apply<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     } else {
-      cudaFuncSetAttribute(k_ic_apply<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-      cudaFuncSetAttribute(k_ic_apply<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+      cudaFuncSetAttribute(k_ic_apply<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_ic_apply<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
-    done_attr = true;
   }
   if (yin) {
     if (fin)
-      { note_launch(); k_ic_apply<T, true, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d,
-                                                             part, done); }
+      { note_launch(); k_ic_apply<T, true, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d, part, done, ldc); }
     else
-      { note_launch(); k_ic_apply<T, true, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                              out_d, part, done); }
+      { note_launch(); k_ic_apply<T, true, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d, part, done, ldc); }
   } else {
     if (fin)
-      { note_launch(); k_ic_apply<T, false, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                              out_d, part, done); }
+      { note_launch(); k_ic_apply<T, false, true><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d, part, done, ldc); }
     else
-      { note_launch(); k_ic_apply<T, false, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t,
-                                                               out_d, part, done); }
+      { note_launch(); k_ic_apply<T, false, false><<<nsub, threads, smem, st>>>(g, subs, tx, ty, tz, diag, inv_d, x, yin, out_t, out_d, part, done, ldc); }
   }
 }
 

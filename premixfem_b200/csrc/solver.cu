@@ -310,6 +310,10 @@ int Solver::build_partition() {
     err = "subdomain too large for the shared-memory sweeps (cells <= 8192, ny*nz <= 256)";
     return 62;
   }
+  if (32 * 8 + 5 * (size_t)((max_cells + 3) & ~3) * (opt.precision == 1 ? 4 : 8) > 227 * 1024) {
+    err = "subdomain too large for the shared-memory IC(0) sweep of this precision (FP64: <= 5600 cells)";
+    return 62;
+  }
   kmax = opt.en_lv1;
   if (kmax > 8 || opt.en_lv1 + opt.eig_guard > 10) {
     err = "en_lv1 must be <= 8 (block size en_lv1 + guard <= 10)";
@@ -502,6 +506,7 @@ int Solver::setup() {
                           max_lines, st);
   cudaEventRecord(e[2], st);
   if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;
+  if (int er = check(cudaGetLastError(), "setup launch")) return er;
   if (prof_eig) {  // diagnostics: cycles per LOBPCG phase, summed over CTAs
     std::vector<long long> hp(16 * eig_blocks);
     cudaMemcpy(hp.data(), d_prof, sizeof(long long) * hp.size(), cudaMemcpyDeviceToHost);
@@ -612,6 +617,7 @@ int Solver::setup() {
   launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
   cudaEventRecord(e[5], st);
   if (int er = check(cudaStreamSynchronize(st), "coarse setup")) return er;
+  if (int er = check(cudaGetLastError(), "coarse setup launch")) return er;
   cudaFree(d_ks3);
   float ms[5];
   for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], e[i], e[i + 1]);
@@ -748,6 +754,7 @@ int Solver::pc_apply(const double* x_in, double* y_out, bool on_device) {
   cudaEventRecord(ev1, st);
   if (!on_device) cudaMemcpyAsync(y_out, ys, n * 8, cudaMemcpyDeviceToHost, st);
   int e = check(cudaStreamSynchronize(st), "PC_apply_vec");
+  if (!e) e = check(cudaGetLastError(), "PC_apply_vec launch");
   float ms = 0;
   cudaEventElapsedTime(&ms, ev0, ev1);
   t_stages[ST_AV] += ms * 1e-3;
@@ -785,6 +792,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
     }
     cudaMemcpyAsync(h_state, state, sizeof(PcgState), cudaMemcpyDeviceToHost, st);
     if (int e = check(cudaStreamSynchronize(st), "KSPSolve")) return e;
+    if (int e = check(cudaGetLastError(), "KSPSolve launch")) return e;
     if (h_state->done) break;
     if (++guard > opt.max_it + 8) break;
   }
