@@ -158,14 +158,14 @@ __global__ void k_pcg_start(long long n, const double* b, double* x, double* r, 
   v = block_sum(v, red);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
-__global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double rtol, int max_it) {
+__global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double rtol, double atol, int max_it) {
   __shared__ double red[32];
   const double v = fixed_sum(part, nb, red);
   if (threadIdx.x == 0) {
     const double dp = sqrt(v);
     s->dp = dp;
     s->rnorm0 = dp;
-    s->ttol = fmax(rtol * dp, 1.0e-50);  // KSPConvergedDefault: max(rtol*rnorm0, abstol)
+    s->ttol = fmax(rtol * dp, atol);  // KSPConvergedDefault: max(rtol*rnorm0, abstol)
     s->its = 0;
     s->max_it = max_it;
     s->first = 1;
@@ -174,10 +174,10 @@ __global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double 
   }
 }
 void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,
-                      int max_it, cudaStream_t st) {
+                      double atol, int max_it, cudaStream_t st) {
   int nb = cell_blocks(g.ncell);
   { note_launch(); k_pcg_start<<<nb, kCellThreads, 0, st>>>(g.ncell, b, x, r, part); }
-  { note_launch(); k_pcg_start_fin<<<1, 256, 0, st>>>(part, nb, s, rtol, max_it); }
+  { note_launch(); k_pcg_start_fin<<<1, 256, 0, st>>>(part, nb, s, rtol, atol, max_it); }
 }
 
 // beta = z.r (the dot is written per block by the preconditioner's last kernel

@@ -40,7 +40,7 @@ void launch_spmv(const Grid& g, const double* tx, const double* ty, const double
 
 // ---- PCG -----------------------------------------------------------------------
 void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,
-                      int max_it, cudaStream_t st);
+                      double atol, int max_it, cudaStream_t st);
 // beta = z.r from nparts per-block partials (written by the preconditioner's last kernel).
 void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream_t st);
 // same, computing the partials itself

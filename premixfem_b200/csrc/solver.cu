@@ -94,6 +94,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   o->use_full_Cholesky_lv1 = db.has("use_full_Cholesky_lv1");
   o->use_2level = db.has("use_2level");
   db.get_real("ksp_rtol", &o->rtol);
+  db.get_real("ksp_atol", &o->atol);
   db.get_int("ksp_max_it", &o->max_it);
   std::string prec;
   auto it = db.kv.find("pmf_precision");
@@ -404,6 +405,36 @@ std::vector<int> Solver::schedule() const {
   return s;
 }
 
+// Face transmissibilities, diagonal and Dirichlet terms of the operator on
+// the solver stream (PC_create_A, src/PreMixFEM_3D.c:1757-1824).
+void Solver::assemble_launch() {
+  AssembleArgs aa;
+  aa.g = g;
+  aa.kx = kx;
+  aa.ky = ky;
+  aa.kz = kz;
+  const double meas = H[0] * H[1] * H[2];
+  const double fyz = H[1] * H[2], fzx = H[2] * H[0], fxy = H[0] * H[1];
+  aa.cx = fyz * fyz / meas;
+  aa.cy = fzx * fzx / meas;
+  aa.cz = fxy * fxy / meas;
+  for (int f = 0; f < 6; ++f) {
+    aa.dir_on[f] = dir_on_[f];
+    aa.dir_val[f] = dir_val_[f];
+  }
+  launch_assemble(aa, tx, ty, tz, diag, db, bval, st);
+}
+
+int Solver::assemble() {
+  if (!kx) {
+    err = "kappa not set";
+    return 73;
+  }
+  if (!tx) alloc_fine();
+  assemble_launch();
+  return check(cudaStreamSynchronize(st), "assemble");
+}
+
 int Solver::setup() {
   if (!kx) {
     err = "kappa not set (PC_init contract: the caller constructs kappa before setup)";
@@ -417,23 +448,10 @@ int Solver::setup() {
   cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
   cudaEventRecord(e[0], st);
   // operator (PC_create_A) and level 1
-  AssembleArgs aa;
-  aa.g = g;
-  aa.kx = kx;
-  aa.ky = ky;
-  aa.kz = kz;
-  const double meas = H[0] * H[1] * H[2];
-  const double fyz = H[1] * H[2], fzx = H[2] * H[0], fxy = H[0] * H[1];
-  aa.cx = fyz * fyz / meas;
-  aa.cy = fzx * fzx / meas;
-  aa.cz = fxy * fxy / meas;
+  assemble_launch();
   int dmask = 0;
-  for (int f = 0; f < 6; ++f) {
-    aa.dir_on[f] = dir_on_[f];
-    aa.dir_val[f] = dir_val_[f];
+  for (int f = 0; f < 6; ++f)
     if (dir_on_[f]) dmask |= 1 << f;
-  }
-  launch_assemble(aa, tx, ty, tz, diag, db, bval, st);
   if (!d_flag) cudaMalloc(&d_flag, 4 * sizeof(int));
   cudaMemsetAsync(d_flag, 0, 4 * sizeof(int), st);
   launch_ic_factor(g, d_subs, nsub, max_lines, tx, ty, tz, diag, inv64, d_flag, st);
@@ -479,7 +497,7 @@ int Solver::setup() {
   la.Hx = H[0];
   la.Hy = H[1];
   la.Hz = H[2];
-  la.meas = meas;
+  la.meas = H[0] * H[1] * H[2];
   la.xinit = nullptr;
   la.dirichlet_mask = dmask;
   la.ld = 0;
@@ -707,8 +725,8 @@ void Solver::apply(const double* x, double* out, double* partial, const int* don
 }
 
 int Solver::rhs(const double* source, double* out, bool on_device) {
-  if (!is_setup) {
-    err = "setup not done";
+  if (!tx) {
+    err = "operator not assembled";
     return 73;
   }
   const size_t n = (size_t)g.ncell;
@@ -775,7 +793,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
     xs = vx;
   }
   cudaEventRecord(ev0, st);
-  launch_pcg_start(g, bs, xs, r, part, state, opt.rtol, opt.max_it, st);
+  launch_pcg_start(g, bs, xs, r, part, state, opt.rtol, opt.atol, opt.max_it, st);
   const int* done = &state->done;
   apply(r, z, part, done);
   launch_pcg_beta_fin(part, nparts_apply(), state, st);

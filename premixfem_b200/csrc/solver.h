@@ -23,6 +23,7 @@ struct Options {
   bool use_W_cycle = false, no_shift_A_cc = false, use_full_Cholesky_lv1 = false, use_2level = false;
   int precision = 0;  // 0 plain FP64, 1 FP32 preconditioner inside FP64 PCG
   double rtol = 1e-8;
+  double atol = 1e-50;  // KSP abstol (PETSc default)
   int max_it = 10000;
   int eig_max_it = 300;
   double eig_tol = -1.0;  // < 0: 1e-8 for the FP64 setup, 1e-6 for the FP32 setup
@@ -66,6 +67,7 @@ class Solver {
 
   int set_kappa(const double* kx, const double* ky, const double* kz, bool on_device);
   int set_dirichlet(int face, double value);
+  int assemble();  // operator only (PC_create_A); setup() assembles as well
   int setup();
   int rhs(const double* source, double* out, bool on_device);
   int apply_A(const double* x, double* y, bool on_device);
@@ -110,6 +112,7 @@ class Solver {
   int check(cudaError_t e, const char* what);
   int build_partition();
   void alloc_fine();
+  void assemble_launch();
   template <typename T>
   void apply_impl(const double* x, double* out, double* partial, const int* done);
   void apply(const double* x, double* out, double* partial, const int* done);

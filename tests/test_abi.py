@@ -28,3 +28,20 @@ def test_no_device_calls_fail_cleanly_without_gpu():
     lib = _native.load()
     # pmf_device_count never faults; on a CPU-only host it reports 0
     assert lib.pmf_device_count() >= 0
+
+
+def test_library_exports_reference_interface_and_petsc_subset():
+    """PreMixFEM_3D.h (the reference's entry points) and pmf_petsc_compat.h."""
+    lib = _native.load()
+    ref = declared_functions("PreMixFEM_3D.h")
+    assert set(ref) >= {"PC_init", "PC_setup", "PC_create_A", "PC_apply_vec", "PC_get_range",
+                        "PC_print_info", "PC_print_stat", "PC_final", "PC_final_default", "_PC_setup"}
+    compat = declared_functions("pmf_petsc_compat.h")
+    assert {"KSPSolve", "DMDAVecGetArray", "MatMult", "PCShellSetApply"} <= set(compat)
+    for n in ref + compat:
+        assert hasattr(lib, n), f"missing export {n}"
+
+
+def test_every_header_is_covered():
+    headers = sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
+    assert headers == ["PreMixFEM_3D.h", "pmf_b200.h", "pmf_petsc_compat.h"]
