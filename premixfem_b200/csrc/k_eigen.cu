@@ -1019,6 +1019,31 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     __syncthreads();
     const int num = sm.ival[1];
     if (threadIdx.x < k) evals[(long long)s * k + threadIdx.x] = sm.lam[threadIdx.x];
+    // FP32 storage: on a subdomain that touches no Dirichlet face, the lowest
+    // eigenvector of A_i^N v = lambda M_i v is exactly the constant (A_i^N 1 = 0),
+    // but FP32 iterations only reach it to ~1e-6.  Write the exact M-normalised
+    // constant instead, so that the coarse spaces contain the global null vector
+    // of a pure-Neumann operator exactly and its coarse pivot stays negligible.
+    bool snap = false;
+    double cval = 0.0;
+    if (sizeof(T) == 4 && num >= 1) {
+      const int dm = a.dirichlet_mask;
+      const bool touches = ((dm & 1) && S.x0 == 0) || ((dm & 2) && S.x0 + nx == g.M) || ((dm & 4) && S.y0 == 0) ||
+                           ((dm & 8) && S.y0 + ny == g.N) || ((dm & 16) && S.z0 == 0) || ((dm & 32) && S.z0 + nz == g.P);
+      if (!touches) {
+        double msum = 0.0, vsum = 0.0;
+        for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+          double v0 = 0.0;
+          for (int b = 0; b < m; ++b) v0 += (double)X[(size_t)b * ld + cl] * mt.Y[b * LB_LD];
+          msum += Md[cl];
+          vsum += Md[cl] * v0;
+        }
+        msum = block_sum(msum, sm.res);
+        vsum = block_sum(vsum, sm.res);
+        snap = msum > 0.0;
+        cval = snap ? copysign(1.0 / sqrt(msum), vsum) : 0.0;
+      }
+    }
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
       const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
       const long long cg = ((long long)(S.z0 + kz_) * g.N + (S.y0 + jy)) * g.M + (S.x0 + i);
@@ -1032,6 +1057,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
           for (int b = 0; b < LB_MM; ++b)
             if (b < m) v += xr[b] * mt.Y[b * LB_LD + j];
         }
+        if (snap && j == 0) v = cval;
         phi[cg * a.kmax + j] = (T)v;
       }
     }
