@@ -69,6 +69,33 @@ int pmf_get_stages(pmf_solver* s, double t[10]);
 /* last setup and solve time measured with CUDA events on the solver stream (ms) */
 int pmf_get_timing(pmf_solver* s, double* setup_ms, double* solve_ms);
 
+/*
+ * pmf_residual_noalloc -- has no counterpart in the reference (its residual is
+ * a MatMult into a Vec it allocates, then VecAXPY and VecNorm).
+ *
+ * r = b - A x and rnorm[0] = ||r||_2 for DEVICE vectors b, x, r and a DEVICE
+ * scalar rnorm, enqueued on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream); the call returns without waiting.  It allocates nothing,
+ * host or device, on its success path: the reduction scratch is a static
+ * device array inside the library.  For callers that cannot allocate at that
+ * point: a device pool that owns all free memory, a per-iteration monitor
+ * where cudaMalloc would synchronise the device, or a fixed launch sequence
+ * that must not change between recordings.
+ *   - meshes of more than PMF_NOALLOC_MAX_CELLS cells are rejected (error 62);
+ *   - the operator must be assembled (pmf_setup done; else error 73), and the
+ *     current device must be the solver's (else error 62);
+ *   - the first call on each device resolves and zeroes the scratch (with
+ *     cudaGetSymbolAddress and cudaMemset, synchronising the device): make that
+ *     first call before any stream capture begins;
+ *   - the scratch's ticket counter must be zero when a call starts; set-up
+ *     zeroes it and every completed call leaves it at zero;
+ *   - all calls on one device share the scratch: overlapping calls (two
+ *     streams, two threads) race and return wrong results; serialise them.
+ */
+#define PMF_NOALLOC_MAX_BLOCKS 16384
+#define PMF_NOALLOC_MAX_CELLS 33554432LL /* PMF_NOALLOC_MAX_BLOCKS x 2048 cells */
+int pmf_residual_noalloc(pmf_solver* s, const double* b, const double* x, double* r, double* rnorm, void* stream);
+
 /* total number of CUDA kernels launched by this library in this process */
 unsigned long long pmf_launch_count(void);
 

@@ -35,6 +35,7 @@ SIGNATURES = {
     "pmf_get_coarse_blocks": (C.c_int, [_vp, _vp]),
     "pmf_get_stages": (C.c_int, [_vp, _vp]),
     "pmf_get_timing": (C.c_int, [_vp, _dp, _dp]),
+    "pmf_residual_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pmf_launch_count": (C.c_ulonglong, []),
     "pmf_last_error": (C.c_char_p, []),
     "pmf_device_count": (C.c_int, []),

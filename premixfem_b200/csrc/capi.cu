@@ -28,6 +28,10 @@ static int wrap(pmf_solver* h, int code) {
     if (!(h) || !(h)->s) return fail(62, "null solver handle");    \
   } while (0)
 
+// accessors for entry points defined in other translation units (noalloc.cu)
+pmf::Solver* pmf_internal_solver(pmf_solver* h) { return h ? h->s : nullptr; }
+int pmf_internal_fail(int code, const char* msg) { return fail(code, msg); }
+
 extern "C" {
 
 int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out) {
