@@ -67,6 +67,10 @@ WORKLOADS = {
 # Algorithmic bytes per cell of the FP64 operator kernel k_spmv (y = A x):
 # reads x, tx, ty, tz, diag (5 x 8 B), writes y (8 B).
 SPMV_BYTES_PER_CELL = 6 * 8
+# DRAM bytes per (subdomain x LOBPCG iteration) of k_lobpcg<float>, 16^3 subdomains, m = 8: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum = 32.3 GB for 512 subdomains x 29.4 iterations
+# (profiles/k_lobpcg_fracture128_mixed.md).
+LOBPCG_TRAFFIC_PER_SUB_ITER = 32.3e9 / (512 * 29.36)
 
 
 def _peaks():
@@ -212,6 +216,7 @@ def run_b200(args):
         res = float(torch.linalg.norm(b - torch.from_numpy(s.apply_A(x.cpu().numpy())).cuda())) / bn
         results[prec] = dict(steps=steps, launches=launches, clocks=clk.summary(), stages=stages,
                              eig_iters_mean=float(it1.mean()), eig_iters_max=int(it1.max()),
+                             eig_iters_sum=int(it1.sum()), cells_per_sub=n / len(it1),
                              eig_unconverged=int((st1 != 0).sum()), rel_residual=res, x=x.cpu().numpy())
         if prec == "mixed":
             # e2e through the C ABI with host buffers (copies inside the timed region)
@@ -250,6 +255,11 @@ def run_b200(args):
     st = results["mixed"]["stages"]
     eig_s = st["su_lv2_1"] / (args.steps + args.warmup)
     spmv_ms = results["spmv_ms"]
+    # LOBPCG algorithmic FLOPs of this launch: sum over subdomains of iterations x n_s x (60 m^2 + 31 m)
+    m_blk = wl["opts"]["en_lv1"] + 2
+    lob_sub_iters = results["mixed"]["eig_iters_sum"]
+    lob_flops = float(lob_sub_iters) * results["mixed"]["cells_per_sub"] * (60 * m_blk ** 2 + 31 * m_blk)
+    biter = n * (104 + 4 * (25 + 6 * wl["opts"]["en_lv1"]))
     spmv_gbs = SPMV_BYTES_PER_CELL * n / (spmv_ms * 1e-3) / 1e9
     line = {
         "metric": METRIC,
@@ -286,13 +296,27 @@ def run_b200(args):
         "roofline": {
             "kernel": "k_lobpcg<float> (batched local eigensolver, dominant share of the step)",
             "bound": "tensor",
-            "achieved": None,
+            "achieved": round(lob_flops / eig_s / 1e12, 3),
             "peak": bf16,
             "unit": "TFLOP/s",
-            "frac": None,
-            "traffic": None,
+            "frac": round(lob_flops / eig_s / 1e12 / bf16, 6),
+            "traffic": round(LOBPCG_TRAFFIC_PER_SUB_ITER * lob_sub_iters, 0),
             "time_s_per_step": round(eig_s, 6),
-            "note": "FP64-accumulated Gram/Rayleigh-Ritz on CUDA cores; latency-bound, see profiles/",
+            "flops_per_launch": lob_flops,
+            "note": "algorithmic FLOPs n*(60 m^2 + 31 m) per subdomain-iteration (Grams, basis and A-image "
+                    "updates, stencil, IC(0) sweeps), FP64 arithmetic on the FP64 tensor pipe (DMMA) and CUDA "
+                    "cores; the denominator is the measured bf16 peak, the only tensor peak measured.  traffic: "
+                    "ncu dram bytes per subdomain-iteration on the 128^3 case, scaled by this launch's "
+                    "subdomain-iterations.  Latency-bound; see profiles/k_lobpcg_fracture128_mixed.md",
+        },
+        "roofline_solve_model": {
+            "phase": "PCG solve (all kernels), algorithmic bytes B_iter = N*[104 + w*(25+6k)], w=4, k=6",
+            "bound": "hbm",
+            "achieved": round(biter * its_m / so_m / 1e9, 1),
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": round(biter * its_m / so_m / 1e9 / hbm, 4),
+            "bytes_per_iteration": biter,
         },
         "roofline_solve": {
             "kernel": "k_spmv (7-point FP64 operator, y = A x)",
