@@ -37,7 +37,12 @@ typedef struct pmf_solver pmf_solver;
  * -eb_lv1, -eb_lv2, -si_lv1, -si_lv2, -eg_op, -use_W_cycle, -no_shift_A_cc,
  * -ksp_rtol, -ksp_max_it; B200 extensions: -pmf_sd sx,sy,sz (subdomains per
  * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
- * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it. */
+ * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it, -pmf_learned
+ * <weights file> (learned initial blocks for the local eigensolves),
+ * -pmf_learned_its N and -pmf_learned_tol t (a subdomain whose LOBPCG from the
+ * learned start has not reached relative residual t within N iterations is
+ * solved again from a random start at the normal tolerance; defaults 30 and
+ * 1e-4). */
 int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out);
 int pmf_destroy(pmf_solver* s);
 
@@ -68,6 +73,40 @@ int pmf_get_coarse_blocks(pmf_solver* s, double* out);
 int pmf_get_stages(pmf_solver* s, double t[10]);
 /* last setup and solve time measured with CUDA events on the solver stream (ms) */
 int pmf_get_timing(pmf_solver* s, double* setup_ms, double* solve_ms);
+
+/*
+ * Learned set-up (no counterpart in the reference, whose local eigensolves
+ * always start from SLEPc's default vectors).  A 3-D convolutional
+ * encoder-decoder maps each subdomain's log-permeability patch (16^3, zero
+ * padded) to k initial vectors for LOBPCG.  All array arguments are device
+ * memory, work runs on the legacy default stream; feats are BF16
+ * [nsub][4096][16], V are FP32 [nsub][4096][k], M FP32 [nsub][4096], network
+ * outputs y and gradients dy FP32 [B][4096][16].
+ */
+typedef struct pmf_net pmf_net;
+int pmf_net_create(unsigned long long seed, pmf_net** out);   /* random (He) weights */
+int pmf_net_load(const char* path, pmf_net** out);
+int pmf_net_save(pmf_net* net, const char* path);
+int pmf_net_destroy(pmf_net* net);
+int pmf_net_params(pmf_net* net);                              /* parameter count */
+/* info: type (0 conv3, 1 down2, 2 up2, 3 conv1), cin, cout, s_in, s_out, taps */
+int pmf_net_layer_info(int layer, int info[6]);
+int pmf_net_forward(pmf_net* net, const void* x, int B, float* y);
+int pmf_net_backward(pmf_net* net, const float* dy, int B);   /* after pmf_net_forward of the same batch */
+int pmf_net_adam(pmf_net* net, float lr, float beta1, float beta2, float eps, float weight_decay);
+/* FP32 weights W[tap][cin][cout] and biases of one layer (host memory) */
+int pmf_net_get_weights(pmf_net* net, int layer, float* w, float* b);
+int pmf_net_set_weights(pmf_net* net, int layer, const float* w, const float* b);
+int pmf_net_get_grads(pmf_net* net, int layer, float* gw, float* gb);
+/* subspace loss per sample: loss[b] = ||V - Y C||_M^2 / k with C = (Y^T M Y)^-1 Y^T M V, and dL/dy
+ * of the batch mean */
+int pmf_net_loss(const float* y, const float* V, const float* M, int B, int k, float* loss, float* dy);
+/* after pmf_setup: network inputs of every subdomain and, as training targets, its local
+ * eigenvectors and mass diagonal (any of the three pointers may be NULL) */
+int pmf_learned_patches(pmf_solver* s, void* feats, float* V, float* M);
+/* stats: learned start used, subdomains that fell back, LOBPCG iterations from the learned start,
+ * iterations of the fallbacks; net_ms: network inference time of the last set-up */
+int pmf_get_learned_stats(pmf_solver* s, long long stats[4], double* net_ms);
 
 /*
  * pmf_residual_noalloc -- has no counterpart in the reference (its residual is

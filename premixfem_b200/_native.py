@@ -35,6 +35,21 @@ SIGNATURES = {
     "pmf_get_coarse_blocks": (C.c_int, [_vp, _vp]),
     "pmf_get_stages": (C.c_int, [_vp, _vp]),
     "pmf_get_timing": (C.c_int, [_vp, _dp, _dp]),
+    "pmf_net_create": (C.c_int, [C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "pmf_net_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "pmf_net_save": (C.c_int, [_vp, C.c_char_p]),
+    "pmf_net_destroy": (C.c_int, [_vp]),
+    "pmf_net_params": (C.c_int, [_vp]),
+    "pmf_net_layer_info": (C.c_int, [C.c_int, _vp]),
+    "pmf_net_forward": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "pmf_net_backward": (C.c_int, [_vp, _vp, C.c_int]),
+    "pmf_net_adam": (C.c_int, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "pmf_net_get_weights": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "pmf_net_set_weights": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "pmf_net_get_grads": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "pmf_net_loss": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp]),
+    "pmf_learned_patches": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "pmf_get_learned_stats": (C.c_int, [_vp, _vp, _dp]),
     "pmf_residual_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pmf_launch_count": (C.c_ulonglong, []),
     "pmf_last_error": (C.c_char_p, []),

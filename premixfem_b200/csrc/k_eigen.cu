@@ -650,7 +650,17 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
   PhaseClock pc{a.prof ? a.prof + (size_t)blockIdx.x * 16 : nullptr, 0};
   pc.start();
 
-  for (int s = blockIdx.x; s < a.nsub; s += gridDim.x) {
+  const int count = a.sub_list ? *a.nlist : a.nsub;
+  __shared__ int s_next;
+  for (int idx = blockIdx.x;; idx += gridDim.x) {
+    if (a.queue) {  // dynamic schedule: take the next unclaimed subdomain
+      __syncthreads();
+      if (threadIdx.x == 0) s_next = atomicAdd(a.queue, 1);
+      __syncthreads();
+      idx = s_next;
+    }
+    if (idx >= count) break;
+    const int s = a.sub_list ? a.sub_list[idx] : idx;
     const SubInfo S = a.subs[s];
     const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
     T* X = reinterpret_cast<T*>(wb);
@@ -752,7 +762,10 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     for (int e = threadIdx.x; e < m * nc; e += blockDim.x) {
       const int j = e / nc, cl = e % nc;
       double v;
-      if (a.xinit) {
+      if (a.xinit_patch && j < a.xinit_k) {
+        const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+        v = a.xinit_patch[((size_t)s * 4096 + (kz_ * 16 + jy) * 16 + i) * 16 + j];
+      } else if (a.xinit) {
         const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
         const long long cg = ((long long)(S.z0 + kz_) * g.N + (S.y0 + jy)) * g.M + (S.x0 + i);
         v = a.xinit[cg * m + j];
@@ -1073,7 +1086,7 @@ void launch_lobpcg(const LobpcgArgs& a_in, int nblocks, void* work, T* phi, doub
   a.ld = lb_ld(max_cells);
   a.ldc = (max_cells + 3) & ~3;
   const size_t fixed = sizeof(LbSmall) + (size_t)16 * a.ldc;
-  const size_t limit = 227 * 1024;
+  const size_t limit = 227 * 1024 - 256;  // leave room for the kernel's static shared memory
   const size_t avail = limit > fixed ? limit - fixed : 0;
   int mb = (int)std::min<size_t>(a.m, avail / ((size_t)4 * a.ldc));
   if (mb < 1) mb = 1;
@@ -1084,6 +1097,7 @@ void launch_lobpcg(const LobpcgArgs& a_in, int nblocks, void* work, T* phi, doub
   (void)max_lines;
   cudaFuncSetAttribute(k_lobpcg<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const size_t stride = (lobpcg_work_bytes(max_cells, a.m, sizeof(T)) + 255) & ~(size_t)255;
+  if (a.queue) cudaMemsetAsync(a.queue, 0, sizeof(int), st);
   { note_launch(); k_lobpcg<T><<<nblocks, threads, smem, st>>>(a, (unsigned char*)work, stride, phi, evals, iters, status, ks, eb); }
 }
 template void launch_lobpcg<float>(const LobpcgArgs&, int, void*, float*, double*, int*, int*, int*, double, int, int,

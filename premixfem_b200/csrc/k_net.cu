@@ -1,0 +1,834 @@
+// Kernels of the learned-initialisation network (layer table in pmf_net.h).
+//
+// Forward: every layer is one implicit GEMM, out[row][cout] = sum over
+// (tap, cin) of in[gather(row, tap)][cin] * W[tap][cin][cout], computed on
+// the BF16 tensor cores (mma.sync m16n8k16, FP32 accumulation) with the bias,
+// skip addition, ReLU and the BF16 rounding fused in the epilogue.  A CTA owns
+// 64 output voxels of one sample and all output channels; per tap it stages
+// the 64 gathered input rows and the tap's weight slice in shared memory.
+// Transposed (up2) layers order their rows by (sample, parity, coarse voxel)
+// so that one tile uses one weight slice.
+//
+// Backward (training only, FP32 CUDA cores): the input gradient is a gather
+// over the taps that touched each input voxel, fused with the skip-gradient
+// addition and the ReLU mask of the input activation; the weight gradient is
+// a tiled reduction over output rows with FP32 atomics per chunk.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "pmf_kernels.h"
+#include "pmf_net.h"
+
+namespace pmf {
+
+const NetLayer kNetLayers[NET_LAYERS] = {
+    // type     cin cout s_in s_out relu skip in out
+    {NL_CONV3, 16, 32, 16, 16, 1, -1, 0, 1},
+    {NL_DOWN2, 32, 64, 16, 8, 1, -1, 1, 2},
+    {NL_CONV3, 64, 64, 8, 8, 1, -1, 2, 3},
+    {NL_DOWN2, 64, 96, 8, 4, 1, -1, 3, 4},
+    {NL_CONV3, 96, 96, 4, 4, 1, -1, 4, 5},
+    {NL_UP2, 96, 64, 4, 8, 1, 3, 5, 6},
+    {NL_UP2, 64, 32, 8, 16, 1, 1, 6, 7},
+    {NL_CONV3, 32, 32, 16, 16, 1, -1, 7, 8},
+    {NL_CONV1, 32, 16, 16, 16, 0, -1, 8, 9},
+};
+const NetActShape kNetActs[NET_ACTS] = {{16, 16}, {16, 32}, {8, 64}, {8, 64}, {4, 96},
+                                        {4, 96},  {8, 64},  {16, 32}, {16, 32}, {16, 16}};
+
+namespace {
+
+__device__ __forceinline__ int cube(int s) { return s * s * s; }
+
+// Input voxel read by output voxel o through tap t (-1: zero padding / not this tap).
+__device__ __forceinline__ int in_vox(int type, int s_in, int s_out, int o, int t) {
+  int x = o % s_out, y = (o / s_out) % s_out, z = o / (s_out * s_out);
+  if (type == NL_CONV3) {
+    x += t % 3 - 1;
+    y += (t / 3) % 3 - 1;
+    z += t / 9 - 1;
+    if (x < 0 || y < 0 || z < 0 || x >= s_in || y >= s_in || z >= s_in) return -1;
+    return (z * s_in + y) * s_in + x;
+  }
+  if (type == NL_DOWN2) return ((2 * z + (t >> 2)) * s_in + 2 * y + ((t >> 1) & 1)) * s_in + 2 * x + (t & 1);
+  if (type == NL_CONV1) return o;
+  const int par = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+  if (par != t) return -1;
+  return ((z >> 1) * s_in + (y >> 1)) * s_in + (x >> 1);
+}
+
+// Fine voxel of coarse voxel v (edge s_in) and parity d.
+__device__ __forceinline__ int up_vox(int v, int d, int s_in) {
+  const int x = v % s_in, y = (v / s_in) % s_in, z = v / (s_in * s_in), s = 2 * s_in;
+  return ((2 * z + (d >> 2)) * s + 2 * y + ((d >> 1) & 1)) * s + 2 * x + (d & 1);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct FwdArgs {
+  int type, cin, cout, s_in, s_out, relu;
+  const __nv_bfloat16* in;
+  const __nv_bfloat16* W;
+  const float* bias;
+  const __nv_bfloat16* skip;
+  __nv_bfloat16* out;
+  float* outf;
+};
+
+constexpr int kTileRows = 64;
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_net_fwd(FwdArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ int rowout[kTileRows];
+  const int lda = a.cin + 8, ldb = a.cout + 8;
+  __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smraw);
+  __nv_bfloat16* Bs = As + kTileRows * lda;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int so3 = cube(a.s_out), si3 = cube(a.s_in);
+  const long long r0 = (long long)blockIdx.x * kTileRows;
+  const int b = (int)(r0 / so3);
+  const int rem0 = (int)(r0 % so3);
+  const bool up = a.type == NL_UP2;
+  const int d_tile = up ? rem0 / si3 : 0;
+  if (tid < kTileRows) rowout[tid] = up ? up_vox((rem0 + tid) % si3, d_tile, a.s_in) : rem0 + tid;
+  const int ntap = (up || a.type == NL_CONV1) ? 1 : net_taps(a.type);
+  float acc[NT][4];
+#pragma unroll
+  for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+  const int vin = a.cin >> 3, vout = a.cout >> 3;
+  for (int ti = 0; ti < ntap; ++ti) {
+    const int t = up ? d_tile : ti;
+    __syncthreads();
+    for (int e = tid; e < kTileRows * vin; e += blockDim.x) {
+      const int rr = e / vin, cv = e % vin;
+      const int iv = up ? (rem0 + rr) % si3 : in_vox(a.type, a.s_in, a.s_out, rowout[rr], t);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (iv >= 0) v = *reinterpret_cast<const uint4*>(a.in + ((size_t)b * si3 + iv) * a.cin + cv * 8);
+      *reinterpret_cast<uint4*>(As + rr * lda + cv * 8) = v;
+    }
+    for (int e = tid; e < a.cin * vout; e += blockDim.x) {
+      const int k = e / vout, cv = e % vout;
+      *reinterpret_cast<uint4*>(Bs + k * ldb + cv * 8) =
+          *reinterpret_cast<const uint4*>(a.W + ((size_t)t * a.cin + k) * a.cout + cv * 8);
+    }
+    __syncthreads();
+    for (int kc = 0; kc < a.cin; kc += 16) {
+      uint32_t a0, a1, a2, a3;
+      ldsm_x4(smem_u32(As + (warp * 16 + (lane & 15)) * lda + kc + (lane >> 4) * 8), a0, a1, a2, a3);
+#pragma unroll
+      for (int np = 0; np < NT / 2; ++np) {
+        uint32_t b0, b1, b2, b3;
+        ldsm_x4_t(smem_u32(Bs + (kc + (lane & 7) + ((lane >> 3) & 1) * 8) * ldb + np * 16 + (lane >> 4) * 8), b0, b1,
+                  b2, b3);
+        mma_bf16(acc[2 * np], a0, a1, a2, a3, b0, b1);
+        mma_bf16(acc[2 * np + 1], a0, a1, a2, a3, b2, b3);
+      }
+    }
+  }
+  // epilogue: bias, skip, ReLU, store
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int rr = warp * 16 + (lane >> 2) + h * 8;
+    const size_t rowbase = ((size_t)b * so3 + rowout[rr]) * a.cout;
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+      const int col = n * 8 + (lane & 3) * 2;
+      float v0 = acc[n][2 * h] + a.bias[col];
+      float v1 = acc[n][2 * h + 1] + a.bias[col + 1];
+      if (a.skip) {
+        const __nv_bfloat162 s2 = *reinterpret_cast<const __nv_bfloat162*>(a.skip + rowbase + col);
+        v0 += __bfloat162float(s2.x);
+        v1 += __bfloat162float(s2.y);
+      }
+      if (a.relu) {
+        v0 = fmaxf(v0, 0.f);
+        v1 = fmaxf(v1, 0.f);
+      }
+      if (a.outf) {
+        *reinterpret_cast<float2*>(a.outf + rowbase + col) = make_float2(v0, v1);
+      } else {
+        *reinterpret_cast<__nv_bfloat162*>(a.out + rowbase + col) = __floats2bfloat162_rn(v0, v1);
+      }
+    }
+  }
+}
+
+// ---- backward -------------------------------------------------------------------------------
+struct DgradArgs {
+  int type, cin, cout, s_in, s_out, B;
+  const float* dz;                // pre-activation gradient of this layer's output [B][s_out^3][cout]
+  const float* wt;                // W[tap][cout][cin] (FP32)
+  const __nv_bfloat16* in_act;    // this layer's input activation (ReLU mask), may be null
+  const float* add;               // gradient reaching the input through a skip, may be null
+  float* din;                     // pre-activation gradient of the previous layer's output
+};
+
+__global__ void k_net_dgrad(DgradArgs a) {
+  const int si3 = cube(a.s_in), so3 = cube(a.s_out);
+  const long long total = (long long)a.B * si3 * a.cin;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ci = (int)(idx % a.cin);
+    const int i = (int)((idx / a.cin) % si3);
+    const int b = (int)(idx / ((long long)a.cin * si3));
+    if (a.in_act && !(__bfloat162float(a.in_act[idx]) > 0.f)) {
+      a.din[idx] = 0.f;
+      continue;
+    }
+    const int x = i % a.s_in, y = (i / a.s_in) % a.s_in, z = i / (a.s_in * a.s_in);
+    float s = 0.f;
+    auto tap = [&](int o, int t) {
+      const float* dzr = a.dz + ((size_t)b * so3 + o) * a.cout;
+      const float* w = a.wt + (size_t)t * a.cout * a.cin + ci;
+      for (int co = 0; co < a.cout; ++co) s += dzr[co] * w[(size_t)co * a.cin];
+    };
+    if (a.type == NL_CONV3) {
+      for (int t = 0; t < 27; ++t) {
+        const int ox = x - (t % 3 - 1), oy = y - ((t / 3) % 3 - 1), oz = z - (t / 9 - 1);
+        if (ox < 0 || oy < 0 || oz < 0 || ox >= a.s_out || oy >= a.s_out || oz >= a.s_out) continue;
+        tap((oz * a.s_out + oy) * a.s_out + ox, t);
+      }
+    } else if (a.type == NL_DOWN2) {
+      tap(((z >> 1) * a.s_out + (y >> 1)) * a.s_out + (x >> 1), (x & 1) | ((y & 1) << 1) | ((z & 1) << 2));
+    } else if (a.type == NL_CONV1) {
+      tap(i, 0);
+    } else {
+      for (int d = 0; d < 8; ++d) tap(up_vox(i, d, a.s_in), d);
+    }
+    if (a.add) s += a.add[idx];
+    a.din[idx] = s;
+  }
+}
+
+struct WgradArgs {
+  int type, cin, cout, s_in, s_out, B, rows_per_chunk;
+  const __nv_bfloat16* in;  // layer input activation
+  const float* dz;          // pre-activation gradient of the output
+  float* gw;                // [tap][cin][cout], accumulated
+};
+
+// dW[t][ci][co] = sum over output rows of in[gather(row, t)][ci] * dz[row][co].
+// blockIdx.y = tap, blockIdx.x = chunk of rows; 16 x 16 threads, each TA x TB outputs.
+template <int TA, int TB>
+__global__ void __launch_bounds__(256) k_net_wgrad(WgradArgs a) {
+  constexpr int CIN = 16 * TA, COUT = 16 * TB, RT = 32;
+  __shared__ float xs[RT][CIN + 1];
+  __shared__ float zs[RT][COUT + 1];
+  const int t = blockIdx.y;
+  const bool up = a.type == NL_UP2;
+  const int so3 = cube(a.s_out), si3 = cube(a.s_in);
+  const long long nrows = (long long)a.B * (up ? si3 : so3);
+  const long long rbeg = (long long)blockIdx.x * a.rows_per_chunk;
+  const long long rend = min(nrows, rbeg + a.rows_per_chunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float acc[TA][TB];
+#pragma unroll
+  for (int i = 0; i < TA; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) acc[i][j] = 0.f;
+  for (long long r0 = rbeg; r0 < rend; r0 += RT) {
+    for (int e = threadIdx.x; e < RT * CIN; e += 256) {
+      const int rr = e / CIN, c = e % CIN;
+      const long long row = r0 + rr;
+      float v = 0.f;
+      if (row < rend) {
+        int b, iv;
+        if (up) {
+          b = (int)(row / si3);
+          iv = (int)(row % si3);
+        } else {
+          b = (int)(row / so3);
+          iv = in_vox(a.type, a.s_in, a.s_out, (int)(row % so3), t);
+        }
+        if (iv >= 0) v = __bfloat162float(a.in[((size_t)b * si3 + iv) * CIN + c]);
+      }
+      xs[rr][c] = v;
+    }
+    for (int e = threadIdx.x; e < RT * COUT; e += 256) {
+      const int rr = e / COUT, c = e % COUT;
+      const long long row = r0 + rr;
+      float v = 0.f;
+      if (row < rend) {
+        int b, o;
+        if (up) {
+          b = (int)(row / si3);
+          o = up_vox((int)(row % si3), t, a.s_in);
+        } else {
+          b = (int)(row / so3);
+          o = (int)(row % so3);
+        }
+        v = a.dz[((size_t)b * so3 + o) * COUT + c];
+      }
+      zs[rr][c] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int rr = 0; rr < RT; ++rr) {
+      float xv[TA], zv[TB];
+#pragma unroll
+      for (int i = 0; i < TA; ++i) xv[i] = xs[rr][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < TB; ++j) zv[j] = zs[rr][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < TA; ++i)
+#pragma unroll
+        for (int j = 0; j < TB; ++j) acc[i][j] += xv[i] * zv[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < TA; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) atomicAdd(&a.gw[((size_t)t * CIN + ty + 16 * i) * COUT + tx + 16 * j], acc[i][j]);
+}
+
+__global__ void k_net_bgrad(const float* dz, long long rows, int cout, float* gb) {
+  __shared__ double red[32];
+  const int co = blockIdx.x;
+  double s = 0.0;
+  for (long long r = threadIdx.x; r < rows; r += blockDim.x) s += dz[r * cout + co];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) gb[co] = (float)s;
+}
+
+__global__ void k_net_adam(long long n, float* w, const float* g, float* m, float* v, float lr, float b1, float b2,
+                           float eps, float wd, float bc1, float bc2) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  }
+}
+
+// BF16 copy W16[t][ci][co] and FP32 transpose Wt[t][co][ci] of the master weights.
+__global__ void k_net_refresh(int taps, int cin, int cout, const float* w, __nv_bfloat16* w16, float* wt) {
+  const long long n = (long long)taps * cin * cout;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int co = (int)(i % cout), ci = (int)((i / cout) % cin), t = (int)(i / ((long long)cin * cout));
+    w16[i] = __float2bfloat16_rn(w[i]);
+    wt[((size_t)t * cout + co) * cin + ci] = w[i];
+  }
+}
+
+// ---- subspace loss ----------------------------------------------------------------------------
+constexpr int kLossK = 8;
+
+__global__ void __launch_bounds__(256) k_net_loss(const float* y, const float* V, const float* Mw, int k, int B,
+                                                  float* loss, float* dy) {
+  __shared__ double red[32];
+  __shared__ double G[kLossK * kLossK], H[kLossK * kLossK], C[kLossK * kLossK];
+  const int b = blockIdx.x;
+  const float* yb = y + (size_t)b * NET_VOX * NET_COUT;
+  const float* vb = V + (size_t)b * NET_VOX * k;
+  const float* mb = Mw + (size_t)b * NET_VOX;
+  // G and H, one entry per pass over the patch (k <= 8: at most 128 passes)
+  for (int e = 0; e < 2 * k * k; ++e) {
+    const int i = (e % (k * k)) / k, j = e % k;
+    const bool g = e < k * k;
+    double s = 0.0;
+    for (int v = threadIdx.x; v < NET_VOX; v += blockDim.x) {
+      const float m = mb[v];
+      if (m == 0.f) continue;
+      s += (double)m * yb[(size_t)v * NET_COUT + i] * (g ? yb[(size_t)v * NET_COUT + j] : vb[(size_t)v * k + j]);
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) (g ? G : H)[i * kLossK + j] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // C = (G + eps I)^-1 H by Cholesky
+    double tr = 0.0;
+    for (int i = 0; i < k; ++i) tr += G[i * kLossK + i];
+    const double eps = 1e-6 * tr / k + 1e-30;
+    double L[kLossK * kLossK];
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = G[i * kLossK + j] + (i == j ? eps : 0.0);
+        for (int q = 0; q < j; ++q) s -= L[i * kLossK + q] * L[j * kLossK + q];
+        L[i * kLossK + j] = (i == j) ? sqrt(fmax(s, 1e-300)) : s / L[j * kLossK + j];
+      }
+    for (int c = 0; c < k; ++c) {
+      double z[kLossK];
+      for (int i = 0; i < k; ++i) {
+        double s = H[i * kLossK + c];
+        for (int q = 0; q < i; ++q) s -= L[i * kLossK + q] * z[q];
+        z[i] = s / L[i * kLossK + i];
+      }
+      for (int i = k - 1; i >= 0; --i) {
+        double s = z[i];
+        for (int q = i + 1; q < k; ++q) s -= L[q * kLossK + i] * C[q * kLossK + c];
+        C[i * kLossK + c] = s / L[i * kLossK + i];
+      }
+    }
+  }
+  __syncthreads();
+  const float scale = -2.f / (float)(B * k);
+  double lacc = 0.0;
+  for (int v = threadIdx.x; v < NET_VOX; v += blockDim.x) {
+    const float m = mb[v];
+    float r[kLossK];
+    for (int j = 0; j < k; ++j) {
+      double p = 0.0;
+      for (int i = 0; i < k; ++i) p += (double)yb[(size_t)v * NET_COUT + i] * C[i * kLossK + j];
+      r[j] = vb[(size_t)v * k + j] - (float)p;
+      lacc += (double)m * r[j] * r[j];
+    }
+    float* d = dy + ((size_t)b * NET_VOX + v) * NET_COUT;
+    for (int i = 0; i < NET_COUT; ++i) {
+      float s = 0.f;
+      if (i < k)
+        for (int j = 0; j < k; ++j) s += r[j] * (float)C[i * kLossK + j];
+      d[i] = scale * m * s;
+    }
+  }
+  lacc = block_sum(lacc, red);
+  if (threadIdx.x == 0) loss[b] = (float)(lacc / k);
+}
+
+// ---- patches -------------------------------------------------------------------------------------
+__global__ void k_net_features(Grid g, const SubInfo* subs, const double* kx, const double* ky, const double* kz,
+                               int dmask, __nv_bfloat16* feats) {
+  __shared__ double red[32];
+  const SubInfo S = subs[blockIdx.x];
+  const int nc = S.nx * S.ny * S.nz;
+  double s = 0.0;
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+    const int i = cl % S.nx, j = (cl / S.nx) % S.ny, q = cl / (S.nx * S.ny);
+    const long long cg = ((long long)(S.z0 + q) * g.N + (S.y0 + j)) * g.M + (S.x0 + i);
+    s += log(kx[cg]) + log(ky[cg]) + log(kz[cg]);
+  }
+  const double mean = block_sum(s, red) / (3.0 * nc);
+  for (int v = threadIdx.x; v < NET_VOX; v += blockDim.x) {
+    const int x = v % NET_S, y = (v / NET_S) % NET_S, z = v / (NET_S * NET_S);
+    float f[NET_CIN];
+#pragma unroll
+    for (int c = 0; c < NET_CIN; ++c) f[c] = 0.f;
+    if (x < S.nx && y < S.ny && z < S.nz) {
+      const int ex = S.x0 + x, ey = S.y0 + y, ez = S.z0 + z;
+      const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+      f[0] = (float)((log(kx[cg]) - mean) * 0.25);
+      f[1] = (float)((log(ky[cg]) - mean) * 0.25);
+      f[2] = (float)((log(kz[cg]) - mean) * 0.25);
+      const bool dir = ((dmask & 1) && ex == 0) || ((dmask & 2) && ex == g.M - 1) || ((dmask & 4) && ey == 0) ||
+                       ((dmask & 8) && ey == g.N - 1) || ((dmask & 16) && ez == 0) || ((dmask & 32) && ez == g.P - 1);
+      f[3] = dir ? 1.f : 0.f;
+      f[4] = 1.f;
+    }
+    __nv_bfloat16* o = feats + ((size_t)blockIdx.x * NET_VOX + v) * NET_CIN;
+#pragma unroll
+    for (int c = 0; c < NET_CIN; c += 2)
+      *reinterpret_cast<__nv_bfloat162*>(o + c) = __floats2bfloat162_rn(f[c], f[c + 1]);
+  }
+}
+
+__device__ __forceinline__ double harm(double a, double b) { return 2.0 / (1.0 / a + 1.0 / b); }
+
+// Mass diagonal of the local eigenproblem (src/PreMixFEM_3D.c:243-346), the same
+// expression, term for term, as the batched eigensolver's.
+__global__ void k_net_targets(NetTargetArgs a) {
+  const SubInfo S = a.subs[blockIdx.x];
+  const Grid g = a.g;
+  for (int v = threadIdx.x; v < NET_VOX; v += blockDim.x) {
+    const int i = v % NET_S, j = (v / NET_S) % NET_S, kk = v / (NET_S * NET_S);
+    float* Vo = a.V + ((size_t)blockIdx.x * NET_VOX + v) * a.k;
+    if (!(i < S.nx && j < S.ny && kk < S.nz)) {
+      for (int c = 0; c < a.k; ++c) Vo[c] = 0.f;
+      a.Mw[(size_t)blockIdx.x * NET_VOX + v] = 0.f;
+      continue;
+    }
+    const int nx = S.nx, ny = S.ny, nz = S.nz;
+    const int ex = S.x0 + i, ey = S.y0 + j, ez = S.z0 + kk;
+    const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    double mv;
+    if (a.eg_op == 1) {
+      mv = a.kx[cg] + a.ky[cg] + a.kz[cg];
+    } else if (a.eg_op == 2) {
+      double dn = a.db[cg];
+      if (i > 0) dn += a.tx[cg];
+      if (i < nx - 1) dn += a.tx[cg + 1];
+      if (j > 0) dn += a.ty[cg];
+      if (j < ny - 1) dn += a.ty[cg + g.M];
+      if (kk > 0) dn += a.tz[cg];
+      if (kk < nz - 1) dn += a.tz[cg + g.MN];
+      mv = dn;
+    } else {
+      mv = 0.0;
+      if (i == 0 && ex >= 1) mv += 2.0 * harm(a.kx[cg - 1], a.kx[cg]) / a.Hx / a.Hx;
+      if (ex + 1 != g.M) mv += 2.0 * harm(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
+      if (ey >= 1) mv += 2.0 * harm(a.ky[cg - g.M], a.ky[cg]) / a.Hy / a.Hy;
+      if (ey + 1 != g.N) mv += 2.0 * harm(a.ky[cg], a.ky[cg + g.M]) / a.Hy / a.Hy;
+      if (ez >= 1) mv += 2.0 * harm(a.kz[cg - g.MN], a.kz[cg]) / a.Hz / a.Hz;
+      if (ez + 1 != g.P) mv += 2.0 * harm(a.kz[cg], a.kz[cg + g.MN]) / a.Hz / a.Hz;
+      if (i + 1 < nx) mv += 2.0 * harm(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
+      const int dm = a.dirichlet_mask;
+      if (dm & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+      if (dm & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+      if (dm & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+      if (dm & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+      if (dm & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
+      if (dm & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
+      mv *= a.meas;
+    }
+    a.Mw[(size_t)blockIdx.x * NET_VOX + v] = (float)mv;
+    for (int c = 0; c < a.k; ++c)
+      Vo[c] = a.phi_f32 ? reinterpret_cast<const float*>(a.phi)[cg * a.kmax + c]
+                        : (float)reinterpret_cast<const double*>(a.phi)[cg * a.kmax + c];
+  }
+}
+
+// Subdomains whose eigensolve did not converge (status 1), in index order.
+__global__ void k_failed_list(const int* status, int nsub, int* list, int* count) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int s = 0; s < nsub; ++s)
+    if (status[s] == 1) list[c++] = s;
+  *count = c;
+}
+
+}  // namespace
+
+void launch_net_targets(const NetTargetArgs& a, cudaStream_t st) {
+  { note_launch(); k_net_targets<<<a.nsub, 256, 0, st>>>(a); }
+}
+
+void launch_failed_list(const int* status, int nsub, int* list, int* count, cudaStream_t st) {
+  { note_launch(); k_failed_list<<<1, 32, 0, st>>>(status, nsub, list, count); }
+}
+
+void launch_net_features(const Grid& g, const SubInfo* subs, int nsub, const double* kx, const double* ky,
+                         const double* kz, int dirichlet_mask, __nv_bfloat16* feats, cudaStream_t st) {
+  { note_launch(); k_net_features<<<nsub, 256, 0, st>>>(g, subs, kx, ky, kz, dirichlet_mask, feats); }
+}
+
+void launch_net_loss(const float* y, const float* V, const float* Mw, int B, int k, float* loss, float* dy,
+                     cudaStream_t st) {
+  { note_launch(); k_net_loss<<<B, 256, 0, st>>>(y, V, Mw, k, B, loss, dy); }
+}
+
+// ---- host side ---------------------------------------------------------------------------------
+static size_t wcount(const NetLayer& L) { return (size_t)net_taps(L.type) * L.cin * L.cout; }
+static size_t act_elems(int a) { return (size_t)kNetActs[a].s * kNetActs[a].s * kNetActs[a].s * kNetActs[a].c; }
+
+Net::Net() {}
+
+Net::~Net() {
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    void* p[] = {w32_[l], b32_[l], w16_[l], wt_[l], gw_[l], gb_[l], mw_[l], vw_[l], mb_[l], vb_[l]};
+    for (void* q : p)
+      if (q) cudaFree(q);
+  }
+  for (int a = 0; a < NET_ACTS; ++a) {
+    if (a > 0 && act_[a]) cudaFree(act_[a]);
+    if (dact_[a]) cudaFree(dact_[a]);
+  }
+}
+
+int Net::params() const {
+  int n = 0;
+  for (const NetLayer& L : kNetLayers) n += (int)wcount(L) + L.cout;
+  return n;
+}
+
+int Net::alloc_params() {
+  if (w32_[0]) return 0;
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const size_t nw = wcount(kNetLayers[l]), nb = kNetLayers[l].cout;
+    bool ok = cudaMalloc(&w32_[l], nw * 4) == cudaSuccess && cudaMalloc(&b32_[l], nb * 4) == cudaSuccess &&
+              cudaMalloc(&w16_[l], nw * 2) == cudaSuccess && cudaMalloc(&wt_[l], nw * 4) == cudaSuccess &&
+              cudaMalloc(&gw_[l], nw * 4) == cudaSuccess && cudaMalloc(&gb_[l], nb * 4) == cudaSuccess &&
+              cudaMalloc(&mw_[l], nw * 4) == cudaSuccess && cudaMalloc(&vw_[l], nw * 4) == cudaSuccess &&
+              cudaMalloc(&mb_[l], nb * 4) == cudaSuccess && cudaMalloc(&vb_[l], nb * 4) == cudaSuccess;
+    if (!ok) {
+      err = "cudaMalloc of the network parameters failed";
+      return 76;
+    }
+    cudaMemset(mw_[l], 0, nw * 4);
+    cudaMemset(vw_[l], 0, nw * 4);
+    cudaMemset(mb_[l], 0, nb * 4);
+    cudaMemset(vb_[l], 0, nb * 4);
+  }
+  return 0;
+}
+
+void Net::refresh(int l, cudaStream_t st) {
+  const NetLayer& L = kNetLayers[l];
+  const long long n = (long long)wcount(L);
+  { note_launch(); k_net_refresh<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(net_taps(L.type), L.cin, L.cout, w32_[l], w16_[l], wt_[l]); }
+}
+
+int Net::set_weights(int l, const float* w, const float* b) {
+  if (l < 0 || l >= NET_LAYERS) {
+    err = "layer index out of range";
+    return 62;
+  }
+  if (int e = alloc_params()) return e;
+  const NetLayer& L = kNetLayers[l];
+  if (w) cudaMemcpy(w32_[l], w, wcount(L) * 4, cudaMemcpyHostToDevice);
+  if (b) cudaMemcpy(b32_[l], b, L.cout * 4, cudaMemcpyHostToDevice);
+  refresh(l, 0);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    err = "set_weights failed";
+    return 76;
+  }
+  return 0;
+}
+
+int Net::get_weights(int l, float* w, float* b) const {
+  if (l < 0 || l >= NET_LAYERS || !w32_[l]) return 62;
+  if (w) cudaMemcpy(w, w32_[l], wcount(kNetLayers[l]) * 4, cudaMemcpyDeviceToHost);
+  if (b) cudaMemcpy(b, b32_[l], kNetLayers[l].cout * 4, cudaMemcpyDeviceToHost);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : 76;
+}
+
+int Net::get_grads(int l, float* gw, float* gb) const {
+  if (l < 0 || l >= NET_LAYERS || !gw_[l]) return 62;
+  if (gw) cudaMemcpy(gw, gw_[l], wcount(kNetLayers[l]) * 4, cudaMemcpyDeviceToHost);
+  if (gb) cudaMemcpy(gb, gb_[l], kNetLayers[l].cout * 4, cudaMemcpyDeviceToHost);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : 76;
+}
+
+int Net::init(unsigned long long seed) {
+  if (int e = alloc_params()) return e;
+  std::mt19937_64 rng(seed);
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const NetLayer& L = kNetLayers[l];
+    const int fan_in = (L.type == NL_UP2 ? 1 : net_taps(L.type)) * (l == 0 ? 5 : L.cin);
+    std::normal_distribution<float> nd(0.f, std::sqrt((L.relu ? 2.f : 1.f) / fan_in));
+    std::vector<float> w(wcount(L)), b(L.cout, 0.f);
+    for (auto& x : w) x = nd(rng);
+    if (int e = set_weights(l, w.data(), b.data())) return e;
+  }
+  step_ = 0;
+  return 0;
+}
+
+static const char kMagic[8] = {'P', 'M', 'F', 'N', 'E', 'T', '0', '1'};
+
+int Net::save(const char* path) const {
+  FILE* f = fopen(path, "wb");
+  if (!f) return 62;
+  fwrite(kMagic, 1, 8, f);
+  const int hdr[2] = {1, NET_LAYERS};
+  fwrite(hdr, 4, 2, f);
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const NetLayer& L = kNetLayers[l];
+    const int d[4] = {L.type, L.cin, L.cout, net_taps(L.type)};
+    fwrite(d, 4, 4, f);
+    std::vector<__nv_bfloat16> w(wcount(L));
+    std::vector<float> b(L.cout);
+    cudaMemcpy(w.data(), w16_[l], w.size() * 2, cudaMemcpyDeviceToHost);
+    cudaMemcpy(b.data(), b32_[l], b.size() * 4, cudaMemcpyDeviceToHost);
+    fwrite(w.data(), 2, w.size(), f);
+    fwrite(b.data(), 4, b.size(), f);
+  }
+  const bool ok = fclose(f) == 0;
+  return ok ? 0 : 76;
+}
+
+int Net::load(const char* path) {
+  FILE* f = fopen(path, "rb");
+  if (!f) {
+    err = std::string("cannot open network weights ") + path;
+    return 62;
+  }
+  auto fail = [&](const char* why) {
+    fclose(f);
+    err = std::string(path) + ": " + why;
+    return 62;
+  };
+  char mg[8];
+  int hdr[2];
+  if (fread(mg, 1, 8, f) != 8 || memcmp(mg, kMagic, 8) != 0) return fail("not a weight file");
+  if (fread(hdr, 4, 2, f) != 2 || hdr[0] != 1 || hdr[1] != NET_LAYERS) return fail("unsupported version or layout");
+  if (int e = alloc_params()) {
+    fclose(f);
+    return e;
+  }
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const NetLayer& L = kNetLayers[l];
+    int d[4];
+    if (fread(d, 4, 4, f) != 4 || d[0] != L.type || d[1] != L.cin || d[2] != L.cout || d[3] != net_taps(L.type))
+      return fail("layer shapes differ from this build's network");
+    std::vector<__nv_bfloat16> w(wcount(L));
+    std::vector<float> w32(w.size()), b(L.cout);
+    if (fread(w.data(), 2, w.size(), f) != w.size() || fread(b.data(), 4, b.size(), f) != b.size())
+      return fail("truncated");
+    for (size_t i = 0; i < w.size(); ++i) w32[i] = __bfloat162float(w[i]);
+    if (int e = set_weights(l, w32.data(), b.data())) {
+      fclose(f);
+      return e;
+    }
+  }
+  fclose(f);
+  return 0;
+}
+
+int Net::ensure(int B) {
+  if (B <= cap_) return 0;
+  for (int a = 1; a < NET_ACTS; ++a) {
+    if (act_[a]) cudaFree(act_[a]);
+    if (dact_[a]) cudaFree(dact_[a]);
+    act_[a] = nullptr;
+    dact_[a] = nullptr;
+  }
+  for (int a = 1; a < NET_ACTS - 1; ++a)
+    if (cudaMalloc(&act_[a], act_elems(a) * B * 2) != cudaSuccess) {
+      err = "cudaMalloc of the network activations failed";
+      cap_ = 0;
+      return 76;
+    }
+  cap_ = B;
+  return 0;
+}
+
+int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_t st) {
+  if (!w32_[0]) {
+    err = "network weights not initialised or loaded";
+    return 73;
+  }
+  if (int e = ensure(B)) return e;
+  x_ = x;
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const NetLayer& L = kNetLayers[l];
+    FwdArgs a;
+    a.type = L.type;
+    a.cin = L.cin;
+    a.cout = L.cout;
+    a.s_in = L.s_in;
+    a.s_out = L.s_out;
+    a.relu = L.relu;
+    a.in = L.in_act == 0 ? x : act_[L.in_act];
+    a.W = w16_[l];
+    a.bias = b32_[l];
+    a.skip = L.skip >= 0 ? act_[L.skip] : nullptr;
+    a.out = L.out_act == NET_ACTS - 1 ? nullptr : act_[L.out_act];
+    a.outf = L.out_act == NET_ACTS - 1 ? y : nullptr;
+    const long long rows = (long long)B * L.s_out * L.s_out * L.s_out;
+    const int grid = (int)(rows / kTileRows);
+    const size_t smem = ((size_t)kTileRows * (L.cin + 8) + (size_t)L.cin * (L.cout + 8)) * 2;
+    note_launch();
+    switch (L.cout / 8) {
+      case 2: k_net_fwd<2><<<grid, 128, smem, st>>>(a); break;
+      case 4: k_net_fwd<4><<<grid, 128, smem, st>>>(a); break;
+      case 8: k_net_fwd<8><<<grid, 128, smem, st>>>(a); break;
+      case 12: k_net_fwd<12><<<grid, 128, smem, st>>>(a); break;
+      default: err = "unsupported layer width"; return 56;
+    }
+  }
+  (void)keep;
+  return 0;
+}
+
+int Net::backward(const float* dy, int B, cudaStream_t st) {
+  if (B > cap_ || !x_) {
+    err = "backward needs the activations of a forward pass of the same batch";
+    return 73;
+  }
+  for (int a = 1; a < NET_ACTS - 1; ++a)
+    if (!dact_[a] && cudaMalloc(&dact_[a], act_elems(a) * cap_ * 4) != cudaSuccess) {
+      err = "cudaMalloc of the network gradients failed";
+      return 76;
+    }
+  // dpre[l]: pre-activation gradient of layer l's output; layer 8's is dy.
+  auto dpre = [&](int l) -> float* {
+    return l == NET_LAYERS - 1 ? const_cast<float*>(dy) : dact_[kNetLayers[l].out_act];
+  };
+  for (int l = NET_LAYERS - 1; l >= 0; --l) {
+    const NetLayer& L = kNetLayers[l];
+    const __nv_bfloat16* in = L.in_act == 0 ? x_ : act_[L.in_act];
+    cudaMemsetAsync(gw_[l], 0, wcount(L) * 4, st);
+    // weight gradient
+    WgradArgs w;
+    w.type = L.type;
+    w.cin = L.cin;
+    w.cout = L.cout;
+    w.s_in = L.s_in;
+    w.s_out = L.s_out;
+    w.B = B;
+    w.rows_per_chunk = 2048;
+    w.in = in;
+    w.dz = dpre(l);
+    w.gw = gw_[l];
+    const long long rows = (long long)B * (L.type == NL_UP2 ? L.s_in * L.s_in * L.s_in : L.s_out * L.s_out * L.s_out);
+    dim3 grid((unsigned)((rows + w.rows_per_chunk - 1) / w.rows_per_chunk), net_taps(L.type));
+    const int ta = L.cin / 16, tb = L.cout / 16;
+    note_launch();
+    if (ta == 1 && tb == 2) k_net_wgrad<1, 2><<<grid, 256, 0, st>>>(w);
+    else if (ta == 2 && tb == 4) k_net_wgrad<2, 4><<<grid, 256, 0, st>>>(w);
+    else if (ta == 4 && tb == 4) k_net_wgrad<4, 4><<<grid, 256, 0, st>>>(w);
+    else if (ta == 4 && tb == 6) k_net_wgrad<4, 6><<<grid, 256, 0, st>>>(w);
+    else if (ta == 6 && tb == 6) k_net_wgrad<6, 6><<<grid, 256, 0, st>>>(w);
+    else if (ta == 6 && tb == 4) k_net_wgrad<6, 4><<<grid, 256, 0, st>>>(w);
+    else if (ta == 4 && tb == 2) k_net_wgrad<4, 2><<<grid, 256, 0, st>>>(w);
+    else if (ta == 2 && tb == 2) k_net_wgrad<2, 2><<<grid, 256, 0, st>>>(w);
+    else if (ta == 2 && tb == 1) k_net_wgrad<2, 1><<<grid, 256, 0, st>>>(w);
+    else {
+      err = "unsupported layer shape in backward";
+      return 56;
+    }
+    const long long orows = (long long)B * L.s_out * L.s_out * L.s_out;
+    { note_launch(); k_net_bgrad<<<L.cout, 256, 0, st>>>(dpre(l), orows, L.cout, gb_[l]); }
+    if (l == 0) break;
+    // gradient reaching the input activation, masked by its ReLU, plus skip gradients
+    DgradArgs d;
+    d.type = L.type;
+    d.cin = L.cin;
+    d.cout = L.cout;
+    d.s_in = L.s_in;
+    d.s_out = L.s_out;
+    d.B = B;
+    d.dz = dpre(l);
+    d.wt = wt_[l];
+    d.in_act = in;
+    d.add = nullptr;
+    for (int j = 0; j < NET_LAYERS; ++j)
+      if (kNetLayers[j].skip == L.in_act) d.add = dpre(j);
+    d.din = dact_[L.in_act];
+    const long long tot = (long long)B * L.s_in * L.s_in * L.s_in * L.cin;
+    { note_launch(); k_net_dgrad<<<(int)std::min<long long>((tot + 255) / 256, 1 << 20), 256, 0, st>>>(d); }
+  }
+  return 0;
+}
+
+void Net::adam(float lr, float b1, float b2, float eps, float wd, cudaStream_t st) {
+  ++step_;
+  const float bc1 = 1.f - powf(b1, (float)step_), bc2 = 1.f - powf(b2, (float)step_);
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const NetLayer& L = kNetLayers[l];
+    const long long nw = (long long)wcount(L);
+    { note_launch(); k_net_adam<<<(int)std::min<long long>((nw + 255) / 256, 4096), 256, 0, st>>>(nw, w32_[l], gw_[l], mw_[l], vw_[l], lr, b1, b2, eps, wd, bc1, bc2); }
+    { note_launch(); k_net_adam<<<1, 256, 0, st>>>(L.cout, b32_[l], gb_[l], mb_[l], vb_[l], lr, b1, b2, eps, 0.f, bc1, bc2); }
+    refresh(l, st);
+  }
+}
+
+}  // namespace pmf

@@ -120,6 +120,16 @@ struct LobpcgArgs {
   const double *kx, *ky, *kz;              // permeability (for the MOD/MEAN mass)
   double Hx, Hy, Hz, meas;
   const double* xinit;  // optional initial block (per cell, m values), may be null
+  // optional per-subdomain initial columns from the learned network: patch
+  // layout [s][16^3 voxels][16 channels], columns 0..xinit_k-1 used, the rest random
+  const float* xinit_patch;
+  int xinit_k;
+  // optional subset of subdomains to solve: sub_list[0 .. *nlist-1] (device), may be null
+  const int* sub_list;
+  const int* nlist;
+  // optional work queue (one device int, zeroed by the launcher): CTAs take the
+  // next subdomain with atomicAdd instead of the fixed stride blockIdx.x + k*gridDim.x
+  int* queue;
   int dirichlet_mask;   // bit f set: face f (x-,x+,y-,y+,z-,z+) is a Dirichlet face
   int ld;               // column stride of the work block vectors (set by the launcher)
   int ldc;              // stride of the shared-memory sweep arrays (set by the launcher)

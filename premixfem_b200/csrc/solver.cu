@@ -8,6 +8,7 @@
 #include <cstring>
 #include <sstream>
 
+#include "pmf_net.h"
 #include "solver.h"
 
 namespace pmf {
@@ -113,6 +114,24 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_real("pmf_eig_sigma", &o->eig_sigma);
   db.get_int("pmf_eig_guard", &o->eig_guard);
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
+  {
+    auto it2 = db.kv.find("pmf_learned");
+    if (it2 != db.kv.end()) {
+      if (it2->second.empty()) {
+        *err = "-pmf_learned needs the path of a network weight file";
+        return 62;
+      }
+      o->learned_path = it2->second;
+    }
+  }
+  if (db.get_real("pmf_learned_tol", &o->learned_tol) && !(o->learned_tol > 0.0)) {
+    *err = "-pmf_learned_tol must be > 0";
+    return 62;
+  }
+  if (db.get_int("pmf_learned_its", &o->learned_its) && o->learned_its < 1) {
+    *err = "-pmf_learned_its must be >= 1";
+    return 62;
+  }
   if (o->use_full_Cholesky_lv1) {
     *err = "-use_full_Cholesky_lv1 is not supported by this build (IC(0) only)";
     return 56;  // PETSC_ERR_SUP
@@ -229,6 +248,10 @@ Solver::~Solver() {
                   state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (void* p : {(void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
+                  (void*)d_status_learned})
+    if (p) cudaFree(p);
+  delete net;
   if (h_state) cudaFreeHost(h_state);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -314,6 +337,13 @@ int Solver::build_partition() {
   if (32 * 8 + 5 * (size_t)((max_cells + 3) & ~3) * (opt.precision == 1 ? 4 : 8) > 227 * 1024) {
     err = "subdomain too large for the shared-memory IC(0) sweep of this precision (FP64: <= 5600 cells)";
     return 62;
+  }
+  if (!opt.learned_path.empty()) {
+    for (const SubInfo& S : subs)
+      if (S.nx > NET_S || S.ny > NET_S || S.nz > NET_S) {
+        err = "-pmf_learned needs subdomains of at most 16 x 16 x 16 cells";
+        return 62;
+      }
   }
   kmax = opt.en_lv1;
   if (kmax > 8 || opt.en_lv1 + opt.eig_guard > 10) {
@@ -435,6 +465,79 @@ int Solver::assemble() {
   return check(cudaStreamSynchronize(st), "assemble");
 }
 
+// Local eigensolves from the network's initial blocks: one LOBPCG launch
+// capped at learned_its iterations, then a second launch, from a random start
+// with the full budget, over the subdomains the first one left unconverged
+// (the list is built on the device, so no host round trip is needed).
+int Solver::run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1) {
+  const bool mixed = opt.precision == 1;
+  if (!net) {
+    net = new Net();
+    if (int e = net->load(opt.learned_path.c_str())) {
+      err = net->err;
+      delete net;
+      net = nullptr;
+      return e;
+    }
+  }
+  const int chunk = std::min(nsub, 1024);
+  if (!net_y) {
+    if (int e = check(cudaMalloc(&net_y, (size_t)nsub * NET_VOX * NET_COUT * sizeof(float)), "cudaMalloc net output"))
+      return e;
+    if (int e = check(cudaMalloc(&net_x, (size_t)chunk * NET_VOX * NET_CIN * 2), "cudaMalloc net input")) return e;
+    cudaMalloc(&d_fail_list, sizeof(int) * nsub);
+    cudaMalloc(&d_fail_count, sizeof(int));
+    cudaMalloc(&d_iters_learned, sizeof(int) * nsub);
+    cudaMalloc(&d_status_learned, sizeof(int) * nsub);
+  }
+  int dmask = 0;
+  for (int f = 0; f < 6; ++f)
+    if (dir_on_[f]) dmask |= 1 << f;
+  cudaEvent_t n0, n1;
+  cudaEventCreate(&n0);
+  cudaEventCreate(&n1);
+  cudaEventRecord(n0, st);
+  for (int c0 = 0; c0 < nsub; c0 += chunk) {
+    const int cb = std::min(chunk, nsub - c0);
+    launch_net_features(g, d_subs + c0, cb, kx, ky, kz, dmask, (__nv_bfloat16*)net_x, st);
+    if (int e = net->forward((const __nv_bfloat16*)net_x, cb, net_y + (size_t)c0 * NET_VOX * NET_COUT, false, st)) {
+      err = net->err;
+      return e;
+    }
+  }
+  cudaEventRecord(n1, st);
+  LobpcgArgs l1 = la;
+  l1.xinit_patch = net_y;
+  l1.xinit_k = opt.en_lv1;
+  l1.max_it = std::min(opt.learned_its, opt.eig_max_it);
+  l1.tol = std::max(opt.learned_tol, la.tol);
+  LobpcgArgs l2 = la;
+  l2.sub_list = d_fail_list;
+  l2.nlist = d_fail_count;
+  if (mixed)
+    launch_lobpcg<float>(l1, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                         max_lines, st);
+  else
+    launch_lobpcg<double>(l1, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                          max_lines, st);
+  cudaMemcpyAsync(d_iters_learned, d_iters, sizeof(int) * nsub, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(d_status_learned, d_status, sizeof(int) * nsub, cudaMemcpyDeviceToDevice, st);
+  launch_failed_list(d_status, nsub, d_fail_list, d_fail_count, st);
+  if (mixed)
+    launch_lobpcg<float>(l2, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                         max_lines, st);
+  else
+    launch_lobpcg<double>(l2, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                          max_lines, st);
+  float ms = 0.f;
+  cudaEventSynchronize(n1);
+  cudaEventElapsedTime(&ms, n0, n1);
+  net_ms = ms;
+  cudaEventDestroy(n0);
+  cudaEventDestroy(n1);
+  return 0;
+}
+
 int Solver::setup() {
   if (!kx) {
     err = "kappa not set (PC_init contract: the caller constructs kappa before setup)";
@@ -499,6 +602,12 @@ int Solver::setup() {
   la.Hz = H[2];
   la.meas = H[0] * H[1] * H[2];
   la.xinit = nullptr;
+  la.xinit_patch = nullptr;
+  la.xinit_k = 0;
+  la.sub_list = nullptr;
+  la.nlist = nullptr;
+  if (!d_queue) cudaMalloc(&d_queue, sizeof(int));
+  la.queue = d_queue;
   la.dirichlet_mask = dmask;
   la.ld = 0;
   la.prof = nullptr;
@@ -516,12 +625,15 @@ int Solver::setup() {
     eig_work_bytes = need;
   }
   const double eb1 = opt.eb_lv1 < 0 ? 1.0e12 : opt.eb_lv1;  // 1/NIL
-  if (mixed)
+  if (!opt.learned_path.empty()) {
+    if (int er = run_learned_eigen(la, eig_blocks, eb1)) return er;
+  } else if (mixed) {
     launch_lobpcg<float>(la, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
                          max_lines, st);
-  else
+  } else {
     launch_lobpcg<double>(la, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
                           max_lines, st);
+  }
   cudaEventRecord(e[2], st);
   if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;
   if (int er = check(cudaGetLastError(), "setup launch")) return er;
@@ -550,6 +662,23 @@ int Solver::setup() {
   eig1.resize((size_t)nsub * opt.en_lv1);
   cudaMemcpy(ks.data(), d_ks, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
   cudaMemcpy(eig_iters.data(), d_iters, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+  if (!opt.learned_path.empty()) {
+    // iterations from the learned start, plus the random restart where it was needed
+    std::vector<int> it_l(nsub), st_l(nsub);
+    cudaMemcpy(it_l.data(), d_iters_learned, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+    cudaMemcpy(st_l.data(), d_status_learned, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
+    learned_used = 1;
+    learned_fallbacks = 0;
+    learned_iters = fallback_iters = 0;
+    for (int s_ = 0; s_ < nsub; ++s_) {
+      learned_iters += it_l[s_];
+      if (st_l[s_] == 1) {
+        ++learned_fallbacks;
+        fallback_iters += eig_iters[s_];
+        eig_iters[s_] += it_l[s_];
+      }
+    }
+  }
   cudaMemcpy(eig_status.data(), d_status, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
   cudaMemcpy(eig1.data(), d_eig1, sizeof(double) * eig1.size(), cudaMemcpyDeviceToHost);
   int bad_pivots = 0;

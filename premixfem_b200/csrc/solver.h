@@ -33,6 +33,13 @@ struct Options {
   double l3_tol = 1e-10;
   unsigned long long seed = 20240611ull;
   int pcg_chunk = 4;
+  // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
+  // LOBPCG starts from the network's output and may take learned_its
+  // iterations; subdomains that have not converged by then are solved again
+  // from a random start with the full iteration budget
+  std::string learned_path;
+  int learned_its = 30;
+  double learned_tol = 1e-4;  // Ritz-residual gate of the learned start
 };
 
 // PETSc-style options database ("-name value" pairs); flags carry an empty value.
@@ -59,6 +66,8 @@ enum Stage {
   ST_AV,
   ST_COUNT
 };
+
+class Net;
 
 class Solver {
  public:
@@ -121,6 +130,16 @@ class Solver {
   double dir_val_[6] = {0, 0, 0, 0, 0, 0};
   double last_setup_ms = 0, last_solve_ms = 0;
   int last_its = 0;
+  // learned set-up
+  Net* net = nullptr;
+  void* net_x = nullptr;  // BF16 feature patches of one chunk of subdomains
+  float* net_y = nullptr;  // network output for every subdomain [nsub][4096][16]
+  int* d_queue = nullptr;
+  int *d_fail_list = nullptr, *d_fail_count = nullptr, *d_iters_learned = nullptr, *d_status_learned = nullptr;
+  int learned_used = 0, learned_fallbacks = 0;
+  long long learned_iters = 0, fallback_iters = 0;
+  double net_ms = 0.0;
+  int run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1);
   int nparts_apply() const { return nsub; }
 };
 

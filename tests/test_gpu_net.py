@@ -1,0 +1,149 @@
+"""GPU checks of the learned-initialisation network against the CPU oracle.
+
+Tolerances: forward output within 2e-2 relative L2 of the oracle run with the
+same BF16 rounding of weights and activations (the GPU accumulates in FP32,
+the oracle in FP64, and either may round an activation one BF16 ulp apart);
+weight and bias gradients within 5e-2 relative L2 and at cosine >= 0.998 per
+layer (the rounding differences compound through the eight ReLU layers the
+gradient crosses on its way to the first layer); the subspace
+loss and its gradient within 1e-4.  The learned start must leave the set-up's
+results unchanged: local eigenvalues within 1e-6 relative (mixed-precision
+tolerance) and PCG iterations within +-1 of the random start.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import net_oracle as NO
+from premixfem_b200 import _native, fields, learned
+from premixfem_b200.solver import DarcySolver, options_string
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def torch():
+    return pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def net_and_batch(native, torch):
+    net = learned.Net(seed=7)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((2, 16, 16, 16, 16)).astype(np.float32)
+    x[..., 5:] = 0.0
+    xt = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    xb = xt.float().cpu().numpy().astype(np.float64)
+    W, b = [], []
+    for l in range(9):
+        w_, b_ = net.weights(l)
+        W.append(w_.astype(np.float64))
+        b.append(b_.astype(np.float64))
+    return net, xt, xb, W, b
+
+
+def test_forward_matches_oracle(net_and_batch, torch):
+    net, xt, xb, W, b = net_and_batch
+    y = torch.empty((2, 4096, 16), dtype=torch.float32, device="cuda")
+    net.forward(xt, y)
+    torch.cuda.synchronize()
+    acts = NO.forward(xb, W, b, bf16=True)
+    ref = acts[-1].reshape(2, 4096, 16)
+    assert _rel(y.cpu().numpy(), ref) < 2e-2
+
+
+def test_backward_matches_oracle(net_and_batch, torch):
+    net, xt, xb, W, b = net_and_batch
+    y = torch.empty((2, 4096, 16), dtype=torch.float32, device="cuda")
+    net.forward(xt, y)
+    rng = np.random.default_rng(5)
+    dy = rng.standard_normal((2, 4096, 16)).astype(np.float32)
+    net.backward(torch.from_numpy(dy).cuda())
+    torch.cuda.synchronize()
+    acts = NO.forward(xb, W, b, bf16=True)
+    dW, db = NO.backward(acts, W, dy.astype(np.float64).reshape(2, 16, 16, 16, 16), bf16=True)
+    for l in range(9):
+        gw, gb = net.grads(l)
+        cos = float(np.dot(gw.ravel(), dW[l].ravel()) / (np.linalg.norm(gw) * np.linalg.norm(dW[l])))
+        assert _rel(gw, dW[l]) < 5e-2 and cos > 0.998, (l, _rel(gw, dW[l]), cos)
+        assert _rel(gb, db[l]) < 5e-2, (l, _rel(gb, db[l]))
+
+
+def test_loss_matches_oracle(native, torch):
+    rng = np.random.default_rng(11)
+    B, k = 3, 6
+    y = rng.standard_normal((B, 4096, 16)).astype(np.float32)
+    V = rng.standard_normal((B, 4096, k)).astype(np.float32)
+    M = rng.uniform(0.1, 2.0, (B, 4096)).astype(np.float32)
+    M[:, ::7] = 0.0
+    yt, Vt, Mt = (torch.from_numpy(a).cuda() for a in (y, V, M))
+    loss = torch.empty(B, dtype=torch.float32, device="cuda")
+    dy = torch.empty_like(yt)
+    learned.loss_and_grad(yt, Vt, Mt, k, loss, dy)
+    torch.cuda.synchronize()
+    rl, rdy = NO.subspace_loss(y.astype(np.float64), V, M, k)
+    assert _rel(loss.cpu().numpy(), rl) < 1e-4
+    assert _rel(dy.cpu().numpy(), rdy) < 1e-4
+
+
+def test_patches_hold_m_orthonormal_eigenvectors(native, torch):
+    feats, V, M = learned.patches(64, seed=9)
+    V = V.double().cpu().numpy()
+    M = M.double().cpu().numpy()
+    f = feats.float().cpu().numpy()
+    assert V.shape == (64, 4096, 6) and np.all(np.isfinite(f))
+    inside = f[:, :, 4] > 0.5
+    assert np.array_equal(inside, M > 0)
+    for s in range(V.shape[0]):
+        G = V[s].T @ (M[s][:, None] * V[s])
+        assert np.abs(G - np.eye(6)).max() < 1e-3, s
+
+
+def test_learned_start_keeps_results(native, torch, tmp_path):
+    """A network with random weights still gives the same preconditioner:
+    subdomains that do not converge from its output fall back to a random start."""
+    net = learned.Net(seed=123)
+    path = str(tmp_path / "random.pmfnet")
+    net.save(path)
+    prob = fields.fracture256(64, seed=21)
+    res = {}
+    for mode in ("plain", "learned"):
+        opts = {"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": "mixed"}
+        if mode == "learned":
+            opts.update(pmf_learned=path, pmf_learned_its=3, pmf_learned_tol=1e-6)
+        s = DarcySolver.from_problem(prob, options_string(opts))
+        s.setup()
+        b = s.rhs(prob["source"].ravel())
+        x, its, rn, reason = s.solve(b)
+        ev, ks, it1, st1 = s.eigen_lv1()
+        stats = (C.c_longlong * 4)()
+        nm = C.c_double()
+        _native.check(s.lib.pmf_get_learned_stats(s.h, stats, C.byref(nm)))
+        res[mode] = dict(its=its, ev=ev, st=st1, stats=list(stats), x=x)
+        s.close()
+    assert res["learned"]["stats"][0] == 1 and res["plain"]["stats"][0] == 0
+    assert res["learned"]["stats"][1] > 0  # random weights: most subdomains fall back
+    assert np.all(res["learned"]["st"] != 1)
+    ev_p, ev_l = res["plain"]["ev"], res["learned"]["ev"]
+    scale = np.abs(ev_p).max()
+    assert np.all(np.abs(ev_l - ev_p) <= 1e-6 * np.abs(ev_p) + 1e-9 * scale)
+    assert abs(res["learned"]["its"] - res["plain"]["its"]) <= 1
+
+
+def test_trained_network_reduces_eigensolver_iterations(native, torch):
+    """What the trained network gains over the randomly started eigensolve, on a
+    field it was not trained on (seed 77; training used seeds 101-110): fewer
+    LOBPCG iterations at the same PCG iteration count (+-1) and solution."""
+    assert os.path.exists(learned.DEFAULT_WEIGHTS)
+    res = learned.evaluate(learned.DEFAULT_WEIGHTS, n=128, seed=77)
+    r, l = res["random"], res["learned"]
+    assert l["eig_iters_mean"] <= 0.7 * r["eig_iters_mean"], res
+    assert l["fallbacks"] <= 0.05 * 512, res
+    assert abs(l["pcg_iters"] - r["pcg_iters"]) <= 1, res
+    assert res["solution_rel_diff"] < 1e-6, res
