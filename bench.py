@@ -3,14 +3,16 @@
 preconditioner on one B200 (per rank), through libpremixfem_b200.so.
 
 Metric: setup+solve seconds at 1e-8 relative residual and PCG iterations,
-mixed precision (FP32 preconditioner / FP32 eigensolver vectors, FP64 PCG and
-coarse factorisations) against the plain FP64 GPU form.
+mixed precision with the learned eigensolver start (FP32 preconditioner and
+eigensolver vectors, FP64 PCG, Rayleigh-Ritz and coarse factorisations;
+local eigensolves started from the trained network's blocks, Ritz-gated,
+random restart on failure) against the plain FP64 GPU form.
 
 One step = one full setup (operator assembly, level-1 IC(0), batched local
 eigensolves, Galerkin level 2, level-3 eigensolve + Galerkin, coarse
 inverses) plus one PCG solve to 1e-8 on the workload's seeded synthetic field.
 
-  value   mixed form, inputs resident in HBM (kappa and rhs on the device)
+  value   mixed/learned form, inputs resident in HBM (kappa and rhs on the device)
   e2e     mixed form through the C ABI with host buffers (host->device copy
           of kappa and source, device->host copy of the solution, inside the
           timed region)
@@ -27,6 +29,7 @@ a bounded sample of the same workload and scales it to the full size.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -51,8 +54,11 @@ WORKLOADS = {
     "fracture256": dict(
         make=lambda seed: fields.fracture256(256, seed=seed),
         opts={"sd": 4, "pmf_vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
+        learned=os.path.join(ROOT, "premixfem_b200", "weights", "fracture16_k6.pmfnet"),
         desc="fracture256: 256^3 unit cells, 200 fractures k=1e4, 5% barriers k=1e-4, p=1|0 on x faces; "
-             "16^3 subdomains of 16^3 cells (virtual rank grid 4x4x4, -sd 4), en_lv1=6, en_lv2=4, V-cycle",
+             "16^3 subdomains of 16^3 cells (virtual rank grid 4x4x4, -sd 4), en_lv1=6, en_lv2=4, V-cycle; "
+             "mixed form with the learned eigensolver start (network trained on seeds 101-110, this field is "
+             "seed 4)",
         sample_n=64, sample_opts={"sd": 4, "en_lv1": 6, "en_lv2": 4},
     ),
     # 32^3 unit cube GRF.
@@ -168,7 +174,10 @@ def run_b200(args):
     x_host = torch.empty(n, dtype=torch.float64).pin_memory()
 
     def make_solver(prec):
-        s = DarcySolver(prob["dom"], prob["mesh"], options_string(dict(wl["opts"], pmf_precision=prec)))
+        o = dict(wl["opts"], pmf_precision=prec)
+        if prec == "mixed" and wl.get("learned"):
+            o["pmf_learned"] = wl["learned"]
+        s = DarcySolver(prob["dom"], prob["mesh"], options_string(o))
         for f, v in prob["dirichlet"].items():
             s.set_dirichlet(f, v)
         return s
@@ -212,12 +221,16 @@ def run_b200(args):
         launches = lib.pmf_launch_count() - launches0
         stages = s.stages()
         ev1, ks, it1, st1 = s.eigen_lv1()
+        lst = (C.c_longlong * 4)()
+        net_ms = C.c_double()
+        _native.check(lib.pmf_get_learned_stats(s.h, lst, C.byref(net_ms)))
         bn = float(torch.linalg.norm(b))
         res = float(torch.linalg.norm(b - torch.from_numpy(s.apply_A(x.cpu().numpy())).cuda())) / bn
         results[prec] = dict(steps=steps, launches=launches, clocks=clk.summary(), stages=stages,
                              eig_iters_mean=float(it1.mean()), eig_iters_max=int(it1.max()),
                              eig_iters_sum=int(it1.sum()), cells_per_sub=n / len(it1),
-                             eig_unconverged=int((st1 != 0).sum()), rel_residual=res, x=x.cpu().numpy())
+                             eig_unconverged=int((st1 != 0).sum()), rel_residual=res, x=x.cpu().numpy(),
+                             learned=dict(used=int(lst[0]), fallbacks=int(lst[1]), net_ms=round(net_ms.value, 3)))
         if prec == "mixed":
             # e2e through the C ABI with host buffers (copies inside the timed region)
             e2e = []
@@ -288,7 +301,10 @@ def run_b200(args):
         "rel_residual": {"mixed": results["mixed"]["rel_residual"], "plain_fp64": results["fp64"]["rel_residual"]},
         "solution_rel_diff_mixed_vs_fp64": xdiff,
         "eigensolver": {"iters_mean": results["mixed"]["eig_iters_mean"], "iters_max": results["mixed"]["eig_iters_max"],
-                        "unconverged": results["mixed"]["eig_unconverged"]},
+                        "unconverged": results["mixed"]["eig_unconverged"],
+                        "plain_fp64_iters_mean": results["fp64"]["eig_iters_mean"],
+                        "plain_fp64_iters_max": results["fp64"]["eig_iters_max"],
+                        "learned_start": results["mixed"]["learned"]},
         # host buffers: kappa x3 + source + rhs in (5n doubles); rhs + solution out (2n doubles)
         "e2e": {"value": round(t_e2e, 6), "unit": "s", "h2d_bytes_per_step": int(5 * n * 8),
                 "d2h_bytes_per_step": int(2 * n * 8)},

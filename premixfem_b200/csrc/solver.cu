@@ -248,7 +248,7 @@ Solver::~Solver() {
                   state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  for (void* p : {(void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
+  for (void* p : {(void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
                   (void*)d_status_learned})
     if (p) cudaFree(p);
   delete net;
@@ -720,14 +720,11 @@ int Solver::setup() {
   { note_launch(); k_add_diag<<<nrank, 256, 0, st>>>(nrank, nr, ANinv, 1e-8, 1); }
   launch_spd_inverse(nrank, nr, ANinv, 1e-14, d_flag + 2, st);
   const int p = std::min(nr, std::min(32, 2 * en2 + 4));
-  double* l3work = nullptr;
-  if (int er = check(cudaMalloc(&l3work, sizeof(double) * nrank * 3 * nr * p), "cudaMalloc l3 work")) return er;
-  launch_dense_smallest_eig(nrank, nr, en2, p, AN, ANinv, V3, d_eig3, d_l3it, opt.l3_tol, opt.l3_max_it, l3work, st);
-  if (int er = check(cudaStreamSynchronize(st), "level-3 eigensolve")) {
-    cudaFree(l3work);
-    return er;
+  if (!l3work) {
+    if (int er = check(cudaMalloc(&l3work, sizeof(double) * nrank * 3 * nr * p), "cudaMalloc l3 work")) return er;
   }
-  cudaFree(l3work);
+  launch_dense_smallest_eig(nrank, nr, en2, p, AN, ANinv, V3, d_eig3, d_l3it, opt.l3_tol, opt.l3_max_it, l3work, st);
+  if (int er = check(cudaStreamSynchronize(st), "level-3 eigensolve")) return er;
   eig3.resize((size_t)nrank * en2);
   l3_iters.resize(nrank);
   cudaMemcpy(eig3.data(), d_eig3, sizeof(double) * eig3.size(), cudaMemcpyDeviceToHost);

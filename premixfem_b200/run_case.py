@@ -49,11 +49,15 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--opts", default="", help="extra options appended to the generated option string")
+    ap.add_argument("--learned", action="store_true", help="start the local eigensolves from the trained network")
     args = ap.parse_args()
 
     import torch
 
     prob, opts = make_case(args.case, args.n, args.seed)
+    if args.learned:
+        from premixfem_b200.learned import DEFAULT_WEIGHTS
+        opts["pmf_learned"] = DEFAULT_WEIGHTS
     o = options_string(dict(opts, pmf_precision=args.precision)) + " " + args.opts
     s = DarcySolver(prob["dom"], prob["mesh"], o)
     for f, v in prob["dirichlet"].items():
@@ -71,10 +75,14 @@ def main():
         _, its, rn, reason = s.solve(b, x)
         su, so = s.timing()
         _, _, it1, st1 = s.eigen_lv1()
+        _, _, it3 = s.eigen_lv2()
+        stages = {k_: round(v_ * 1e3, 2) for k_, v_ in s.stages().items()}
         print(json.dumps({"case": args.case, "n": args.n, "precision": args.precision, "rep": rep,
                           "setup_ms": round(su, 3), "solve_ms": round(so, 3), "pcg_iters": its,
+                          "stages_ms_cumulative": stages,
                           "reason": reason, "eig_iters_mean": float(it1.mean()), "eig_iters_max": int(it1.max()),
-                          "eig_not_converged": int((st1 == 1).sum())}), flush=True)
+                          "eig_not_converged": int((st1 == 1).sum()), "lv3_iters_max": int(it3.max()),
+                          "lv3_iters_mean": float(it3.mean())}), flush=True)
     s.close()
 
 
