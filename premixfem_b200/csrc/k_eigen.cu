@@ -283,56 +283,66 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 // its B fragment (column of S / AS): no shared-memory staging.  The per-warp
 // partial tiles are reduced in a fixed order through shared memory, so the
 // result is deterministic.  red: >= 8 * 32 * 32 doubles.
-template <typename TS, typename TA>
+template <typename TS, typename TA, int NT>
 __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, const double* wgt, int ncells,
                                            double* GM, double* GA, double* red) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int r = lane >> 2, cq = lane & 3;
   const int ns = S.total();
   const int nt = (ns + 7) >> 3;
-  const TS* sp[4];
-  const TA* ap[4];
+  const TS* sp[NT];
+  const TA* ap[NT];
 #pragma unroll
-  for (int ta = 0; ta < 4; ++ta) {
+  for (int ta = 0; ta < NT; ++ta) {
     const int a = 8 * ta + r;
     sp[ta] = (ta < nt && a < ns) ? S.col(a) : nullptr;
     ap[ta] = (ta < nt && a < ns) ? AS.col(a) : nullptr;
   }
-  double cm[4][4][2], ca[4][4][2];
+  double cm[NT][NT][2], ca[NT][NT][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < NT; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) cm[i][j][0] = cm[i][j][1] = ca[i][j][0] = ca[i][j][1] = 0.0;
-  double s[4], as[4], wv;
+    for (int j = 0; j < NT; ++j) cm[i][j][0] = cm[i][j][1] = ca[i][j][0] = ca[i][j][1] = 0.0;
+  // Each warp step covers 8 cells (two k-steps of 4): lane l reads cells
+  // c0 + l%4 and c0 + 4 + l%4, so a column's two loads fill whole 32-byte
+  // sectors, and the next step's 16 loads per lane are in flight during the MMAs.
+  double s[NT], as[NT], s2[NT], as2[NT], wv, wv2;
   auto load = [&](int c0) {
-    const int c = c0 + cq;
-    const bool in = c < ncells;
+    const int c = c0 + cq, c2 = c0 + 4 + cq;
+    const bool in = c < ncells, in2 = c2 < ncells;
     wv = in ? wgt[c] : 0.0;
+    wv2 = in2 ? wgt[c2] : 0.0;
 #pragma unroll
-    for (int ta = 0; ta < 4; ++ta) {
+    for (int ta = 0; ta < NT; ++ta) {
       s[ta] = (in && sp[ta]) ? (double)sp[ta][c] : 0.0;
       as[ta] = (in && ap[ta]) ? (double)ap[ta][c] : 0.0;
+      s2[ta] = (in2 && sp[ta]) ? (double)sp[ta][c2] : 0.0;
+      as2[ta] = (in2 && ap[ta]) ? (double)ap[ta][c2] : 0.0;
     }
   };
-  load(4 * w);
-  for (int c0 = 4 * w; c0 < ncells; c0 += 4 * nwarp) {
-    double cs[4], cas[4];
+  load(8 * w);
+  for (int c0 = 8 * w; c0 < ncells; c0 += 8 * nwarp) {
+    double cs[NT], cas[NT], cs2[NT], cas2[NT];
 #pragma unroll
-    for (int ta = 0; ta < 4; ++ta) {
+    for (int ta = 0; ta < NT; ++ta) {
       cs[ta] = s[ta];
       cas[ta] = as[ta];
+      cs2[ta] = s2[ta];
+      cas2[ta] = as2[ta];
     }
-    const double cw = wv;
-    if (c0 + 4 * nwarp < ncells) load(c0 + 4 * nwarp);  // next group in flight during the MMAs
+    const double cw = wv, cw2 = wv2;
+    if (c0 + 8 * nwarp < ncells) load(c0 + 8 * nwarp);  // next step in flight during the MMAs
 #pragma unroll
-    for (int ta = 0; ta < 4; ++ta) {
+    for (int ta = 0; ta < NT; ++ta) {
       if (ta >= nt) break;
-      const double ws = cs[ta] * cw;
+      const double ws = cs[ta] * cw, ws2 = cs2[ta] * cw2;
 #pragma unroll
-      for (int tb = 0; tb < 4; ++tb) {
+      for (int tb = 0; tb < NT; ++tb) {
         if (tb >= nt) break;
         dmma884(cm[ta][tb][0], cm[ta][tb][1], ws, cs[tb]);
         dmma884(ca[ta][tb][0], ca[ta][tb][1], cs[ta], cas[tb]);
+        dmma884(cm[ta][tb][0], cm[ta][tb][1], ws2, cs2[tb]);
+        dmma884(ca[ta][tb][0], ca[ta][tb][1], cs2[ta], cas2[tb]);
       }
     }
   }
@@ -341,9 +351,9 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
   for (int which = 0; which < 2; ++which) {
     __syncthreads();
 #pragma unroll
-    for (int ta = 0; ta < 4; ++ta)
+    for (int ta = 0; ta < NT; ++ta)
 #pragma unroll
-      for (int tb = 0; tb < 4; ++tb) {
+      for (int tb = 0; tb < NT; ++tb) {
         if (ta < nt && tb < nt) {
           const int row = 8 * ta + r, col = 8 * tb + 2 * cq;
           red[(w * 32 + row) * 32 + col] = which ? ca[ta][tb][0] : cm[ta][tb][0];
@@ -368,7 +378,7 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
 // for j < m (m <= 16).  Warp w handles groups of 8 cells; lane l's A fragment
 // is S_{k0 + l%4} at cell 8g + l/4 and its B fragments come from Y in shared
 // memory.  Every warp reads all ns columns of its 8 cells before writing them.
-template <typename T>
+template <typename T, int NK, int NJ, int STAGES>
 __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1, int n2, int m, const double* Y,
                                             int ncells, size_t ld) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -377,12 +387,13 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
   const int nk = (ns + 3) >> 2;
   const int nj = (m + 7) >> 3;
   const int ngrp = (ncells + 7) >> 3;
-  double av[8], an[8];
+  // STAGES groups ahead are loading while group gi is multiplied.
+  double av[NK], an[NK], an2[NK];
   auto load = [&](int gi, double* dst) {
     const int cell = 8 * gi + r;
     const bool in = cell < ncells;
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
+    for (int kk = 0; kk < NK; ++kk) {
       const int b = 4 * kk + cq;
       double v = 0.0;
       if (kk < nk && in && b < ns) {
@@ -397,18 +408,28 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
     }
   };
   if (w < ngrp) load(w, an);
+  if (STAGES > 1 && w + nwarp < ngrp) load(w + nwarp, an2);
   for (int gi = w; gi < ngrp; gi += nwarp) {
     const int cell = 8 * gi + r;
     const bool in = cell < ncells;
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) av[kk] = an[kk];
-    if (gi + nwarp < ngrp) load(gi + nwarp, an);
-    double dx[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, dp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int kk = 0; kk < NK; ++kk) {
+      av[kk] = an[kk];
+      if (STAGES > 1) an[kk] = an2[kk];
+    }
+    if (STAGES > 1) {
+      if (gi + 2 * nwarp < ngrp) load(gi + 2 * nwarp, an2);
+    } else {
+      if (gi + nwarp < ngrp) load(gi + nwarp, an);
+    }
+    double dx[NJ][2], dp[NJ][2];
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
+    for (int tj = 0; tj < NJ; ++tj) dx[tj][0] = dx[tj][1] = dp[tj][0] = dp[tj][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < NK; ++kk) {
       if (kk >= nk) break;
 #pragma unroll
-      for (int tj = 0; tj < 2; ++tj) {
+      for (int tj = 0; tj < NJ; ++tj) {
         if (tj >= nj) break;
         const int bb = 4 * kk + cq, jj = 8 * tj + r;
         const double y = (bb < ns && jj < m) ? Y[bb * LB_LD + jj] : 0.0;
@@ -419,7 +440,7 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
     }
     // D fragment: rows = cells 8gi + r, columns j = 8tj + 2cq + {0, 1}
 #pragma unroll
-    for (int tj = 0; tj < 2; ++tj) {
+    for (int tj = 0; tj < NJ; ++tj) {
       if (tj >= nj) break;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -970,7 +991,10 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       {
         Seg3<T> sS{{X, W, P}, {m, nact, np}, ld};
         Seg3<double> sA{{AX, AW, AP}, {m, nact, np}, ld};
-        cta_gram2_mma(sS, sA, Md, nc, mt.GM, mt.GA, mt.U);
+        if (nS <= 24)
+          cta_gram2_mma<T, double, 3>(sS, sA, Md, nc, mt.GM, mt.GA, mt.U);
+        else
+          cta_gram2_mma<T, double, 4>(sS, sA, Md, nc, mt.GM, mt.GA, mt.U);
       }
       pc.lap(4);
       pc.lap(5);
@@ -982,9 +1006,10 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       // ---- X <- S Y, P <- [W P] Y_WP, same for AX / AP (per cell, in place)
       // X <- S Y, P <- [W P] Y_WP and the same combination of the FP64 A-images, on the
       // FP64 tensor cores
-      cta_update_mma<T>(X, W, P, m, nact, np, m, mt.Y, nc, ld);
+      cta_update_mma<T, 8, 2, 1>(X, W, P, m, nact, np, m, mt.Y, nc, ld);
+      pc.lap(14);
       if (sizeof(T) == 8) {
-        cta_update_mma<double>(AX, AW, AP, m, nact, np, m, mt.Y, nc, ld);
+        cta_update_mma<double, 8, 2, 1>(AX, AW, AP, m, nact, np, m, mt.Y, nc, ld);
         __syncthreads();
       } else {
         // FP32 storage rounds X and P: their A-images are recomputed from the stored values

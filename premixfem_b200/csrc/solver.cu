@@ -114,6 +114,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_real("pmf_eig_sigma", &o->eig_sigma);
   db.get_int("pmf_eig_guard", &o->eig_guard);
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
+  db.get_int("pmf_eig_ctas", &o->eig_ctas);
   {
     auto it2 = db.kv.find("pmf_learned");
     if (it2 != db.kv.end()) {
@@ -576,7 +577,7 @@ int Solver::setup() {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int eig_blocks = std::min(nsub, nsm);
+  const int eig_blocks = std::min(nsub, opt.eig_ctas > 0 ? opt.eig_ctas : nsm);
   LobpcgArgs la;
   la.g = g;
   la.subs = d_subs;
@@ -640,8 +641,9 @@ int Solver::setup() {
   if (prof_eig) {  // diagnostics: cycles per LOBPCG phase, summed over CTAs
     std::vector<long long> hp(16 * eig_blocks);
     cudaMemcpy(hp.data(), d_prof, sizeof(long long) * hp.size(), cudaMemcpyDeviceToHost);
-    const char* names[14] = {"init",    "residual",  "precond",   "stencil",  "gram",     "pre_rr",   "update",
-                             "final",   "rr_scale",  "rr_chol",   "rr_basis", "rr_proj",  "rr_jacobi", "rr_coef"};
+    const char* names[15] = {"init",    "residual",  "precond",   "stencil",  "gram",     "pre_rr",   "update_aimg",
+                             "final",   "rr_scale",  "rr_chol",   "rr_basis", "rr_proj",  "rr_jacobi", "rr_coef",
+                             "update_mma"};
     long long tot[16] = {0}, mx = 0;
     for (int b = 0; b < eig_blocks; ++b) {
       long long sb = 0;
@@ -652,7 +654,7 @@ int Solver::setup() {
       mx = std::max(mx, sb);
     }
     fprintf(stderr, "[premixfem_b200] LOBPCG cycles per phase (sum over %d CTAs; slowest CTA %lld):", eig_blocks, mx);
-    for (int p = 0; p < 14; ++p) fprintf(stderr, " %s=%lld", names[p], tot[p]);
+    for (int p = 0; p < 15; ++p) fprintf(stderr, " %s=%lld", names[p], tot[p]);
     fprintf(stderr, "\n");
     cudaFree(d_prof);
   }

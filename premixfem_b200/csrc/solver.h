@@ -33,6 +33,7 @@ struct Options {
   double l3_tol = 1e-10;
   unsigned long long seed = 20240611ull;
   int pcg_chunk = 4;
+  int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
