@@ -840,7 +840,7 @@ PetscErrorCode PC_init(PCCtx* s_ctx, PetscScalar* dom, PetscInt* mesh) {
   s_ctx->use_W_cycle = o.use_W_cycle ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->no_shift_A_cc = o.no_shift_A_cc ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->use_full_Cholesky_lv1 = PETSC_FALSE;
-  s_ctx->use_2level = PETSC_FALSE;
+  s_ctx->use_2level = o.use_2level ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->H_x = dom[0] / (double)mesh[0];
   s_ctx->H_y = dom[1] / (double)mesh[1];
   s_ctx->H_z = dom[2] / (double)mesh[2];
@@ -901,6 +901,7 @@ PetscErrorCode PC_print_info(PCCtx* s_ctx) {
                         s_ctx->eigen_bd_lv1));
   PetscCall(PetscPrintf(PETSC_COMM_WORLD, "max_eigen_num_lv2=%d, eigen_bd_lv2=%.5E\n", s_ctx->max_eigen_num_lv2,
                         s_ctx->eigen_bd_lv2));
+  if (s_ctx->use_2level) PetscCall(PetscPrintf(PETSC_COMM_WORLD, "Only use the 2-level version!\n"));
   return 0;
 }
 
@@ -1017,7 +1018,7 @@ PetscErrorCode PC_print_stat(PCCtx* s_ctx) {
   }
   double mx2[2] = {0, 0}, mn2[2] = {0, 0};
   int num2[2] = {0, 0}, size3 = 0;
-  for (int r = 0; r < s->nrank; ++r) {
+  for (int r = 0; r < (int)s->ks3.size(); ++r) {
     const int k3 = s->ks3[r];
     const double a = s->eig3[(size_t)r * s->en2 + (k3 > 0 ? k3 - 1 : 0)], b = s->eig3[(size_t)r * s->en2];
     size3 += k3;

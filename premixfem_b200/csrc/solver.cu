@@ -137,10 +137,6 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
     *err = "-use_full_Cholesky_lv1 is not supported by this build (IC(0) only)";
     return 56;  // PETSC_ERR_SUP
   }
-  if (o->use_2level) {
-    *err = "-use_2level is not supported by this build (three-level cycle only)";
-    return 56;
-  }
   return 0;
 }
 
@@ -249,7 +245,7 @@ Solver::~Solver() {
                   state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  for (void* p : {(void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
+  for (void* p : {(void*)A2g, (void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
                   (void*)d_status_learned})
     if (p) cudaFree(p);
   delete net;
@@ -358,7 +354,13 @@ int Solver::build_partition() {
   nr = spr * kmax;
   en2 = std::min(opt.en_lv2, nr);
   n3 = nrank * en2;
-  if (nr > 4096 || n3 > 8192) {
+  if (opt.use_2level) {
+    if ((long long)nsub * kmax > 8192) {
+      err = "-use_2level: the global coarse problem (subdomains * en_lv1) must have <= 8192 unknowns for the "
+            "dense coarse solver";
+      return 56;
+    }
+  } else if (nr > 4096 || n3 > 8192) {
     err = "coarse blocks too large (subdomains per rank * en_lv1 <= 4096, ranks * en_lv2 <= 8192)";
     return 62;
   }
@@ -424,6 +426,12 @@ int Solver::set_dirichlet(int face, double value) {
 
 std::vector<int> Solver::schedule() const {
   std::vector<int> s;
+  if (opt.use_2level) {  // :1918-1922: [1] * si1, global coarse solve, [1] * si1
+    for (int i = 0; i < opt.si_lv1; ++i) s.push_back(1);
+    s.push_back(4);
+    for (int i = 0; i < opt.si_lv1; ++i) s.push_back(1);
+    return s;
+  }
   for (int i = 0; i < opt.si_lv1; ++i) s.push_back(1);
   for (int i = 0; i < opt.si_lv2; ++i) s.push_back(2);
   s.push_back(3);
@@ -713,6 +721,45 @@ int Solver::setup() {
     launch_galerkin<float>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const float*)phi, blk, gface, st);
   else
     launch_galerkin<double>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const double*)phi, blk, gface, st);
+  auto finish = [&]() -> int {
+    if (int er = check(cudaStreamSynchronize(st), "coarse setup")) return er;
+    if (int er = check(cudaGetLastError(), "coarse setup launch")) return er;
+    float ms[5];
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], e[i], e[i + 1]);
+    t_stages[ST_SU_LV1] += ms[0] * 1e-3;
+    t_stages[ST_SU_LV2_1] += ms[1] * 1e-3;
+    t_stages[ST_SU_LV2_2] += ms[2] * 1e-3;
+    t_stages[ST_SU_LV3_1] += ms[3] * 1e-3;
+    t_stages[ST_SU_LV3_2] += ms[4] * 1e-3;
+    float tot;
+    cudaEventElapsedTime(&tot, e[0], e[5]);
+    t_stages[ST_SU] += tot * 1e-3;
+    last_setup_ms = tot;
+    for (auto& x : e) cudaEventDestroy(x);
+    is_setup = true;
+    return 0;
+  };
+  if (opt.use_2level) {
+    // _PC_setup_lv2_c (:423-735): the global Galerkin matrix Phi^T A Phi over all
+    // subdomains (+ NIL I unless -no_shift_A_cc), inverted densely
+    const long long nc = (long long)nsub * kmax;
+    if (!A2g) {
+      if (int er = check(cudaMalloc(&A2g, sizeof(double) * nc * nc), "cudaMalloc global coarse matrix")) return er;
+    }
+    launch_assemble_dense(d_subs, nsub, 1, nsub, kmax, blk, gface, 0, A2g, st);
+    if (!opt.no_shift_A_cc) {
+      note_launch();
+      k_add_diag<<<1, 256, 0, st>>>(1, (int)nc, A2g, 1.0e-12, 0);
+    }
+    launch_spd_inverse(1, (int)nc, A2g, 1e-14, d_flag + 1, st);
+    cudaEventRecord(e[3], st);
+    cudaEventRecord(e[4], st);
+    cudaEventRecord(e[5], st);
+    eig3.clear();
+    ks3.clear();
+    l3_iters.clear();
+    return finish();
+  }
   launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 0, A2inv, st);
   launch_spd_inverse(nrank, nr, A2inv, 1e-14, d_flag + 1, st);
   cudaEventRecord(e[3], st);
@@ -751,8 +798,7 @@ int Solver::setup() {
     rnb[rr * 6 + 4] = at(rx, ry, rz - 1);
     rnb[rr * 6 + 5] = at(rx, ry, rz + 1);
   }
-  int* d_ks3 = nullptr;
-  cudaMalloc(&d_ks3, sizeof(int) * nrank);
+  if (!d_ks3) cudaMalloc(&d_ks3, sizeof(int) * nrank);
   cudaMemcpyAsync(d_ks3, ks3.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_rank_nb, rnb.data(), sizeof(int) * nrank * 6, cudaMemcpyHostToDevice, st);
   { note_launch(); k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3); }
@@ -762,23 +808,7 @@ int Solver::setup() {
                                        opt.no_shift_A_cc ? 0.0 : 1.0e-12); }
   launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
   cudaEventRecord(e[5], st);
-  if (int er = check(cudaStreamSynchronize(st), "coarse setup")) return er;
-  if (int er = check(cudaGetLastError(), "coarse setup launch")) return er;
-  cudaFree(d_ks3);
-  float ms[5];
-  for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], e[i], e[i + 1]);
-  t_stages[ST_SU_LV1] += ms[0] * 1e-3;
-  t_stages[ST_SU_LV2_1] += ms[1] * 1e-3;
-  t_stages[ST_SU_LV2_2] += ms[2] * 1e-3;
-  t_stages[ST_SU_LV3_1] += ms[3] * 1e-3;
-  t_stages[ST_SU_LV3_2] += ms[4] * 1e-3;
-  float tot;
-  cudaEventElapsedTime(&tot, e[0], e[5]);
-  t_stages[ST_SU] += tot * 1e-3;
-  last_setup_ms = tot;
-  for (auto& x : e) cudaEventDestroy(x);
-  is_setup = true;
-  return 0;
+  return finish();
 }
 
 template <typename T>
@@ -826,6 +856,8 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
       }
       if (v == 2) {
         launch_block_gemv(nrank, nr, A2inv, c, dz, 0, done, st);
+      } else if (v == 4) {  // _PC_apply_vec_lv2_2level (:1481-1537)
+        launch_block_gemv(1, (int)ncoarse, A2g, c, dz, 0, done, st);
       } else {
         launch_lv3_restrict(nrank, nr, en2, V3, c, d3, done, st);
         launch_block_gemv(1, n3, A3inv, d3, w3, 0, done, st);

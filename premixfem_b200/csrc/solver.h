@@ -137,6 +137,8 @@ class Solver {
   float* net_y = nullptr;  // network output for every subdomain [nsub][4096][16]
   int* d_queue = nullptr;
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
+  int* d_ks3 = nullptr;
+  double* A2g = nullptr;  // -use_2level: inverse of the global coarse matrix
   int *d_fail_list = nullptr, *d_fail_count = nullptr, *d_iters_learned = nullptr, *d_status_learned = nullptr;
   int learned_used = 0, learned_fallbacks = 0;
   long long learned_iters = 0, fallback_iters = 0;

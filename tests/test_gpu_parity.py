@@ -160,3 +160,33 @@ def test_bad_arguments_return_errors(native):
         s.setup()  # kappa not set
     assert e.value.code == 73
     s.close()
+
+
+TWO_LEVEL = {
+    "grf16_2level": (lambda: fields.unit_cube_grf(16, seed=2),
+                     {"sd": 2, "pmf_vranks": (2, 2, 1), "en_lv1": 4, "use_2level": True}),
+    "aniso_2level_si2": (lambda: dict(fields.aniso_const(8, 8, 8), dirichlet={"z+": 1.0}),
+                         {"sd": 2, "en_lv1": 3, "use_2level": True, "si_lv1": 2}),
+}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", list(TWO_LEVEL))
+def test_two_level_matches_oracle(native, name, precision):
+    """-use_2level (_PC_setup_lv2_c / _PC_apply_vec_lv2_2level): one preconditioner
+    application (FP64 only, 1e-6) and the PCG iterations (+-1) and solution (1e-8)."""
+    mk, d = TWO_LEVEL[name]
+    prob = mk()
+    ref = O.solve(prob, _oracle_opts(d))
+    s = _gpu(prob, dict(d, pmf_precision=precision))
+    if precision == "fp64":
+        x = np.random.default_rng(12).standard_normal(ref["op"].n)
+        y, yr = s.pc_apply(x), ref["pc"].apply(x)
+        assert np.linalg.norm(y - yr) <= 1e-6 * np.linalg.norm(yr)
+    b = s.rhs(prob["source"].ravel())
+    x, its, rnorm, reason = s.solve(b)
+    assert reason == "converged"
+    assert abs(its - ref["its"]) <= 1, f"iterations {its} vs oracle {ref['its']}"
+    xd = O.direct_solve(ref["op"], ref["b"])
+    assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+    s.close()
