@@ -20,6 +20,8 @@
 // returned eigenvalues and the normalisation v^T M v = 1 (the GHEP
 // normalisation SLEPc returns).
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "pmf_dense.cuh"
 #include "pmf_kernels.h"
@@ -46,8 +48,9 @@ __host__ __device__ inline int lb_ld(int max_cells) { return (max_cells + 63) & 
 
 size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes) {
   const size_t ld = lb_ld(max_cells);
-  // X, W, P in the storage precision; their A-images always FP64; M, Neumann diagonal
-  return (size_t)3 * m * ld * prec_bytes + (size_t)3 * m * ld * sizeof(double) + (size_t)3 * ld * sizeof(double);
+  // X, W, P in the storage precision; their A-images always FP64; M, Neumann diagonals
+  return (size_t)3 * m * ld * prec_bytes + (size_t)3 * m * ld * sizeof(double) + (size_t)3 * ld * sizeof(double) +
+         (size_t)4 * ld * sizeof(float);  // + IC(0) sweep coefficients (batched solver)
 }
 
 __device__ __forceinline__ double avg_k(double a, double b) { return 2.0 / (1.0 / a + 1.0 / b); }
@@ -650,6 +653,14 @@ __device__ __forceinline__ void neumann_apply_col(const Grid& g, const SubInfo& 
   }
 }
 
+// Per-subdomain iteration state of the phase-batched solver (global memory).
+struct EbState {
+  double lam[LB_MM];
+  double lscale, best;
+  int act[LB_MM];
+  int nact, np, nS, hasP, done, conv, stag, it, last_improve, restart;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned char* work, size_t work_stride, T* phi,
                                                 double* evals, int* iters, int* status, int* ks, double eb) {
@@ -671,7 +682,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
   PhaseClock pc{a.prof ? a.prof + (size_t)blockIdx.x * 16 : nullptr, 0};
   pc.start();
 
-  const int count = a.sub_list ? *a.nlist : a.nsub;
+  const int count = (a.sub_list && a.nlist) ? *a.nlist : a.nsub;
   __shared__ int s_next;
   for (int idx = blockIdx.x;; idx += gridDim.x) {
     if (a.queue) {  // dynamic schedule: take the next unclaimed subdomain
@@ -684,7 +695,8 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     const int s = a.sub_list ? a.sub_list[idx] : idx;
     const SubInfo S = a.subs[s];
     const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
-    T* X = reinterpret_cast<T*>(wb);
+    unsigned char* wbs = a.mode ? a.slab + (size_t)s * a.slab_stride : wb;
+    T* X = reinterpret_cast<T*>(wbs);
     T* W = X + (size_t)m * ld;
     T* P = W + (size_t)m * ld;
     double* AX = reinterpret_cast<double*>(P + (size_t)m * ld);
@@ -694,6 +706,16 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     double* dN = Md + ld;
     double* dN32 = dN + ld;  // diagonal matching the FP32-rounded couplings (FP32 storage)
 
+    bool hasP = false;
+    int it = 0;
+    bool conv = false;
+    if (a.mode == 2) {  // final phase of the batched solver: the state comes from the slab
+      const EbState* es = reinterpret_cast<const EbState*>(a.state) + s;
+      it = es->it;
+      conv = es->conv != 0;
+      if (threadIdx.x == 0) sm.ival[6] = es->stag;
+      __syncthreads();
+    } else {
     // ---- mass diagonal (src/PreMixFEM_3D.c:243-346), Neumann diagonal, sweep coefficients
     double ratio = 0.0;
     for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
@@ -839,9 +861,6 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     }
     __syncthreads();
 
-    bool hasP = false;
-    int it = 0;
-    bool conv = false;
     if (threadIdx.x == 0) {
       sm.scal[2] = 1e300;
       sm.ival[5] = 0;
@@ -849,6 +868,32 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     }
     __syncthreads();
     pc.lap(0);
+    if (a.mode == 1) {  // set-up phase of the batched solver: keep coefficients and state
+      EbState* es = reinterpret_cast<EbState*>(a.state) + s;
+      float* gc = reinterpret_cast<float*>(dN32 + ld);
+      for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+        gc[cl] = ctx[cl];
+        gc[(size_t)ld + cl] = cty[cl];
+        gc[(size_t)2 * ld + cl] = ctz[cl];
+        gc[(size_t)3 * ld + cl] = cinv[cl];
+      }
+      if (threadIdx.x < m) es->lam[threadIdx.x] = sm.lam[threadIdx.x];
+      if (threadIdx.x == 0) {
+        es->lscale = lscale;
+        es->best = 1e300;
+        es->last_improve = 0;
+        es->hasP = 0;
+        es->done = 0;
+        es->conv = 0;
+        es->stag = 0;
+        es->it = 0;
+        es->restart = 0;
+        es->nact = 0;
+        es->np = 0;
+        es->nS = m;
+      }
+      continue;
+    }
     for (; it < a.max_it; ++it) {
       // ---- residuals R = AX - M X Lambda (into W) and ||R_j||_{M^-1}
       double racc[LB_MM];
@@ -1029,6 +1074,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       hasP = true;
       pc.lap(6);
     }
+    }  // mode != 2
 
     // ---- final FP64 Rayleigh-Ritz on X (A X recomputed in FP64 over the W|P slab)
     double* AX64 = AX;
@@ -1129,5 +1175,447 @@ template void launch_lobpcg<float>(const LobpcgArgs&, int, void*, float*, double
                                    cudaStream_t);
 template void launch_lobpcg<double>(const LobpcgArgs&, int, void*, double*, double*, int*, int*, int*, double, int,
                                     int, cudaStream_t);
+
+
+// ============================================================================
+// Phase-batched LOBPCG.  The iteration of k_lobpcg, one launch per phase over
+// every active subdomain, the block vectors of all subdomains resident in HBM
+// (per-subdomain slabs: X, W, P, their FP64 A-images, M, the Neumann
+// diagonals and the IC(0) sweep coefficients).  Set-up and the final
+// Rayleigh-Ritz are k_lobpcg's own code (modes 1 and 2).  Each phase is a
+// separate grid (subdomain x cell chunk or column batch), so many more warps
+// per SM are in flight than in the one-CTA-per-SM persistent kernel; partial
+// sums are reduced in a fixed order, so results do not depend on scheduling.
+
+namespace {
+
+constexpr int EB_CHUNK = 1024;  // cells per Gram / residual / update chunk
+
+template <typename T>
+struct EbSlab {
+  T *X, *W, *P;
+  double *AX, *AW, *AP, *Md, *dN, *dN32;
+  float *ctx, *cty, *ctz, *cinv;
+  __device__ EbSlab(unsigned char* base, int m, int ld) {
+    X = reinterpret_cast<T*>(base);
+    W = X + (size_t)m * ld;
+    P = W + (size_t)m * ld;
+    AX = reinterpret_cast<double*>(P + (size_t)m * ld);
+    AW = AX + (size_t)m * ld;
+    AP = AW + (size_t)m * ld;
+    Md = AP + (size_t)m * ld;
+    dN = Md + ld;
+    dN32 = dN + ld;
+    ctx = reinterpret_cast<float*>(dN32 + ld);
+    cty = ctx + ld;
+    ctz = cty + ld;
+    cinv = ctz + ld;
+  }
+};
+
+struct EbArgs {
+  Grid g;
+  const SubInfo* subs;
+  const int* list;
+  int m, k, ld, ldc, mb, nchunk, max_it;
+  double tol;
+  unsigned char* slab;
+  size_t slab_stride;
+  EbState* state;
+  double* Ybuf;
+  double* gpart;
+  double* rpart;
+  int* nactive;
+  int* alist;  // subdomains still iterating, compacted by k_eb_control
+  const double *tx, *ty, *tz;
+};
+
+// Phase kernels index the compacted active list; the control kernel the full list.
+__device__ __forceinline__ int eb_sub(const EbArgs& a, int idx) { return a.alist[idx]; }
+
+// Partial ||AX_j - lambda_j M X_j||^2_{M^-1} over one chunk of cells.
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_resid(EbArgs a, int use_alist) {
+  __shared__ double red[32];
+  const int s = use_alist ? a.alist[blockIdx.y] : (a.list ? a.list[blockIdx.y] : (int)blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK, c1 = min(nc, c0 + EB_CHUNK);
+  double* out = a.rpart + ((size_t)s * a.nchunk + blockIdx.x) * LB_MM;
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  for (int j = 0; j < a.m; ++j) {
+    const double lam = es.lam[j];
+    double acc = 0.0;
+    for (int cl = c0 + threadIdx.x; cl < c1; cl += blockDim.x) {
+      const double mv = sl.Md[cl];
+      const double r = sl.AX[(size_t)j * a.ld + cl] - lam * mv * (double)sl.X[(size_t)j * a.ld + cl];
+      acc += r * r / mv;
+    }
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) out[j] = acc;
+  }
+}
+
+// Convergence, soft locking and the rounding-floor test of k_lobpcg, one
+// thread per subdomain.
+__global__ void k_eb_control(EbArgs a, int nlist, int it) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nlist) return;
+  const int s = a.list ? a.list[idx] : idx;
+  EbState& es = a.state[s];
+  if (es.done) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int nch = (nc + EB_CHUNK - 1) / EB_CHUNK;
+  const int m = a.m, k = a.k;
+  int na = 0, cv = 1;
+  double worst = 0.0;
+  for (int j = 0; j < m; ++j) {
+    double v = 0.0;
+    for (int c = 0; c < nch; ++c) v += a.rpart[((size_t)s * a.nchunk + c) * LB_MM + j];
+    const double res = sqrt(v) / es.lscale;
+    const bool done_j = res <= a.tol;
+    if (j < k) worst = fmax(worst, res);
+    if (j < k && !done_j) cv = 0;
+    if (!done_j || j >= k) es.act[na++] = j;
+  }
+  if (!cv) {
+    if (worst < 0.5 * es.best) {
+      es.best = worst;
+      es.last_improve = it;
+    } else if (it - es.last_improve >= 12 && worst <= 10.0 * a.tol) {
+      cv = 1;
+      es.stag = 1;
+    }
+  }
+  if (cv) {
+    es.done = 1;
+    es.conv = 1;
+    es.it = it;
+    return;
+  }
+  es.nact = na;
+  es.np = es.hasP ? m : 0;
+  es.nS = m + na + es.np;
+  es.it = it + 1;  // iterations counted if the iteration limit ends the solve
+  a.alist[atomicAdd(a.nactive, 1)] = s;  // order is irrelevant: subdomains are independent
+}
+
+// W_c = T (AX_a - lambda_a M X_a) for active columns c (a = act[c]) of one
+// column batch: IC(0) sweeps of A^N + sigma M in shared memory (FP32), and in
+// FP32 storage the FP64 A-image with the FP32-rounded couplings.
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_precond(EbArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int s = eb_sub(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done) return;
+  const int c0 = blockIdx.x * a.mb;
+  const int nb = min(a.mb, es.nact - c0);
+  if (nb <= 0) return;
+  const SubInfo S = a.subs[s];
+  const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
+  const int ldc = a.ldc, ld = a.ld;
+  float* ctx = reinterpret_cast<float*>(smraw);
+  float* cty = ctx + ldc;
+  float* ctz = cty + ldc;
+  float* cinv = ctz + ldc;
+  float* u = cinv + ldc;
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, ld);
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+    ctx[cl] = sl.ctx[cl];
+    cty[cl] = sl.cty[cl];
+    ctz[cl] = sl.ctz[cl];
+    cinv[cl] = sl.cinv[cl];
+  }
+  for (int b = 0; b < nb; ++b) {
+    const int col = es.act[c0 + b];
+    const double lam = es.lam[col];
+    for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+      const double r = sl.AX[(size_t)col * ld + cl] - lam * sl.Md[cl] * (double)sl.X[(size_t)col * ld + cl];
+      u[(size_t)b * ldc + cl] = (float)(T)r;
+    }
+  }
+  __syncthreads();
+  const int t = threadIdx.x, jj = t % ny, kk = t / ny;
+  const bool line = t < ny * nz;
+  const int nplanes = nx + ny + nz - 2;
+  for (int d = 0; d < nplanes; ++d) {
+    const int i = d - jj - kk;
+    if (line && i >= 0 && i < nx) {
+      const int cl = (kk * ny + jj) * nx + i;
+      const float cz_ = ctz[cl], cy_ = cty[cl], cx_ = ctx[cl], ci = cinv[cl];
+#pragma unroll 4
+      for (int b = 0; b < nb; ++b) {
+        float* ub = u + b * ldc;
+        float sacc = ub[cl];
+        if (kk > 0) sacc += cz_ * ub[cl - nxny];
+        if (jj > 0) sacc += cy_ * ub[cl - nx];
+        if (i > 0) sacc += cx_ * ub[cl - 1];
+        ub[cl] = sacc * ci;
+      }
+    }
+    __syncthreads();
+  }
+  for (int d = nplanes - 1; d >= 0; --d) {
+    const int i = d - jj - kk;
+    if (line && i >= 0 && i < nx) {
+      const int cl = (kk * ny + jj) * nx + i;
+      const float cxp = i < nx - 1 ? ctx[cl + 1] : 0.0f;
+      const float cyp = jj < ny - 1 ? cty[cl + nx] : 0.0f;
+      const float czp = kk < nz - 1 ? ctz[cl + nxny] : 0.0f;
+      const float ci = cinv[cl];
+#pragma unroll 4
+      for (int b = 0; b < nb; ++b) {
+        float* ub = u + b * ldc;
+        float sacc = 0.0f;
+        if (i < nx - 1) sacc += cxp * ub[cl + 1];
+        if (jj < ny - 1) sacc += cyp * ub[cl + nx];
+        if (kk < nz - 1) sacc += czp * ub[cl + nxny];
+        ub[cl] = ub[cl] + sacc * ci;
+      }
+    }
+    __syncthreads();
+  }
+  if (sizeof(T) == 4) smem_neumann64(u, ldc, nb, nx, ny, nz, ctx, cty, ctz, sl.dN32, sl.AW + (size_t)c0 * ld, ld);
+  store_cols_from_smem(sl.W + (size_t)c0 * ld, ld, nb, nc, u, ldc);
+}
+
+// FP64 A-images: out_j = A v_j for columns j of the block chosen by `which`
+// (0: W -> AW, FP64 operator; 1: X -> AX and P -> AP, FP32-rounded couplings).
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_aimg(EbArgs a, int which) {
+  const int s = eb_sub(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done || (which == 1 && es.restart)) return;
+  const int col = blockIdx.x;
+  const SubInfo S = a.subs[s];
+  const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
+  const int ld = a.ld;
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, ld);
+  if (which == 0) {
+    if (col >= es.nact) return;
+    neumann_apply_col(a.g, S, a.tx, a.ty, a.tz, sl.dN, sl.W + (size_t)col * ld, sl.AW + (size_t)col * ld, nc);
+    return;
+  }
+  const bool isP = col >= a.m;
+  const int j = isP ? col - a.m : col;
+  const T* v = (isP ? sl.P : sl.X) + (size_t)j * ld;
+  double* out = (isP ? sl.AP : sl.AX) + (size_t)j * ld;
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+    const int i = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
+    double r = sl.dN32[cl] * (double)(float)v[cl];
+    if (i > 0) r -= (double)sl.ctx[cl] * (double)(float)v[cl - 1];
+    if (i < nx - 1) r -= (double)sl.ctx[cl + 1] * (double)(float)v[cl + 1];
+    if (jj > 0) r -= (double)sl.cty[cl] * (double)(float)v[cl - nx];
+    if (jj < ny - 1) r -= (double)sl.cty[cl + nx] * (double)(float)v[cl + nx];
+    if (kk > 0) r -= (double)sl.ctz[cl] * (double)(float)v[cl - nxny];
+    if (kk < nz - 1) r -= (double)sl.ctz[cl + nxny] * (double)(float)v[cl + nxny];
+    out[cl] = r;
+  }
+}
+
+// Partial Grams (w S)^T S and S^T (A S), S = [X W P], over one chunk of cells.
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_eb_gram(EbArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* red = reinterpret_cast<double*>(smraw);
+  const int s = eb_sub(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int cn = min(nc - c0, EB_CHUNK);
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  double* G = a.gpart + ((size_t)s * a.nchunk + blockIdx.x) * 2 * LB_LD * LB_LD;
+  Seg3<T> sS{{sl.X + c0, sl.W + c0, sl.P + c0}, {a.m, es.nact, es.np}, a.ld};
+  Seg3<double> sA{{sl.AX + c0, sl.AW + c0, sl.AP + c0}, {a.m, es.nact, es.np}, a.ld};
+  if (es.nS <= 24)
+    cta_gram2_mma<T, double, 3>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+  else
+    cta_gram2_mma<T, double, 4>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+}
+
+// Rayleigh-Ritz on the chunk-summed Grams (k_lobpcg's cta_rayleigh_ritz).
+__global__ void __launch_bounds__(256) k_eb_rr(EbArgs a, double drop) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  LbSmall& sm = *reinterpret_cast<LbSmall*>(smraw);
+  LbMats& mt = *reinterpret_cast<LbMats*>(smraw + sizeof(LbSmall));
+  const int s = eb_sub(a, blockIdx.x);
+  EbState& es = a.state[s];
+  if (es.done) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int nch = (nc + EB_CHUNK - 1) / EB_CHUNK;
+  const int nS = es.nS, m = a.m;
+  for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
+    const int r = e / nS, c = e % nS;
+    double gm = 0.0, ga = 0.0;
+    for (int q = 0; q < nch; ++q) {
+      const double* G = a.gpart + ((size_t)s * a.nchunk + q) * 2 * LB_LD * LB_LD;
+      gm += G[r * LB_LD + c];
+      ga += G[LB_LD * LB_LD + r * LB_LD + c];
+    }
+    mt.GM[r * LB_LD + c] = gm;
+    mt.GA[r * LB_LD + c] = ga;
+  }
+  if (threadIdx.x < LB_MM) sm.lam[threadIdx.x] = threadIdx.x < m ? es.lam[threadIdx.x] : 0.0;
+  if (threadIdx.x == 0) sm.scal[0] = es.lscale;
+  __syncthreads();
+  const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop, 1e-11);
+  double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int e = threadIdx.x; e < nS * m; e += blockDim.x) {
+    const int r = e / m, c = e % m;
+    Y[r * LB_LD + c] = mt.Y[r * LB_LD + c];
+  }
+  if (threadIdx.x < m) es.lam[threadIdx.x] = sm.lam[threadIdx.x];
+  if (threadIdx.x == 0) {
+    es.restart = q < m ? 1 : 0;  // basis collapsed: no update, next iteration without P
+    es.hasP = q < m ? 0 : 1;
+  }
+}
+
+// X <- S Y, P <- [W P] Y_WP (and the FP64 A-images in FP64 storage), per chunk.
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_eb_update(EbArgs a) {
+  __shared__ double Ys[LB_LD * LB_LD];
+  const int s = eb_sub(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done || es.restart) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int cn = min(nc - c0, EB_CHUNK);
+  const double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int e = threadIdx.x; e < es.nS * LB_LD; e += blockDim.x) Ys[e] = Y[e];
+  __syncthreads();
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  const int m = a.m;
+  cta_update_mma<T, 8, 2, 1>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+  if (sizeof(T) == 8) cta_update_mma<double, 8, 2, 1>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+}
+
+}  // namespace
+
+size_t lobpcg_batched_slab_bytes(int max_cells, int m, int prec_bytes) {
+  return (lobpcg_work_bytes(max_cells, m, prec_bytes) + 255) & ~(size_t)255;
+}
+size_t lobpcg_batched_state_bytes() { return sizeof(EbState); }
+int lobpcg_batched_nchunk(int max_cells) { return (max_cells + EB_CHUNK - 1) / EB_CHUNK; }
+
+template <typename T>
+int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int* list, int nlist, T* phi,
+                          double* evals, int* iters, int* status, int* ks, double eb, int max_cells, int max_lines,
+                          cudaStream_t st) {
+  if (nlist <= 0) return 0;
+  // set-up phase: k_lobpcg mode 1 into the per-subdomain slabs
+  LobpcgArgs a = a_in;
+  a.slab = b.slab;
+  a.slab_stride = b.slab_stride;
+  a.state = b.state;
+  a.sub_list = list;
+  a.nlist = nullptr;
+  a.nsub = list ? nlist : a_in.nsub;
+  const int ctas = 148;
+  a.mode = 1;
+  launch_lobpcg<T>(a, std::min(ctas, nlist), nullptr, phi, evals, iters, status, ks, eb, max_cells, max_lines, st);
+  EbArgs e;
+  e.g = a.g;
+  e.subs = a.subs;
+  e.list = list;
+  e.m = a.m;
+  e.k = a.k;
+  e.ld = lb_ld(max_cells);
+  e.ldc = (max_cells + 3) & ~3;
+  e.nchunk = b.nchunk;
+  e.max_it = a.max_it;
+  e.tol = a.tol;
+  e.slab = b.slab;
+  e.slab_stride = b.slab_stride;
+  e.state = reinterpret_cast<EbState*>(b.state);
+  e.Ybuf = b.Ybuf;
+  e.gpart = b.gpart;
+  e.rpart = b.rpart;
+  e.nactive = b.nactive;
+  e.alist = b.alist;
+  e.tx = a.tx;
+  e.ty = a.ty;
+  e.tz = a.tz;
+  // column batch of the preconditioner: coefficients + mb vectors within ~113 KB (2 CTAs per SM)
+  const size_t coef = (size_t)16 * e.ldc;
+  e.mb = (int)std::max<size_t>(1, std::min<size_t>(a.m, (112 * 1024 - coef) / ((size_t)4 * e.ldc)));
+  const size_t pre_smem = coef + (size_t)4 * e.ldc * e.mb;
+  const size_t gram_smem = (size_t)8 * 32 * 32 * sizeof(double);
+  const size_t rr_smem = sizeof(LbSmall) + sizeof(LbMats);
+  cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem);
+  cudaFuncSetAttribute(k_eb_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem);
+  cudaFuncSetAttribute(k_eb_rr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem);
+  const double drop = sizeof(T) == 4 ? 1e-9 : 1e-13;
+  // optional diagnostics (PMF_PROFILE_EIGEN): device time per phase
+  const bool prof = getenv("PMF_PROFILE_EIGEN") != nullptr;
+  cudaEvent_t pev[9];
+  float ptot[8] = {0};
+  if (prof)
+    for (auto& x : pev) cudaEventCreate(&x);
+  auto mark = [&](int i) {
+    if (prof) cudaEventRecord(pev[i], st);
+  };
+  mark(0);
+  int nact = nlist;
+  for (int it = 0; it < a.max_it; ++it) {
+    // residual norms of the subdomains still iterating (all of them at it = 0)
+    mark(1);
+    { note_launch(); k_eb_resid<T><<<dim3(e.nchunk, nact), 256, 0, st>>>(e, it > 0 ? 1 : 0); }
+    cudaMemsetAsync(b.nactive, 0, sizeof(int), st);
+    { note_launch(); k_eb_control<<<(nlist + 127) / 128, 128, 0, st>>>(e, nlist, it); }
+    cudaMemcpyAsync(b.h_nactive, b.nactive, sizeof(int), cudaMemcpyDeviceToHost, st);
+    mark(2);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 76;
+    if (prof) {
+      float ms;
+      cudaEventElapsedTime(&ms, pev[1], pev[2]);
+      ptot[0] += ms;
+    }
+    nact = *b.h_nactive;
+    if (nact == 0) break;
+    const dim3 gchunk(e.nchunk, nact), gpre((a.m + e.mb - 1) / e.mb, nact);
+    { note_launch(); k_eb_precond<T><<<gpre, 256, pre_smem, st>>>(e); }
+    if (sizeof(T) == 8) { note_launch(); k_eb_aimg<T><<<dim3(a.m, nact), 256, 0, st>>>(e, 0); }
+    mark(3);
+    { note_launch(); k_eb_gram<T><<<gchunk, 256, gram_smem, st>>>(e); }
+    mark(4);
+    { note_launch(); k_eb_rr<<<nact, 256, rr_smem, st>>>(e, drop); }
+    mark(5);
+    { note_launch(); k_eb_update<T><<<gchunk, 256, 0, st>>>(e); }
+    if (sizeof(T) == 4) { note_launch(); k_eb_aimg<T><<<dim3(2 * a.m, nact), 256, 0, st>>>(e, 1); }
+    mark(6);
+    if (prof) {
+      cudaEventSynchronize(pev[6]);
+      float ms;
+      for (int q = 2; q < 6; ++q) {
+        cudaEventElapsedTime(&ms, pev[q], pev[q + 1]);
+        ptot[q - 1] += ms;
+      }
+    }
+  }
+  if (prof) {
+    fprintf(stderr, "[premixfem_b200] batched LOBPCG ms: resid+control %.2f precond %.2f gram %.2f rr %.2f update %.2f\n",
+            ptot[0], ptot[1], ptot[2], ptot[3], ptot[4]);
+    for (auto& x : pev) cudaEventDestroy(x);
+  }
+  // final phase: k_lobpcg mode 2 (FP64 Rayleigh-Ritz, adaptive count, output)
+  a.mode = 2;
+  launch_lobpcg<T>(a, std::min(ctas, nlist), nullptr, phi, evals, iters, status, ks, eb, max_cells, max_lines, st);
+  return cudaGetLastError() == cudaSuccess ? 0 : 76;
+}
+template int launch_lobpcg_batched<float>(const LobpcgArgs&, const EbBuffers&, const int*, int, float*, double*, int*,
+                                          int*, int*, double, int, int, cudaStream_t);
+template int launch_lobpcg_batched<double>(const LobpcgArgs&, const EbBuffers&, const int*, int, double*, double*,
+                                           int*, int*, int*, double, int, int, cudaStream_t);
 
 }  // namespace pmf

@@ -130,6 +130,13 @@ struct LobpcgArgs {
   // optional work queue (one device int, zeroed by the launcher): CTAs take the
   // next subdomain with atomicAdd instead of the fixed stride blockIdx.x + k*gridDim.x
   int* queue;
+  // phase-batched solver: 0 = whole solve in this kernel (per-CTA work slab);
+  // 1 = set-up only (mass, IC(0) pivots, initial block and Rayleigh-Ritz) into
+  // the per-subdomain slab and state; 2 = final Rayleigh-Ritz and output from them
+  int mode;
+  unsigned char* slab;  // per-subdomain work slabs (modes 1, 2), stride slab_stride
+  size_t slab_stride;
+  void* state;          // per-subdomain EbState array (modes 1, 2)
   int dirichlet_mask;   // bit f set: face f (x-,x+,y-,y+,z-,z+) is a Dirichlet face
   int ld;               // column stride of the work block vectors (set by the launcher)
   int ldc;              // stride of the shared-memory sweep arrays (set by the launcher)
@@ -145,6 +152,30 @@ size_t lobpcg_work_bytes(int max_cells, int m, int prec_bytes);
 template <typename T>
 void launch_lobpcg(const LobpcgArgs& a, int nblocks, void* work, T* phi, double* evals, int* iters, int* status,
                    int* ks, double eb, int max_cells, int max_lines, cudaStream_t st);
+
+// Phase-batched LOBPCG: the same iteration as launch_lobpcg, but each phase
+// (residual norms, convergence control, IC(0)-preconditioned directions,
+// A-images, Grams, Rayleigh-Ritz, basis update) is its own launch over every
+// active subdomain, with the block vectors of all subdomains resident in HBM.
+struct EbBuffers {
+  unsigned char* slab = nullptr;  // nsub x slab_stride
+  size_t slab_stride = 0;
+  void* state = nullptr;          // nsub EbState
+  double* Ybuf = nullptr;         // nsub x 32 x 32 Rayleigh-Ritz coefficients
+  double* gpart = nullptr;        // nsub x nchunk x 2 x 32 x 32 partial Grams
+  double* rpart = nullptr;        // nsub x nchunk x LB_MM partial residual norms
+  int* nactive = nullptr;         // device counter
+  int* alist = nullptr;           // nsub: compacted list of subdomains still iterating
+  int* h_nactive = nullptr;       // pinned host copy
+  int nchunk = 0;
+};
+size_t lobpcg_batched_slab_bytes(int max_cells, int m, int prec_bytes);
+size_t lobpcg_batched_state_bytes();
+int lobpcg_batched_nchunk(int max_cells);
+// list (device) / nlist (host): subdomains to solve, or nullptr for all a.nsub.
+template <typename T>
+int launch_lobpcg_batched(const LobpcgArgs& a, const EbBuffers& b, const int* list, int nlist, T* phi, double* evals,
+                          int* iters, int* status, int* ks, double eb, int max_cells, int max_lines, cudaStream_t st);
 
 // Level-3 eigenpairs: smallest en2 of dense symmetric A[r] (nr x nr), via subspace
 // iteration with the inverse of (A + mu I) (given as inv) and Rayleigh-Ritz.

@@ -115,6 +115,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_guard", &o->eig_guard);
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
   db.get_int("pmf_eig_ctas", &o->eig_ctas);
+  db.get_int("pmf_eig_batched", &o->eig_batched);
   {
     auto it2 = db.kv.find("pmf_learned");
     if (it2 != db.kv.end()) {
@@ -245,6 +246,10 @@ Solver::~Solver() {
                   state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart, (void*)eb.nactive,
+                  (void*)eb.alist})
+    if (p) cudaFree(p);
+  if (eb.h_nactive) cudaFreeHost(eb.h_nactive);
   for (void* p : {(void*)A2g, (void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
                   (void*)d_status_learned})
     if (p) cudaFree(p);
@@ -474,6 +479,59 @@ int Solver::assemble() {
   return check(cudaStreamSynchronize(st), "assemble");
 }
 
+int Solver::alloc_eb(int m, bool mixed) {
+  const size_t stride = lobpcg_batched_slab_bytes(max_cells, m, mixed ? 4 : 8);
+  if (eb.slab && eb.slab_stride == stride) return 0;
+  for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart})
+    if (p) cudaFree(p);
+  eb.slab_stride = stride;
+  eb.nchunk = lobpcg_batched_nchunk(max_cells);
+  const size_t ns = (size_t)nsub;
+  if (int e = check(cudaMalloc(&eb.slab, ns * stride), "cudaMalloc eigensolver slabs")) return e;
+  if (int e = check(cudaMalloc(&eb.state, ns * lobpcg_batched_state_bytes()), "cudaMalloc eigensolver state")) return e;
+  if (int e = check(cudaMalloc(&eb.Ybuf, ns * 32 * 32 * sizeof(double)), "cudaMalloc eigensolver Y")) return e;
+  if (int e = check(cudaMalloc(&eb.gpart, ns * eb.nchunk * 2 * 32 * 32 * sizeof(double)), "cudaMalloc Grams"))
+    return e;
+  if (int e = check(cudaMalloc(&eb.rpart, ns * eb.nchunk * 10 * sizeof(double)), "cudaMalloc residuals")) return e;
+  if (!eb.nactive) cudaMalloc(&eb.nactive, sizeof(int));
+  if (eb.alist) cudaFree(eb.alist);
+  cudaMalloc(&eb.alist, ns * sizeof(int));
+  if (!eb.h_nactive) cudaMallocHost(&eb.h_nactive, sizeof(int));
+  return 0;
+}
+
+// The batched local eigensolves over `list` (nullptr: every subdomain), with
+// the phase-batched solver or the single persistent launch.
+int Solver::run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1) {
+  const bool mixed = opt.precision == 1;
+  if (!opt.eig_batched) {
+    if (list) {
+      la.sub_list = list;
+      la.nlist = d_fail_count;
+    }
+    if (mixed)
+      launch_lobpcg<float>(la, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                           max_lines, st);
+    else
+      launch_lobpcg<double>(la, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
+                            max_cells, max_lines, st);
+    return 0;
+  }
+  if (int e = alloc_eb(la.m, mixed)) return e;
+  int r;
+  if (mixed)
+    r = launch_lobpcg_batched<float>(la, eb, list, nlist, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
+                                     max_cells, max_lines, st);
+  else
+    r = launch_lobpcg_batched<double>(la, eb, list, nlist, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
+                                      max_cells, max_lines, st);
+  if (r) {
+    err = "batched eigensolve: a CUDA call failed";
+    return r;
+  }
+  return 0;
+}
+
 // Local eigensolves from the network's initial blocks: one LOBPCG launch
 // capped at learned_its iterations, then a second launch, from a random start
 // with the full budget, over the subdomains the first one left unconverged
@@ -523,21 +581,20 @@ int Solver::run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1) {
   LobpcgArgs l2 = la;
   l2.sub_list = d_fail_list;
   l2.nlist = d_fail_count;
-  if (mixed)
-    launch_lobpcg<float>(l1, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                         max_lines, st);
-  else
-    launch_lobpcg<double>(l1, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                          max_lines, st);
+  if (int er = run_eigen(l1, nullptr, nsub, eig_blocks, eb1)) return er;
   cudaMemcpyAsync(d_iters_learned, d_iters, sizeof(int) * nsub, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(d_status_learned, d_status, sizeof(int) * nsub, cudaMemcpyDeviceToDevice, st);
   launch_failed_list(d_status, nsub, d_fail_list, d_fail_count, st);
-  if (mixed)
-    launch_lobpcg<float>(l2, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                         max_lines, st);
-  else
-    launch_lobpcg<double>(l2, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                          max_lines, st);
+  if (opt.eig_batched) {
+    int nfail = 0;
+    cudaMemcpyAsync(eb.h_nactive, d_fail_count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int er = check(cudaStreamSynchronize(st), "learned eigensolve")) return er;
+    nfail = *eb.h_nactive;
+    LobpcgArgs l3 = la;
+    if (int er = run_eigen(l3, d_fail_list, nfail, eig_blocks, eb1)) return er;
+  } else {
+    if (int er = run_eigen(l2, nullptr, nsub, eig_blocks, eb1)) return er;
+  }
   float ms = 0.f;
   cudaEventSynchronize(n1);
   cudaEventElapsedTime(&ms, n0, n1);
@@ -617,6 +674,10 @@ int Solver::setup() {
   la.nlist = nullptr;
   if (!d_queue) cudaMalloc(&d_queue, sizeof(int));
   la.queue = d_queue;
+  la.mode = 0;
+  la.slab = nullptr;
+  la.slab_stride = 0;
+  la.state = nullptr;
   la.dirichlet_mask = dmask;
   la.ld = 0;
   la.prof = nullptr;
@@ -636,12 +697,8 @@ int Solver::setup() {
   const double eb1 = opt.eb_lv1 < 0 ? 1.0e12 : opt.eb_lv1;  // 1/NIL
   if (!opt.learned_path.empty()) {
     if (int er = run_learned_eigen(la, eig_blocks, eb1)) return er;
-  } else if (mixed) {
-    launch_lobpcg<float>(la, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                         max_lines, st);
   } else {
-    launch_lobpcg<double>(la, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
-                          max_lines, st);
+    if (int er = run_eigen(la, nullptr, nsub, eig_blocks, eb1)) return er;
   }
   cudaEventRecord(e[2], st);
   if (int er = check(cudaStreamSynchronize(st), "local eigensolves")) return er;

@@ -34,6 +34,7 @@ struct Options {
   unsigned long long seed = 20240611ull;
   int pcg_chunk = 4;
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
+  int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
@@ -136,6 +137,9 @@ class Solver {
   void* net_x = nullptr;  // BF16 feature patches of one chunk of subdomains
   float* net_y = nullptr;  // network output for every subdomain [nsub][4096][16]
   int* d_queue = nullptr;
+  EbBuffers eb;  // phase-batched eigensolver storage
+  int alloc_eb(int m, bool mixed);
+  int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;
   double* A2g = nullptr;  // -use_2level: inverse of the global coarse matrix
