@@ -311,7 +311,6 @@ __global__ void k_spd_inverse(int n, double* a_all, double tol, int* nnull) {
     __syncthreads();
   }
   const double scale = red[0] > 0 ? red[0] : 1.0;
-  const long long nn = (long long)n * n;
   for (int k = 0; k < n; ++k) {
     const double piv = a[(long long)k * n + k];
     const bool isnull = !(piv > tol * scale);
@@ -327,23 +326,28 @@ __global__ void k_spd_inverse(int n, double* a_all, double tol, int* nnull) {
       }
       if (threadIdx.x == 0) nul += 1;
     } else {
-      for (long long e = threadIdx.x; e < nn; e += blockDim.x) {
-        const int i = (int)(e / n), j = (int)(e % n);
-        if (i == k)
-          a[e] = rowk[j];
-        else
-          a[e] = (j == k ? 0.0 : a[e]) - colk[i] * rowk[j];
+      // rank-1 update, one warp per row (no index division in the inner loop)
+      const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      for (int i = threadIdx.x >> 5; i < n; i += nw) {
+        double* row = a + (long long)i * n;
+        if (i == k) {
+          for (int j = lane; j < n; j += 32) row[j] = rowk[j];
+        } else {
+          const double ci = colk[i];
+          for (int j = lane; j < n; j += 32) row[j] = (j == k ? 0.0 : row[j]) - ci * rowk[j];
+        }
       }
     }
     __syncthreads();
   }
-  for (long long e = threadIdx.x; e < nn; e += blockDim.x) {
-    const int i = (int)(e / n), j = (int)(e % n);
-    if (i < j) {
-      const double v = 0.5 * (a[e] + a[(long long)j * n + i]);
-      a[e] = v;
-      a[(long long)j * n + i] = v;
-    }
+  {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i < n; i += nw)
+      for (int j = i + 1 + lane; j < n; j += 32) {
+        const double v = 0.5 * (a[(long long)i * n + j] + a[(long long)j * n + i]);
+        a[(long long)i * n + j] = v;
+        a[(long long)j * n + i] = v;
+      }
   }
   if (threadIdx.x == 0 && nnull) atomicAdd(nnull, nul);
 }
