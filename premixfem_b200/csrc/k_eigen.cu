@@ -1404,8 +1404,23 @@ __global__ void __launch_bounds__(256) k_eb_aimg(EbArgs a, int which) {
   const int j = isP ? col - a.m : col;
   const T* v = (isP ? sl.P : sl.X) + (size_t)j * ld;
   double* out = (isP ? sl.AP : sl.AX) + (size_t)j * ld;
+  // cell coordinates advanced incrementally (no division per cell)
+  const int sti = blockDim.x % nx, stl = blockDim.x / nx;
+  int i = threadIdx.x % nx, jj = (threadIdx.x / nx) % ny, kk = threadIdx.x / nxny;
   for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-    const int i = cl % nx, tt = cl / nx, jj = tt % ny, kk = tt / ny;
+    if (cl != (int)threadIdx.x) {
+      i += sti;
+      int dl = stl;
+      if (i >= nx) {
+        i -= nx;
+        ++dl;
+      }
+      jj += dl;
+      while (jj >= ny) {
+        jj -= ny;
+        ++kk;
+      }
+    }
     double r = sl.dN32[cl] * (double)(float)v[cl];
     if (i > 0) r -= (double)sl.ctx[cl] * (double)(float)v[cl - 1];
     if (i < nx - 1) r -= (double)sl.ctx[cl + 1] * (double)(float)v[cl + 1];
@@ -1480,8 +1495,9 @@ __global__ void __launch_bounds__(256) k_eb_rr(EbArgs a, double drop) {
 }
 
 // X <- S Y, P <- [W P] Y_WP (and the FP64 A-images in FP64 storage), per chunk.
-template <typename T>
-__global__ void __launch_bounds__(256, 2) k_eb_update(EbArgs a) {
+// NK / NJ: k-steps and 8-column tiles of the tensor-core update (6 / 1 for m <= 8).
+template <typename T, int NK, int NJ>
+__global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
   __shared__ double Ys[LB_LD * LB_LD];
   const int s = eb_sub(a, blockIdx.y);
   const EbState& es = a.state[s];
@@ -1496,8 +1512,9 @@ __global__ void __launch_bounds__(256, 2) k_eb_update(EbArgs a) {
   __syncthreads();
   EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
   const int m = a.m;
-  cta_update_mma<T, 8, 2, 1>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
-  if (sizeof(T) == 8) cta_update_mma<double, 8, 2, 1>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+  cta_update_mma<T, NK, NJ, 1>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+  if (sizeof(T) == 8)
+    cta_update_mma<double, NK, NJ, 1>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
 }
 
 }  // namespace
@@ -1591,7 +1608,11 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     mark(4);
     { note_launch(); k_eb_rr<<<nact, 256, rr_smem, st>>>(e, drop); }
     mark(5);
-    { note_launch(); k_eb_update<T><<<gchunk, 256, 0, st>>>(e); }
+    note_launch();
+    if (a.m <= 8)
+      k_eb_update<T, 6, 1><<<gchunk, 256, 0, st>>>(e);
+    else
+      k_eb_update<T, 8, 2><<<gchunk, 256, 0, st>>>(e);
     if (sizeof(T) == 4) { note_launch(); k_eb_aimg<T><<<dim3(2 * a.m, nact), 256, 0, st>>>(e, 1); }
     mark(6);
     if (prof) {
