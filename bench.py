@@ -73,10 +73,6 @@ WORKLOADS = {
 # Algorithmic bytes per cell of the FP64 operator kernel k_spmv (y = A x):
 # reads x, tx, ty, tz, diag (5 x 8 B), writes y (8 B).
 SPMV_BYTES_PER_CELL = 6 * 8
-# DRAM bytes per (subdomain x LOBPCG iteration) of k_lobpcg<float>, 16^3 subdomains, m = 8: ncu
-# dram__bytes_read.sum + dram__bytes_write.sum = 32.3 GB for 512 subdomains x 29.4 iterations
-# (profiles/k_lobpcg_fracture128_mixed.md).
-LOBPCG_TRAFFIC_PER_SUB_ITER = 32.3e9 / (512 * 29.36)
 
 
 def _peaks():
@@ -177,6 +173,8 @@ def run_b200(args):
         o = dict(wl["opts"], pmf_precision=prec)
         if prec == "mixed" and wl.get("learned"):
             o["pmf_learned"] = wl["learned"]
+        if prec == "mixed":
+            o["pmf_eig_profile"] = 1  # per-phase CUDA events of the batched eigensolver (roofline below)
         s = DarcySolver(prob["dom"], prob["mesh"], options_string(o))
         for f, v in prob["dirichlet"].items():
             s.set_dirichlet(f, v)
@@ -224,13 +222,17 @@ def run_b200(args):
         lst = (C.c_longlong * 4)()
         net_ms = C.c_double()
         _native.check(lib.pmf_get_learned_stats(s.h, lst, C.byref(net_ms)))
+        phases = (C.c_double * 8)()
+        colcells = C.c_ulonglong()
+        _native.check(lib.pmf_get_eig_phases(s.h, phases, C.byref(colcells)))
         bn = float(torch.linalg.norm(b))
         res = float(torch.linalg.norm(b - torch.from_numpy(s.apply_A(x.cpu().numpy())).cuda())) / bn
         results[prec] = dict(steps=steps, launches=launches, clocks=clk.summary(), stages=stages,
                              eig_iters_mean=float(it1.mean()), eig_iters_max=int(it1.max()),
                              eig_iters_sum=int(it1.sum()), cells_per_sub=n / len(it1),
                              eig_unconverged=int((st1 != 0).sum()), rel_residual=res, x=x.cpu().numpy(),
-                             learned=dict(used=int(lst[0]), fallbacks=int(lst[1]), net_ms=round(net_ms.value, 3)))
+                             learned=dict(used=int(lst[0]), fallbacks=int(lst[1]), net_ms=round(net_ms.value, 3)),
+                             eig_phases=list(phases), eig_colcells=int(colcells.value))
         if prec == "mixed":
             # e2e through the C ABI with host buffers (copies inside the timed region)
             e2e = []
@@ -268,10 +270,15 @@ def run_b200(args):
     st = results["mixed"]["stages"]
     eig_s = st["su_lv2_1"] / (args.steps + args.warmup)
     spmv_ms = results["spmv_ms"]
-    # LOBPCG algorithmic FLOPs of this launch: sum over subdomains of iterations x n_s x (60 m^2 + 31 m)
+    # dominant kernel of the step: the batched eigensolver's basis update k_eb_update<float>
+    # (X <- [X W P] Y, P <- [W P] Y per subdomain).  Algorithmic bytes per subdomain-iteration:
+    # read the nS basis columns and write X and P (2m columns), 4 bytes per FP32 value; the library
+    # counts sum(nS x cells) over subdomain-iterations (colcells) and times the phase with events.
     m_blk = wl["opts"]["en_lv1"] + 2
     lob_sub_iters = results["mixed"]["eig_iters_sum"]
-    lob_flops = float(lob_sub_iters) * results["mixed"]["cells_per_sub"] * (60 * m_blk ** 2 + 31 * m_blk)
+    ph = results["mixed"]["eig_phases"]
+    upd_bytes = 4.0 * (results["mixed"]["eig_colcells"] + 2 * m_blk * results["mixed"]["cells_per_sub"] * lob_sub_iters)
+    upd_s = ph[4] * 1e-3
     biter = n * (104 + 4 * (25 + 6 * wl["opts"]["en_lv1"]))
     spmv_gbs = SPMV_BYTES_PER_CELL * n / (spmv_ms * 1e-3) / 1e9
     line = {
@@ -310,21 +317,21 @@ def run_b200(args):
                 "d2h_bytes_per_step": int(2 * n * 8)},
         "gpu_launches": int(results["mixed"]["launches"] / max(1, args.steps)),
         "roofline": {
-            "kernel": "k_lobpcg<float> (batched local eigensolver, dominant share of the step)",
-            "bound": "tensor",
-            "achieved": round(lob_flops / eig_s / 1e12, 3),
-            "peak": bf16,
-            "unit": "TFLOP/s",
-            "frac": round(lob_flops / eig_s / 1e12 / bf16, 6),
-            "traffic": round(LOBPCG_TRAFFIC_PER_SUB_ITER * lob_sub_iters, 0),
-            "time_s_per_step": round(eig_s, 6),
-            "flops_per_launch": lob_flops,
-            "note": "algorithmic FLOPs n*(60 m^2 + 31 m) per subdomain-iteration (Grams, basis and A-image "
-                    "updates, stencil, IC(0) sweeps), FP64 arithmetic on the FP64 tensor pipe (DMMA) and CUDA "
-                    "cores; the denominator is the measured bf16 peak, the only tensor peak measured.  traffic: "
-                    "ncu dram bytes per subdomain-iteration on the 128^3 case, scaled by this launch's "
-                    "subdomain-iterations.  Latency-bound; see profiles/k_lobpcg_fracture128_mixed.md",
+            "kernel": "k_eb_update<float> (batched LOBPCG basis update, largest single kernel of the step)",
+            "bound": "hbm",
+            "achieved": round(upd_bytes / upd_s / 1e9, 1) if upd_s > 0 else None,
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": round(upd_bytes / upd_s / 1e9 / hbm, 4) if upd_s > 0 else None,
+            "traffic": None,
+            "bytes_per_step": upd_bytes,
+            "time_s_per_step": round(upd_s, 6),
+            "peak_kind": peak_kind,
         },
+        "lobpcg_phases_ms": {"resid_control": round(ph[0], 2), "precond": round(ph[1], 2), "gram": round(ph[2], 2),
+                             "rayleigh_ritz": round(ph[3], 2), "update": round(ph[4], 2),
+                             "a_images": round(ph[5], 2), "lockstep_iterations": int(ph[6]),
+                             "eigen_stage_s": round(eig_s, 6)},
         "roofline_solve_model": {
             "phase": "PCG solve (all kernels), algorithmic bytes B_iter = N*[104 + w*(25+6k)], w=4, k=6",
             "bound": "hbm",

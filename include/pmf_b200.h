@@ -135,6 +135,12 @@ int pmf_get_learned_stats(pmf_solver* s, long long stats[4], double* net_ms);
 #define PMF_NOALLOC_MAX_CELLS 33554432LL /* PMF_NOALLOC_MAX_BLOCKS x 2048 cells */
 int pmf_residual_noalloc(pmf_solver* s, const double* b, const double* x, double* r, double* rnorm, void* stream);
 
+/* Phase-batched local eigensolver of the last pmf_setup (option -pmf_eig_profile 1 enables the
+ * timing): ms[0..5] device ms of residual norms + control, IC(0)-preconditioned directions, Grams,
+ * Rayleigh-Ritz, basis update, FP32 A-images; ms[6] lockstep iterations.  colcells: sum over
+ * subdomain-iterations of (basis columns x cells), the unit of the Gram and update traffic. */
+int pmf_get_eig_phases(pmf_solver* s, double ms[8], unsigned long long* colcells);
+
 /* total number of CUDA kernels launched by this library in this process */
 unsigned long long pmf_launch_count(void);
 

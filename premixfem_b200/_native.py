@@ -50,6 +50,7 @@ SIGNATURES = {
     "pmf_net_loss": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp]),
     "pmf_learned_patches": (C.c_int, [_vp, _vp, _vp, _vp]),
     "pmf_get_learned_stats": (C.c_int, [_vp, _vp, _dp]),
+    "pmf_get_eig_phases": (C.c_int, [_vp, _vp, C.POINTER(C.c_ulonglong)]),
     "pmf_residual_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pmf_launch_count": (C.c_ulonglong, []),
     "pmf_last_error": (C.c_char_p, []),

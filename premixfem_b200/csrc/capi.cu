@@ -202,6 +202,14 @@ int pmf_get_timing(pmf_solver* h, double* setup_ms, double* solve_ms) {
   return 0;
 }
 
+int pmf_get_eig_phases(pmf_solver* h, double ms[8], unsigned long long* colcells) {
+  PMF_CHECK_HANDLE(h);
+  if (ms)
+    for (int i = 0; i < 8; ++i) ms[i] = h->s->eig_phase_ms[i];
+  if (colcells) *colcells = h->s->eig_colcells;
+  return 0;
+}
+
 unsigned long long pmf_launch_count(void) { return __atomic_load_n(&pmf::g_launches, __ATOMIC_RELAXED); }
 
 const char* pmf_last_error(void) { return g_last_error.c_str(); }

@@ -1227,6 +1227,7 @@ struct EbArgs {
   double* rpart;
   int* nactive;
   int* alist;  // subdomains still iterating, compacted by k_eb_control
+  unsigned long long* colcells;  // sum over active subdomain-iterations of (basis columns x cells)
   const double *tx, *ty, *tz;
 };
 
@@ -1301,6 +1302,7 @@ __global__ void k_eb_control(EbArgs a, int nlist, int it) {
   es.nS = m + na + es.np;
   es.it = it + 1;  // iterations counted if the iteration limit ends the solve
   a.alist[atomicAdd(a.nactive, 1)] = s;  // order is irrelevant: subdomains are independent
+  if (a.colcells) atomicAdd(a.colcells, (unsigned long long)es.nS * (unsigned long long)nc);
 }
 
 // W_c = T (AX_a - lambda_a M X_a) for active columns c (a = act[c]) of one
@@ -1560,6 +1562,8 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   e.rpart = b.rpart;
   e.nactive = b.nactive;
   e.alist = b.alist;
+  e.colcells = b.colcells;
+  if (b.colcells) cudaMemsetAsync(b.colcells, 0, sizeof(unsigned long long), st);
   e.tx = a.tx;
   e.ty = a.ty;
   e.tz = a.tz;
@@ -1573,8 +1577,8 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   cudaFuncSetAttribute(k_eb_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem);
   cudaFuncSetAttribute(k_eb_rr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem);
   const double drop = sizeof(T) == 4 ? 1e-9 : 1e-13;
-  // optional diagnostics (PMF_PROFILE_EIGEN): device time per phase
-  const bool prof = getenv("PMF_PROFILE_EIGEN") != nullptr;
+  // optional phase timing (b.phase_ms, or PMF_PROFILE_EIGEN): device time per phase
+  const bool prof = b.phase_ms != nullptr || getenv("PMF_PROFILE_EIGEN") != nullptr;
   cudaEvent_t pev[9];
   float ptot[8] = {0};
   if (prof)
@@ -1583,7 +1587,7 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     if (prof) cudaEventRecord(pev[i], st);
   };
   mark(0);
-  int nact = nlist;
+  int nact = nlist, lockstep = 0;
   for (int it = 0; it < a.max_it; ++it) {
     // residual norms of the subdomains still iterating (all of them at it = 0)
     mark(1);
@@ -1600,7 +1604,9 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     }
     nact = *b.h_nactive;
     if (nact == 0) break;
+    ++lockstep;
     const dim3 gchunk(e.nchunk, nact), gpre((a.m + e.mb - 1) / e.mb, nact);
+    mark(2);
     { note_launch(); k_eb_precond<T><<<gpre, 256, pre_smem, st>>>(e); }
     if (sizeof(T) == 8) { note_launch(); k_eb_aimg<T><<<dim3(a.m, nact), 256, 0, st>>>(e, 0); }
     mark(3);
@@ -1613,20 +1619,28 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
       k_eb_update<T, 6, 1><<<gchunk, 256, 0, st>>>(e);
     else
       k_eb_update<T, 8, 2><<<gchunk, 256, 0, st>>>(e);
-    if (sizeof(T) == 4) { note_launch(); k_eb_aimg<T><<<dim3(2 * a.m, nact), 256, 0, st>>>(e, 1); }
     mark(6);
+    if (sizeof(T) == 4) { note_launch(); k_eb_aimg<T><<<dim3(2 * a.m, nact), 256, 0, st>>>(e, 1); }
+    mark(7);
     if (prof) {
-      cudaEventSynchronize(pev[6]);
+      cudaEventSynchronize(pev[7]);
       float ms;
-      for (int q = 2; q < 6; ++q) {
+      for (int q = 2; q < 7; ++q) {
         cudaEventElapsedTime(&ms, pev[q], pev[q + 1]);
         ptot[q - 1] += ms;
       }
     }
   }
   if (prof) {
-    fprintf(stderr, "[premixfem_b200] batched LOBPCG ms: resid+control %.2f precond %.2f gram %.2f rr %.2f update %.2f\n",
-            ptot[0], ptot[1], ptot[2], ptot[3], ptot[4]);
+    if (b.phase_ms) {
+      for (int q = 0; q < 6; ++q) b.phase_ms[q] += ptot[q];
+      b.phase_ms[6] += lockstep;
+    }
+    if (getenv("PMF_PROFILE_EIGEN"))
+      fprintf(stderr,
+              "[premixfem_b200] batched LOBPCG ms: resid+control %.2f precond %.2f gram %.2f rr %.2f update %.2f "
+              "a-images %.2f (%d lockstep iterations)\n",
+              ptot[0], ptot[1], ptot[2], ptot[3], ptot[4], ptot[5], lockstep);
     for (auto& x : pev) cudaEventDestroy(x);
   }
   // final phase: k_lobpcg mode 2 (FP64 Rayleigh-Ritz, adaptive count, output)

@@ -166,6 +166,9 @@ struct EbBuffers {
   double* rpart = nullptr;        // nsub x nchunk x LB_MM partial residual norms
   int* nactive = nullptr;         // device counter
   int* alist = nullptr;           // nsub: compacted list of subdomains still iterating
+  unsigned long long* colcells = nullptr;  // device: sum of (basis columns x cells) over sub-iterations
+  double* phase_ms = nullptr;     // host, optional: accumulated ms of resid+control, preconditioner,
+                                  // Gram, Rayleigh-Ritz, update, A-images; [6] lockstep iterations
   int* h_nactive = nullptr;       // pinned host copy
   int nchunk = 0;
 };

@@ -116,6 +116,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
   db.get_int("pmf_eig_ctas", &o->eig_ctas);
   db.get_int("pmf_eig_batched", &o->eig_batched);
+  db.get_int("pmf_eig_profile", &o->eig_profile);
   {
     auto it2 = db.kv.find("pmf_learned");
     if (it2 != db.kv.end()) {
@@ -247,7 +248,7 @@ Solver::~Solver() {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart, (void*)eb.nactive,
-                  (void*)eb.alist})
+                  (void*)eb.alist, (void*)eb.colcells})
     if (p) cudaFree(p);
   if (eb.h_nactive) cudaFreeHost(eb.h_nactive);
   for (void* p : {(void*)A2g, (void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
@@ -494,6 +495,7 @@ int Solver::alloc_eb(int m, bool mixed) {
     return e;
   if (int e = check(cudaMalloc(&eb.rpart, ns * eb.nchunk * 10 * sizeof(double)), "cudaMalloc residuals")) return e;
   if (!eb.nactive) cudaMalloc(&eb.nactive, sizeof(int));
+  if (!eb.colcells) cudaMalloc(&eb.colcells, sizeof(unsigned long long));
   if (eb.alist) cudaFree(eb.alist);
   cudaMalloc(&eb.alist, ns * sizeof(int));
   if (!eb.h_nactive) cudaMallocHost(&eb.h_nactive, sizeof(int));
@@ -518,6 +520,7 @@ int Solver::run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks
     return 0;
   }
   if (int e = alloc_eb(la.m, mixed)) return e;
+  eb.phase_ms = opt.eig_profile ? eig_phase_ms : nullptr;
   int r;
   if (mixed)
     r = launch_lobpcg_batched<float>(la, eb, list, nlist, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
@@ -529,6 +532,10 @@ int Solver::run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks
     err = "batched eigensolve: a CUDA call failed";
     return r;
   }
+  unsigned long long cc = 0;
+  cudaMemcpyAsync(&cc, eb.colcells, sizeof(cc), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  eig_colcells += cc;
   return 0;
 }
 
@@ -695,6 +702,8 @@ int Solver::setup() {
     eig_work_bytes = need;
   }
   const double eb1 = opt.eb_lv1 < 0 ? 1.0e12 : opt.eb_lv1;  // 1/NIL
+  for (double& x : eig_phase_ms) x = 0.0;
+  eig_colcells = 0;
   if (!opt.learned_path.empty()) {
     if (int er = run_learned_eigen(la, eig_blocks, eb1)) return er;
   } else {

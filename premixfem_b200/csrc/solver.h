@@ -35,6 +35,7 @@ struct Options {
   int pcg_chunk = 4;
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
+  int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
@@ -138,6 +139,8 @@ class Solver {
   float* net_y = nullptr;  // network output for every subdomain [nsub][4096][16]
   int* d_queue = nullptr;
   EbBuffers eb;  // phase-batched eigensolver storage
+  double eig_phase_ms[8] = {0};
+  unsigned long long eig_colcells = 0;
   int alloc_eb(int m, bool mixed);
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
