@@ -100,67 +100,161 @@ struct FwdArgs {
   float* outf;
 };
 
-constexpr int kTileRows = 64;
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  // 16-byte global->shared copy; zero-filled when !valid (src-size 0)
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
 
-template <int NT>
-__global__ void __launch_bounds__(128) k_net_fwd(FwdArgs a) {
+// ROWS output voxels of one sample per CTA (ROWS / (16 MT) warps, each MT
+// 16-row tiles x all output channels, sharing the weight fragments); the
+// gathered input rows and the weight slice of the next tap are copied with
+// cp.async while the current tap is multiplied.
+template <int NT, int ROWS, int MT>
+__global__ void __launch_bounds__(ROWS * 2 / MT) k_net_fwd(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ int rowout[kTileRows];
+  __shared__ int rowout[ROWS];
   const int lda = a.cin + 8, ldb = a.cout + 8;
-  __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smraw);
-  __nv_bfloat16* Bs = As + kTileRows * lda;
+  __nv_bfloat16* As0 = reinterpret_cast<__nv_bfloat16*>(smraw);
+  __nv_bfloat16* Bs0 = As0 + 2 * ROWS * lda;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nthr = ROWS * 2 / MT;
   const int so3 = cube(a.s_out), si3 = cube(a.s_in);
-  const long long r0 = (long long)blockIdx.x * kTileRows;
+  const long long r0 = (long long)blockIdx.x * ROWS;
   const int b = (int)(r0 / so3);
   const int rem0 = (int)(r0 % so3);
   const bool up = a.type == NL_UP2;
   const int d_tile = up ? rem0 / si3 : 0;
-  if (tid < kTileRows) rowout[tid] = up ? up_vox((rem0 + tid) % si3, d_tile, a.s_in) : rem0 + tid;
+  for (int q = tid; q < ROWS; q += nthr) rowout[q] = up ? up_vox((rem0 + q) % si3, d_tile, a.s_in) : rem0 + q;
+  __syncthreads();
   const int ntap = (up || a.type == NL_CONV1) ? 1 : net_taps(a.type);
-  float acc[NT][4];
-#pragma unroll
-  for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
   const int vin = a.cin >> 3, vout = a.cout >> 3;
-  for (int ti = 0; ti < ntap; ++ti) {
-    const int t = up ? d_tile : ti;
-    __syncthreads();
-    for (int e = tid; e < kTileRows * vin; e += blockDim.x) {
+  // Per-thread copy assignments, fixed for all taps: up to EA input-row
+  // vectors and EB weight vectors, with their coordinates precomputed so the
+  // per-tap gather needs no division.
+  constexpr int NTHR = ROWS * 2 / MT;
+  constexpr int EA = (ROWS * 12 + NTHR - 1) / NTHR;  // cin <= 96: 12 vectors per row
+  constexpr int EB = (96 * 12 + NTHR - 1) / NTHR;
+  int a_dst[EA], a_xyz[EA], a_src[EA];
+  int b_dst[EB];
+  const int sin = a.s_in;
+#pragma unroll
+  for (int j = 0; j < EA; ++j) {
+    const int e = tid + j * nthr;
+    a_dst[j] = -1;
+    if (e < ROWS * vin) {
       const int rr = e / vin, cv = e % vin;
-      const int iv = up ? (rem0 + rr) % si3 : in_vox(a.type, a.s_in, a.s_out, rowout[rr], t);
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (iv >= 0) v = *reinterpret_cast<const uint4*>(a.in + ((size_t)b * si3 + iv) * a.cin + cv * 8);
-      *reinterpret_cast<uint4*>(As + rr * lda + cv * 8) = v;
+      a_dst[j] = rr * lda + cv * 8;
+      if (up) {
+        a_src[j] = ((rem0 + rr) % si3) * a.cin + cv * 8;
+        a_xyz[j] = 0;
+      } else {
+        const int o = rowout[rr], so = a.s_out;
+        int x = o % so, y = (o / so) % so, z = o / (so * so);
+        if (a.type == NL_DOWN2) {
+          x *= 2;
+          y *= 2;
+          z *= 2;
+        }
+        a_xyz[j] = x | (y << 10) | (z << 20);
+        a_src[j] = ((z * sin + y) * sin + x) * a.cin + cv * 8;
+      }
     }
-    for (int e = tid; e < a.cin * vout; e += blockDim.x) {
-      const int k = e / vout, cv = e % vout;
-      *reinterpret_cast<uint4*>(Bs + k * ldb + cv * 8) =
-          *reinterpret_cast<const uint4*>(a.W + ((size_t)t * a.cin + k) * a.cout + cv * 8);
+  }
+#pragma unroll
+  for (int j = 0; j < EB; ++j) {
+    const int e = tid + j * nthr;
+    b_dst[j] = e < a.cin * vout ? (e / vout) * ldb + (e % vout) * 8 : -1;
+  }
+  const __nv_bfloat16* inb = a.in + (size_t)b * si3 * a.cin;
+  auto stage = [&](int ti, int buf) {
+    const int t = up ? d_tile : ti;
+    __nv_bfloat16* As = As0 + buf * ROWS * lda;
+    __nv_bfloat16* Bs = Bs0 + buf * a.cin * ldb;
+    int dx = 0, dy = 0, dz = 0;
+    if (a.type == NL_CONV3) {
+      dx = t % 3 - 1;
+      dy = (t / 3) % 3 - 1;
+      dz = t / 9 - 1;
+    } else if (a.type == NL_DOWN2) {
+      dx = t & 1;
+      dy = (t >> 1) & 1;
+      dz = t >> 2;
+    }
+    const int off = ((dz * sin + dy) * sin + dx) * a.cin;
+#pragma unroll
+    for (int j = 0; j < EA; ++j) {
+      if (a_dst[j] < 0) continue;
+      bool ok = true;
+      if (a.type == NL_CONV3) {
+        const int x = (a_xyz[j] & 1023) + dx, y = ((a_xyz[j] >> 10) & 1023) + dy, z = (a_xyz[j] >> 20) + dz;
+        ok = x >= 0 && y >= 0 && z >= 0 && x < sin && y < sin && z < sin;
+      }
+      const int src = ok ? a_src[j] + (up || a.type == NL_CONV1 ? 0 : off) : 0;
+      cp_async16(As + a_dst[j], inb + src, ok);
+    }
+    const __nv_bfloat16* wt = a.W + (size_t)t * a.cin * a.cout;
+#pragma unroll
+    for (int j = 0; j < EB; ++j) {
+      if (b_dst[j] < 0) continue;
+      cp_async16(Bs + b_dst[j], wt + 8 * (tid + j * nthr), true);
+    }
+    cp_async_commit();
+  };
+  float acc[MT][NT][4];
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+    for (int n = 0; n < NT; ++n) acc[mt][n][0] = acc[mt][n][1] = acc[mt][n][2] = acc[mt][n][3] = 0.f;
+  stage(0, 0);
+  for (int ti = 0; ti < ntap; ++ti) {
+    if (ti + 1 < ntap) {
+      stage(ti + 1, (ti + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const __nv_bfloat16* As = As0 + (ti & 1) * ROWS * lda;
+    const __nv_bfloat16* Bs = Bs0 + (ti & 1) * a.cin * ldb;
     for (int kc = 0; kc < a.cin; kc += 16) {
-      uint32_t a0, a1, a2, a3;
-      ldsm_x4(smem_u32(As + (warp * 16 + (lane & 15)) * lda + kc + (lane >> 4) * 8), a0, a1, a2, a3);
+      uint32_t af[MT][4];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+        ldsm_x4(smem_u32(As + ((warp * MT + mt) * 16 + (lane & 15)) * lda + kc + (lane >> 4) * 8), af[mt][0],
+                af[mt][1], af[mt][2], af[mt][3]);
 #pragma unroll
       for (int np = 0; np < NT / 2; ++np) {
         uint32_t b0, b1, b2, b3;
         ldsm_x4_t(smem_u32(Bs + (kc + (lane & 7) + ((lane >> 3) & 1) * 8) * ldb + np * 16 + (lane >> 4) * 8), b0, b1,
                   b2, b3);
-        mma_bf16(acc[2 * np], a0, a1, a2, a3, b0, b1);
-        mma_bf16(acc[2 * np + 1], a0, a1, a2, a3, b2, b3);
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          mma_bf16(acc[mt][2 * np], af[mt][0], af[mt][1], af[mt][2], af[mt][3], b0, b1);
+          mma_bf16(acc[mt][2 * np + 1], af[mt][0], af[mt][1], af[mt][2], af[mt][3], b2, b3);
+        }
       }
     }
+    __syncthreads();  // the buffer just read is refilled two taps later
   }
   // epilogue: bias, skip, ReLU, store
 #pragma unroll
+  for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const int rr = warp * 16 + (lane >> 2) + h * 8;
+    const int rr = (warp * MT + mt) * 16 + (lane >> 2) + h * 8;
     const size_t rowbase = ((size_t)b * so3 + rowout[rr]) * a.cout;
 #pragma unroll
     for (int n = 0; n < NT; ++n) {
       const int col = n * 8 + (lane & 3) * 2;
-      float v0 = acc[n][2 * h] + a.bias[col];
-      float v1 = acc[n][2 * h + 1] + a.bias[col + 1];
+      float v0 = acc[mt][n][2 * h] + a.bias[col];
+      float v1 = acc[mt][n][2 * h + 1] + a.bias[col + 1];
       if (a.skip) {
         const __nv_bfloat162 s2 = *reinterpret_cast<const __nv_bfloat162*>(a.skip + rowbase + col);
         v0 += __bfloat162float(s2.x);
@@ -733,16 +827,32 @@ int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_
     a.out = L.out_act == NET_ACTS - 1 ? nullptr : act_[L.out_act];
     a.outf = L.out_act == NET_ACTS - 1 ? y : nullptr;
     const long long rows = (long long)B * L.s_out * L.s_out * L.s_out;
-    const int grid = (int)(rows / kTileRows);
-    const size_t smem = ((size_t)kTileRows * (L.cin + 8) + (size_t)L.cin * (L.cout + 8)) * 2;
+    // 128-row tiles where a tile stays inside one sample (and one parity class for up2)
+    const int per = L.type == NL_UP2 ? L.s_in * L.s_in * L.s_in : L.s_out * L.s_out * L.s_out;
+    const bool big = per % 256 == 0;
+    const int R = big ? 256 : 64;
+    const int grid = (int)(rows / R);
+    const size_t smem = (2 * (size_t)R * (L.cin + 8) + 2 * (size_t)L.cin * (L.cout + 8)) * 2;
     note_launch();
+    // 256-row tiles: 8 warps x two 16-row tiles; 64-row tiles (4^3 layers): 4 warps x one
+#define PMF_FWD(NTV)                                                                                      \
+  do {                                                                                                    \
+    if (big) {                                                                                            \
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k_net_fwd<NTV, 256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+      k_net_fwd<NTV, 256, 2><<<grid, 256, smem, st>>>(a);                                                 \
+    } else {                                                                                              \
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k_net_fwd<NTV, 64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+      k_net_fwd<NTV, 64, 1><<<grid, 128, smem, st>>>(a);                                                  \
+    }                                                                                                     \
+  } while (0)
     switch (L.cout / 8) {
-      case 2: k_net_fwd<2><<<grid, 128, smem, st>>>(a); break;
-      case 4: k_net_fwd<4><<<grid, 128, smem, st>>>(a); break;
-      case 8: k_net_fwd<8><<<grid, 128, smem, st>>>(a); break;
-      case 12: k_net_fwd<12><<<grid, 128, smem, st>>>(a); break;
+      case 2: PMF_FWD(2); break;
+      case 4: PMF_FWD(4); break;
+      case 8: PMF_FWD(8); break;
+      case 12: PMF_FWD(12); break;
       default: err = "unsupported layer width"; return 56;
     }
+#undef PMF_FWD
   }
   (void)keep;
   return 0;
