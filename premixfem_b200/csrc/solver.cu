@@ -117,6 +117,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_ctas", &o->eig_ctas);
   db.get_int("pmf_eig_batched", &o->eig_batched);
   db.get_int("pmf_eig_profile", &o->eig_profile);
+  db.get_int("pmf_pcg_graph", &o->pcg_graph);
   {
     auto it2 = db.kv.find("pmf_learned");
     if (it2 != db.kv.end()) {
@@ -247,6 +248,7 @@ Solver::~Solver() {
                   state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
   for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart, (void*)eb.nactive,
                   (void*)eb.alist, (void*)eb.colcells})
     if (p) cudaFree(p);
@@ -483,6 +485,7 @@ int Solver::assemble() {
 int Solver::alloc_eb(int m, bool mixed) {
   const size_t stride = lobpcg_batched_slab_bytes(max_cells, m, mixed ? 4 : 8);
   if (eb.slab && eb.slab_stride == stride) return 0;
+  if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
   for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart})
     if (p) cudaFree(p);
   eb.slab_stride = stride;
@@ -1026,13 +1029,43 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   double* pin = p0;
   double* pout = p1;
   int guard = 0;
-  for (;;) {
-    for (int c_ = 0; c_ < std::max(1, opt.pcg_chunk); ++c_) {
+  const int chunk = std::max(1, opt.pcg_chunk);
+  auto enqueue_chunk = [&]() {
+    for (int c_ = 0; c_ < chunk; ++c_) {
       launch_pcg_iter_a(g, tx, ty, tz, diag, z, pin, pout, w, part, state, st);
       launch_pcg_iter_b(g.ncell, xs, r, pout, w, part, state, st);
       apply(r, z, part, done);
       launch_pcg_beta_fin(part, nparts_apply(), state, st);
       std::swap(pin, pout);
+    }
+  };
+  // A chunk of PCG iterations (each: p-update + A p, x/r update, the whole
+  // preconditioner application, beta) as one CUDA graph: captured once per
+  // solution buffer and replayed until the device-side `done` flag is set.
+  // An even chunk returns the p buffers to their roles, so replays chain.
+  const bool use_graph = opt.pcg_graph && chunk % 2 == 0;
+  if (use_graph && (!pcg_exec || pcg_graph_x != xs)) {
+    if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
+    pcg_exec = nullptr;
+    const unsigned long long l0 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+    cudaGraph_t graph = nullptr;
+    if (int e = check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return e;
+    enqueue_chunk();
+    if (int e = check(cudaStreamEndCapture(st, &graph), "graph capture")) return e;
+    const unsigned long long l1 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+    pcg_graph_kernels = l1 - l0;
+    __atomic_fetch_sub(&g_launches, pcg_graph_kernels, __ATOMIC_RELAXED);  // captured, not launched
+    const cudaError_t ie = cudaGraphInstantiate(&pcg_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (int e = check(ie, "graph instantiate")) return e;
+    pcg_graph_x = xs;
+  }
+  for (;;) {
+    if (use_graph) {
+      if (int e = check(cudaGraphLaunch(pcg_exec, st), "graph launch")) return e;
+      __atomic_fetch_add(&g_launches, pcg_graph_kernels, __ATOMIC_RELAXED);
+    } else {
+      enqueue_chunk();
     }
     cudaMemcpyAsync(h_state, state, sizeof(PcgState), cudaMemcpyDeviceToHost, st);
     if (int e = check(cudaStreamSynchronize(st), "KSPSolve")) return e;

@@ -33,6 +33,7 @@ struct Options {
   double l3_tol = 1e-10;
   unsigned long long seed = 20240611ull;
   int pcg_chunk = 4;
+  int pcg_graph = 1;  // replay each chunk of PCG iterations as one CUDA graph
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
@@ -140,6 +141,9 @@ class Solver {
   int* d_queue = nullptr;
   EbBuffers eb;  // phase-batched eigensolver storage
   double eig_phase_ms[8] = {0};
+  cudaGraphExec_t pcg_exec = nullptr;  // one chunk of PCG iterations
+  const double* pcg_graph_x = nullptr;
+  unsigned long long pcg_graph_kernels = 0;
   unsigned long long eig_colcells = 0;
   int alloc_eb(int m, bool mixed);
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
