@@ -1,6 +1,8 @@
 // Coarse-space kernels (FP64): level-2 Galerkin assembly, batched dense SPD
 // inverses, the level-3 eigenproblem and the small coarse products used by the
 // cycle executor.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 #include "pmf_dense.cuh"
@@ -351,7 +353,184 @@ __global__ void k_spd_inverse(int n, double* a_all, double tol, int* nnull) {
   }
   if (threadIdx.x == 0 && nnull) atomicAdd(nnull, nul);
 }
+// The same Gauss-Jordan inverse by a cluster of kSpdCl CTAs per matrix, for
+// n <= 32 * NM.  CTA c of the cluster owns rows [c R, c R + R), R = ceil(n /
+// kSpdCl); warp w holds rows c R + w + 16 s (s < RW) in registers, lane l the
+// columns l + 32 m.  Per pivot the owning warp publishes the scaled pivot row
+// in its CTA's shared memory, one cluster barrier makes it visible, and every
+// CTA copies it through distributed shared memory and updates its rows.  The
+// arithmetic per element is that of k_spd_inverse, so the results agree bit
+// for bit.
+constexpr int kSpdCl = 8;
+constexpr int kSpdWarps = 16;
+
+template <int NM, int RW>
+__global__ void __launch_bounds__(kSpdWarps * 32, 1)
+    k_spd_inverse_cl(int n, double* a_all, double tol, int* nnull) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const int mat = blockIdx.x / kSpdCl;
+  double* a = a_all + (long long)mat * n * n;
+  const int R = (n + kSpdCl - 1) / kSpdCl;
+  const int r0 = crank * R;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __shared__ double pub[2][NM * 32];  // published pivot rows (read by the whole cluster)
+  __shared__ double prow[NM * 32];    // local copy of the current pivot row
+  __shared__ int pnull[2];
+  __shared__ double cmax[kSpdWarps];
+  __shared__ double smax;
+  double v[RW][NM];
+  int rows[RW];
+#pragma unroll
+  for (int s = 0; s < RW; ++s) {
+    const int i = r0 + w + kSpdWarps * s;
+    rows[s] = (w + kSpdWarps * s < R && i < n) ? i : -1;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const int j = lane + 32 * m;
+      v[s][m] = (rows[s] >= 0 && j < n) ? a[(long long)i * n + j] : 0.0;
+    }
+  }
+  // scale = max |a_ii| over the whole matrix
+  double mx = 0.0;
+#pragma unroll
+  for (int s = 0; s < RW; ++s)
+#pragma unroll
+    for (int m = 0; m < NM; ++m)
+      if (rows[s] >= 0 && lane + 32 * m == rows[s]) mx = fmax(mx, fabs(v[s][m]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) cmax[w] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m2 = 0.0;
+    for (int q = 0; q < kSpdWarps; ++q) m2 = fmax(m2, cmax[q]);
+    smax = m2;
+  }
+  cluster.sync();
+  if (threadIdx.x == 0) {
+    double m2 = 0.0;
+    for (int c = 0; c < kSpdCl; ++c) m2 = fmax(m2, *cluster.map_shared_rank(&smax, c));
+    cmax[0] = m2 > 0 ? m2 : 1.0;
+  }
+  cluster.sync();  // every CTA has read the others' maxima before smax is reused
+  const double scale = cmax[0];
+  int nul = 0;
+  for (int k = 0; k < n; ++k) {
+    const int o = k / R, ok = k - o * R;
+    const int ow = ok % kSpdWarps, os = ok / kSpdWarps;
+    const int km = k >> 5, kl = k & 31;
+    if (crank == o && w == ow) {  // owner warp: publish row k scaled by its pivot
+#pragma unroll
+      for (int s = 0; s < RW; ++s)
+        if (s == os) {
+          double pv = 0.0;
+#pragma unroll
+          for (int m = 0; m < NM; ++m)
+            if (m == km) pv = v[s][m];
+          const double piv = __shfl_sync(0xffffffffu, pv, kl);
+          const bool isnull = !(piv > tol * scale);
+#pragma unroll
+          for (int m = 0; m < NM; ++m) {
+            const int j = lane + 32 * m;
+            pub[k & 1][j] = isnull ? 0.0 : (j == k ? 1.0 : v[s][m]) / piv;
+          }
+          if (lane == 0) pnull[k & 1] = isnull ? 1 : 0;
+        }
+    }
+    cluster.sync();
+    {
+      const double* src = cluster.map_shared_rank(&pub[k & 1][0], o);
+      for (int j = threadIdx.x; j < NM * 32; j += blockDim.x) prow[j] = src[j];
+    }
+    const bool isnull = *cluster.map_shared_rank(&pnull[k & 1], o) != 0;
+    __syncthreads();
+    if (isnull) {
+      if (crank == o && threadIdx.x == 0) ++nul;
+#pragma unroll
+      for (int s = 0; s < RW; ++s) {
+        if (rows[s] < 0) continue;
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+          if (rows[s] == k || (m == km && lane == kl)) v[s][m] = 0.0;
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < RW; ++s) {
+        if (rows[s] < 0) continue;
+        if (rows[s] == k) {
+#pragma unroll
+          for (int m = 0; m < NM; ++m) v[s][m] = prow[lane + 32 * m];
+        } else {
+          double cv = 0.0;
+#pragma unroll
+          for (int m = 0; m < NM; ++m)
+            if (m == km) cv = v[s][m];
+          const double ci = __shfl_sync(0xffffffffu, cv, kl);
+#pragma unroll
+          for (int m = 0; m < NM; ++m) {
+            const int j = lane + 32 * m;
+            v[s][m] = (j == k ? 0.0 : v[s][m]) - ci * prow[j];
+          }
+        }
+      }
+    }
+  }
+  // rows back to global memory, then the symmetrisation of k_spd_inverse by the
+  // owner of the lower row index of each pair
+#pragma unroll
+  for (int s = 0; s < RW; ++s)
+    if (rows[s] >= 0)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) {
+        const int j = lane + 32 * m;
+        if (j < n) a[(long long)rows[s] * n + j] = v[s][m];
+      }
+  cluster.sync();
+#pragma unroll
+  for (int s = 0; s < RW; ++s) {
+    const int i = rows[s];
+    if (i < 0) continue;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const int j = lane + 32 * m;
+      if (j > i && j < n) {
+        const double sv = 0.5 * (v[s][m] + a[(long long)j * n + i]);
+        a[(long long)i * n + j] = sv;
+        a[(long long)j * n + i] = sv;
+      }
+    }
+  }
+  if (threadIdx.x == 0 && nnull && nul) atomicAdd(nnull, nul);
+}
+
+template <int NM, int RW>
+static bool spd_inverse_cl(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb * kSpdCl);
+  cfg.blockDim = dim3(kSpdWarps * 32);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kSpdCl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, k_spd_inverse_cl<NM, RW>, n, a, tol, nnull) != cudaSuccess) {
+    (void)cudaGetLastError();  // cluster launch refused: the caller falls back to one CTA per matrix
+    return false;
+  }
+  note_launch();
+  return true;
+}
+
 void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
+  const int R = (n + kSpdCl - 1) / kSpdCl;
+  if (n <= 128 && R <= kSpdWarps && spd_inverse_cl<4, 1>(nb, n, a, tol, nnull, st)) return;
+  if (n > 128 && n <= 256 && R <= 2 * kSpdWarps && spd_inverse_cl<8, 2>(nb, n, a, tol, nnull, st)) return;
+  if (n > 256 && n <= 384 && R <= 3 * kSpdWarps && spd_inverse_cl<12, 3>(nb, n, a, tol, nnull, st)) return;
   const int smem = 2 * n * sizeof(double);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   { note_launch(); k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull); }
@@ -365,9 +544,49 @@ void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaSt
 // eigenvectors come out orthonormal in the 2-norm as SLEPc returns them.
 // work: 3 * nr * p doubles per rank.
 #define PMF_L3_MAXP 32
+
+// Out[i * p + c] = sum_l M[i][l] Xs[l * ldx + c] (- shift[c] Xs[i * ldx + c]) for c < q, with the
+// block Xs staged in shared memory: one warp per row, lanes along l (coalesced
+// row reads), eight column accumulators per pass, warp reductions.
+__device__ void cta_rows_mm(const double* __restrict__ M, int nr, const double* Xs, int ldx, int q, double* Out,
+                            int p, const double* shift) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = wid; i < nr; i += nw) {
+    const double* row = M + (long long)i * nr;
+    for (int c0 = 0; c0 < q; c0 += 8) {
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+      for (int l = lane; l < nr; l += 32) {
+        const double mv = row[l];
+        const double* xr = Xs + l * ldx + c0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c0 + c < q) acc[c] += mv * xr[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const double v = warp_sum(acc[c]);
+        if (lane == 0 && c0 + c < q)
+          Out[(long long)i * p + c0 + c] = shift ? v - shift[c0 + c] * Xs[i * ldx + c0 + c] : v;
+      }
+    }
+  }
+}
+
+// Xs[l * ldx + c] = X[l * p + c], c < q
+__device__ __forceinline__ void cta_stage_block(const double* X, int nr, int p, int q, double* Xs, int ldx) {
+  for (int e = threadIdx.x; e < nr * q; e += blockDim.x) {
+    const int l = e / q, c = e - l * q;
+    Xs[l * ldx + c] = X[(long long)l * p + c];
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int p, const double* A_all, const double* inv_all,
                                      double* V_all, double* evals_all, int* iters, double tol, int max_it,
-                                     double* work_all) {
+                                     double* work_all, int ldx) {
+  extern __shared__ double xs[];  // nr x ldx staging block when ldx > 0
   const int r = blockIdx.x;
   const double* A = A_all + (long long)r * nr * nr;
   const double* inv = inv_all + (long long)r * nr * nr;
@@ -392,12 +611,17 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
   int it = 0;
   for (; it < max_it; ++it) {
     // Y = inv X
-    for (long long e = tid; e < (long long)nr * p; e += nt) {
-      const int i = (int)(e / p), j = (int)(e % p);
-      const double* row = inv + (long long)i * nr;
-      double acc = 0.0;
-      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + j];
-      Y[e] = acc;
+    if (ldx > 0) {
+      cta_stage_block(X, nr, p, p, xs, ldx);
+      cta_rows_mm(inv, nr, xs, ldx, p, Y, p, nullptr);
+    } else {
+      for (long long e = tid; e < (long long)nr * p; e += nt) {
+        const int i = (int)(e / p), j = (int)(e % p);
+        const double* row = inv + (long long)i * nr;
+        double acc = 0.0;
+        for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + j];
+        Y[e] = acc;
+      }
     }
     __syncthreads();
     // SVQB: G = Y^T Y, D^-1/2 G D^-1/2 = U w U^T, X = Y D^-1/2 U w^-1/2 (kept columns)
@@ -439,12 +663,17 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
     }
     __syncthreads();
     // AY = A X (q columns), H = X^T A X
-    for (long long e = tid; e < (long long)nr * q; e += nt) {
-      const int i = (int)(e / q), c = (int)(e % q);
-      const double* row = A + (long long)i * nr;
-      double acc = 0.0;
-      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
-      AY[(long long)i * p + c] = acc;
+    if (ldx > 0) {
+      cta_stage_block(X, nr, p, q, xs, ldx);
+      cta_rows_mm(A, nr, xs, ldx, q, AY, p, nullptr);
+    } else {
+      for (long long e = tid; e < (long long)nr * q; e += nt) {
+        const int i = (int)(e / q), c = (int)(e % q);
+        const double* row = A + (long long)i * nr;
+        double acc = 0.0;
+        for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
+        AY[(long long)i * p + c] = acc;
+      }
     }
     __syncthreads();
     for (int e = tid; e < q * q; e += nt) {
@@ -478,12 +707,17 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
     }
     __syncthreads();
     // recompute AY for the Ritz vectors and the residuals of the wanted ones
-    for (long long e = tid; e < (long long)nr * q; e += nt) {
-      const int i = (int)(e / q), c = (int)(e % q);
-      const double* row = A + (long long)i * nr;
-      double acc = 0.0;
-      for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
-      AY[(long long)i * p + c] = acc - w[c] * X[(long long)i * p + c];
+    if (ldx > 0) {
+      cta_stage_block(X, nr, p, q, xs, ldx);
+      cta_rows_mm(A, nr, xs, ldx, q, AY, p, w);
+    } else {
+      for (long long e = tid; e < (long long)nr * q; e += nt) {
+        const int i = (int)(e / q), c = (int)(e % q);
+        const double* row = A + (long long)i * nr;
+        double acc = 0.0;
+        for (int l = 0; l < nr; ++l) acc += row[l] * X[(long long)l * p + c];
+        AY[(long long)i * p + c] = acc - w[c] * X[(long long)i * p + c];
+      }
     }
     __syncthreads();
     if (tid == 0) conv = 1;
@@ -515,7 +749,16 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
 
 void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
                                double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st) {
-  { note_launch(); k_dense_smallest_eig<<<nrank, 512, 0, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work); }
+  // stage the iteration block in shared memory (odd leading dimension: no bank conflicts) when it fits
+  int ldx = p | 1;
+  size_t smem = (size_t)nr * ldx * sizeof(double);
+  if (smem > 160 * 1024) {
+    ldx = 0;
+    smem = 0;
+  } else {  // the kernel also holds ~26 KB of static shared memory
+    cudaFuncSetAttribute(k_dense_smallest_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  { note_launch(); k_dense_smallest_eig<<<nrank, 512, smem, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work, ldx); }
 }
 
 }  // namespace pmf
