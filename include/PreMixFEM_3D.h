@@ -30,9 +30,11 @@
  * preconditioned CG on the device; any other PC or norm type runs PETSc's CG
  * recurrence on the host over the same callbacks.
  *
- * Differences a caller can see: -use_full_Cholesky_lv1 is rejected with
- * PETSC_ERR_SUP, and -use_2level needs a global coarse problem of at most 8192
- * unknowns (it is solved densely); the multiscale bases stay in device memory, so
+ * Differences a caller can see: -use_full_Cholesky_lv1 factors every
+ * subdomain block as a banded Cholesky in natural order (bandwidth nx*ny, at
+ * most 1800; the factors take cells * (nx*ny + 1) values of device memory), and
+ * -use_2level needs a global coarse problem of at most 8192 unknowns (it is
+ * solved densely); the multiscale bases stay in device memory, so
  * s_ctx->ms_bases_c / ms_bases_cc / ksp_lv1 hold NULL handles (the flat ABI's
  * pmf_get_phi reads the bases); the per-subdomain arrays (eigen_num_lv1, ...)
  * cover every subdomain of every virtual rank, and coarse_start/len* list the

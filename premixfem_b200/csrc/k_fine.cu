@@ -584,6 +584,200 @@ void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, cons
     { note_launch(); k_prolong<T, 16><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
 }
 
+// ---------------------------------------------------------------------------
+// Exact level-1 local solves (-use_full_Cholesky_lv1, src/PreMixFEM_3D.c:205-207,
+// where the reference switches the local KSP from ICC(0) to a full Cholesky):
+// banded Cholesky L L^T of every subdomain's principal block in natural
+// order.  The lower bandwidth is b = nx*ny; column j of L holds L(j + d, j),
+// d = 0..b, at band[boff[s] + j * ld + d] with ld = band_ld(b) (a multiple of
+// 4, zero past the last row).
+constexpr int kCholW = 8;  // panel width of the factorisation
+
+__host__ __device__ inline int band_ld(int b) { return (b + 1 + 3) & ~3; }
+int band_ld_host(int b) { return band_ld(b); }
+
+// Blocked left-looking factorisation, one CTA per subdomain, FP64.  For each
+// panel of kCholW columns: the panel rows (b + kCholW of them) start from A and
+// subtract sum_q L(i, q) L(j0 + c, q) over the previous b columns (one thread
+// per row, the multipliers staged in shared memory), then the panel is
+// factored in shared memory and written out.  Non-positive pivots are counted
+// in *bad (and replaced by 1 so that the factor stays finite).
+__global__ void __launch_bounds__(256) k_band_chol_factor(Grid g, const SubInfo* subs, const double* tx,
+                                                          const double* ty, const double* tz, const double* diag,
+                                                          const long long* boff, double* band, int* bad) {
+  extern __shared__ double chs[];
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  const int n = q.ncells, b = q.nxny, ld = band_ld(b);
+  double* L = band + boff[blockIdx.x];
+  double* P = chs;                     // (b + kCholW) x kCholW panel, P[r * kCholW + c]
+  double* Mq = P + (b + kCholW) * kCholW;  // Mq[(qc - qlo) * kCholW + c] = L(j0 + c, qc)
+  int nbad = 0;
+  for (int j0 = 0; j0 < n; j0 += kCholW) {
+    const int wc = min(kCholW, n - j0);
+    const int rows = min(n - j0, b + wc);
+    const int qlo = max(0, j0 - b);
+    const int nq = j0 - qlo;
+    for (int e = threadIdx.x; e < nq * kCholW; e += blockDim.x) {
+      const int qq = e / kCholW, c = e - qq * kCholW;
+      const int qc = qlo + qq, d = j0 + c - qc;
+      Mq[e] = (c < wc && d <= b) ? L[(long long)qc * ld + d] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      const int i = j0 + r;
+      const int ii = i % q.nx, tt = i / q.nx, jj = tt % q.ny, kk = tt / q.ny;
+      const long long cg = ((long long)(q.z0 + kk) * g.N + (q.y0 + jj)) * g.M + (q.x0 + ii);
+      double acc[kCholW];
+#pragma unroll
+      for (int c = 0; c < kCholW; ++c) {
+        const int dd = i - (j0 + c);
+        double a = 0.0;
+        if (c < wc) {
+          if (dd == 0)
+            a = diag[cg];
+          else if (dd == 1 && ii > 0)
+            a = -tx[cg];
+          else if (dd == q.nx && jj > 0)
+            a = -ty[cg];
+          else if (dd == q.nxny && kk > 0)
+            a = -tz[cg];
+        }
+        acc[c] = a;
+      }
+      for (int qc = max(qlo, i - b); qc < j0; ++qc) {
+        const double lv = L[(long long)qc * ld + (i - qc)];
+        const double* m = Mq + (qc - qlo) * kCholW;
+#pragma unroll
+        for (int c = 0; c < kCholW; ++c) acc[c] -= lv * m[c];
+      }
+#pragma unroll
+      for (int c = 0; c < kCholW; ++c) P[r * kCholW + c] = acc[c];
+    }
+    __syncthreads();
+    for (int c = 0; c < wc; ++c) {
+      if (threadIdx.x == 0) {
+        double d = P[c * kCholW + c];
+        if (!(d > 0.0)) {
+          ++nbad;
+          d = 1.0;
+        }
+        P[c * kCholW + c] = sqrt(d);
+      }
+      __syncthreads();
+      const double piv = P[c * kCholW + c];
+      for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) P[r * kCholW + c] /= piv;
+      __syncthreads();
+      for (int r = c + 1 + threadIdx.x; r < rows; r += blockDim.x) {
+        const double lrc = P[r * kCholW + c];
+        for (int c2 = c + 1; c2 < wc; ++c2)
+          if (r >= c2) P[r * kCholW + c2] -= lrc * P[c2 * kCholW + c];
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < wc * ld; e += blockDim.x) {
+      const int c = e / ld, d = e - c * ld;
+      L[(long long)(j0 + c) * ld + d] = (d <= b && c + d < rows) ? P[(c + d) * kCholW + c] : 0.0;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && nbad) atomicAdd(bad, nbad);
+}
+
+void launch_band_chol_factor(const Grid& g, const SubInfo* subs, int nsub, int max_b, const double* tx,
+                             const double* ty, const double* tz, const double* diag, const long long* boff,
+                             double* band, int* bad, cudaStream_t st) {
+  const int smem = (2 * max_b + kCholW) * kCholW * (int)sizeof(double);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_band_chol_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  { note_launch(); k_band_chol_factor<<<nsub, 256, smem, st>>>(g, subs, tx, ty, tz, diag, boff, band, bad); }
+}
+
+// out = yin + (L L^T)^-1 (x - A yin), one warp per subdomain: the right-hand
+// side goes to shared memory, then a column-oriented forward substitution
+// (w_j = u_j / L_jj; u_{j+d} -= L(j+d, j) w_j across the lanes) and a dot-
+// product backward substitution (z_j = (w_j - sum_d L(j+d, j) z_{j+d}) / L_jj).
+template <typename T, bool HAS_Y, bool FINAL>
+__global__ void __launch_bounds__(32) k_band_chol_apply(Grid g, const SubInfo* subs, const T* tx, const T* ty,
+                                                        const T* tz, const T* diag, const long long* boff,
+                                                        const T* band, const double* x, const T* yin, T* out_t,
+                                                        double* out_d, double* part, const int* done) {
+  if (done && *done) return;
+  extern __shared__ __align__(16) unsigned char chu_raw[];
+  T* u = reinterpret_cast<T*>(chu_raw);
+  const SubGeom q = sub_geom(subs[blockIdx.x]);
+  const int n = q.ncells, b = q.nxny, ld = band_ld(b);
+  const T* L = band + boff[blockIdx.x];
+  const int lane = threadIdx.x;
+  for (int cl = lane; cl < n; cl += 32) {
+    const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
+    const int ex = q.x0 + i, ey = q.y0 + j, ez = q.z0 + k;
+    const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    T r = (T)x[cg];
+    if (HAS_Y) r -= apply_A(g, cg, ex, ey, ez, tx, ty, tz, diag, yin);
+    u[cl] = r;
+  }
+  __syncwarp();
+  for (int j = 0; j < n; ++j) {
+    const T* col = L + (long long)j * ld;
+    const T wj = u[j] / col[0];
+    const int dmax = min(b, n - 1 - j);
+    __syncwarp();
+    if (lane == 0) u[j] = wj;
+#pragma unroll 4
+    for (int d = 1 + lane; d <= dmax; d += 32) u[j + d] -= col[d] * wj;
+    __syncwarp();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    const T* col = L + (long long)j * ld;
+    const int dmax = min(b, n - 1 - j);
+    T sacc = (T)0;
+#pragma unroll 4
+    for (int d = 1 + lane; d <= dmax; d += 32) sacc += col[d] * u[j + d];
+    sacc = warp_sum(sacc);
+    if (lane == 0) u[j] = (u[j] - sacc) / col[0];
+    __syncwarp();
+  }
+  double dot = 0.0;
+  for (int cl = lane; cl < n; cl += 32) {
+    const int i = cl % q.nx, tt = cl / q.nx, j = tt % q.ny, k = tt / q.ny;
+    const long long cg = ((long long)(q.z0 + k) * g.N + (q.y0 + j)) * g.M + (q.x0 + i);
+    T o = u[cl];
+    if (HAS_Y) o += yin[cg];
+    if (FINAL) {
+      const double od = (double)o;
+      out_d[cg] = od;
+      dot += x[cg] * od;
+    } else {
+      out_t[cg] = o;
+    }
+  }
+  if (FINAL) {
+    dot = warp_sum(dot);
+    if (lane == 0) part[blockIdx.x] = dot;
+  }
+}
+
+template <typename T>
+void launch_band_chol_apply(const Grid& g, const SubInfo* subs, int nsub, int max_cells, const T* tx, const T* ty,
+                            const T* tz, const T* diag, const long long* boff, const T* band, const double* x,
+                            const T* yin, T* out_t, double* out_d, double* part, const int* done, cudaStream_t st) {
+  const int smem = max_cells * (int)sizeof(T);
+  const bool fin = out_d != nullptr;
+#define PMF_BCH(HY, FN)                                                                                        \
+  {                                                                                                            \
+    if (smem > 48 * 1024)                                                                                      \
+      cudaFuncSetAttribute(k_band_chol_apply<T, HY, FN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);   \
+    note_launch();                                                                                             \
+    k_band_chol_apply<T, HY, FN><<<nsub, 32, smem, st>>>(g, subs, tx, ty, tz, diag, boff, band, x, yin, out_t, \
+                                                         out_d, part, done);                                   \
+  }
+  if (yin) {
+    if (fin) PMF_BCH(true, true) else PMF_BCH(true, false)
+  } else {
+    if (fin) PMF_BCH(false, true) else PMF_BCH(false, false)
+  }
+#undef PMF_BCH
+}
+
 #define PMF_INST(T)                                                                                              \
   template void launch_ic_apply<T>(const Grid&, const SubInfo*, int, int, int, const T*, const T*, const T*,      \
                                    const T*, const T*, const double*, const T*, T*, double*, double*, const int*, \
@@ -592,7 +786,10 @@ void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, cons
                                          const T*, const T*, const double*, const T*, double*, const int*,        \
                                          cudaStream_t);                                                           \
   template void launch_prolong<T>(const Grid&, const SubInfo*, int, int, const T*, const double*, T*, const int*, \
-                                  cudaStream_t);
+                                  cudaStream_t);                                                                \
+  template void launch_band_chol_apply<T>(const Grid&, const SubInfo*, int, int, const T*, const T*, const T*,   \
+                                          const T*, const long long*, const T*, const double*, const T*, T*,     \
+                                          double*, double*, const int*, cudaStream_t);
 PMF_INST(float)
 PMF_INST(double)
 #undef PMF_INST

@@ -839,7 +839,7 @@ PetscErrorCode PC_init(PCCtx* s_ctx, PetscScalar* dom, PetscInt* mesh) {
   s_ctx->eigen_bd_lv2 = o.eb_lv2 < 0.0 ? 1.0 / NIL : o.eb_lv2;
   s_ctx->use_W_cycle = o.use_W_cycle ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->no_shift_A_cc = o.no_shift_A_cc ? PETSC_TRUE : PETSC_FALSE;
-  s_ctx->use_full_Cholesky_lv1 = PETSC_FALSE;
+  s_ctx->use_full_Cholesky_lv1 = o.use_full_Cholesky_lv1 ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->use_2level = o.use_2level ? PETSC_TRUE : PETSC_FALSE;
   s_ctx->H_x = dom[0] / (double)mesh[0];
   s_ctx->H_y = dom[1] / (double)mesh[1];

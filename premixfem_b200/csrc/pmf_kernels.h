@@ -64,6 +64,19 @@ void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines
                      const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
                      T* out_t, double* out_d, double* part, const int* done, cudaStream_t st);
 
+// Exact level-1 solves (-use_full_Cholesky_lv1): banded Cholesky of every
+// subdomain block in natural order, column j of L at band[boff[s] + j*band_ld(b)],
+// b = nx*ny; bad counts non-positive pivots.
+int band_ld_host(int b);
+void launch_band_chol_factor(const Grid& g, const SubInfo* subs, int nsub, int max_b, const double* tx,
+                             const double* ty, const double* tz, const double* diag, const long long* boff,
+                             double* band, int* bad, cudaStream_t st);
+// out = yin + (L L^T)^-1 (x - A yin), the same contract as launch_ic_apply.
+template <typename T>
+void launch_band_chol_apply(const Grid& g, const SubInfo* subs, int nsub, int max_cells, const T* tx, const T* ty,
+                            const T* tz, const T* diag, const long long* boff, const T* band, const double* x,
+                            const T* yin, T* out_t, double* out_d, double* part, const int* done, cudaStream_t st);
+
 // c[s*kmax + j] = sum_{cells of s} phi[c*kmax + j] * (x - A y)[c]   (y may be null)
 template <typename T>
 void launch_resid_restrict(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,

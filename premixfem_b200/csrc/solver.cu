@@ -136,10 +136,6 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
     *err = "-pmf_learned_its must be >= 1";
     return 62;
   }
-  if (o->use_full_Cholesky_lv1) {
-    *err = "-use_full_Cholesky_lv1 is not supported by this build (IC(0) only)";
-    return 56;  // PETSC_ERR_SUP
-  }
   return 0;
 }
 
@@ -254,7 +250,7 @@ Solver::~Solver() {
     if (p) cudaFree(p);
   if (eb.h_nactive) cudaFreeHost(eb.h_nactive);
   for (void* p : {(void*)A2g, (void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
-                  (void*)d_status_learned})
+                  (void*)d_status_learned, (void*)d_boff, (void*)band64, (void*)band32})
     if (p) cudaFree(p);
   delete net;
   if (h_state) cudaFreeHost(h_state);
@@ -633,7 +629,11 @@ int Solver::setup() {
     if (dir_on_[f]) dmask |= 1 << f;
   if (!d_flag) cudaMalloc(&d_flag, 4 * sizeof(int));
   cudaMemsetAsync(d_flag, 0, 4 * sizeof(int), st);
-  launch_ic_factor(g, d_subs, nsub, max_lines, tx, ty, tz, diag, inv64, d_flag, st);
+  if (opt.use_full_Cholesky_lv1) {
+    if (int er = setup_band_cholesky(mixed)) return er;
+  } else {
+    launch_ic_factor(g, d_subs, nsub, max_lines, tx, ty, tz, diag, inv64, d_flag, st);
+  }
   if (mixed) {
     launch_to_f32(tx, tx32, g.ncell, st);
     launch_to_f32(ty, ty32, g.ncell, st);
@@ -763,7 +763,8 @@ int Solver::setup() {
   int bad_pivots = 0;
   cudaMemcpy(&bad_pivots, d_flag, sizeof(int), cudaMemcpyDeviceToHost);
   if (bad_pivots) {
-    err = "non-positive IC(0) pivot in a level-1 factorisation";
+    err = opt.use_full_Cholesky_lv1 ? "non-positive pivot in a level-1 Cholesky factorisation"
+                                    : "non-positive IC(0) pivot in a level-1 factorisation";
     return 71;  // PETSC_ERR_MAT_LU_ZRPVT
   }
   for (int s = 0; s < nsub; ++s) subs[s].k = ks[s];
@@ -880,6 +881,48 @@ int Solver::setup() {
   return finish();
 }
 
+// -use_full_Cholesky_lv1 (src/PreMixFEM_3D.c:205-207): banded Cholesky factors
+// of every subdomain block, FP64 (plus an FP32 copy for the mixed form).
+int Solver::setup_band_cholesky(bool mixed) {
+  std::vector<long long> off(nsub);
+  long long len = 0;
+  int mb = 0;
+  for (int s = 0; s < nsub; ++s) {
+    const SubInfo& S = subs[s];
+    const int b = S.nx * S.ny;
+    off[s] = len;
+    len += (long long)S.nx * S.ny * S.nz * band_ld_host(b);
+    mb = std::max(mb, b);
+  }
+  if ((2LL * mb + 8) * 8 * 8 > 227 * 1024) {
+    err = "subdomain too wide for the banded Cholesky factorisation (nx*ny <= 1800)";
+    return 62;
+  }
+  if (len != band_len) {
+    if (band64) cudaFree(band64);
+    if (band32) cudaFree(band32);
+    band64 = nullptr;
+    band32 = nullptr;
+    size_t freeb = 0, totb = 0;
+    cudaMemGetInfo(&freeb, &totb);
+    const size_t need = (size_t)len * (8 + (mixed ? 4 : 0));
+    if (need + (256u << 20) > freeb) {
+      err = "not enough device memory for the level-1 Cholesky factors";
+      return 55;  // PETSC_ERR_MEM
+    }
+    if (int er = check(cudaMalloc(&band64, sizeof(double) * len), "cudaMalloc Cholesky factors")) return er;
+    band_len = len;
+  }
+  if (mixed && !band32)
+    if (int er = check(cudaMalloc(&band32, sizeof(float) * len), "cudaMalloc Cholesky factors (FP32)")) return er;
+  if (!d_boff) cudaMalloc(&d_boff, sizeof(long long) * nsub);
+  cudaMemcpyAsync(d_boff, off.data(), sizeof(long long) * nsub, cudaMemcpyHostToDevice, st);
+  launch_band_chol_factor(g, d_subs, nsub, mb, tx, ty, tz, diag, d_boff, band64, d_flag, st);
+  if (mixed) launch_to_f32(band64, band32, len, st);
+  // the host vector must outlive the asynchronous copy
+  return check(cudaStreamSynchronize(st), "level-1 Cholesky factorisation");
+}
+
 template <typename T>
 void Solver::apply_impl(const double* x, double* out, double* partial, const int* done) {
   const bool f32 = sizeof(T) == 4;
@@ -903,7 +946,17 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
         z_pend = false;
       }
       const T* yin = y_zero ? nullptr : yb[cur];
-      if (last)
+      if (opt.use_full_Cholesky_lv1) {
+        const T* tband = f32 ? (const T*)band32 : (const T*)band64;
+        if (last)
+          launch_band_chol_apply<T>(g, d_subs, nsub, max_cells, ttx, tty, ttz, tdg, d_boff, tband, x, yin, nullptr,
+                                    out, partial, done, st);
+        else {
+          launch_band_chol_apply<T>(g, d_subs, nsub, max_cells, ttx, tty, ttz, tdg, d_boff, tband, x, yin,
+                                    yb[1 - cur], nullptr, nullptr, done, st);
+          cur = 1 - cur;
+        }
+      } else if (last)
         launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, nullptr, out,
                            partial, done, st);
       else {

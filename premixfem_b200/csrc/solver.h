@@ -107,6 +107,11 @@ class Solver {
   double *tx = nullptr, *ty = nullptr, *tz = nullptr, *diag = nullptr, *db = nullptr, *bval = nullptr;
   float *tx32 = nullptr, *ty32 = nullptr, *tz32 = nullptr, *diag32 = nullptr, *inv32 = nullptr;
   double* inv64 = nullptr;
+  // -use_full_Cholesky_lv1: banded Cholesky factors of the subdomain blocks
+  long long* d_boff = nullptr;
+  double* band64 = nullptr;
+  float* band32 = nullptr;
+  long long band_len = 0;
   void* phi = nullptr;
   double *blk = nullptr, *gface = nullptr, *A2inv = nullptr, *AN = nullptr, *ANinv = nullptr, *V3 = nullptr,
          *A3inv = nullptr, *d_eig1 = nullptr, *d_eig3 = nullptr;
@@ -146,6 +151,7 @@ class Solver {
   unsigned long long pcg_graph_kernels = 0;
   unsigned long long eig_colcells = 0;
   int alloc_eb(int m, bool mixed);
+  int setup_band_cholesky(bool mixed);
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;

@@ -190,3 +190,38 @@ def test_two_level_matches_oracle(native, name, precision):
     xd = O.direct_solve(ref["op"], ref["b"])
     assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
     s.close()
+
+
+CHOL_CASES = {
+    "grf16_chol": (lambda: fields.unit_cube_grf(16, seed=1),
+                   {"sd": 2, "en_lv1": 4, "en_lv2": 4, "use_full_Cholesky_lv1": True}),
+    "ragged_vr_chol": (lambda: fields.random_box((13, 11, 9), seed=7, sigma=2.0),
+                       {"pmf_sd": (2, 2, 1), "pmf_vranks": (2, 1, 3), "en_lv1": 3, "en_lv2": 2,
+                        "use_full_Cholesky_lv1": True}),
+}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", list(CHOL_CASES))
+def test_full_cholesky_level1_matches_oracle(native, name, precision):
+    """-use_full_Cholesky_lv1: exact banded Cholesky local solves against the
+    oracle's exact local Cholesky (preconditioner output in FP64, PCG
+    iterations +-1 and the solution within 1e-8 of a direct solve in both
+    precisions)."""
+    mk, d = CHOL_CASES[name]
+    prob = mk()
+    ref = O.solve(prob, _oracle_opts(d))
+    s = _gpu(prob, dict(d, pmf_precision=precision))
+    if precision == "fp64":
+        x = np.random.default_rng(11).standard_normal(ref["op"].n)
+        yr = ref["pc"].apply(x)
+        rel = np.linalg.norm(s.pc_apply(x) - yr) / np.linalg.norm(yr)
+        assert rel <= 1e-6, f"PC_apply_vec relative difference {rel:.2e}"
+    b = s.rhs(prob["source"].ravel())
+    x, its, rnorm, reason = s.solve(b)
+    assert reason == "converged"
+    assert abs(its - ref["its"]) <= 1, f"iterations {its} vs oracle {ref['its']}"
+    xd = O.direct_solve(ref["op"], ref["b"])
+    err = np.linalg.norm(x - xd) / np.linalg.norm(xd)
+    assert err <= 1e-8, f"solution error vs direct {err:.2e}"
+    s.close()
