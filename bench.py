@@ -357,6 +357,7 @@ def run_b200(args):
             "peak_kind": peak_kind,
         },
         "clocks": results["mixed"]["clocks"],
+        "autotune": _tune_choices(lib),
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, wl, prob, its_p)
@@ -365,6 +366,18 @@ def run_b200(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _tune_choices(lib):
+    """The launch-shape tuner's choices of this process: {kernel|shape: [choice, per-candidate us]}."""
+    n = lib.pmf_tune_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib.pmf_tune_report(buf, n + 1)
+    try:
+        table = json.loads(buf.value.decode())
+    except ValueError:
+        return None
+    return {k.rsplit("|", 1)[0]: [v["choice"], v["us"]] for k, v in table.items()}
 
 
 def time_spmv(s, n):

@@ -141,6 +141,12 @@ int pmf_residual_noalloc(pmf_solver* s, const double* b, const double* x, double
  * subdomain-iterations of (basis columns x cells), the unit of the Gram and update traffic. */
 int pmf_get_eig_phases(pmf_solver* s, double ms[8], unsigned long long* colcells);
 
+/* Launch-shape tuner table of this process as JSON ({"<kernel>|<shape>|<device>": {"choice": c,
+ * "us": [per-candidate microseconds]}, ...}).  Copies at most len-1 bytes and a terminating zero into
+ * buf (buf may be NULL); returns the full length.  The tuner is on unless PMF_AUTOTUNE=0 or
+ * -pmf_autotune 0; PMF_TUNE_FILE=<path> keeps the table across processes. */
+int pmf_tune_report(char* buf, int len);
+
 /* total number of CUDA kernels launched by this library in this process */
 unsigned long long pmf_launch_count(void);
 

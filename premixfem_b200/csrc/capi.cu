@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/pmf_b200.h"
+#include "tune.h"
 #include "solver.h"
 
 struct pmf_solver {
@@ -208,6 +209,16 @@ int pmf_get_eig_phases(pmf_solver* h, double ms[8], unsigned long long* colcells
     for (int i = 0; i < 8; ++i) ms[i] = h->s->eig_phase_ms[i];
   if (colcells) *colcells = h->s->eig_colcells;
   return 0;
+}
+
+int pmf_tune_report(char* buf, int len) {
+  const std::string r = pmf::tune_report();
+  if (buf && len > 0) {
+    const int n = std::min<int>(len - 1, (int)r.size());
+    memcpy(buf, r.data(), n);
+    buf[n] = 0;
+  }
+  return (int)r.size();
 }
 
 unsigned long long pmf_launch_count(void) { return __atomic_load_n(&pmf::g_launches, __ATOMIC_RELAXED); }

@@ -464,8 +464,8 @@ __global__ void k_ic_apply(Grid g, const SubInfo* subs, const T* tx, const T* ty
 template <typename T>
 void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines, int max_cells, const T* tx,
                      const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
-                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st) {
-  int threads = std::max(64, ((max_lines + 31) / 32) * 32);
+                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st, int threads) {
+  threads = std::max(threads, std::max(64, ((max_lines + 31) / 32) * 32));
   const int ldc = (max_cells + 3) & ~3;
   size_t smem = 32 * sizeof(double) + (size_t)5 * ldc * sizeof(T);
   const bool fin = out_d != nullptr;
@@ -533,23 +533,24 @@ __global__ void k_resid_restrict(Grid g, const SubInfo* subs, int kmax, const T*
 template <typename T, int KM>
 static void rr_dispatch(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
                         const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
-                        const int* done, cudaStream_t st) {
+                        const int* done, cudaStream_t st, int threads) {
   if (y)
-    { note_launch(); k_resid_restrict<T, KM, true><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
+    { note_launch(); k_resid_restrict<T, KM, true><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
   else
-    { note_launch(); k_resid_restrict<T, KM, false><<<nsub, 256, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
+    { note_launch(); k_resid_restrict<T, KM, false><<<nsub, threads, 0, st>>>(g, subs, kmax, tx, ty, tz, diag, phi, x, y, c, done); }
 }
 
 template <typename T>
 void launch_resid_restrict(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
                            const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
-                           const int* done, cudaStream_t st) {
+                           const int* done, cudaStream_t st, int threads) {
+  threads = (threads >= 32 && threads <= 1024 && threads % 32 == 0) ? threads : 256;
   if (kmax <= 4)
-    rr_dispatch<T, 4>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+    rr_dispatch<T, 4>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st, threads);
   else if (kmax <= 8)
-    rr_dispatch<T, 8>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+    rr_dispatch<T, 8>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st, threads);
   else
-    rr_dispatch<T, 16>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st);
+    rr_dispatch<T, 16>(g, subs, nsub, kmax, tx, ty, tz, diag, phi, x, y, c, done, st, threads);
 }
 
 // Prolongation y += Phi_s Z_s (VecMAXPY in _PC_apply_vec_lv2, :1578).
@@ -575,13 +576,14 @@ __global__ void k_prolong(Grid g, const SubInfo* subs, int kmax, const T* phi, c
 
 template <typename T>
 void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* phi, const double* Z, T* y,
-                    const int* done, cudaStream_t st) {
+                    const int* done, cudaStream_t st, int threads) {
+  threads = (threads >= 32 && threads <= 1024 && threads % 32 == 0) ? threads : 256;
   if (kmax <= 4)
-    { note_launch(); k_prolong<T, 4><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
+    { note_launch(); k_prolong<T, 4><<<nsub, threads, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
   else if (kmax <= 8)
-    { note_launch(); k_prolong<T, 8><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
+    { note_launch(); k_prolong<T, 8><<<nsub, threads, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
   else
-    { note_launch(); k_prolong<T, 16><<<nsub, 256, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
+    { note_launch(); k_prolong<T, 16><<<nsub, threads, 0, st>>>(g, subs, kmax, phi, Z, y, done); }
 }
 
 // ---------------------------------------------------------------------------
@@ -781,12 +783,12 @@ void launch_band_chol_apply(const Grid& g, const SubInfo* subs, int nsub, int ma
 #define PMF_INST(T)                                                                                              \
   template void launch_ic_apply<T>(const Grid&, const SubInfo*, int, int, int, const T*, const T*, const T*,      \
                                    const T*, const T*, const double*, const T*, T*, double*, double*, const int*, \
-                                   cudaStream_t);                                                                \
+                                   cudaStream_t, int);                                                           \
   template void launch_resid_restrict<T>(const Grid&, const SubInfo*, int, int, const T*, const T*, const T*,     \
                                          const T*, const T*, const double*, const T*, double*, const int*,        \
-                                         cudaStream_t);                                                           \
+                                         cudaStream_t, int);                                                      \
   template void launch_prolong<T>(const Grid&, const SubInfo*, int, int, const T*, const double*, T*, const int*, \
-                                  cudaStream_t);                                                                \
+                                  cudaStream_t, int);                                                           \
   template void launch_band_chol_apply<T>(const Grid&, const SubInfo*, int, int, const T*, const T*, const T*,   \
                                           const T*, const long long*, const T*, const double*, const T*, T*,     \
                                           double*, double*, const int*, cudaStream_t);

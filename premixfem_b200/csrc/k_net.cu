@@ -24,6 +24,7 @@
 
 #include "pmf_kernels.h"
 #include "pmf_net.h"
+#include "tune.h"
 
 namespace pmf {
 
@@ -804,6 +805,34 @@ int Net::ensure(int B) {
   return 0;
 }
 
+// One forward layer with ROWS-row tiles and MT 16-row m-tiles per warp.
+template <int NT, int ROWS, int MT>
+static bool fwd_launch_t(const FwdArgs& a, long long rows, cudaStream_t st) {
+  const size_t smem = (2 * (size_t)ROWS * (a.cin + 8) + 2 * (size_t)a.cin * (a.cout + 8)) * 2;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_net_fwd<NT, ROWS, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_net_fwd<NT, ROWS, MT><<<(int)(rows / ROWS), ROWS * 2 / MT, smem, st>>>(a);
+  return true;
+}
+
+template <int NT>
+static bool fwd_launch_nt(int R, int MT, const FwdArgs& a, long long rows, cudaStream_t st) {
+  if (R == 256 && MT == 2) return fwd_launch_t<NT, 256, 2>(a, rows, st);
+  if (R == 128 && MT == 1) return fwd_launch_t<NT, 128, 1>(a, rows, st);
+  if (R == 128 && MT == 2) return fwd_launch_t<NT, 128, 2>(a, rows, st);
+  if (R == 64 && MT == 1) return fwd_launch_t<NT, 64, 1>(a, rows, st);
+  return false;
+}
+
+static bool fwd_launch(int ntv, int R, int MT, const FwdArgs& a, long long rows, cudaStream_t st) {
+  switch (ntv) {
+    case 2: return fwd_launch_nt<2>(R, MT, a, rows, st);
+    case 4: return fwd_launch_nt<4>(R, MT, a, rows, st);
+    case 8: return fwd_launch_nt<8>(R, MT, a, rows, st);
+    case 12: return fwd_launch_nt<12>(R, MT, a, rows, st);
+  }
+  return false;
+}
+
 int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_t st) {
   if (!w32_[0]) {
     err = "network weights not initialised or loaded";
@@ -827,32 +856,26 @@ int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_
     a.out = L.out_act == NET_ACTS - 1 ? nullptr : act_[L.out_act];
     a.outf = L.out_act == NET_ACTS - 1 ? y : nullptr;
     const long long rows = (long long)B * L.s_out * L.s_out * L.s_out;
-    // 128-row tiles where a tile stays inside one sample (and one parity class for up2)
+    // tiles stay inside one sample (and one parity class for up2); candidate 0
+    // is the built-in choice, the tuner may pick another for this layer and batch
     const int per = L.type == NL_UP2 ? L.s_in * L.s_in * L.s_in : L.s_out * L.s_out * L.s_out;
-    const bool big = per % 256 == 0;
-    const int R = big ? 256 : 64;
-    const int grid = (int)(rows / R);
-    const size_t smem = (2 * (size_t)R * (L.cin + 8) + 2 * (size_t)L.cin * (L.cout + 8)) * 2;
-    note_launch();
-    // 256-row tiles: 8 warps x two 16-row tiles; 64-row tiles (4^3 layers): 4 warps x one
-#define PMF_FWD(NTV)                                                                                      \
-  do {                                                                                                    \
-    if (big) {                                                                                            \
-      if (smem > 48 * 1024) cudaFuncSetAttribute(k_net_fwd<NTV, 256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-      k_net_fwd<NTV, 256, 2><<<grid, 256, smem, st>>>(a);                                                 \
-    } else {                                                                                              \
-      if (smem > 48 * 1024) cudaFuncSetAttribute(k_net_fwd<NTV, 64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-      k_net_fwd<NTV, 64, 1><<<grid, 128, smem, st>>>(a);                                                  \
-    }                                                                                                     \
-  } while (0)
-    switch (L.cout / 8) {
-      case 2: PMF_FWD(2); break;
-      case 4: PMF_FWD(4); break;
-      case 8: PMF_FWD(8); break;
-      case 12: PMF_FWD(12); break;
-      default: err = "unsupported layer width"; return 56;
+    static const int kTiles[4][2] = {{256, 2}, {128, 1}, {128, 2}, {64, 1}};
+    int cand[4], nc = 0;
+    const int def = per % 256 == 0 ? 0 : 3;
+    cand[nc++] = def;
+    for (int t = 0; t < 4; ++t)
+      if (t != def && per % kTiles[t][0] == 0) cand[nc++] = t;
+    const int ntv = L.cout / 8;
+    if (ntv != 2 && ntv != 4 && ntv != 8 && ntv != 12) {
+      err = "unsupported layer width";
+      return 56;
     }
-#undef PMF_FWD
+    auto launch = [&](int c) -> bool { return fwd_launch(ntv, kTiles[cand[c]][0], kTiles[cand[c]][1], a, rows, st); };
+    char key[96];
+    snprintf(key, sizeof(key), "net_fwd|L%d|B%d", l, B);
+    const int c = tune_choose(key, nc, launch, st);
+    note_launch();
+    launch(c);
   }
   (void)keep;
   return 0;

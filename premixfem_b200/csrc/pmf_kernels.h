@@ -62,7 +62,7 @@ void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_line
 template <typename T>
 void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines, int max_cells, const T* tx,
                      const T* ty, const T* tz, const T* diag, const T* inv_d, const double* x, const T* yin,
-                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st);
+                     T* out_t, double* out_d, double* part, const int* done, cudaStream_t st, int threads = 0);
 
 // Exact level-1 solves (-use_full_Cholesky_lv1): banded Cholesky of every
 // subdomain block in natural order, column j of L at band[boff[s] + j*band_ld(b)],
@@ -81,12 +81,12 @@ void launch_band_chol_apply(const Grid& g, const SubInfo* subs, int nsub, int ma
 template <typename T>
 void launch_resid_restrict(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* tx, const T* ty,
                            const T* tz, const T* diag, const T* phi, const double* x, const T* y, double* c,
-                           const int* done, cudaStream_t st);
+                           const int* done, cudaStream_t st, int threads = 256);
 
 // y[c] += sum_j phi[c*kmax + j] * Z[s*kmax + j]
 template <typename T>
 void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, const T* phi, const double* Z, T* y,
-                    const int* done, cudaStream_t st);
+                    const int* done, cudaStream_t st, int threads = 256);
 
 // ---- coarse (FP64) -------------------------------------------------------------
 // out = alpha*v_in_out_base - A2 * v   where A2 is block sparse: blk[s][b][kmax][kmax],

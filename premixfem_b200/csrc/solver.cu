@@ -10,6 +10,7 @@
 
 #include "pmf_net.h"
 #include "solver.h"
+#include "tune.h"
 
 namespace pmf {
 
@@ -118,6 +119,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_batched", &o->eig_batched);
   db.get_int("pmf_eig_profile", &o->eig_profile);
   db.get_int("pmf_pcg_graph", &o->pcg_graph);
+  db.get_int("pmf_autotune", &o->autotune);
   {
     auto it2 = db.kv.find("pmf_learned");
     if (it2 != db.kv.end()) {
@@ -615,6 +617,7 @@ int Solver::setup() {
     err = "kappa not set (PC_init contract: the caller constructs kappa before setup)";
     return 73;  // PETSC_ERR_ARG_WRONGSTATE
   }
+  if (opt.autotune >= 0) tune_set_enabled(opt.autotune == 1);
   cudaEvent_t e[8];
   for (auto& x : e) cudaEventCreate(&x);
   const bool mixed = opt.precision == 1;
@@ -806,6 +809,12 @@ int Solver::setup() {
     t_stages[ST_SU] += tot * 1e-3;
     last_setup_ms = tot;
     for (auto& x : e) cudaEventDestroy(x);
+    // launch shapes of the preconditioner kernels (first set-up of a shape only)
+    if (mixed)
+      tune_pc<float>();
+    else
+      tune_pc<double>();
+    if (int er = check(cudaStreamSynchronize(st), "launch-shape tuning")) return er;
     is_setup = true;
     return 0;
   };
@@ -923,6 +932,57 @@ int Solver::setup_band_cholesky(bool mixed) {
   return check(cudaStreamSynchronize(st), "level-1 Cholesky factorisation");
 }
 
+// Threads per subdomain of the level-1 solve and of the level-2 restriction /
+// prolongation, chosen by the launch-shape tuner on scratch buffers (the first
+// set-up of a shape times every candidate; later set-ups reuse the choice).
+template <typename T>
+void Solver::tune_pc() {
+  const bool f32 = sizeof(T) == 4;
+  const T* ttx = f32 ? (const T*)tx32 : (const T*)tx;
+  const T* tty = f32 ? (const T*)ty32 : (const T*)ty;
+  const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
+  const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
+  const T* tinv = f32 ? (const T*)inv32 : (const T*)inv64;
+  const T* tphi = (const T*)phi;
+  T* ya = (T*)y0;
+  T* yo = (T*)y1;
+  cudaMemsetAsync(ya, 0, sizeof(T) * g.ncell, st);
+  cudaMemsetAsync(z, 0, sizeof(double) * g.ncell, st);
+  cudaMemsetAsync(Zacc, 0, sizeof(double) * nsub * kmax, st);
+  const int old[3] = {ic_threads, rr_threads, pr_threads};
+  char key[192];
+  const char* prec = f32 ? "f32" : "f64";
+  if (!opt.use_full_Cholesky_lv1) {
+    const int base = std::max(64, ((max_lines + 31) / 32) * 32);
+    std::vector<int> cand = {base};
+    for (int t : {512, 1024})
+      if (t > base) cand.push_back(t);
+    snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d", prec, nsub, max_cells, max_lines);
+    const int ci = tune_choose(key, (int)cand.size(), [&](int i) {
+      launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, ya, yo, nullptr,
+                         nullptr, nullptr, st, cand[i]);
+      return true;
+    }, st);
+    ic_threads = cand[ci];
+  }
+  const int rcand[3] = {256, 128, 512};
+  snprintf(key, sizeof(key), "resid_restrict|%s|n%d|c%d|k%d", prec, nsub, max_cells, kmax);
+  rr_threads = rcand[tune_choose(key, 3, [&](int i) {
+    launch_resid_restrict<T>(g, d_subs, nsub, kmax, ttx, tty, ttz, tdg, tphi, z, ya, c, nullptr, st, rcand[i]);
+    return true;
+  }, st)];
+  snprintf(key, sizeof(key), "prolong|%s|n%d|c%d|k%d", prec, nsub, max_cells, kmax);
+  pr_threads = rcand[tune_choose(key, 3, [&](int i) {
+    launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yo, nullptr, st, rcand[i]);
+    return true;
+  }, st)];
+  if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads)) {
+    cudaGraphExecDestroy(pcg_exec);  // captured with other launch shapes
+    pcg_exec = nullptr;
+    pcg_graph_x = nullptr;
+  }
+}
+
 template <typename T>
 void Solver::apply_impl(const double* x, double* out, double* partial, const int* done) {
   const bool f32 = sizeof(T) == 4;
@@ -942,7 +1002,7 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
     const bool last = idx + 1 == sch.size();
     if (v == 1) {
       if (z_pend) {
-        launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st);
+        launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st, pr_threads);
         z_pend = false;
       }
       const T* yin = y_zero ? nullptr : yb[cur];
@@ -958,10 +1018,10 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
         }
       } else if (last)
         launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, nullptr, out,
-                           partial, done, st);
+                           partial, done, st, ic_threads);
       else {
         launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, yb[1 - cur],
-                           nullptr, nullptr, done, st);
+                           nullptr, nullptr, done, st, ic_threads);
         cur = 1 - cur;
       }
       y_zero = false;
@@ -969,11 +1029,11 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
     } else {
       if (!c_valid) {
         if (z_pend) {
-          launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st);
+          launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st, pr_threads);
           z_pend = false;
         }
         launch_resid_restrict<T>(g, d_subs, nsub, kmax, ttx, tty, ttz, tdg, tphi, x, y_zero ? nullptr : yb[cur], c,
-                                 done, st);
+                                 done, st, rr_threads);
         c_valid = true;
       }
       if (v == 2) {

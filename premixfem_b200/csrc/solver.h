@@ -34,6 +34,7 @@ struct Options {
   unsigned long long seed = 20240611ull;
   int pcg_chunk = 4;
   int pcg_graph = 1;  // replay each chunk of PCG iterations as one CUDA graph
+  int autotune = -1;  // launch-shape tuning: 1 on, 0 off, -1 the process default (PMF_AUTOTUNE)
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
@@ -152,6 +153,9 @@ class Solver {
   unsigned long long eig_colcells = 0;
   int alloc_eb(int m, bool mixed);
   int setup_band_cholesky(bool mixed);
+  template <typename T>
+  void tune_pc();
+  int ic_threads = 0, rr_threads = 256, pr_threads = 256;  // tuned launch shapes
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;

@@ -1,0 +1,85 @@
+"""The launch-shape tuner: every candidate it may pick computes the same thing.
+
+The tuner chooses by speed alone, so each candidate launch shape is checked
+here by forcing it (PMF_TUNE_FORCE=c): the network forward pass of each row
+tile against the CPU oracle (2e-2, the forward-pass tolerance of
+test_gpu_net.py), and the preconditioner application with each thread count
+of the level-1 solve and the level-2 restriction / prolongation against the
+built-in shape (1e-12 in FP64, 1e-5 in mixed precision: only the order of the
+block reductions changes).  The report of a tuned set-up lists its choices.
+"""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+
+from oracle import net_oracle as NO
+from premixfem_b200 import _native, fields, learned
+from premixfem_b200.solver import DarcySolver, options_string
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
+
+
+@pytest.mark.parametrize("cand", [0, 1, 2, 3])
+def test_net_forward_every_tile(native, monkeypatch, cand):
+    torch = pytest.importorskip("torch")
+    monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
+    net = learned.Net(seed=7)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((2, 16, 16, 16, 16)).astype(np.float32)
+    x[..., 5:] = 0.0
+    xt = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    xb = xt.float().cpu().numpy().astype(np.float64)
+    W, b = [], []
+    for l in range(9):
+        w_, b_ = net.weights(l)
+        W.append(w_.astype(np.float64))
+        b.append(b_.astype(np.float64))
+    y = torch.empty((2, 4096, 16), dtype=torch.float32, device="cuda")
+    net.forward(xt, y)
+    torch.cuda.synchronize()
+    ref = NO.forward(xb, W, b, bf16=True)[-1].reshape(2, 4096, 16)
+    assert _rel(y.cpu().numpy(), ref) < 2e-2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pc_apply_every_thread_shape(native, monkeypatch, precision):
+    prob = fields.fracture256(64, seed=3)
+    opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
+    x = np.random.default_rng(5).standard_normal(64 ** 3)
+    out = []
+    for cand in (0, 1, 2):
+        monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
+        s = DarcySolver.from_problem(prob, opts)
+        s.setup()
+        out.append(s.pc_apply(x))
+        s.close()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    for cand in (1, 2):
+        assert _rel(out[cand], out[0]) <= tol, (cand, _rel(out[cand], out[0]))
+
+
+def test_report_lists_the_tuned_shapes(native, monkeypatch):
+    monkeypatch.delenv("PMF_TUNE_FORCE", raising=False)
+    lib = _native.load()
+    prob = fields.unit_cube_grf(32, seed=2)
+    s = DarcySolver.from_problem(prob, "-sd 4 -pmf_autotune 1")
+    s.setup()
+    s.close()
+    n = lib.pmf_tune_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    assert lib.pmf_tune_report(buf, n + 1) == n
+    table = json.loads(buf.value.decode())
+    # 32^3 with -sd 4: 64 subdomains of 8^3 cells (64 x-lines each), 4 eigenvectors
+    shapes = ("ic_apply|f64|n64|c512|l64|", "resid_restrict|f64|n64|c512|k4|", "prolong|f64|n64|c512|k4|")
+    keys = [k for k in table if k.startswith(shapes)]
+    assert len(keys) == 3, list(table)
+    for k in keys:
+        e = table[k]
+        assert 0 <= e["choice"] < len(e["us"])
+        assert e["us"][e["choice"]] == min(t for t in e["us"] if t >= 0)
