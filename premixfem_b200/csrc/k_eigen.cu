@@ -25,6 +25,7 @@
 
 #include "pmf_dense.cuh"
 #include "pmf_kernels.h"
+#include "tune.h"
 
 namespace pmf {
 
@@ -1302,6 +1303,8 @@ __global__ void k_eb_control(EbArgs a, int nlist, int it) {
   es.nS = m + na + es.np;
   es.it = it + 1;  // iterations counted if the iteration limit ends the solve
   a.alist[atomicAdd(a.nactive, 1)] = s;  // order is irrelevant: subdomains are independent
+  atomicAdd(a.nactive + 1, na);          // active columns: the preconditioner's work
+  atomicAdd(a.nactive + 2, es.nS);       // basis columns: the Gram's and the update's work
   if (a.colcells) atomicAdd(a.colcells, (unsigned long long)es.nS * (unsigned long long)nc);
 }
 
@@ -1567,13 +1570,39 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   e.tx = a.tx;
   e.ty = a.ty;
   e.tz = a.tz;
-  // column batch of the preconditioner: coefficients + mb vectors within ~113 KB (2 CTAs per SM)
+  // column batch of the preconditioner: the built-in one keeps coefficients + mb
+  // vectors within ~113 KB (2 CTAs per SM); the online tuner also tries all m
+  // columns in one CTA (fewer barriers per column, 1 CTA per SM) and one column
   const size_t coef = (size_t)16 * e.ldc;
   e.mb = (int)std::max<size_t>(1, std::min<size_t>(a.m, (112 * 1024 - coef) / ((size_t)4 * e.ldc)));
-  const size_t pre_smem = coef + (size_t)4 * e.ldc * e.mb;
+  int mb_c[3], nmb = 0;
+  mb_c[nmb++] = e.mb;
+  if (a.m != e.mb && coef + (size_t)4 * e.ldc * a.m <= 220 * 1024) mb_c[nmb++] = a.m;
+  if (e.mb != 1) mb_c[nmb++] = 1;
+  size_t pre_smem_max = 0;
+  for (int q = 0; q < nmb; ++q) pre_smem_max = std::max(pre_smem_max, coef + (size_t)4 * e.ldc * mb_c[q]);
   const size_t gram_smem = (size_t)8 * 32 * 32 * sizeof(double);
   const size_t rr_smem = sizeof(LbSmall) + sizeof(LbMats);
-  cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem);
+  cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem_max);
+  // basis update tiles: <6,1> (3 CTAs per SM) is the built-in for m <= 8, <8,2> the alternative
+  const int nupd = a.m <= 8 ? 2 : 1;
+  char kpre[96], kupd[96];
+  snprintf(kpre, sizeof(kpre), "eb_precond|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
+  snprintf(kupd, sizeof(kupd), "eb_update|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
+  cudaEvent_t tev[4];
+  for (auto& x : tev) cudaEventCreate(&x);
+  int prev_pc = -1, prev_uc = -1, prev_cols = 0, prev_ns = 0;
+  // time per unit of work of the previous iteration's launches, read after the
+  // iteration's own synchronisation (no extra host waits)
+  auto report_prev = [&]() {
+    if (prev_pc < 0) return;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, tev[0], tev[1]) == cudaSuccess && prev_cols > 0)
+      tune_online_report(kpre, nmb, prev_pc, 1e3f * ms / (float)prev_cols);
+    if (cudaEventElapsedTime(&ms, tev[2], tev[3]) == cudaSuccess && prev_ns > 0)
+      tune_online_report(kupd, nupd, prev_uc, 1e3f * ms / (float)prev_ns);
+    prev_pc = -1;
+  };
   cudaFuncSetAttribute(k_eb_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem);
   cudaFuncSetAttribute(k_eb_rr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem);
   const double drop = sizeof(T) == 4 ? 1e-9 : 1e-13;
@@ -1592,22 +1621,28 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     // residual norms of the subdomains still iterating (all of them at it = 0)
     mark(1);
     { note_launch(); k_eb_resid<T><<<dim3(e.nchunk, nact), 256, 0, st>>>(e, it > 0 ? 1 : 0); }
-    cudaMemsetAsync(b.nactive, 0, sizeof(int), st);
+    cudaMemsetAsync(b.nactive, 0, 3 * sizeof(int), st);
     { note_launch(); k_eb_control<<<(nlist + 127) / 128, 128, 0, st>>>(e, nlist, it); }
-    cudaMemcpyAsync(b.h_nactive, b.nactive, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(b.h_nactive, b.nactive, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
     mark(2);
     if (cudaStreamSynchronize(st) != cudaSuccess) return 76;
+    report_prev();
     if (prof) {
       float ms;
       cudaEventElapsedTime(&ms, pev[1], pev[2]);
       ptot[0] += ms;
     }
-    nact = *b.h_nactive;
+    nact = b.h_nactive[0];
     if (nact == 0) break;
     ++lockstep;
-    const dim3 gchunk(e.nchunk, nact), gpre((a.m + e.mb - 1) / e.mb, nact);
+    const int pc = tune_online_pick(kpre, nmb), uc = tune_online_pick(kupd, nupd);
+    EbArgs ep = e;
+    ep.mb = mb_c[pc];
+    const dim3 gchunk(e.nchunk, nact), gpre((a.m + ep.mb - 1) / ep.mb, nact);
     mark(2);
-    { note_launch(); k_eb_precond<T><<<gpre, 256, pre_smem, st>>>(e); }
+    cudaEventRecord(tev[0], st);
+    { note_launch(); k_eb_precond<T><<<gpre, 256, coef + (size_t)4 * e.ldc * ep.mb, st>>>(ep); }
+    cudaEventRecord(tev[1], st);
     if (sizeof(T) == 8) { note_launch(); k_eb_aimg<T><<<dim3(a.m, nact), 256, 0, st>>>(e, 0); }
     mark(3);
     { note_launch(); k_eb_gram<T><<<gchunk, 256, gram_smem, st>>>(e); }
@@ -1615,10 +1650,16 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     { note_launch(); k_eb_rr<<<nact, 256, rr_smem, st>>>(e, drop); }
     mark(5);
     note_launch();
-    if (a.m <= 8)
+    cudaEventRecord(tev[2], st);
+    if (a.m <= 8 && uc == 0)
       k_eb_update<T, 6, 1><<<gchunk, 256, 0, st>>>(e);
     else
       k_eb_update<T, 8, 2><<<gchunk, 256, 0, st>>>(e);
+    cudaEventRecord(tev[3], st);
+    prev_pc = pc;
+    prev_uc = uc;
+    prev_cols = b.h_nactive[1];
+    prev_ns = b.h_nactive[2];
     mark(6);
     if (sizeof(T) == 4) { note_launch(); k_eb_aimg<T><<<dim3(2 * a.m, nact), 256, 0, st>>>(e, 1); }
     mark(7);
@@ -1631,6 +1672,9 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
       }
     }
   }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return 76;
+  report_prev();
+  for (auto& x : tev) cudaEventDestroy(x);
   if (prof) {
     if (b.phase_ms) {
       for (int q = 0; q < 6; ++q) b.phase_ms[q] += ptot[q];

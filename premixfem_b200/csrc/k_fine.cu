@@ -253,9 +253,80 @@ __global__ void k_pcg_iter_a_fin(const double* part, int nb, PcgState* s) {
     }
   }
 }
+// The same step as a 2.5-D march: a CTA owns a 32 x 16 tile of x-lines and a
+// stretch of z-planes; the new p of the current plane sits in shared memory
+// with a one-cell halo, the planes below and above in registers, so z and p
+// are read once per cell (plus the tile halo) instead of at all seven stencil
+// points.  The operator is evaluated in apply_A's order (same w bit for bit).
+constexpr int kPaX = 32, kPaY = 16;
+__global__ void __launch_bounds__(kPaX * kPaY) k_pcg_iter_a25(Grid g, const double* __restrict__ tx,
+                                                             const double* __restrict__ ty,
+                                                             const double* __restrict__ tz,
+                                                             const double* __restrict__ diag,
+                                                             const double* __restrict__ z,
+                                                             const double* __restrict__ pin, double* pout,
+                                                             double* w, double* part, const PcgState* s, int zc) {
+  __shared__ double sp[kPaY + 2][kPaX + 2];
+  __shared__ double red[32];
+  if (s->done) return;
+  const bool first = s->first != 0;
+  const double b = first ? 0.0 : s->beta / s->betaold;
+  const int lx = threadIdx.x % kPaX, ly = threadIdx.x / kPaX;
+  const int ex = blockIdx.x * kPaX + lx, ey = blockIdx.y * kPaY + ly;
+  const int zb = blockIdx.z * zc, ze = min(g.P, zb + zc);
+  const bool in = ex < g.M && ey < g.N;
+  auto pn = [&](long long c) { return first ? z[c] : z[c] + b * pin[c]; };
+  const long long row = (long long)ey * g.M + ex;
+  double pprev = 0.0, pcur = 0.0;
+  if (in) {
+    pcur = pn((long long)zb * g.MN + row);
+    if (zb > 0) pprev = pn((long long)(zb - 1) * g.MN + row);
+  }
+  double v = 0.0;
+  for (int ez = zb; ez < ze; ++ez) {
+    const long long c = (long long)ez * g.MN + row;
+    const double pnext = (in && ez + 1 < g.P) ? pn(c + g.MN) : 0.0;
+    sp[ly + 1][lx + 1] = pcur;
+    if (lx == 0) sp[ly + 1][0] = (in && ex > 0) ? pn(c - 1) : 0.0;
+    if (lx == kPaX - 1) sp[ly + 1][kPaX + 1] = (in && ex + 1 < g.M) ? pn(c + 1) : 0.0;
+    if (ly == 0) sp[0][lx + 1] = (in && ey > 0) ? pn(c - g.M) : 0.0;
+    if (ly == kPaY - 1) sp[kPaY + 1][lx + 1] = (in && ey + 1 < g.N) ? pn(c + g.M) : 0.0;
+    __syncthreads();
+    if (in) {
+      double a = diag[c] * pcur;
+      if (ex > 0) a -= tx[c] * sp[ly + 1][lx];
+      if (ex < g.M - 1) a -= tx[c + 1] * sp[ly + 1][lx + 2];
+      if (ey > 0) a -= ty[c] * sp[ly][lx + 1];
+      if (ey < g.N - 1) a -= ty[c + g.M] * sp[ly + 2][lx + 1];
+      if (ez > 0) a -= tz[c] * pprev;
+      if (ez < g.P - 1) a -= tz[c + g.MN] * pnext;
+      pout[c] = pcur;
+      w[c] = a;
+      v += pcur * a;
+    }
+    __syncthreads();  // the next plane overwrites sp
+    pprev = pcur;
+    pcur = pnext;
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = v;
+}
+
 void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
                        const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
                        cudaStream_t st) {
+  // partials: at most cell_blocks(ncell) blocks (the size the caller's buffer is guaranteed to hold)
+  const int cap = cell_blocks(g.ncell);
+  const int bx = (g.M + kPaX - 1) / kPaX, by = (g.N + kPaY - 1) / kPaY;
+  const int per_z = std::max(1, cap / std::max(1, bx * by));
+  const int zc = std::max(16, (g.P + per_z - 1) / per_z);
+  const int bz = (g.P + zc - 1) / zc;
+  const long long nb25 = (long long)bx * by * bz;
+  if (nb25 <= cap && by <= 65535 && bz <= 65535) {
+    { note_launch(); k_pcg_iter_a25<<<dim3(bx, by, bz), kPaX * kPaY, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s, zc); }
+    { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, (int)nb25, s); }
+    return;
+  }
   int nb = cell_blocks(g.ncell);
   { note_launch(); k_pcg_iter_a<<<nb, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s); }
   { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s); }

@@ -495,11 +495,11 @@ int Solver::alloc_eb(int m, bool mixed) {
   if (int e = check(cudaMalloc(&eb.gpart, ns * eb.nchunk * 2 * 32 * 32 * sizeof(double)), "cudaMalloc Grams"))
     return e;
   if (int e = check(cudaMalloc(&eb.rpart, ns * eb.nchunk * 10 * sizeof(double)), "cudaMalloc residuals")) return e;
-  if (!eb.nactive) cudaMalloc(&eb.nactive, sizeof(int));
+  if (!eb.nactive) cudaMalloc(&eb.nactive, 4 * sizeof(int));
   if (!eb.colcells) cudaMalloc(&eb.colcells, sizeof(unsigned long long));
   if (eb.alist) cudaFree(eb.alist);
   cudaMalloc(&eb.alist, ns * sizeof(int));
-  if (!eb.h_nactive) cudaMallocHost(&eb.h_nactive, sizeof(int));
+  if (!eb.h_nactive) cudaMallocHost(&eb.h_nactive, 4 * sizeof(int));
   return 0;
 }
 

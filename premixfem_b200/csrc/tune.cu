@@ -153,6 +153,58 @@ int tune_choose(const std::string& key0, int ncand, const std::function<bool(int
   return ent.choice;
 }
 
+int tune_online_pick(const std::string& key0, int ncand) {
+  if (ncand <= 1) return 0;
+  if (const char* f = getenv("PMF_TUNE_FORCE")) {
+    const int c = atoi(f);
+    return c < 0 ? 0 : (c >= ncand ? ncand - 1 : c);
+  }
+  if (!tune_enabled()) return 0;
+  const std::string key = key0 + "|" + tune_device();
+  Table& t = table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  if (!t.loaded) load_locked(t);
+  auto it = t.rows.find(key);
+  if (it == t.rows.end()) return 0;
+  Entry& e = it->second;
+  if ((int)e.us.size() != ncand) return 0;
+  for (int c = 0; c < ncand; ++c)
+    if (e.us[c] < 0.0f) return c;  // not measured yet
+  return e.choice;
+}
+
+void tune_online_report(const std::string& key0, int ncand, int cand, float us_per_unit) {
+  if (ncand <= 1 || cand < 0 || cand >= ncand || getenv("PMF_TUNE_FORCE") || !tune_enabled()) return;
+  const std::string key = key0 + "|" + tune_device();
+  Table& t = table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  Entry& e = t.rows[key];
+  if ((int)e.us.size() != ncand) {
+    e.us.assign(ncand, -1.0f);
+    e.choice = 0;
+  }
+  const bool complete_before = [&] {
+    for (float u : e.us)
+      if (u < 0.0f) return false;
+    return true;
+  }();
+  if (complete_before) return;  // decided: later steps do not move the choice
+  e.us[cand] = us_per_unit;
+  float best = 1e30f;
+  bool complete = true;
+  for (int c = 0; c < ncand; ++c) {
+    if (e.us[c] < 0.0f) {
+      complete = false;
+      continue;
+    }
+    if (e.us[c] < best) {
+      best = e.us[c];
+      e.choice = c;
+    }
+  }
+  if (complete) save_locked(t);
+}
+
 std::string tune_report() {
   Table& t = table();
   std::lock_guard<std::mutex> lk(t.mu);

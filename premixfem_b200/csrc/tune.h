@@ -26,6 +26,14 @@ namespace pmf {
 // candidate c on `st` and returns false when c does not apply to this shape.
 int tune_choose(const std::string& key, int ncand, const std::function<bool(int)>& launch, cudaStream_t st,
                 int reps = 3);
+// Online form for kernels that change their data and run once per step of a
+// loop (the lock-step eigensolver phases): tune_online_pick returns the
+// candidate to launch now -- each candidate in turn until all have run once,
+// then the fastest -- and the caller reports the measured time per unit of
+// work (e.g. per active subdomain) with tune_online_report.  Every launch is
+// a real step of the computation, so nothing is run twice.
+int tune_online_pick(const std::string& key, int ncand);
+void tune_online_report(const std::string& key, int ncand, int cand, float us_per_unit);
 // Turn tuning on or off for the whole process (the solver option -pmf_autotune).
 void tune_set_enabled(bool on);
 bool tune_enabled();

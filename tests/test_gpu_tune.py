@@ -83,3 +83,28 @@ def test_report_lists_the_tuned_shapes(native, monkeypatch):
         e = table[k]
         assert 0 <= e["choice"] < len(e["us"])
         assert e["us"][e["choice"]] == min(t for t in e["us"] if t >= 0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_eigensolver_every_online_shape(native, monkeypatch, precision):
+    """The lock-step eigensolver's online candidates (preconditioner column batch
+    3 / 8 / 1, update tiles <6,1> / <8,2>) give the same local eigenvalues
+    (1e-6 relative) and the same PCG iteration count (+-1)."""
+    prob = fields.fracture256(64, seed=3)
+    opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
+    res = []
+    for cand in (0, 1, 2):
+        monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
+        s = DarcySolver.from_problem(prob, opts)
+        s.setup()
+        ev = s.eigen_lv1()[0].copy()
+        b = s.rhs(prob["source"].ravel())
+        _, its, _, reason = s.solve(b)
+        assert reason == "converged"
+        res.append((ev, its))
+        s.close()
+    for cand in (1, 2):
+        ev0, ev = res[0][0], res[cand][0]
+        rel = np.abs(ev - ev0) / np.maximum(np.abs(ev0), 1e-9 * np.abs(ev0).max())
+        assert rel.max() <= 1e-6, (cand, rel.max())
+        assert abs(res[cand][1] - res[0][1]) <= 1, (cand, res[cand][1], res[0][1])
