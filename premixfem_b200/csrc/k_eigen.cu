@@ -1522,6 +1522,154 @@ __global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
     cta_update_mma<double, NK, NJ, 1>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
 }
 
+// ---- final phase (k_lobpcg mode 2 as phase kernels over every subdomain of
+// the list): FP64 A-images of X, Grams of X, the FP64 Rayleigh-Ritz with the
+// adaptive count (:369-383) and the output of the k_i wanted vectors.  Run at
+// full occupancy instead of one register-heavy CTA per SM.  After this phase
+// the state's nact / np / best hold the kept count, the snap flag and the
+// value of the snapped constant vector.
+__device__ __forceinline__ int eb_full(const EbArgs& a, int idx) { return a.list ? a.list[idx] : idx; }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_fin_aimg(EbArgs a) {
+  const int s = eb_full(a, blockIdx.y);
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  const int col = blockIdx.x;
+  neumann_apply_col(a.g, S, a.tx, a.ty, a.tz, sl.dN, sl.X + (size_t)col * a.ld, sl.AX + (size_t)col * a.ld, nc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_eb_fin_gram(EbArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* red = reinterpret_cast<double*>(smraw);
+  const int s = eb_full(a, blockIdx.y);
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int cn = min(nc - c0, EB_CHUNK);
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  double* G = a.gpart + ((size_t)s * a.nchunk + blockIdx.x) * 2 * LB_LD * LB_LD;
+  Seg3<T> sS{{sl.X + c0, sl.X + c0, sl.X + c0}, {a.m, 0, 0}, a.ld};
+  Seg3<double> sA{{sl.AX + c0, sl.AX + c0, sl.AX + c0}, {a.m, 0, 0}, a.ld};
+  cta_gram2_mma<T, double, 3>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_fin_rr(EbArgs a, double eb, int dmask, double* evals, int* iters,
+                                                   int* status, int* ks) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  LbSmall& sm = *reinterpret_cast<LbSmall*>(smraw);
+  LbMats& mt = *reinterpret_cast<LbMats*>(smraw + sizeof(LbSmall));
+  const int s = eb_full(a, blockIdx.x);
+  EbState& es = a.state[s];
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int nch = (nc + EB_CHUNK - 1) / EB_CHUNK;
+  const int m = a.m, k = a.k;
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+    const int r = e / m, c = e % m;
+    double gm = 0.0, ga = 0.0;
+    for (int q = 0; q < nch; ++q) {
+      const double* G = a.gpart + ((size_t)s * a.nchunk + q) * 2 * LB_LD * LB_LD;
+      gm += G[r * LB_LD + c];
+      ga += G[LB_LD * LB_LD + r * LB_LD + c];
+    }
+    mt.GM[r * LB_LD + c] = gm;
+    mt.GA[r * LB_LD + c] = ga;
+  }
+  if (threadIdx.x < LB_MM) sm.lam[threadIdx.x] = threadIdx.x < m ? es.lam[threadIdx.x] : 0.0;
+  if (threadIdx.x == 0) sm.scal[0] = es.lscale;
+  __syncthreads();
+  cta_rayleigh_ritz(sm, mt, m, m, 1e-14, 1e-14);
+  if (threadIdx.x == 0) {
+    int num = k;
+    for (int j = 0; j < k; ++j)
+      if (sm.lam[j] >= eb) {
+        num = j + 1;
+        break;
+      }
+    sm.ival[1] = num;
+    ks[s] = num;
+    iters[s] = es.it;
+    status[s] = es.conv ? (es.stag ? 2 : 0) : 1;
+  }
+  __syncthreads();
+  const int num = sm.ival[1];
+  if (threadIdx.x < k) evals[(long long)s * k + threadIdx.x] = sm.lam[threadIdx.x];
+  double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+    const int r = e / m, c = e % m;
+    Y[r * LB_LD + c] = mt.Y[r * LB_LD + c];
+  }
+  // FP32 storage, subdomain touching no Dirichlet face: the lowest vector is
+  // the constant; write it exactly (M-normalised, sign of the computed one)
+  bool snap = false;
+  double cval = 0.0;
+  if (sizeof(T) == 4 && num >= 1) {
+    const bool touches = ((dmask & 1) && S.x0 == 0) || ((dmask & 2) && S.x0 + S.nx == a.g.M) ||
+                         ((dmask & 4) && S.y0 == 0) || ((dmask & 8) && S.y0 + S.ny == a.g.N) ||
+                         ((dmask & 16) && S.z0 == 0) || ((dmask & 32) && S.z0 + S.nz == a.g.P);
+    if (!touches) {
+      EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+      double msum = 0.0, vsum = 0.0;
+      for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+        double v0 = 0.0;
+        for (int b = 0; b < m; ++b) v0 += (double)sl.X[(size_t)b * a.ld + cl] * mt.Y[b * LB_LD];
+        msum += sl.Md[cl];
+        vsum += sl.Md[cl] * v0;
+      }
+      msum = block_sum(msum, sm.res);
+      vsum = block_sum(vsum, sm.res);
+      snap = msum > 0.0;
+      cval = snap ? copysign(1.0 / sqrt(msum), vsum) : 0.0;
+    }
+  }
+  if (threadIdx.x == 0) {
+    es.nact = num;
+    es.np = snap ? 1 : 0;
+    es.best = cval;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_fin_out(EbArgs a, int kmax, T* phi) {
+  __shared__ double Ys[LB_LD * LB_LD];
+  const int s = eb_full(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  const SubInfo S = a.subs[s];
+  const int nx = S.nx, ny = S.ny, nc = nx * ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int c1 = min(nc, c0 + EB_CHUNK);
+  const double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int e = threadIdx.x; e < a.m * LB_LD; e += blockDim.x) Ys[e] = Y[e];
+  __syncthreads();
+  const int m = a.m, num = es.nact;
+  const bool snap = es.np != 0;
+  const double cval = es.best;
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  for (int cl = c0 + threadIdx.x; cl < c1; cl += blockDim.x) {
+    const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+    const long long cg = ((long long)(S.z0 + kz_) * a.g.N + (S.y0 + jy)) * a.g.M + (S.x0 + i);
+    double xr[LB_MM];
+#pragma unroll
+    for (int b = 0; b < LB_MM; ++b) xr[b] = b < m ? (double)sl.X[(size_t)b * a.ld + cl] : 0.0;
+    for (int j = 0; j < kmax; ++j) {
+      double v = 0.0;
+      if (j < num) {
+#pragma unroll
+        for (int b = 0; b < LB_MM; ++b)
+          if (b < m) v += xr[b] * Ys[b * LB_LD + j];
+      }
+      if (snap && j == 0) v = cval;
+      phi[cg * kmax + j] = (T)v;
+    }
+  }
+}
+
 }  // namespace
 
 size_t lobpcg_batched_slab_bytes(int max_cells, int m, int prec_bytes) {
@@ -1687,7 +1835,18 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
               ptot[0], ptot[1], ptot[2], ptot[3], ptot[4], ptot[5], lockstep);
     for (auto& x : pev) cudaEventDestroy(x);
   }
-  // final phase: k_lobpcg mode 2 (FP64 Rayleigh-Ritz, adaptive count, output)
+  // final phase: FP64 Rayleigh-Ritz, adaptive count, output
+  if (a.final_batched) {
+    const size_t fin_rr_smem = sizeof(LbSmall) + sizeof(LbMats);
+    cudaFuncSetAttribute(k_eb_fin_rr<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fin_rr_smem);
+    cudaFuncSetAttribute(k_eb_fin_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem);
+    { note_launch(); k_eb_fin_aimg<T><<<dim3(a.m, nlist), 256, 0, st>>>(e); }
+    { note_launch(); k_eb_fin_gram<T><<<dim3(e.nchunk, nlist), 256, gram_smem, st>>>(e); }
+    { note_launch(); k_eb_fin_rr<T><<<nlist, 256, fin_rr_smem, st>>>(e, eb, a.dirichlet_mask, evals, iters, status, ks); }
+    { note_launch(); k_eb_fin_out<T><<<dim3(e.nchunk, nlist), 256, 0, st>>>(e, a.kmax, phi); }
+    return cudaGetLastError() == cudaSuccess ? 0 : 76;
+  }
+  // final phase as one persistent launch: k_lobpcg mode 2
   a.mode = 2;
   launch_lobpcg<T>(a, std::min(ctas, nlist), nullptr, phi, evals, iters, status, ks, eb, max_cells, max_lines, st);
   return cudaGetLastError() == cudaSuccess ? 0 : 76;

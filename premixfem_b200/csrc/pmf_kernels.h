@@ -147,6 +147,7 @@ struct LobpcgArgs {
   // 1 = set-up only (mass, IC(0) pivots, initial block and Rayleigh-Ritz) into
   // the per-subdomain slab and state; 2 = final Rayleigh-Ritz and output from them
   int mode;
+  int final_batched;    // batched solver: 1 = final Rayleigh-Ritz and output as phase kernels, 0 = mode 2
   unsigned char* slab;  // per-subdomain work slabs (modes 1, 2), stride slab_stride
   size_t slab_stride;
   void* state;          // per-subdomain EbState array (modes 1, 2)

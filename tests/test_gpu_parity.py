@@ -225,3 +225,30 @@ def test_full_cholesky_level1_matches_oracle(native, name, precision):
     err = np.linalg.norm(x - xd) / np.linalg.norm(xd)
     assert err <= 1e-8, f"solution error vs direct {err:.2e}"
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_final_phase_matches_persistent(native, precision):
+    """The eigensolver's final Rayleigh-Ritz and output as phase kernels
+    (-pmf_eig_final 1, the default) against the persistent mode-2 launch: the
+    same local eigenvalues (1e-9 relative), preconditioner (1e-9 FP64, 1e-5
+    mixed) and PCG iteration count (+-1)."""
+    prob = fields.random_box((32, 24, 20), seed=4, sigma=1.5, dirichlet={"x-": 1.0})
+    out = []
+    for fin in (0, 1):
+        s = _gpu(prob, {"pmf_sd": (4, 3, 2), "en_lv1": 5, "en_lv2": 3, "pmf_precision": precision, "pmf_eig_final": fin})
+        ev = s.eigen_lv1()[0].copy()
+        x = np.random.default_rng(2).standard_normal(32 * 24 * 20)
+        y = s.pc_apply(x)
+        b = s.rhs(prob["source"].ravel())
+        _, its, _, reason = s.solve(b)
+        assert reason == "converged"
+        out.append((ev, y, its))
+        s.close()
+    ev0, ev1 = out[0][0], out[1][0]
+    rel = np.abs(ev1 - ev0) / np.maximum(np.abs(ev0), 1e-9 * np.abs(ev0).max())
+    assert rel.max() <= 1e-9, rel.max()
+    tol = 1e-9 if precision == "fp64" else 1e-5
+    ry = np.linalg.norm(out[1][1] - out[0][1]) / np.linalg.norm(out[0][1])
+    assert ry <= tol, ry
+    assert abs(out[1][2] - out[0][2]) <= 1
