@@ -35,6 +35,7 @@ typedef struct pmf_solver pmf_solver;
 
 /* Options use the reference's PETSc option names: -sd, -en_lv1, -en_lv2,
  * -eb_lv1, -eb_lv2, -si_lv1, -si_lv2, -eg_op, -use_W_cycle, -no_shift_A_cc,
+ * -use_full_Cholesky_lv1 (banded Cholesky local solves), -use_2level,
  * -ksp_rtol, -ksp_max_it; B200 extensions: -pmf_sd sx,sy,sz (subdomains per
  * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
  * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it, -pmf_learned
@@ -42,7 +43,11 @@ typedef struct pmf_solver pmf_solver;
  * -pmf_learned_its N and -pmf_learned_tol t (a subdomain whose LOBPCG from the
  * learned start has not reached relative residual t within N iterations is
  * solved again from a random start at the normal tolerance; defaults 30 and
- * 1e-4). */
+ * 1e-4), -pmf_eig_batched 0|1 and -pmf_eig_final 0|1 (phase-batched
+ * eigensolver and its batched final phase, both on by default),
+ * -pmf_eig_profile 1 (per-phase timing, pmf_get_eig_phases), -pmf_pcg_graph
+ * 0|1 (PCG iterations replayed as CUDA graphs, on by default), -pmf_autotune
+ * 0|1 (launch-shape tuning, on by default; pmf_tune_report). */
 int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out);
 int pmf_destroy(pmf_solver* s);
 
