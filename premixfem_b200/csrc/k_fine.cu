@@ -312,9 +312,9 @@ __global__ void __launch_bounds__(kPaX * kPaY) k_pcg_iter_a25(Grid g, const doub
   if (threadIdx.x == 0) part[((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = v;
 }
 
-void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
-                       const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
-                       cudaStream_t st) {
+int launch_pcg_iter_a_main(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                           const double* z, const double* pin, double* pout, double* w, double* part,
+                           const PcgState* s, cudaStream_t st, int variant) {
   // partials: at most cell_blocks(ncell) blocks (the size the caller's buffer is guaranteed to hold)
   const int cap = cell_blocks(g.ncell);
   const int bx = (g.M + kPaX - 1) / kPaX, by = (g.N + kPaY - 1) / kPaY;
@@ -322,13 +322,18 @@ void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const 
   const int zc = std::max(16, (g.P + per_z - 1) / per_z);
   const int bz = (g.P + zc - 1) / zc;
   const long long nb25 = (long long)bx * by * bz;
-  if (nb25 <= cap && by <= 65535 && bz <= 65535) {
+  if (variant == 0 && nb25 <= cap && by <= 65535 && bz <= 65535) {
     { note_launch(); k_pcg_iter_a25<<<dim3(bx, by, bz), kPaX * kPaY, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s, zc); }
-    { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, (int)nb25, s); }
-    return;
+    return (int)nb25;
   }
-  int nb = cell_blocks(g.ncell);
-  { note_launch(); k_pcg_iter_a<<<nb, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s); }
+  { note_launch(); k_pcg_iter_a<<<cap, kCellThreads, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s); }
+  return cap;
+}
+
+void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                       const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
+                       cudaStream_t st, int variant) {
+  const int nb = launch_pcg_iter_a_main(g, tx, ty, tz, diag, z, pin, pout, w, part, s, st, variant);
   { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s); }
 }
 

@@ -47,7 +47,13 @@ void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream
 void launch_pcg_beta(const double* r, const double* z, long long n, double* part, PcgState* s, cudaStream_t st);
 void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
                        const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
-                       cudaStream_t st);
+                       cudaStream_t st, int variant = 0);
+// The main kernel of launch_pcg_iter_a alone (no state update): variant 0 the
+// 2.5-D march where the mesh allows it, 1 the grid-stride kernel.  Returns the
+// number of partial sums written.
+int launch_pcg_iter_a_main(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
+                           const double* z, const double* pin, double* pout, double* w, double* part,
+                           const PcgState* s, cudaStream_t st, int variant);
 void launch_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
                        PcgState* s, cudaStream_t st);
 void launch_dot(const double* a, const double* b, long long n, double* part, double* out, cudaStream_t st);

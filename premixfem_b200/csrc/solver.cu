@@ -951,7 +951,7 @@ void Solver::tune_pc() {
   cudaMemsetAsync(ya, 0, sizeof(T) * g.ncell, st);
   cudaMemsetAsync(z, 0, sizeof(double) * g.ncell, st);
   cudaMemsetAsync(Zacc, 0, sizeof(double) * nsub * kmax, st);
-  const int old[3] = {ic_threads, rr_threads, pr_threads};
+  const int old[4] = {ic_threads, rr_threads, pr_threads, pcga_variant};
   char key[192];
   const char* prec = f32 ? "f32" : "f64";
   if (!opt.use_full_Cholesky_lv1) {
@@ -978,7 +978,20 @@ void Solver::tune_pc() {
     launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yo, nullptr, st, rcand[i]);
     return true;
   }, st)];
-  if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads)) {
+  // the CG step's fused p-update + operator kernel: 2.5-D march or grid-stride
+  // (the main kernel alone is timed; the state says first step, not done)
+  {
+    PcgState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.first = 1;
+    cudaMemcpy(state, &hs, sizeof(hs), cudaMemcpyHostToDevice);
+    snprintf(key, sizeof(key), "pcg_iter_a|M%d|N%d|P%d", g.M, g.N, g.P);
+    pcga_variant = tune_choose(key, 2, [&](int i) {
+      launch_pcg_iter_a_main(g, tx, ty, tz, diag, z, p0, p1, w, part, state, st, i);
+      return true;
+    }, st);
+  }
+  if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads || old[3] != pcga_variant)) {
     cudaGraphExecDestroy(pcg_exec);  // captured with other launch shapes
     pcg_exec = nullptr;
     pcg_graph_x = nullptr;
@@ -1147,7 +1160,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   const int chunk = std::max(1, opt.pcg_chunk);
   auto enqueue_chunk = [&]() {
     for (int c_ = 0; c_ < chunk; ++c_) {
-      launch_pcg_iter_a(g, tx, ty, tz, diag, z, pin, pout, w, part, state, st);
+      launch_pcg_iter_a(g, tx, ty, tz, diag, z, pin, pout, w, part, state, st, pcga_variant);
       launch_pcg_iter_b(g.ncell, xs, r, pout, w, part, state, st);
       apply(r, z, part, done);
       launch_pcg_beta_fin(part, nparts_apply(), state, st);

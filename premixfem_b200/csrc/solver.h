@@ -156,7 +156,7 @@ class Solver {
   int setup_band_cholesky(bool mixed);
   template <typename T>
   void tune_pc();
-  int ic_threads = 0, rr_threads = 256, pr_threads = 256;  // tuned launch shapes
+  int ic_threads = 0, rr_threads = 256, pr_threads = 256, pcga_variant = 0;  // tuned launch shapes
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;

@@ -108,3 +108,26 @@ def test_eigensolver_every_online_shape(native, monkeypatch, precision):
         rel = np.abs(ev - ev0) / np.maximum(np.abs(ev0), 1e-9 * np.abs(ev0).max())
         assert rel.max() <= 1e-6, (cand, rel.max())
         assert abs(res[cand][1] - res[0][1]) <= 1, (cand, res[cand][1], res[0][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_every_pcg_kernel(native, monkeypatch, precision):
+    """Both candidates of the CG step's fused p-update + operator kernel (the
+    2.5-D march and the grid-stride kernel; forced together with the other
+    shapes' candidates 0 / 1) converge in the same number of iterations (+-1)
+    to the same solution (1e-7 relative: only the order of the dot-product
+    partial sums differs)."""
+    prob = fields.fracture256(64, seed=3)
+    opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
+    res = []
+    for cand in (0, 1):
+        monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
+        s = DarcySolver.from_problem(prob, opts)
+        s.setup()
+        b = s.rhs(prob["source"].ravel())
+        x, its, _, reason = s.solve(b)
+        assert reason == "converged"
+        res.append((x.copy(), its))
+        s.close()
+    assert abs(res[1][1] - res[0][1]) <= 1, (res[0][1], res[1][1])
+    assert _rel(res[1][0], res[0][0]) <= 1e-7, _rel(res[1][0], res[0][0])
