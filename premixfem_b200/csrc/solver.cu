@@ -957,7 +957,7 @@ void Solver::tune_pc() {
   if (!opt.use_full_Cholesky_lv1) {
     const int base = std::max(64, ((max_lines + 31) / 32) * 32);
     std::vector<int> cand = {base};
-    for (int t : {512, 1024})
+    for (int t : {384, 512, 768, 1024})
       if (t > base) cand.push_back(t);
     snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d", prec, nsub, max_cells, max_lines);
     const int ci = tune_choose(key, (int)cand.size(), [&](int i) {

@@ -53,14 +53,14 @@ def test_pc_apply_every_thread_shape(native, monkeypatch, precision):
     opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
     x = np.random.default_rng(5).standard_normal(64 ** 3)
     out = []
-    for cand in (0, 1, 2):
+    for cand in (0, 1, 2, 3, 4):  # level 1: 256 / 384 / 512 / 768 / 1024 threads (others clamped)
         monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
         s = DarcySolver.from_problem(prob, opts)
         s.setup()
         out.append(s.pc_apply(x))
         s.close()
     tol = 1e-12 if precision == "fp64" else 1e-5
-    for cand in (1, 2):
+    for cand in (1, 2, 3, 4):
         assert _rel(out[cand], out[0]) <= tol, (cand, _rel(out[cand], out[0]))
 
 
