@@ -52,7 +52,7 @@ from premixfem_b200.solver import options_string  # noqa: E402
 METRIC = "setup+solve s at 1e-8 resid & PCG iters: mixed/learned vs plain FP64, 1 B200"
 
 WORKLOADS = {
-    # 256^3 fracture network, 16^3 subdomains of 16^3 cells, k = 6.
+    # 256^3 fracture network, 16^3 subdomains of 16^3 cells, k = 6 (the benchmarked workload).
     "fracture256": dict(
         make=lambda seed: fields.fracture256(256, seed=seed),
         opts={"sd": 4, "pmf_vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
@@ -64,7 +64,7 @@ WORKLOADS = {
         sample_n=128, sample_opts={"sd": 4, "vranks": (2, 2, 2), "en_lv1": 6, "en_lv2": 4},
         cpu_opts={"sd": 4, "vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
     ),
-    # 32^3 unit cube GRF.
+    # 32^3 unit-cube GRF, the small CPU-runnable case.
     "unit_cube_grf32": dict(
         make=lambda seed: fields.unit_cube_grf(32, seed=seed),
         opts={"sd": 4, "en_lv1": 4, "en_lv2": 4},
