@@ -1670,6 +1670,239 @@ __global__ void __launch_bounds__(256) k_eb_fin_out(EbArgs a, int kmax, T* phi) 
   }
 }
 
+// ---- set-up phase (k_lobpcg mode 1 as phase kernels over every subdomain of
+// the list): mass and Neumann diagonals, FP32 sweep coefficients, IC(0) pivots
+// of A^N + sigma M and the initial block (one CTA per subdomain), the
+// A-images of the block, its Grams, the first Rayleigh-Ritz with the state
+// initialisation, and the rotation of X and A X by the Ritz coefficients.
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_init_a(EbArgs e, LobpcgArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ double red[32];
+  const int ldc = e.ldc;
+  double* Dtmp = reinterpret_cast<double*>(smraw);
+  float* ctx = reinterpret_cast<float*>(Dtmp + ldc);
+  float* cty = ctx + ldc;
+  float* ctz = cty + ldc;
+  const int s = eb_full(e, blockIdx.x);
+  EbState& es = e.state[s];
+  const SubInfo S = e.subs[s];
+  const Grid g = e.g;
+  const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
+  const int m = e.m, ld = e.ld;
+  EbSlab<T> sl(e.slab + (size_t)s * e.slab_stride, m, ld);
+  double ratio = 0.0;
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+    const int i = cl % nx, tt = cl / nx, j = tt % ny, kk = tt / ny;
+    const int ex = S.x0 + i, ey = S.y0 + j, ez = S.z0 + kk;
+    const long long cg = ((long long)ez * g.N + ey) * g.M + ex;
+    double dn = a.db[cg];
+    if (i > 0) dn += a.tx[cg];
+    if (i < nx - 1) dn += a.tx[cg + 1];
+    if (j > 0) dn += a.ty[cg];
+    if (j < ny - 1) dn += a.ty[cg + g.M];
+    if (kk > 0) dn += a.tz[cg];
+    if (kk < nz - 1) dn += a.tz[cg + g.MN];
+    double mv;
+    if (a.eg_op == 1) {  // EIG_OP_MEAN (:332-333)
+      mv = a.kx[cg] + a.ky[cg] + a.kz[cg];
+    } else if (a.eg_op == 2) {  // EIG_OP_DIAG: diag(A_i^N)
+      mv = dn;
+    } else {  // EIG_OP_MOD with the reference's x-direction accumulation (:258-320)
+      mv = 0.0;
+      if (i == 0 && ex >= 1) mv += 2.0 * avg_k(a.kx[cg - 1], a.kx[cg]) / a.Hx / a.Hx;
+      if (ex + 1 != g.M) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
+      if (ey >= 1) mv += 2.0 * avg_k(a.ky[cg - g.M], a.ky[cg]) / a.Hy / a.Hy;
+      if (ey + 1 != g.N) mv += 2.0 * avg_k(a.ky[cg], a.ky[cg + g.M]) / a.Hy / a.Hy;
+      if (ez >= 1) mv += 2.0 * avg_k(a.kz[cg - g.MN], a.kz[cg]) / a.Hz / a.Hz;
+      if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / a.Hz / a.Hz;
+      if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
+      if (a.dirichlet_mask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+      if (a.dirichlet_mask & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
+      if (a.dirichlet_mask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+      if (a.dirichlet_mask & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
+      if (a.dirichlet_mask & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
+      if (a.dirichlet_mask & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
+      mv = mv * a.meas;
+    }
+    sl.Md[cl] = mv;
+    sl.dN[cl] = dn;
+    double d32 = a.db[cg];
+    if (i > 0) d32 += (double)(float)a.tx[cg];
+    if (i < nx - 1) d32 += (double)(float)a.tx[cg + 1];
+    if (j > 0) d32 += (double)(float)a.ty[cg];
+    if (j < ny - 1) d32 += (double)(float)a.ty[cg + g.M];
+    if (kk > 0) d32 += (double)(float)a.tz[cg];
+    if (kk < nz - 1) d32 += (double)(float)a.tz[cg + g.MN];
+    sl.dN32[cl] = d32;
+    const float fx = i > 0 ? (float)a.tx[cg] : 0.0f, fy = j > 0 ? (float)a.ty[cg] : 0.0f,
+                fz = kk > 0 ? (float)a.tz[cg] : 0.0f;
+    ctx[cl] = fx;
+    cty[cl] = fy;
+    ctz[cl] = fz;
+    sl.ctx[cl] = fx;
+    sl.cty[cl] = fy;
+    sl.ctz[cl] = fz;
+    ratio = fmax(ratio, dn / mv);
+  }
+  for (int o = 16; o > 0; o >>= 1) ratio = fmax(ratio, __shfl_xor_sync(0xffffffffu, ratio, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ratio;
+  __syncthreads();
+  double r = 0.0;
+  for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) r = fmax(r, red[wi]);
+  const double lscale = r > 0 ? r : 1.0;
+  const double sigma = a.sigma_rel * lscale;
+  // IC(0) pivots of A^N + sigma M (wavefront, natural order, FP64)
+  const int t = threadIdx.x, jj = t % ny, kk = t / ny;
+  const bool line = t < ny * nz;
+  const int nplanes = nx + ny + nz - 2;
+  for (int d = 0; d < nplanes; ++d) {
+    const int i = d - jj - kk;
+    if (line && i >= 0 && i < nx) {
+      const int cl = (kk * ny + jj) * nx + i;
+      double sacc = 0.0;
+      if (kk > 0) sacc += (double)ctz[cl] * (double)ctz[cl] / Dtmp[cl - nxny];
+      if (jj > 0) sacc += (double)cty[cl] * (double)cty[cl] / Dtmp[cl - nx];
+      if (i > 0) sacc += (double)ctx[cl] * (double)ctx[cl] / Dtmp[cl - 1];
+      double D = sl.dN[cl] + sigma * sl.Md[cl] - sacc;
+      if (!(D > 0.0)) D = sl.dN[cl] + sigma * sl.Md[cl];
+      Dtmp[cl] = D;
+      sl.cinv[cl] = (float)(1.0 / D);
+    }
+    __syncthreads();
+  }
+  // initial block: the learned patch columns, a given block, or random
+  for (int q = threadIdx.x; q < m * nc; q += blockDim.x) {
+    const int j = q / nc, cl = q % nc;
+    double v;
+    if (a.xinit_patch && j < a.xinit_k) {
+      const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+      v = a.xinit_patch[((size_t)s * 4096 + (kz_ * 16 + jy) * 16 + i) * 16 + j];
+    } else if (a.xinit) {
+      const int i = cl % nx, tt = cl / nx, jy = tt % ny, kz_ = tt / ny;
+      const long long cg = ((long long)(S.z0 + kz_) * g.N + (S.y0 + jy)) * g.M + (S.x0 + i);
+      v = a.xinit[cg * m + j];
+    } else {
+      v = hash_uniform(a.seed ^ ((unsigned long long)s << 32) ^ (unsigned long long)q);
+    }
+    sl.X[(size_t)j * ld + cl] = (T)v;
+  }
+  if (threadIdx.x == 0) es.lscale = lscale;
+}
+
+// A X of the initial block: FP64 operator in FP64 storage; in FP32 storage the
+// FP32-rounded couplings and diagonal, as the lock-step A-images use them.
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_init_aimg(EbArgs e) {
+  const int s = eb_full(e, blockIdx.y);
+  const SubInfo S = e.subs[s];
+  const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
+  const int ld = e.ld, col = blockIdx.x;
+  EbSlab<T> sl(e.slab + (size_t)s * e.slab_stride, e.m, ld);
+  if (sizeof(T) == 8) {
+    neumann_apply_col(e.g, S, e.tx, e.ty, e.tz, sl.dN, sl.X + (size_t)col * ld, sl.AX + (size_t)col * ld, nc);
+    return;
+  }
+  const T* v = sl.X + (size_t)col * ld;
+  double* out = sl.AX + (size_t)col * ld;
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
+    const int i = cl % nx, tt = cl / nx, j = tt % ny, k = tt / ny;
+    double r = sl.dN32[cl] * (double)(float)v[cl];
+    if (i > 0) r -= (double)sl.ctx[cl] * (double)(float)v[cl - 1];
+    if (i < nx - 1) r -= (double)sl.ctx[cl + 1] * (double)(float)v[cl + 1];
+    if (j > 0) r -= (double)sl.cty[cl] * (double)(float)v[cl - nx];
+    if (j < ny - 1) r -= (double)sl.cty[cl + nx] * (double)(float)v[cl + nx];
+    if (k > 0) r -= (double)sl.ctz[cl] * (double)(float)v[cl - nxny];
+    if (k < nz - 1) r -= (double)sl.ctz[cl + nxny] * (double)(float)v[cl + nxny];
+    out[cl] = r;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_eb_init_rr(EbArgs e, double drop) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  LbSmall& sm = *reinterpret_cast<LbSmall*>(smraw);
+  LbMats& mt = *reinterpret_cast<LbMats*>(smraw + sizeof(LbSmall));
+  const int s = eb_full(e, blockIdx.x);
+  EbState& es = e.state[s];
+  const SubInfo S = e.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int nch = (nc + EB_CHUNK - 1) / EB_CHUNK;
+  const int m = e.m;
+  for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+    const int r = q / m, c = q % m;
+    double gm = 0.0, ga = 0.0;
+    for (int h = 0; h < nch; ++h) {
+      const double* G = e.gpart + ((size_t)s * e.nchunk + h) * 2 * LB_LD * LB_LD;
+      gm += G[r * LB_LD + c];
+      ga += G[LB_LD * LB_LD + r * LB_LD + c];
+    }
+    mt.GM[r * LB_LD + c] = gm;
+    mt.GA[r * LB_LD + c] = ga;
+  }
+  if (threadIdx.x < LB_MM) sm.lam[threadIdx.x] = 0.0;
+  if (threadIdx.x == 0) sm.scal[0] = es.lscale;
+  __syncthreads();
+  cta_rayleigh_ritz(sm, mt, m, m, drop, 1e-12);
+  double* Y = e.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+    const int r = q / m, c = q % m;
+    Y[r * LB_LD + c] = mt.Y[r * LB_LD + c];
+  }
+  if (threadIdx.x < m) es.lam[threadIdx.x] = sm.lam[threadIdx.x];
+  if (threadIdx.x == 0) {
+    es.best = 1e300;
+    es.last_improve = 0;
+    es.hasP = 0;
+    es.done = 0;
+    es.conv = 0;
+    es.stag = 0;
+    es.it = 0;
+    es.restart = 0;
+    es.nact = 0;
+    es.np = 0;
+    es.nS = m;
+  }
+}
+
+// X <- X Y and A X <- (A X) Y, cell by cell (in place: every cell's m values
+// are read before any is written).
+template <typename T>
+__global__ void __launch_bounds__(256) k_eb_init_rot(EbArgs e) {
+  __shared__ double Ys[LB_LD * LB_LD];
+  const int s = eb_full(e, blockIdx.y);
+  const SubInfo S = e.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int c1 = min(nc, c0 + EB_CHUNK);
+  const double* Y = e.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int q = threadIdx.x; q < e.m * LB_LD; q += blockDim.x) Ys[q] = Y[q];
+  __syncthreads();
+  const int m = e.m, ld = e.ld;
+  EbSlab<T> sl(e.slab + (size_t)s * e.slab_stride, m, ld);
+  for (int cl = c0 + threadIdx.x; cl < c1; cl += blockDim.x) {
+    double xr[LB_MM], ar[LB_MM];
+#pragma unroll
+    for (int b = 0; b < LB_MM; ++b) {
+      xr[b] = b < m ? (double)sl.X[(size_t)b * ld + cl] : 0.0;
+      ar[b] = b < m ? sl.AX[(size_t)b * ld + cl] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < LB_MM; ++j)
+      if (j < m) {
+        double xn = 0.0, an = 0.0;
+#pragma unroll
+        for (int b = 0; b < LB_MM; ++b)
+          if (b < m) {
+            xn += xr[b] * Ys[b * LB_LD + j];
+            an += ar[b] * Ys[b * LB_LD + j];
+          }
+        sl.X[(size_t)j * ld + cl] = (T)xn;
+        sl.AX[(size_t)j * ld + cl] = an;
+      }
+  }
+}
+
 }  // namespace
 
 size_t lobpcg_batched_slab_bytes(int max_cells, int m, int prec_bytes) {
@@ -1692,8 +1925,6 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   a.nlist = nullptr;
   a.nsub = list ? nlist : a_in.nsub;
   const int ctas = 148;
-  a.mode = 1;
-  launch_lobpcg<T>(a, std::min(ctas, nlist), nullptr, phi, evals, iters, status, ks, eb, max_cells, max_lines, st);
   EbArgs e;
   e.g = a.g;
   e.subs = a.subs;
@@ -1718,6 +1949,22 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   e.tx = a.tx;
   e.ty = a.ty;
   e.tz = a.tz;
+  if (a.init_batched) {
+    const size_t init_smem = (size_t)20 * e.ldc;  // FP64 pivots + three FP32 coupling arrays
+    const size_t rr_smem0 = sizeof(LbSmall) + sizeof(LbMats);
+    const size_t gram_smem0 = (size_t)8 * 32 * 32 * sizeof(double);
+    cudaFuncSetAttribute(k_eb_init_a<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)init_smem);
+    cudaFuncSetAttribute(k_eb_init_rr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem0);
+    cudaFuncSetAttribute(k_eb_fin_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem0);
+    { note_launch(); k_eb_init_a<T><<<nlist, 256, init_smem, st>>>(e, a); }
+    { note_launch(); k_eb_init_aimg<T><<<dim3(a.m, nlist), 256, 0, st>>>(e); }
+    { note_launch(); k_eb_fin_gram<T><<<dim3(e.nchunk, nlist), 256, gram_smem0, st>>>(e); }
+    { note_launch(); k_eb_init_rr<<<nlist, 256, rr_smem0, st>>>(e, sizeof(T) == 4 ? 1e-9 : 1e-13); }
+    { note_launch(); k_eb_init_rot<T><<<dim3(e.nchunk, nlist), 256, 0, st>>>(e); }
+  } else {
+    a.mode = 1;
+    launch_lobpcg<T>(a, std::min(ctas, nlist), nullptr, phi, evals, iters, status, ks, eb, max_cells, max_lines, st);
+  }
   // column batch of the preconditioner: the built-in one keeps coefficients + mb
   // vectors within ~113 KB (2 CTAs per SM); the online tuner also tries all m
   // columns in one CTA (fewer barriers per column, 1 CTA per SM) and one column

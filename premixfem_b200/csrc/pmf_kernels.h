@@ -154,6 +154,7 @@ struct LobpcgArgs {
   // the per-subdomain slab and state; 2 = final Rayleigh-Ritz and output from them
   int mode;
   int final_batched;    // batched solver: 1 = final Rayleigh-Ritz and output as phase kernels, 0 = mode 2
+  int init_batched;     // batched solver: 1 = set-up (mass, IC(0), initial block, Rayleigh-Ritz) as phase kernels, 0 = mode 1
   unsigned char* slab;  // per-subdomain work slabs (modes 1, 2), stride slab_stride
   size_t slab_stride;
   void* state;          // per-subdomain EbState array (modes 1, 2)

@@ -118,6 +118,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_ctas", &o->eig_ctas);
   db.get_int("pmf_eig_batched", &o->eig_batched);
   db.get_int("pmf_eig_final", &o->eig_final);
+  db.get_int("pmf_eig_init", &o->eig_init);
   db.get_int("pmf_eig_profile", &o->eig_profile);
   db.get_int("pmf_pcg_graph", &o->pcg_graph);
   db.get_int("pmf_autotune", &o->autotune);
@@ -690,6 +691,7 @@ int Solver::setup() {
   la.queue = d_queue;
   la.mode = 0;
   la.final_batched = opt.eig_final;
+  la.init_batched = opt.eig_init;
   la.slab = nullptr;
   la.slab_stride = 0;
   la.state = nullptr;

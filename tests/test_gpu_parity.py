@@ -11,6 +11,8 @@ Tolerances (FP64 plain form unless stated):
   * mixed precision (FP32 preconditioner, FP64 PCG): iterations within +-1 of
     the oracle, same 1e-8 solution bound.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -19,6 +21,8 @@ from premixfem_b200 import fields
 from premixfem_b200.solver import DarcySolver, options_string
 
 pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _oracle_opts(d):
@@ -252,3 +256,51 @@ def test_batched_final_phase_matches_persistent(native, precision):
     ry = np.linalg.norm(out[1][1] - out[0][1]) / np.linalg.norm(out[0][1])
     assert ry <= tol, ry
     assert abs(out[1][2] - out[0][2]) <= 1
+
+
+INIT_CASES = {
+    # ragged 8 x 8 x 10 subdomains, one Dirichlet face (mass EIG_OP_MOD with the boundary term)
+    "ragged_fp64": (lambda: fields.random_box((32, 24, 20), seed=4, sigma=1.5, dirichlet={"x-": 1.0}),
+                    {"pmf_sd": (4, 3, 2), "en_lv1": 5, "en_lv2": 3, "pmf_precision": "fp64"}),
+    "ragged_mixed": (lambda: fields.random_box((32, 24, 20), seed=4, sigma=1.5, dirichlet={"x-": 1.0}),
+                     {"pmf_sd": (4, 3, 2), "en_lv1": 5, "en_lv2": 3, "pmf_precision": "mixed"}),
+    # learned start from the shipped weights, then the random restart of the subdomains it leaves
+    "fracture64_learned": (lambda: fields.fracture256(64, seed=3),
+                           {"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": "mixed",
+                            "pmf_learned": os.path.join(ROOT, "premixfem_b200", "weights", "fracture16_k6.pmfnet"),
+                            "pmf_learned_its": 30}),
+}
+
+
+@pytest.mark.parametrize("case", sorted(INIT_CASES))
+def test_batched_setup_phase_matches_persistent(native, case):
+    """The eigensolver's set-up (mass and Neumann diagonals, IC(0) pivots, the
+    initial block and its first Rayleigh-Ritz) as phase kernels
+    (-pmf_eig_init 1) against the persistent mode-1 launch (the default):
+    only the summation order of the first Grams differs, so in FP64 the local
+    eigenvalues agree to 1e-6 relative with the floor of 1e-9 x the
+    subdomain's largest wanted eigenvalue for the zero (constant) modes, and
+    the PCG iteration count to +-1.  Mixed precision stores the basis in
+    FP32: where that rounding flips in the first rotation, the two runs stop
+    at different iterates of the 1e-6 residual test (||r||_{M^-1} <= 1e-6 x
+    the largest diagonal-to-mass ratio, or 10 x that for a subdomain accepted
+    at its rounding floor), and the eigenvalues agree to 1e-5 relative with
+    a floor of 1e-6 x the largest wanted one."""
+    make, opts = INIT_CASES[case]
+    prob = make()
+    out = []
+    for ini in (0, 1):
+        s = _gpu(prob, dict(opts, pmf_eig_init=ini))
+        ev = s.eigen_lv1()[0].copy()
+        b = s.rhs(prob["source"].ravel())
+        _, its, _, reason = s.solve(b)
+        assert reason == "converged"
+        out.append((ev, its))
+        s.close()
+    ev0, ev1 = out[0][0], out[1][0]
+    scale = np.abs(ev0).max(axis=1, keepdims=True)
+    rtol, floor = (1e-5, 1e-1) if opts["pmf_precision"] == "mixed" else (1e-6, 1e-3)
+    rel = np.abs(ev1 - ev0) / np.maximum(np.abs(ev0), floor * scale)
+    w = np.unravel_index(np.argmax(rel), rel.shape)
+    assert rel.max() <= rtol, (rel.max(), w, ev0[w], ev1[w], scale[w[0], 0])
+    assert abs(out[1][1] - out[0][1]) <= 1, (out[0][1], out[1][1])
