@@ -36,7 +36,10 @@ typedef struct pmf_solver pmf_solver;
 /* Options use the reference's PETSc option names: -sd, -en_lv1, -en_lv2,
  * -eb_lv1, -eb_lv2, -si_lv1, -si_lv2, -eg_op, -use_W_cycle, -no_shift_A_cc,
  * -use_full_Cholesky_lv1 (banded Cholesky local solves), -use_2level,
- * -ksp_rtol, -ksp_max_it; B200 extensions: -pmf_sd sx,sy,sz (subdomains per
+ * -ksp_rtol, -ksp_max_it, -ksp_constant_null_space (PETSc's: the constant
+ * vector is the operator's null space, removed from every preconditioned
+ * residual of the CG solve; for operators with no Dirichlet face); B200
+ * extensions: -pmf_sd sx,sy,sz (subdomains per
  * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
  * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it, -pmf_learned
  * <weights file> (learned initial blocks for the local eigensolves),

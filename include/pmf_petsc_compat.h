@@ -171,6 +171,9 @@ PetscErrorCode KSPSetType(KSP ksp, KSPType type);
 PetscErrorCode KSPGetPC(KSP ksp, PC* pc);
 PetscErrorCode KSPSetNormType(KSP ksp, KSPNormType normtype);
 PetscErrorCode KSPSetTolerances(KSP ksp, PetscReal rtol, PetscReal abstol, PetscReal dtol, PetscInt maxits);
+/* reads -ksp_type, -pc_type, -ksp_rtol, -ksp_atol, -ksp_divtol, -ksp_max_it,
+ * -ksp_norm_type, -ksp_monitor, -ksp_converged_reason and
+ * -ksp_constant_null_space (constant null space of the operator) */
 PetscErrorCode KSPSetFromOptions(KSP ksp);
 PetscErrorCode KSPSetUp(KSP ksp);
 PetscErrorCode KSPSolve(KSP ksp, Vec b, Vec x);

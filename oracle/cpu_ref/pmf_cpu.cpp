@@ -494,8 +494,17 @@ EigStat lobpcg(const Local& L, int eg_op, int k, double tol, int max_it, double 
         GM[(size_t)b * ns + a] = GM[(size_t)a * ns + b];
         GA[(size_t)a * ns + b] = GA[(size_t)b * ns + a] = 0.5 * (GA[(size_t)a * ns + b] + GB[(size_t)a * ns + b]);
       }
+    // unit M-norm scaling; a column whose M-norm is negligible against the
+    // block's largest (search directions decay geometrically once X stops
+    // moving) carries no direction and is left out (scale 0), as a clamped
+    // scale would blow its rounding up into the projected matrix
     Vec dsc(ns), G2((size_t)ns * ns), ev, EV;
-    for (int a = 0; a < ns; ++a) dsc[a] = 1.0 / std::sqrt(std::max(GM[(size_t)a * ns + a], 1e-300));
+    double gmax = 0.0;
+    for (int a = 0; a < ns; ++a) gmax = std::max(gmax, GM[(size_t)a * ns + a]);
+    for (int a = 0; a < ns; ++a) {
+      const double gaa = GM[(size_t)a * ns + a];
+      dsc[a] = gaa > 1e-28 * gmax ? 1.0 / std::sqrt(gaa) : 0.0;
+    }
     for (int a = 0; a < ns; ++a)
       for (int b = 0; b < ns; ++b) G2[(size_t)a * ns + b] = GM[(size_t)a * ns + b] * dsc[a] * dsc[b];
     sym_eig(G2, ns, ev, EV);
@@ -644,8 +653,9 @@ extern "C" {
 //   mesh[3] M N P; dom[3] domain lengths; kx, ky, kz cell permeabilities (ky / kz may be
 //   null: isotropic); source per cell; dir_on[6] / dir_val[6] Dirichlet faces
 //   x- x+ y- y+ z- z+ and their pressures.
-//   iopt[15]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
-//             eig_max_it, eg_op, threads (<= 0: the OpenMP default)
+//   iopt[16]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
+//             eig_max_it, eg_op, threads (<= 0: the OpenMP default), constant null
+//             space (-ksp_constant_null_space: every preconditioned residual loses its mean)
 //   dopt[3]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii)
 //   x_out[n]: solution; info[10]: its, setup_s, solve_s, threads, eig_its_mean,
 //             eig_its_max, eig_unconverged, ||r_final||, ||r_0||, level-3 size
@@ -658,6 +668,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   const int sd[3] = {iopt[0], iopt[1], iopt[2]}, vr[3] = {iopt[3], iopt[4], iopt[5]};
   const int k = iopt[6], en2_in = iopt[7], si1 = std::max(1, iopt[8]), si2 = std::max(1, iopt[9]);
   const int wcycle = iopt[10], max_it = iopt[11], eig_max_it = iopt[12], eg_op = iopt[13], threads = iopt[14];
+  const bool null_space = iopt[15] != 0;
   const double rtol = dopt[0], eig_tol = dopt[1], eig_sigma = dopt[2];
   for (int i = 0; i < 3; ++i)
     if (mesh[i] < 1 || sd[i] < 1 || vr[i] < 1 || mesh[i] < vr[i] * sd[i]) return -1;
@@ -994,12 +1005,23 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     for (long long i = 0; i < n; ++i) s += a[i] * c[i];
     return s;
   };
+  // MatNullSpaceRemove of the constant null space: z <- z - (sum z / n) 1
+  auto remove_constant = [&](double* v) {
+    if (!null_space) return;
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (long long i = 0; i < n; ++i) s += v[i];
+    s = s / (-(double)n);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < n; ++i) v[i] += s;
+  };
   double dp = std::sqrt(dot(r.data(), r.data()));
   const double r0 = dp;
   const double ttol = std::max(rtol * dp, 1e-50);
   int its = 0;
   if (dp > ttol) {
     pc_apply(r.data(), z.data());
+    remove_constant(z.data());
     double beta = dot(z.data(), r.data()), betaold = 0.0, dpi = 0.0;
     for (int i = 0; i < max_it; ++i) {
       its = i + 1;
@@ -1025,6 +1047,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
       dp = std::sqrt(dot(r.data(), r.data()));
       if (!std::isfinite(dp) || dp <= ttol) break;
       pc_apply(r.data(), z.data());
+      remove_constant(z.data());
       beta = dot(z.data(), r.data());
     }
   }

@@ -71,6 +71,10 @@ class Options:
     use_2level: bool = False
     rtol: float = 1.0e-8
     max_it: int = 10000
+    # -ksp_constant_null_space (PETSc KSPSetFromOptions, read by the drivers'
+    # KSPSetFromOptions call, src/Expe_scal.c:115): the constant vector is the
+    # operator's null space, removed from every preconditioned residual
+    constant_null_space: bool = False
     eig_method: str = "dense"  # "dense": scipy.linalg.eigh; "arpack": eigsh shift-and-invert (SLEPc-like)
 
     def normalized(self):
@@ -603,12 +607,25 @@ class Preconditioner:
         return y
 
 
-def pcg(A, b, apply_pc, rtol=1.0e-8, max_it=10000, abstol=1.0e-50):
+def remove_constant(z):
+    """MatNullSpaceRemove of a constant null space: z <- z - (sum z / n) 1."""
+    return z - z.sum() / z.size
+
+
+def pcg(A, b, apply_pc, rtol=1.0e-8, max_it=10000, abstol=1.0e-50, null_space=False):
     """PETSc KSPSolve_CG with KSP_NORM_UNPRECONDITIONED and KSPConvergedDefault.
 
     Returns (x, its, history, reason).  Convergence when ||r_k|| <= max(rtol
-    ||r_0||, abstol) with r_0 = b (zero initial guess).
+    ||r_0||, abstol) with r_0 = b (zero initial guess).  With ``null_space``
+    (a constant null space attached to the operator) every preconditioned
+    residual loses its mean, as KSP_PCApply does for a left preconditioner;
+    b is not projected (the operator carries no transpose null space).
     """
+    if null_space:
+        inner = apply_pc
+
+        def apply_pc(r):
+            return remove_constant(inner(r))
     x = np.zeros_like(b)
     r = b.copy()
     dp = float(np.linalg.norm(r))
@@ -667,5 +684,6 @@ def solve(problem, opts: Options):
     op = Operator(problem)
     b = op.rhs()
     pc = Preconditioner(op, opts)
-    x, its, hist, reason = pcg(op.A, b, pc.apply, rtol=pc.opts.rtol, max_it=pc.opts.max_it)
+    x, its, hist, reason = pcg(op.A, b, pc.apply, rtol=pc.opts.rtol, max_it=pc.opts.max_it,
+                               null_space=pc.opts.constant_null_space)
     return {"op": op, "pc": pc, "b": b, "x": x, "its": its, "hist": hist, "reason": reason}

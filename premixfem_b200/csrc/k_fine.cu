@@ -203,6 +203,45 @@ void launch_pcg_beta(const double* r, const double* z, long long n, double* part
   { note_launch(); k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nb, s); }
 }
 
+// Constant null space (-ksp_constant_null_space): PETSc's KSP_PCApply removes
+// the operator's null space from every preconditioned residual of a left-
+// preconditioned solve (MatNullSpaceRemove with a constant: z <- z - (sum z / n) 1),
+// then CG takes beta = z.r of the projected z.  Two grid-stride passes: the
+// per-block sums of z, then every block forms the mean from those partials in
+// the same fixed order, shifts z and writes its partial of z.r.  Skipped once
+// the solve is done, like the preconditioner kernels of a replayed graph chunk.
+__global__ void k_null_sum(const double* z, long long n, double* zpart, const int* done) {
+  __shared__ double red[32];
+  if (*done) return;
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v += z[i];
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) zpart[blockIdx.x] = v;
+}
+__global__ void k_null_project(double* z, const double* r, long long n, const double* zpart, int nb, double* part,
+                               const int* done) {
+  __shared__ double red[32];
+  if (*done) return;
+  const double shift = fixed_sum(zpart, nb, red) / (-(double)n);
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double zi = z[i] + shift;
+    z[i] = zi;
+    v += zi * r[i];
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+void launch_pcg_null_beta(double* z, const double* r, long long n, double* part, double* zpart, PcgState* s,
+                          cudaStream_t st) {
+  const int nb = cell_blocks(n);
+  { note_launch(); k_null_sum<<<nb, kCellThreads, 0, st>>>(z, n, zpart, &s->done); }
+  { note_launch(); k_null_project<<<nb, kCellThreads, 0, st>>>(z, r, n, zpart, nb, part, &s->done); }
+  { note_launch(); k_pcg_beta_fin<<<1, 256, 0, st>>>(part, nb, s); }
+}
+
 // p <- z (first) or z + (beta/betaold) p; w <- A p; partial p.w.
 // In-place on p: the stencil reads p at neighbours, so p_new is formed from z
 // and the old p of each neighbour on the fly, and written to pout != pin.

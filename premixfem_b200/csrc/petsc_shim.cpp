@@ -62,6 +62,7 @@ struct _p_KSP {
   double rtol = 1e-5, atol = 1e-50, dtol = 1e5;
   int max_it = 10000;
   bool is_setup = false, monitor = false, view_reason = false;
+  bool null_space = false;  // -ksp_constant_null_space: constant null space on the operator
   int its = 0;
   double rnorm = 0.0;
   KSPConvergedReason reason = KSP_CONVERGED_ITERATING;
@@ -608,6 +609,15 @@ PetscErrorCode KSPSetFromOptions(KSP ksp) {
     else
       return SHIM_ERR(PETSC_ERR_ARG_WRONG, "unknown -ksp_norm_type %s", t->c_str());
   }
+  if (const std::string* t = find_opt(nullptr, "ksp_constant_null_space")) {
+    // PetscOptionsBool: the bare flag or true/yes/on/1 sets it, false/no/off/0 clears it
+    if (t->empty() || *t == "1" || *t == "true" || *t == "yes" || *t == "on")
+      ksp->null_space = true;
+    else if (*t == "0" || *t == "false" || *t == "no" || *t == "off")
+      ksp->null_space = false;
+    else
+      return SHIM_ERR(PETSC_ERR_ARG_WRONG, "unknown -ksp_constant_null_space %s", t->c_str());
+  }
   PetscBool b = PETSC_FALSE;
   PetscCall(PetscOptionsHasName(nullptr, nullptr, "-ksp_monitor", &b));
   ksp->monitor = b;
@@ -652,6 +662,17 @@ static PetscErrorCode cg_host(KSP ksp, Vec b, Vec x) {
     for (PetscInt i = 0; i < n; ++i) t += v->a[i] * v->a[i];
     return sqrt(t);
   };
+  // KSP_PCApply: the preconditioner, then MatNullSpaceRemove of the constant
+  // null space (z <- z - (sum z / n) 1) when the operator carries one
+  auto precondition = [&](Vec rr, Vec zz) -> PetscErrorCode {
+    PetscErrorCode e = pc_apply(&ksp->pc, rr, zz);
+    if (e || !ksp->null_space || n == 0) return e;
+    double sum = 0.0;
+    for (PetscInt i = 0; i < n; ++i) sum += zz->a[i];
+    const double shift = sum / (-(double)n);
+    for (PetscInt i = 0; i < n; ++i) zz->a[i] += shift;
+    return 0;
+  };
   double beta = 0.0, betaold = 0.0, dp = 0.0, ttol = 0.0, dpi = 0.0, dpiold = 0.0;
   // residual test; returns true when the iteration stops
   auto test = [&](int it) {
@@ -675,10 +696,10 @@ static PetscErrorCode cg_host(KSP ksp, Vec b, Vec x) {
       dp = norm2(r);
       ttol = fmax(ksp->rtol * dp, ksp->atol);
       if (test(0)) break;
-      if ((ierr = pc_apply(&ksp->pc, r, z))) break;
+      if ((ierr = precondition(r, z))) break;
       VecDot(z, r, &beta);
     } else {
-      if ((ierr = pc_apply(&ksp->pc, r, z))) break;
+      if ((ierr = precondition(r, z))) break;
       VecDot(z, r, &beta);
       dp = natural ? sqrt(fabs(beta)) : norm2(z);
       ttol = fmax(ksp->rtol * dp, ksp->atol);
@@ -708,10 +729,10 @@ static PetscErrorCode cg_host(KSP ksp, Vec b, Vec x) {
       if (unprec) {
         dp = norm2(r);
         if (test(i + 1)) break;
-        if ((ierr = pc_apply(&ksp->pc, r, z))) break;
+        if ((ierr = precondition(r, z))) break;
         VecDot(z, r, &beta);
       } else {
-        if ((ierr = pc_apply(&ksp->pc, r, z))) break;
+        if ((ierr = precondition(r, z))) break;
         VecDot(z, r, &beta);
         dp = natural ? sqrt(fabs(beta)) : norm2(z);
         if (test(i + 1)) break;
@@ -740,6 +761,7 @@ PetscErrorCode KSPSolve(KSP ksp, Vec b, Vec x) {
     s->opt.rtol = ksp->rtol;
     s->opt.atol = ksp->atol;
     s->opt.max_it = ksp->max_it;
+    s->opt.null_space = ksp->null_space;
     int its = 0, code = 0;
     double rnorm = 0.0;
     const double av0 = s->t_stages[pmf::ST_AV];

@@ -45,6 +45,9 @@ void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, doub
 void launch_pcg_beta_fin(const double* part, int nparts, PcgState* s, cudaStream_t st);
 // same, computing the partials itself
 void launch_pcg_beta(const double* r, const double* z, long long n, double* part, PcgState* s, cudaStream_t st);
+// constant null space: z <- z - mean(z), then beta = z.r (zpart: cell_blocks(n) scratch partials)
+void launch_pcg_null_beta(double* z, const double* r, long long n, double* part, double* zpart, PcgState* s,
+                          cudaStream_t st);
 void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
                        const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
                        cudaStream_t st, int variant = 0);

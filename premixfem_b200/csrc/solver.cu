@@ -95,6 +95,21 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   o->no_shift_A_cc = db.has("no_shift_A_cc");
   o->use_full_Cholesky_lv1 = db.has("use_full_Cholesky_lv1");
   o->use_2level = db.has("use_2level");
+  {
+    // PETSc boolean option: the bare flag or true/yes/on/1 sets it, false/no/off/0 clears it
+    auto itn = db.kv.find("ksp_constant_null_space");
+    if (itn != db.kv.end()) {
+      const std::string& v = itn->second;
+      if (v.empty() || v == "1" || v == "true" || v == "yes" || v == "on")
+        o->null_space = true;
+      else if (v == "0" || v == "false" || v == "no" || v == "off")
+        o->null_space = false;
+      else {
+        *err = "Error in -ksp_constant_null_space (true | false)";
+        return 62;
+      }
+    }
+  }
   db.get_real("ksp_rtol", &o->rtol);
   db.get_real("ksp_atol", &o->atol);
   db.get_int("ksp_max_it", &o->max_it);
@@ -403,7 +418,8 @@ void Solver::alloc_fine() {
     cudaMalloc(&inv32, n * 4);
   }
   const int nparts = std::max(cell_blocks(g.ncell), nsub) + 64;
-  cudaMalloc(&part, nparts * 8);
+  cudaMalloc(&part, (size_t)(nparts + cell_blocks(g.ncell)) * 8);
+  zpart = part + nparts;
   cudaMalloc(&state, sizeof(PcgState));
 }
 
@@ -1154,8 +1170,16 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   cudaEventRecord(ev0, st);
   launch_pcg_start(g, bs, xs, r, part, state, opt.rtol, opt.atol, opt.max_it, st);
   const int* done = &state->done;
+  // beta = z.r from the preconditioner's partials, or of the projected z when
+  // the operator carries the constant null space
+  auto beta = [&]() {
+    if (opt.null_space)
+      launch_pcg_null_beta(z, r, g.ncell, part, zpart, state, st);
+    else
+      launch_pcg_beta_fin(part, nparts_apply(), state, st);
+  };
   apply(r, z, part, done);
-  launch_pcg_beta_fin(part, nparts_apply(), state, st);
+  beta();
   double* pin = p0;
   double* pout = p1;
   int guard = 0;
@@ -1165,7 +1189,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
       launch_pcg_iter_a(g, tx, ty, tz, diag, z, pin, pout, w, part, state, st, pcga_variant);
       launch_pcg_iter_b(g.ncell, xs, r, pout, w, part, state, st);
       apply(r, z, part, done);
-      launch_pcg_beta_fin(part, nparts_apply(), state, st);
+      beta();
       std::swap(pin, pout);
     }
   };
@@ -1174,7 +1198,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   // solution buffer and replayed until the device-side `done` flag is set.
   // An even chunk returns the p buffers to their roles, so replays chain.
   const bool use_graph = opt.pcg_graph && chunk % 2 == 0;
-  if (use_graph && (!pcg_exec || pcg_graph_x != xs)) {
+  if (use_graph && (!pcg_exec || pcg_graph_x != xs || pcg_graph_ns != opt.null_space)) {
     if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
     pcg_exec = nullptr;
     const unsigned long long l0 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
@@ -1189,6 +1213,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
     cudaGraphDestroy(graph);
     if (int e = check(ie, "graph instantiate")) return e;
     pcg_graph_x = xs;
+    pcg_graph_ns = opt.null_space;
   }
   for (;;) {
     if (use_graph) {

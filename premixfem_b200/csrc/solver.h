@@ -21,6 +21,7 @@ struct Options {
   int si_lv1 = 1, si_lv2 = 1;
   int eg_op = 0;
   bool use_W_cycle = false, no_shift_A_cc = false, use_full_Cholesky_lv1 = false, use_2level = false;
+  bool null_space = false;  // -ksp_constant_null_space: the constant is the operator's null space
   int precision = 0;  // 0 plain FP64, 1 FP32 preconditioner inside FP64 PCG
   double rtol = 1e-8;
   double atol = 1e-50;  // KSP abstol (PETSc default)
@@ -126,6 +127,7 @@ class Solver {
   void *y0 = nullptr, *y1 = nullptr;
   double *vb = nullptr, *vx = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *w = nullptr,
          *part = nullptr;
+  double* zpart = nullptr;  // tail of part: per-block sums of z for the constant null space
   PcgState* state = nullptr;
   PcgState* h_state = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -151,6 +153,7 @@ class Solver {
   double eig_phase_ms[8] = {0};
   cudaGraphExec_t pcg_exec = nullptr;  // one chunk of PCG iterations
   const double* pcg_graph_x = nullptr;
+  bool pcg_graph_ns = false;  // the null-space setting the graph was captured with
   unsigned long long pcg_graph_kernels = 0;
   unsigned long long eig_colcells = 0;
   int alloc_eb(int m, bool mixed);

@@ -18,6 +18,10 @@ synthetic fields of the same shapes and value distributions:
                       inclusions (k = 1e-4); p = 1 on x = 0, p = 0 on x = 255.
 * ``large_frac``      512 x 512 x 256, anisotropic GRF (sigma 3) plus 400
                       fracture planes of contrast 1e6; p = 0 on z = 0.
+* ``grf_batch``       64 independent unit-cube problems with per-axis cell
+                      counts U{24..80}, k = exp(GRF) with sigma U[1,3] and
+                      correlation U[0.05,0.2], p = 0 on x = 1, and 4
+                      right-hand sides each (unit source + 3 N(0,1) fields).
 * ``cross``           the reference's own cross field (src/Expe_scal.c:11-42).
 * ``aniso_const``     the reference's test.c field k = (2, 1, 0.5).
 
@@ -242,12 +246,15 @@ def fracture256(n=256, seed=4, n_frac=200, frac_lo=32, frac_hi=160, barrier=0.05
                     name=f"fracture{n}")
 
 
-def large_frac(M=512, N=512, P=256, seed=5, n_frac=400):
-    """Large anisotropic GRF + fracture planes; p = 0 on z = 0, unit source."""
+def large_frac(M=512, N=512, P=256, seed=5, n_frac=400, frac_lo=32, frac_hi=256):
+    """Large anisotropic GRF + fracture planes; p = 0 on z = 0, unit source.
+
+    Fracture planes have in-plane extent U{frac_lo..frac_hi} (clipped to the
+    grid) and k = 1e6 times the background scale."""
     rng = np.random.default_rng(seed)
     g = _grf_periodic((P, N, M), (1.0 / P, 1.0 / N, 1.0 / M), 3.0, (0.02, 0.1, 0.1), rng, embed=1)
     k = np.exp(g)
-    _add_fractures(rng, k, n_frac, 32, 256, 1.0e6)
+    _add_fractures(rng, k, n_frac, frac_lo, frac_hi, 1.0e6)
     src = np.full((P, N, M), 1.0 / (M * N * P))
     return _problem((M, N, P), (1.0, 1.0, 1.0), (k, k, k), src, {"z-": 0.0}, name="large_frac")
 
@@ -267,3 +274,37 @@ def random_box(mesh, seed=0, sigma=1.0, corr=0.2, dirichlet=None, source="unit")
         dirichlet = {"x-": 0.0}
     return _problem((M, N, P), (1.0, 1.0, 1.0), (k, k, k), src, dirichlet, zero_mean=not dirichlet,
                     name=f"random{M}x{N}x{P}")
+
+
+def grf_batch(count=64, seed=3, lo=24, hi=80, n_rhs=4):
+    """The batching workload: ``count`` independent problems on the unit cube.
+
+    Per problem: per-axis cell counts U{lo..hi}; k = exp(g), g a GRF with
+    sigma U[1,3] and isotropic exponential correlation length U[0.05,0.2];
+    p = 0 on x = 1, no-flux elsewhere.  Right-hand sides: the unit source
+    f = 1 and ``n_rhs - 1`` fields of N(0,1) values, all cell-integrated.
+    Returns a list of (problem, [source arrays]); ``problem["source"]`` is the
+    unit source.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        M, N, P = (int(v) for v in rng.integers(lo, hi + 1, size=3))
+        sigma = float(rng.uniform(1.0, 3.0))
+        corr = float(rng.uniform(0.05, 0.2))
+        g = _grf_periodic((P, N, M), (1.0 / P, 1.0 / N, 1.0 / M), sigma, corr, rng, embed=2)
+        k = np.exp(g)
+        meas = 1.0 / (M * N * P)
+        sources = [np.full((P, N, M), meas)]
+        for _ in range(n_rhs - 1):
+            sources.append(rng.standard_normal((P, N, M)) * meas)
+        prob = _problem((M, N, P), (1.0, 1.0, 1.0), (k, k, k), sources[0], {"x+": 0.0},
+                        name=f"grf_batch{M}x{N}x{P}")
+        out.append((prob, sources))
+    return out
+
+
+def tiles(mesh, tile=8):
+    """Subdomains per axis for tiles of about ``tile`` cells (near-equal split,
+    so boundary-adjacent sizes are ragged): ceil(n / tile), at least 2."""
+    return tuple(max(2, -(-int(n) // tile)) for n in mesh)

@@ -76,3 +76,62 @@ def test_thread_count_does_not_change_the_result():
     b = CR.solve(prob, sd=2, threads=4)
     assert a["its"] == b["its"]
     assert np.linalg.norm(a["x"] - b["x"]) <= 1e-10 * np.linalg.norm(a["x"])
+
+
+# Reduced copies of the other benchmark distributions.  The layered channel
+# field keeps the 10 x 10 x 5 subdomains, 20 x 10 x 2 cells and 1e6 channel
+# contrast of the 60 x 220 x 85 workload; the large fracture field keeps
+# sigma 3 and the 1e6 fracture planes of the 512 x 512 x 256 one, with k = 8
+# eigenvectors.
+
+
+def test_layered_channels_match_oracle():
+    # Pure Neumann with a zero-sum injector/producer pair.  Without a null space
+    # the CG recurrence stalls on the constant direction before 1e-8 (PETSc's
+    # DIVERGED_INDEFINITE); with -ksp_constant_null_space both solves converge
+    # to the direct solution.
+    prob = fields.layered(seed=2, M=20, N=30, P=10, smooth_layers=4)
+    opts = dict(sd=(2, 3, 2), en_lv1=4, en_lv2=4)
+    plain = O.solve(prob, O.Options(**opts))
+    assert plain["reason"] == "diverged_indefinite"
+    ref = O.solve(prob, O.Options(**opts, constant_null_space=True))
+    assert ref["reason"] == "converged_rtol"
+    xd = O.direct_solve(ref["op"], ref["b"])
+    a = ref["x"] - ref["x"].mean()
+    assert np.linalg.norm(a - (xd - xd.mean())) <= 1e-8 * np.linalg.norm(xd - xd.mean())
+    got = CR.solve(prob, **opts, constant_null_space=True)
+    assert got["eig_unconverged"] == 0
+    assert got["rnorm"] <= 1e-8 * got["r0"]
+    assert abs(got["its"] - ref["its"]) <= 1, (got["its"], ref["its"])
+    b = got["x"] - got["x"].mean()
+    err = np.linalg.norm(b - a) / np.linalg.norm(a)
+    assert err < 1e-8, err
+
+
+
+def test_large_fracture_field_matches_oracle():
+    prob = fields.large_frac(M=32, N=32, P=16, seed=5, n_frac=8, frac_lo=4, frac_hi=32)
+    opts = dict(sd=(4, 4, 2), en_lv1=8, en_lv2=4)
+    ref = O.solve(prob, O.Options(**opts))
+    got = CR.solve(prob, **opts)
+    assert got["eig_unconverged"] == 0
+    assert abs(got["its"] - ref["its"]) <= 1, (got["its"], ref["its"])
+    err = np.linalg.norm(got["x"] - ref["x"]) / np.linalg.norm(ref["x"])
+    assert err < 1e-8, err
+
+
+def test_problem_batch_every_rhs_matches_oracle():
+    # independent ragged problems of the batching workload, four right-hand
+    # sides each through one preconditioner set-up of the oracle
+    for prob, sources in fields.grf_batch(count=3, seed=3, lo=10, hi=20):
+        opts = dict(sd=fields.tiles(prob["mesh"]), en_lv1=4, en_lv2=4)
+        op = O.Operator(prob)
+        pc = O.Preconditioner(op, O.Options(**opts))
+        for src in sources:
+            b = O.Operator(dict(prob, source=src)).rhs()
+            x_ref, its_ref, _, reason = O.pcg(op.A, b, pc.apply)
+            assert reason == "converged_rtol"
+            got = CR.solve(dict(prob, source=src), **opts)
+            assert abs(got["its"] - its_ref) <= 1, (prob["mesh"], got["its"], its_ref)
+            err = np.linalg.norm(got["x"] - x_ref) / np.linalg.norm(x_ref)
+            assert err < 1e-8, (prob["mesh"], err)

@@ -153,3 +153,25 @@ def test_vranks_reproduce_multi_rank_structure(w_cycle):
     assert len(pc.lay.ranks) == 4 and len(pc.lay.subs) == 32
     assert pc.A3.shape == (12, 12)
     assert res["reason"] == "converged_rtol"
+
+
+def test_constant_null_space_steadies_pure_neumann_cg():
+    # Pure Neumann, default +NIL shift of the level-3 matrix: the constant mode
+    # of z is amplified by 1/NIL, so the plain iteration count at 1e-10 moves
+    # with 1e-15 perturbations of the source.  Removing the constant from z
+    # (-ksp_constant_null_space) makes it deterministic, and every run reaches
+    # the zero-mean direct solution.
+    opts = dict(sd=2, vranks=(1, 2, 2), en_lv1=4, en_lv2=4, rtol=1e-10, constant_null_space=True)
+    rng = np.random.default_rng(0)
+    its = set()
+    for t in range(4):
+        prob = fields.cross(16, 3)
+        src = prob["source"] * (1 + (1e-15 * rng.standard_normal(prob["source"].shape) if t else 0.0))
+        prob["source"] = src / np.linalg.norm(src)
+        r = O.solve(prob, O.Options(**opts))
+        assert r["reason"] == "converged_rtol"
+        its.add(r["its"])
+        xd = O.direct_solve(r["op"], r["b"])
+        xd -= xd.mean()
+        assert np.linalg.norm(r["x"] - r["x"].mean() - xd) <= 1e-9 * np.linalg.norm(xd)
+    assert len(its) == 1, its
