@@ -443,8 +443,8 @@ struct EigStat {
 // Smallest k eigenpairs of A^N v = lambda M v on a box; block size m = k + 2, soft
 // locking of converged wanted columns.  Residual ||A x - lambda M x||_{M^-1} divided by
 // max_i (A^N_ii / M_ii).  Xout: k M-orthonormal columns (column j at [j * n]).
-EigStat lobpcg(const Local& L, int eg_op, int k, double tol, int max_it, double sigma_rel, unsigned long long seed,
-               Vec& Xout) {
+EigStat lobpcg(const Local& L, int eg_op, int k, double tol, int max_it, double sigma_rel, double rel_floor,
+               unsigned long long seed, Vec& Xout) {
   const int n = L.b.n();
   const int m = std::min(k + 2, n);
   constexpr int CH = 64;
@@ -603,7 +603,9 @@ EigStat lobpcg(const Local& L, int eg_op, int k, double tol, int max_it, double 
         rcol[i] = r;
         s += r * r * iMd[i];
       }
-      const bool done = std::sqrt(s) / lscale <= tol;
+      // residual scale: lscale, or max(|lambda_j|, rel_floor lscale) (eigenvalue-relative)
+      const double rs = rel_floor > 0.0 ? std::max(std::fabs(lj), rel_floor * lscale) : lscale;
+      const bool done = std::sqrt(s) / rs <= tol;
       if (j < k && !done) conv = false;
       if (!done || j >= k) {  // soft locking: converged wanted columns leave the search
         ic0_solve(L, D, rcol.data(), &W[(size_t)na * n]);
@@ -656,7 +658,8 @@ extern "C" {
 //   iopt[16]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
 //             eig_max_it, eg_op, threads (<= 0: the OpenMP default), constant null
 //             space (-ksp_constant_null_space: every preconditioned residual loses its mean)
-//   dopt[3]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii)
+//   dopt[4]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii),
+//             eig_rel_floor (> 0: eigen residual test relative to max(|lambda|, floor x lscale))
 //   x_out[n]: solution; info[10]: its, setup_s, solve_s, threads, eig_its_mean,
 //             eig_its_max, eig_unconverged, ||r_final||, ||r_0||, level-3 size
 // Returns 0, or -1 for invalid arguments.
@@ -669,7 +672,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   const int k = iopt[6], en2_in = iopt[7], si1 = std::max(1, iopt[8]), si2 = std::max(1, iopt[9]);
   const int wcycle = iopt[10], max_it = iopt[11], eig_max_it = iopt[12], eg_op = iopt[13], threads = iopt[14];
   const bool null_space = iopt[15] != 0;
-  const double rtol = dopt[0], eig_tol = dopt[1], eig_sigma = dopt[2];
+  const double rtol = dopt[0], eig_tol = dopt[1], eig_sigma = dopt[2], eig_rel_floor = dopt[3];
   for (int i = 0; i < 3; ++i)
     if (mesh[i] < 1 || sd[i] < 1 || vr[i] < 1 || mesh[i] < vr[i] * sd[i]) return -1;
   if (k < 1 || k > 64 || en2_in < 1 || eg_op < 0 || eg_op > 2) return -1;
@@ -738,7 +741,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     Vec dg;
     local_diag(L, false, dg);
     ic0(L, dg, nullptr, 0.0, lv1D[s]);
-    est[s] = lobpcg(L, eg_op, k, eig_tol, eig_max_it, eig_sigma, 0x9E3779B97F4A7C15ull ^ (unsigned long long)(s + 1),
+    est[s] = lobpcg(L, eg_op, k, eig_tol, eig_max_it, eig_sigma, eig_rel_floor, 0x9E3779B97F4A7C15ull ^ (unsigned long long)(s + 1),
                     phi[s]);
   }
 

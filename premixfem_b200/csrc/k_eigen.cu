@@ -941,7 +941,10 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
       if (threadIdx.x < m) {
         double v = 0.0;
         for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += mt.red[threadIdx.x * 33 + wi];
-        sm.res[threadIdx.x] = sqrt(v) / lscale;
+        // residual scale: lscale (the largest diag(A_N)/M), or, with a relative
+        // floor f, max(|lambda_j|, f lscale) as an eigenvalue-relative test
+        const double rs = a.rel_floor > 0.0 ? fmax(fabs(sm.lam[threadIdx.x]), a.rel_floor * lscale) : lscale;
+        sm.res[threadIdx.x] = sqrt(v) / rs;
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -1219,7 +1222,7 @@ struct EbArgs {
   const SubInfo* subs;
   const int* list;
   int m, k, ld, ldc, mb, nchunk, max_it;
-  double tol;
+  double tol, rel_floor;
   unsigned char* slab;
   size_t slab_stride;
   EbState* state;
@@ -1277,7 +1280,8 @@ __global__ void k_eb_control(EbArgs a, int nlist, int it) {
   for (int j = 0; j < m; ++j) {
     double v = 0.0;
     for (int c = 0; c < nch; ++c) v += a.rpart[((size_t)s * a.nchunk + c) * LB_MM + j];
-    const double res = sqrt(v) / es.lscale;
+    const double rs = a.rel_floor > 0.0 ? fmax(fabs(es.lam[j]), a.rel_floor * es.lscale) : es.lscale;
+    const double res = sqrt(v) / rs;
     const bool done_j = res <= a.tol;
     if (j < k) worst = fmax(worst, res);
     if (j < k && !done_j) cv = 0;
@@ -1936,6 +1940,7 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   e.nchunk = b.nchunk;
   e.max_it = a.max_it;
   e.tol = a.tol;
+  e.rel_floor = a.rel_floor;
   e.slab = b.slab;
   e.slab_stride = b.slab_stride;
   e.state = reinterpret_cast<EbState*>(b.state);

@@ -136,6 +136,7 @@ struct LobpcgArgs {
   int eg_op;  // mass matrix variant
   int max_it;
   double tol;
+  double rel_floor;  // > 0: residual test relative to max(|lambda_j|, rel_floor x lscale) instead of lscale
   double sigma_rel;  // IC(0) preconditioner shift, relative
   unsigned long long seed;
   const double *tx, *ty, *tz, *diag, *db;  // FP64 operator

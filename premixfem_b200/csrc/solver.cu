@@ -128,6 +128,10 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_max_it", &o->eig_max_it);
   db.get_real("pmf_eig_tol", &o->eig_tol);
   db.get_real("pmf_eig_sigma", &o->eig_sigma);
+  if (db.get_real("pmf_eig_rel_floor", &o->eig_rel_floor) && !(o->eig_rel_floor >= 0.0 && o->eig_rel_floor < 1.0)) {
+    *err = "Error in -pmf_eig_rel_floor (0 <= f < 1)";
+    return 62;
+  }
   db.get_int("pmf_eig_guard", &o->eig_guard);
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
   db.get_int("pmf_eig_ctas", &o->eig_ctas);
@@ -706,6 +710,7 @@ int Solver::setup() {
   if (!d_queue) cudaMalloc(&d_queue, sizeof(int));
   la.queue = d_queue;
   la.mode = 0;
+  la.rel_floor = opt.eig_rel_floor;
   la.final_batched = opt.eig_final;
   la.init_batched = opt.eig_init;
   la.slab = nullptr;

@@ -36,6 +36,7 @@ struct Options {
   int pcg_chunk = 4;
   int pcg_graph = 1;  // replay each chunk of PCG iterations as one CUDA graph
   int eig_final = 1;  // batched eigensolver: final Rayleigh-Ritz and output as phase kernels (0: one persistent launch)
+  double eig_rel_floor = 0.0;  // > 0: eigen residual test relative to max(|lambda|, floor x lscale)
   int eig_init = 0;   // batched eigensolver: 1 = set-up as phase kernels, 0 = one persistent launch
   int autotune = -1;  // launch-shape tuning: 1 on, 0 off, -1 the process default (PMF_AUTOTUNE)
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)

@@ -135,3 +135,23 @@ def test_problem_batch_every_rhs_matches_oracle():
             assert abs(got["its"] - its_ref) <= 1, (prob["mesh"], got["its"], its_ref)
             err = np.linalg.norm(got["x"] - x_ref) / np.linalg.norm(x_ref)
             assert err < 1e-8, (prob["mesh"], err)
+
+
+def test_eigenvalue_relative_stopping_rule_on_channels():
+    # The local eigensolves stop at ||r_j||_{M^-1} <= tol x lscale (lscale = max
+    # diag(A_N) / M).  On channel fields the smallest eigenvalues lie far below
+    # lscale, the coarse space they give is too loose, and CG stalls above 1e-8.
+    # -pmf_eig_rel_floor 1e-4 tests against max(|lambda_j|, 1e-4 lscale) instead
+    # and reaches the dense-eigensolver oracle's iteration count and solution.
+    prob = fields.layered(seed=2, M=20, N=20, P=10, smooth_layers=4, contrast=1e4)
+    opts = dict(sd=(2, 2, 2), en_lv1=4, en_lv2=4)
+    ref = O.solve(prob, O.Options(**opts, constant_null_space=True))
+    assert ref["reason"] == "converged_rtol"
+    loose = CR.solve(prob, **opts, constant_null_space=True, max_it=300)
+    assert loose["rnorm"] > 1e-8 * loose["r0"]
+    got = CR.solve(prob, **opts, constant_null_space=True, eig_rel_floor=1e-4)
+    assert got["rnorm"] <= 1e-8 * got["r0"]
+    assert abs(got["its"] - ref["its"]) <= 1, (got["its"], ref["its"])
+    a = ref["x"] - ref["x"].mean()
+    err = np.linalg.norm(got["x"] - got["x"].mean() - a) / np.linalg.norm(a)
+    assert err < 1e-8, err
