@@ -8,6 +8,19 @@ Cases (subdomains of 16^3 cells unless stated):
              grid (n/64)^3 with -sd 4
   grf        n^3 unit-cube GRF (sigma 2, correlation 0.1), p = 0 on x = 1,
              unit source, 8^3 subdomains, en_lv1 = 4
+  layered    60 x 220 x 85 layered channel field (cells 20 x 10 x 2, channel
+             contrast 1e6, +/-1 injector/producer, pure Neumann): 6 x 22 x 17
+             subdomains of 10 x 10 x 5 on a 2 x 2 x 1 virtual rank grid (the
+             per-rank dense coarse inverse holds at most 4096 unknowns),
+             en_lv1 = 4, -ksp_constant_null_space; --n is ignored
+  large      n x n x n/2 anisotropic GRF (sigma 3) with fracture planes of
+             contrast 1e6, p = 0 on z = 0 (512 x 512 x 256 at n = 512):
+             16^3 subdomains, -sd 8 on an (n/128, n/128, n/256) virtual rank
+             grid, en_lv1 = 8, en_lv2 = 4
+  batch      --count independent unit-cube GRF problems (per-axis sizes
+             U{24..80}, sigma U[1,3], correlation U[0.05,0.2], p = 0 on
+             x = 1), ~8^3 ragged subdomains, en_lv1 = 4; one set-up and four
+             right-hand sides (unit + 3 N(0,1)) each; --n is ignored
 
 This is the driver the kernel profiles are taken on (a small case of the
 benchmark's kernels under a profiler), and a quick way to try options:
@@ -36,14 +49,58 @@ def make_case(case, n, seed):
             raise SystemExit("--n must be a multiple of 8 for the grf case")
         prob = fields.unit_cube_grf(n, seed=seed)
         opts = {"sd": n // 8, "en_lv1": 4, "en_lv2": 4}
+    elif case == "layered":
+        prob = fields.layered(seed=seed)
+        opts = {"pmf_sd": (3, 11, 17), "pmf_vranks": (2, 2, 1), "en_lv1": 4, "en_lv2": 4,
+                "ksp_constant_null_space": True}
+    elif case == "large":
+        if n % 256:
+            raise SystemExit("--n must be a multiple of 256 for the large case")
+        f = n / 512.0
+        prob = fields.large_frac(M=n, N=n, P=n // 2, seed=seed, n_frac=max(1, int(400 * f * f)),
+                                 frac_lo=max(4, int(32 * f)), frac_hi=int(256 * f))
+        opts = {"sd": 8, "pmf_vranks": (n // 128, n // 128, n // 256), "en_lv1": 8, "en_lv2": 4}
     else:
         raise SystemExit(f"unknown case {case}")
     return prob, opts
 
 
+def run_batch(args):
+    """The batching workload: per problem one set-up and four solves; one JSON
+    line per problem, then the totals."""
+    import torch
+
+    tot_setup = tot_solve = 0.0
+    its_all = []
+    for q, (prob, sources) in enumerate(fields.grf_batch(count=args.count, seed=args.seed)):
+        opts = {"pmf_sd": fields.tiles(prob["mesh"]), "en_lv1": 4, "en_lv2": 4, "pmf_precision": args.precision}
+        s = DarcySolver.from_problem(prob, options_string(opts) + " " + args.opts)
+        s.setup()
+        su, _ = s.timing()
+        its, solve_ms = [], 0.0
+        for src in sources:
+            b = s.rhs(torch.from_numpy(np.ascontiguousarray(src).ravel()).cuda())
+            x = torch.empty_like(b)
+            _, it, _, reason = s.solve(b, x)
+            if reason != "converged":
+                raise SystemExit(f"problem {q} {prob['mesh']}: {reason}")
+            its.append(it)
+            solve_ms += s.timing()[1]
+        s.close()
+        tot_setup += su
+        tot_solve += solve_ms
+        its_all += its
+        print(json.dumps({"case": "batch", "problem": q, "mesh": prob["mesh"], "precision": args.precision,
+                          "setup_ms": round(su, 3), "solve_ms": round(solve_ms, 3), "pcg_iters": its}), flush=True)
+    print(json.dumps({"case": "batch", "problems": args.count, "rhs": 4 * args.count, "precision": args.precision,
+                      "setup_ms_total": round(tot_setup, 3), "solve_ms_total": round(tot_solve, 3),
+                      "pcg_iters_mean": float(np.mean(its_all)), "pcg_iters_max": int(np.max(its_all))}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--case", default="fracture", choices=["fracture", "grf"])
+    ap.add_argument("--case", default="fracture", choices=["fracture", "grf", "layered", "large", "batch"])
+    ap.add_argument("--count", type=int, default=64, help="problems of the batch case")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -52,6 +109,9 @@ def main():
     ap.add_argument("--learned", action="store_true", help="start the local eigensolves from the trained network")
     args = ap.parse_args()
 
+    if args.case == "batch":
+        run_batch(args)
+        return
     import torch
 
     prob, opts = make_case(args.case, args.n, args.seed)
