@@ -17,11 +17,12 @@
 // of A^N + sigma M; the level-3 HEP and the Rayleigh-Ritz problems by
 // Householder tridiagonalisation and the implicit symmetric QR step with a
 // Wilkinson shift (Golub & Van Loan, Matrix Computations, Alg. 8.3.1-8.3.3);
-// MUMPS / SuperLU by a dense Cholesky factorisation that drops null pivots.
-// Not covered: the adaptive eigenvalue bounds (-eb_lv1/-eb_lv2 stay at their
-// defaults, so every subdomain keeps en_lv1 vectors), -use_2level and
-// -use_full_Cholesky_lv1.  tests/test_cpu_ref.py checks it against the NumPy
-// oracle (oracle/pmf_oracle.py).
+// MUMPS / SuperLU by a dense Cholesky factorisation that drops null pivots;
+// CHOLMOD (-use_full_Cholesky_lv1) by a band Cholesky of each subdomain block
+// (Golub & Van Loan, Alg. 4.3.5).  Adaptive eigenvector counts (-eb_lv1,
+// -eb_lv2, :369-383 and :1100-1115) are kept as zero basis columns, which the
+// null-pivot Cholesky factors and the level-3 right-hand sides then ignore.
+// tests/test_cpu_ref.py checks it against the NumPy oracle (oracle/pmf_oracle.py).
 #include <omp.h>
 
 #include <algorithm>
@@ -394,6 +395,63 @@ void ic0_solve(const Local& L, const Vec& iD, const double* r, double* y) {
     }
 }
 
+// Exact Cholesky L L^T of a box's principal block with diagonal dg
+// (-use_full_Cholesky_lv1, :205-207): natural order, half bandwidth hb = nx ny,
+// band[i (hb + 1) + (i - j)] = L(i, j) for i - hb <= j <= i (band Cholesky,
+// Golub & Van Loan Alg. 4.3.5, row by row).  Returns false on a non-positive pivot.
+bool band_chol(const Local& L, const Vec& dg, Vec& band) {
+  const Problem& p = *L.p;
+  const Box& b = L.b;
+  const int n = b.n(), hb = b.nx * b.ny, w = hb + 1;
+  band.assign((size_t)n * w, 0.0);
+  int cl = 0;
+  for (int k = 0; k < b.nz; ++k)
+    for (int j = 0; j < b.ny; ++j) {
+      const long long c0 = p.id(b.x0, b.y0 + j, b.z0 + k);
+      for (int i = 0; i < b.nx; ++i, ++cl) {
+        const long long c = c0 + i;
+        double* row = &band[(size_t)cl * w];
+        row[0] = dg[cl];
+        if (i > 0) row[1] = -p.tx[c];
+        if (j > 0) row[b.nx] = -p.ty[c];
+        if (k > 0) row[hb] = -p.tz[c];
+      }
+    }
+  for (int i = 0; i < n; ++i) {
+    const int j0 = std::max(0, i - hb);
+    double* Li = &band[(size_t)i * w];
+    for (int j = j0; j <= i; ++j) {
+      const double* Lj = &band[(size_t)j * w];
+      double s = Li[i - j];
+      for (int q = j0; q < j; ++q) s -= Li[i - q] * Lj[j - q];
+      if (j < i) {
+        Li[i - j] = s / Lj[0];
+      } else {
+        if (!(s > 0.0)) return false;
+        Li[0] = std::sqrt(s);
+      }
+    }
+  }
+  return true;
+}
+
+// y = (L L^T)^-1 r with the band factor of band_chol.
+void band_solve(const Vec& band, int n, int hb, const double* r, double* y) {
+  const int w = hb + 1;
+  for (int i = 0; i < n; ++i) {
+    const double* Li = &band[(size_t)i * w];
+    double s = r[i];
+    for (int q = std::max(0, i - hb); q < i; ++q) s -= Li[i - q] * y[q];
+    y[i] = s / Li[0];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    const double* Li = &band[(size_t)i * w];
+    const double yi = y[i] / Li[0];
+    y[i] = yi;
+    for (int q = std::max(0, i - hb); q < i; ++q) y[q] -= Li[i - q] * yi;
+  }
+}
+
 // Mass diagonal M_i of the local GHEP (:243-346).  eg_op 0 (MOD) keeps the reference's
 // x-direction accumulation: the face between local cells i-1 and i is added to cell i-1,
 // so a cell counts its right face twice unless it ends its row, and its left face only
@@ -438,6 +496,7 @@ void mass_diag(const Local& L, int eg_op, const Vec& dN, Vec& Md) {
 // ---- local GHEP: LOBPCG -------------------------------------------------------------------
 struct EigStat {
   int its = 0, converged = 0;
+  Vec lam;  // the k lowest Ritz values of the last Rayleigh-Ritz step
 };
 
 // Smallest k eigenpairs of A^N v = lambda M v on a box; block size m = k + 2, soft
@@ -637,6 +696,7 @@ EigStat lobpcg(const Local& L, int eg_op, int k, double tol, int max_it, double 
     hasP = true;
   }
   st.its = it;
+  st.lam.assign(lam.begin(), lam.begin() + k);
   Xout.assign((size_t)n * k, 0.0);
   for (int j = 0; j < k; ++j) {
     double s = 0.0;
@@ -655,14 +715,18 @@ extern "C" {
 //   mesh[3] M N P; dom[3] domain lengths; kx, ky, kz cell permeabilities (ky / kz may be
 //   null: isotropic); source per cell; dir_on[6] / dir_val[6] Dirichlet faces
 //   x- x+ y- y+ z- z+ and their pressures.
-//   iopt[16]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
+//   iopt[19]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
 //             eig_max_it, eg_op, threads (<= 0: the OpenMP default), constant null
-//             space (-ksp_constant_null_space: every preconditioned residual loses its mean)
-//   dopt[4]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii),
-//             eig_rel_floor (> 0: eigen residual test relative to max(|lambda|, floor x lscale))
+//             space (-ksp_constant_null_space: every preconditioned residual loses its
+//             mean), no_shift_A_cc, use_2level, use_full_Cholesky_lv1
+//   dopt[6]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii),
+//             eig_rel_floor (> 0: eigen residual test relative to max(|lambda|, floor x
+//             lscale)), eb_lv1, eb_lv2 (< 0: 1 / NIL, every subdomain keeps en_lv1 and
+//             every rank en_lv2 vectors)
 //   x_out[n]: solution; info[10]: its, setup_s, solve_s, threads, eig_its_mean,
 //             eig_its_max, eig_unconverged, ||r_final||, ||r_0||, level-3 size
-// Returns 0, or -1 for invalid arguments.
+// Returns 0, -1 for invalid arguments, -2 when a subdomain block of
+// -use_full_Cholesky_lv1 is not positive definite.
 int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const double* ky, const double* kz,
                   const double* source, const int* dir_on, const double* dir_val, const int* iopt,
                   const double* dopt, double* x_out, double* info) {
@@ -671,8 +735,10 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   const int sd[3] = {iopt[0], iopt[1], iopt[2]}, vr[3] = {iopt[3], iopt[4], iopt[5]};
   const int k = iopt[6], en2_in = iopt[7], si1 = std::max(1, iopt[8]), si2 = std::max(1, iopt[9]);
   const int wcycle = iopt[10], max_it = iopt[11], eig_max_it = iopt[12], eg_op = iopt[13], threads = iopt[14];
-  const bool null_space = iopt[15] != 0;
+  const bool null_space = iopt[15] != 0, no_shift = iopt[16] != 0, two_level = iopt[17] != 0,
+             full_chol = iopt[18] != 0;
   const double rtol = dopt[0], eig_tol = dopt[1], eig_sigma = dopt[2], eig_rel_floor = dopt[3];
+  const double eb1 = dopt[4] < 0.0 ? 1.0 / NIL : dopt[4], eb2 = dopt[5] < 0.0 ? 1.0 / NIL : dopt[5];
   for (int i = 0; i < 3; ++i)
     if (mesh[i] < 1 || sd[i] < 1 || vr[i] < 1 || mesh[i] < vr[i] * sd[i]) return -1;
   if (k < 1 || k > 64 || en2_in < 1 || eg_op < 0 || eg_op > 2) return -1;
@@ -732,18 +798,33 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
         }
   }
 
-  // level 1 factors and level 2 local eigenvectors
+  // level 1 factors (IC(0), or the exact band Cholesky) and level 2 local
+  // eigenvectors; the adaptive count (:369-383) keeps the first j + 1 vectors at
+  // the first lambda_j >= eb_lv1 and zeroes the rest
   std::vector<Vec> lv1D(nsub), phi(nsub);
   std::vector<EigStat> est(nsub);
-#pragma omp parallel for schedule(dynamic)
+  std::vector<int> ks(nsub, k);
+  int chol_fail = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : chol_fail)
   for (int s = 0; s < nsub; ++s) {
     const Local L{&p, subs[s]};
     Vec dg;
     local_diag(L, false, dg);
-    ic0(L, dg, nullptr, 0.0, lv1D[s]);
+    if (full_chol)
+      chol_fail += band_chol(L, dg, lv1D[s]) ? 0 : 1;
+    else
+      ic0(L, dg, nullptr, 0.0, lv1D[s]);
     est[s] = lobpcg(L, eg_op, k, eig_tol, eig_max_it, eig_sigma, eig_rel_floor, 0x9E3779B97F4A7C15ull ^ (unsigned long long)(s + 1),
                     phi[s]);
+    for (int j = 0; j < k; ++j)
+      if (est[s].lam[j] >= eb1) {
+        ks[s] = j + 1;
+        break;
+      }
+    const int ns = subs[s].n();
+    std::fill(phi[s].begin() + (size_t)ks[s] * ns, phi[s].end(), 0.0);
   }
+  if (chol_fail) return -2;
 
   // Galerkin blocks: blk[s][0] = Phi_s^T A Phi_s, blk[s][1 + f] = Phi_s^T A Phi_nb(s, f);
   // gface[s][f] = sum over face f of t phi_s phi_s^T (the Neumann correction across it).
@@ -811,8 +892,9 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   const int en2 = std::min(en2_in, nr);
   std::vector<Vec> A2L(nrank), V3(nrank);
   std::vector<std::vector<char>> A2null(nrank);
+  std::vector<int> num3(nrank, 0);
 #pragma omp parallel for schedule(dynamic)
-  for (int r = 0; r < nrank; ++r) {
+  for (int r = 0; r < (two_level ? 0 : nrank); ++r) {
     Vec A((size_t)nr * nr, 0.0), AN((size_t)nr * nr, 0.0);
     for (int a = 0; a < spr; ++a) {
       const int s = r * spr + a;
@@ -841,19 +923,34 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     }
     chol_semidef(A, nr, A2null[r]);
     A2L[r].swap(A);
-    Vec w, V;
-    sym_eig(AN, nr, w, V);
+    // HEP on the rank's kept dofs only; adaptive count (:1100-1115) with eb_lv2
+    std::vector<int> act;
+    for (int a = 0; a < spr; ++a)
+      for (int i = 0; i < ks[r * spr + a]; ++i) act.push_back(a * k + i);
+    const int na = (int)act.size();
+    Vec ANc((size_t)na * na), w, V;
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < na; ++j) ANc[(size_t)i * na + j] = AN[(size_t)act[i] * nr + act[j]];
+    sym_eig(ANc, na, w, V);
+    const int k3 = std::min(en2_in, na);
+    int num = k3;
+    for (int j = 0; j < k3; ++j)
+      if (w[j] >= eb2) {
+        num = j + 1;
+        break;
+      }
+    num3[r] = num;
     V3[r].assign((size_t)nr * en2, 0.0);
-    for (int i = 0; i < nr; ++i)
-      for (int j = 0; j < en2; ++j) V3[r][(size_t)i * en2 + j] = V[(size_t)i * nr + j];
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < num; ++j) V3[r][(size_t)act[i] * en2 + j] = V[(size_t)i * na + j];
   }
 
   // A3 = V^T (Phi^T A Phi) V + NIL I, assembled block by block (each thread owns the
   // rows of its rank), and its factor
-  const int n3 = nrank * en2;
+  const int n3 = two_level ? 0 : nrank * en2;
   Vec A3((size_t)n3 * n3, 0.0);
 #pragma omp parallel for schedule(dynamic)
-  for (int r = 0; r < nrank; ++r) {
+  for (int r = 0; r < (two_level ? 0 : nrank); ++r) {
     Vec t(k);
     for (int a = 0; a < spr; ++a) {
       const int s = r * spr + a;
@@ -877,21 +974,47 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
       }
     }
   }
-  for (int i = 0; i < n3; ++i) A3[(size_t)i * n3 + i] += NIL;
+  if (!no_shift)  // :1361-1363
+    for (int i = 0; i < n3; ++i) A3[(size_t)i * n3 + i] += NIL;
   std::vector<char> A3null;
-  chol_semidef(A3, n3, A3null);
+  if (n3) chol_semidef(A3, n3, A3null);
+  // -use_2level (:423-735): the global Phi^T A Phi over every subdomain, cross-rank
+  // blocks included, + NIL I unless -no_shift_A_cc, in place of levels 2 and 3
+  const int nc = two_level ? nsub * k : 0;
+  Vec A2g((size_t)nc * nc, 0.0);
+  std::vector<char> A2gnull;
+  if (two_level) {
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < nsub; ++s)
+      for (int bb = 0; bb < 7; ++bb) {
+        const int s2 = bb == 0 ? s : nbr[(size_t)s * 6 + bb - 1];
+        if (s2 < 0) continue;
+        const double* B = &blk[((size_t)s * 7 + bb) * kk2];
+        for (int i = 0; i < k; ++i)
+          for (int j = 0; j < k; ++j) A2g[(size_t)(s * k + i) * nc + s2 * k + j] = B[i * k + j];
+      }
+    if (!no_shift)
+      for (int i = 0; i < nc; ++i) A2g[(size_t)i * nc + i] += NIL;
+    chol_semidef(A2g, nc, A2gnull);
+  }
+  int n3_kept = 0;
+  for (int r = 0; r < nrank; ++r) n3_kept += num3[r];
   const auto t1 = clk::now();
 
   // ---- preconditioner: y = 0, then r = x - A y and y += B_l r for each visit
-  std::vector<int> sched;
+  std::vector<int> sched;  // 1, 2, 3: the levels; 4: the global 2-level coarse solve
   for (int i = 0; i < si1; ++i) sched.push_back(1);
-  for (int i = 0; i < si2; ++i) sched.push_back(2);
-  sched.push_back(3);
-  if (wcycle) {
+  if (two_level) {  // :1918-1922
+    sched.push_back(4);
+  } else {
     for (int i = 0; i < si2; ++i) sched.push_back(2);
     sched.push_back(3);
+    if (wcycle) {
+      for (int i = 0; i < si2; ++i) sched.push_back(2);
+      sched.push_back(3);
+    }
+    for (int i = 0; i < si2; ++i) sched.push_back(2);
   }
-  for (int i = 0; i < si2; ++i) sched.push_back(2);
   for (int i = 0; i < si1; ++i) sched.push_back(1);
   Vec cvec((size_t)nsub * k), zvec((size_t)nsub * k), rres(n), ay(n), d3(n3);
   auto restrict_ = [&](const double* r) {
@@ -956,7 +1079,10 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
               const long long c0 = p.id(b.x0, b.y0 + jj, b.z0 + kk);
               for (int ii = 0; ii < b.nx; ++ii, ++cl) rl[cl] = rres[c0 + ii];
             }
-          ic0_solve(L, lv1D[s], rl.data(), yl.data());
+          if (full_chol)
+            band_solve(lv1D[s], ns, b.nx * b.ny, rl.data(), yl.data());
+          else
+            ic0_solve(L, lv1D[s], rl.data(), yl.data());
           cl = 0;
           for (int kk = 0; kk < b.nz; ++kk)
             for (int jj = 0; jj < b.ny; ++jj) {
@@ -964,6 +1090,11 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
               for (int ii = 0; ii < b.nx; ++ii, ++cl) y[c0 + ii] += yl[cl];
             }
         }
+      } else if (lvl == 4) {
+        restrict_(rres.data());
+        std::copy(cvec.begin(), cvec.end(), zvec.begin());
+        chol_solve(A2g, A2gnull, nc, zvec.data());
+        prolong(y);
       } else if (lvl == 2) {
         restrict_(rres.data());
 #pragma omp parallel for schedule(dynamic)
@@ -1072,7 +1203,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     info[6] = eunc;
     info[7] = dp;
     info[8] = r0;
-    info[9] = n3;
+    info[9] = two_level ? 0 : n3_kept;
   }
   return 0;
 }

@@ -52,7 +52,8 @@ def _iptr(a):
 
 def solve(problem, sd=(2, 2, 2), vranks=(1, 1, 1), en_lv1=4, en_lv2=4, si_lv1=1, si_lv2=1, use_W_cycle=False,
           eg_op=0, rtol=1e-8, max_it=10000, eig_tol=1e-8, eig_max_it=300, eig_sigma=1e-2, threads=0,
-          constant_null_space=False, eig_rel_floor=0.0):
+          constant_null_space=False, eig_rel_floor=0.0, eb_lv1=-1.0, eb_lv2=-1.0, no_shift_A_cc=False,
+          use_2level=False, use_full_Cholesky_lv1=False):
     """Setup + PCG solve.  Returns dict(x, its, setup_s, solve_s, threads, eig_its_mean,
     eig_its_max, eig_unconverged, rnorm, r0, n3)."""
     lib = load()
@@ -69,9 +70,10 @@ def solve(problem, sd=(2, 2, 2), vranks=(1, 1, 1), en_lv1=4, en_lv2=4, si_lv1=1,
     mesh = np.array([M, N, P], dtype=np.int32)
     dom = np.array(problem["dom"], dtype=np.float64)
     iopt = np.array(list(sd) + list(vranks) + [en_lv1, en_lv2, si_lv1, si_lv2, int(bool(use_W_cycle)), max_it,
-                                               eig_max_it, eg_op, threads, int(bool(constant_null_space))],
-                    dtype=np.int32)
-    dopt = np.array([rtol, eig_tol, eig_sigma, eig_rel_floor], dtype=np.float64)
+                                               eig_max_it, eg_op, threads, int(bool(constant_null_space)),
+                                               int(bool(no_shift_A_cc)), int(bool(use_2level)),
+                                               int(bool(use_full_Cholesky_lv1))], dtype=np.int32)
+    dopt = np.array([rtol, eig_tol, eig_sigma, eig_rel_floor, eb_lv1, eb_lv2], dtype=np.float64)
     x = np.zeros(M * N * P)
     info = np.zeros(10)
     rc = lib.pmf_cpu_solve(_iptr(mesh), _dptr(dom), _dptr(kx), _dptr(ky), _dptr(kz), _dptr(src), _iptr(dir_on),

@@ -33,6 +33,13 @@ CASES = [
      dict(sd=2, vranks=(2, 1, 1), en_lv1=3, en_lv2=3, eg_op=2, use_W_cycle=True, si_lv1=2, si_lv2=2)),
     ("ragged_aniso", lambda: _aniso_box((13, 11, 9), 7, {"y+": 0.5, "z-": -1.0}),
      dict(sd=(2, 2, 1), vranks=(2, 1, 2), en_lv1=3, en_lv2=2, eg_op=0)),
+    ("grf16_2level", lambda: fields.unit_cube_grf(16, seed=2), dict(sd=2, vranks=(2, 2, 1), en_lv1=4, use_2level=True)),
+    ("aniso_2level_si2", lambda: dict(fields.aniso_const(8, 8, 8), dirichlet={"z+": 1.0}),
+     dict(sd=2, en_lv1=3, use_2level=True, si_lv1=2)),
+    ("grf16_full_cholesky", lambda: fields.unit_cube_grf(16, seed=1),
+     dict(sd=2, en_lv1=4, en_lv2=4, use_full_Cholesky_lv1=True)),
+    ("ragged_full_cholesky", lambda: fields.random_box((13, 11, 9), seed=7, sigma=2.0),
+     dict(sd=(2, 2, 1), vranks=(2, 1, 3), en_lv1=3, en_lv2=2, use_full_Cholesky_lv1=True)),
 ]
 
 
@@ -62,6 +69,38 @@ def test_pure_neumann_solution():
     b = got["x"] - got["x"].mean()
     err = np.linalg.norm(b - a) / np.linalg.norm(a)
     assert err < 1e-8, err
+
+
+def test_pure_neumann_without_shift_matches_oracle():
+    # -no_shift_A_cc: the null pivot of the level-3 matrix is dropped, so the
+    # iteration count no longer depends on rounding and must match
+    prob = fields.aniso_const(8, 8, 8)
+    opts = dict(sd=2, en_lv1=4, en_lv2=4, no_shift_A_cc=True)
+    ref = O.solve(prob, O.Options(**opts))
+    got = CR.solve(prob, **opts)
+    assert got["its"] == ref["its"]
+    a, b = ref["x"] - ref["x"].mean(), got["x"] - got["x"].mean()
+    assert np.linalg.norm(b - a) <= 1e-8 * np.linalg.norm(a)
+
+
+def test_adaptive_eigenvector_counts_match_oracle():
+    # -eb_lv1 / -eb_lv2 (:369-383, :1100-1115) halfway between neighbouring order
+    # statistics of the oracle's eigenvalues, so that the counts vary across
+    # subdomains and ranks and no eigenvalue sits on a threshold
+    prob = fields.unit_cube_grf(16, seed=5)
+    base = dict(sd=2, vranks=(2, 2, 1), en_lv1=6, en_lv2=4)
+    pc = O.solve(prob, O.Options(**base))["pc"]
+    w3 = np.sort([w[3] for w in pc.eigvals_lv1])
+    v1 = np.sort([w[1] for w in pc.eigvals_lv2])
+    h = len(w3) // 2
+    opts = dict(base, eb_lv1=0.5 * (w3[h - 1] + w3[h]), eb_lv2=0.5 * (v1[1] + v1[2]))
+    ref = O.solve(prob, O.Options(**opts))
+    counts1, counts2 = ref["pc"].eig_num_lv1, ref["pc"].eig_num_lv2
+    assert min(counts1) < max(counts1) and min(counts2) < 4
+    got = CR.solve(prob, **opts)
+    assert got["n3"] == sum(counts2)
+    assert abs(got["its"] - ref["its"]) <= 1, (got["its"], ref["its"])
+    assert np.linalg.norm(got["x"] - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
 
 
 def test_rejects_too_many_eigenvectors():
