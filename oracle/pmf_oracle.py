@@ -75,6 +75,9 @@ class Options:
     # KSPSetFromOptions call, src/Expe_scal.c:115): the constant vector is the
     # operator's null space, removed from every preconditioned residual
     constant_null_space: bool = False
+    # store the local eigenvectors rounded to FP32, as the mixed form keeps the
+    # coarse basis (the Galerkin products and solves stay FP64)
+    phi_fp32: bool = False
     eig_method: str = "dense"  # "dense": scipy.linalg.eigh; "arpack": eigsh shift-and-invert (SLEPc-like)
 
     def normalized(self):
@@ -481,6 +484,8 @@ class Preconditioner:
                 w, V = w[order], V[:, order]
             else:
                 w, V = sla.eigh(An, np.diag(Md), subset_by_index=[0, k - 1])
+            if o.phi_fp32:
+                V = V.astype(np.float32).astype(np.float64)
             self.eigvals_lv1.append(w)
             # adaptive count, :369-383
             num, vmax = k, w[k - 1]

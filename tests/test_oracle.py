@@ -175,3 +175,17 @@ def test_constant_null_space_steadies_pure_neumann_cg():
         xd -= xd.mean()
         assert np.linalg.norm(r["x"] - r["x"].mean() - xd) <= 1e-9 * np.linalg.norm(xd)
     assert len(its) == 1, its
+
+
+@pytest.mark.parametrize("contrast,mesh,sd,its", [(1e6, (20, 30, 10), (2, 3, 2), 76), (1e4, (20, 20, 10), (2, 2, 2), 43)])
+def test_fp32_stored_basis_keeps_the_channel_iterations(contrast, mesh, sd, its):
+    # The mixed form stores the local eigenvectors in FP32.  On the layered
+    # channel fields, exact eigenvectors rounded to FP32 give the iteration
+    # count of the FP64 ones: the storage is not what limits the mixed form there.
+    M, N, P = mesh
+    prob = fields.layered(seed=2, M=M, N=N, P=P, smooth_layers=4, contrast=contrast)
+    opts = dict(sd=sd, en_lv1=4, en_lv2=4, constant_null_space=True)
+    r64 = O.solve(prob, O.Options(**opts))
+    r32 = O.solve(prob, O.Options(**opts, phi_fp32=True))
+    assert r64["reason"] == r32["reason"] == "converged_rtol"
+    assert r64["its"] == its and abs(r32["its"] - r64["its"]) <= 1
