@@ -40,13 +40,14 @@ int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_
   // PC_init argument checks (src/PreMixFEM_3D.c:1653-1654)
   if (!(dom[0] > 0.0 && dom[1] > 0.0 && dom[2] > 0.0)) return fail(62, "Errors in dom(L, W, H)");
   if (!(mesh[0] > 0 && mesh[1] > 0 && mesh[2] > 0)) return fail(62, "Errors in mesh(M, N, P)");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(76, "no CUDA device available");
+  // options first: their errors do not depend on a device
   pmf::OptionDB db;
   db.parse(options ? options : "");
   pmf::Options o;
   std::string err;
   if (int e = pmf::options_from_db(db, &o, &err)) return fail(e, err);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(76, "no CUDA device available");
   try {
     pmf_solver* h = new pmf_solver;
     h->s = new pmf::Solver(dom, mesh, o);

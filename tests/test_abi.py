@@ -45,3 +45,30 @@ def test_library_exports_reference_interface_and_petsc_subset():
 def test_every_header_is_covered():
     headers = sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
     assert headers == ["PreMixFEM_3D.h", "pmf_b200.h", "pmf_petsc_compat.h"]
+
+
+def test_option_errors_come_before_the_device():
+    """pmf_create checks its options on the host first: a malformed option is
+    argument error 62 with or without a GPU; well-formed options get as far as
+    the device (0 with a GPU, 76 without one)."""
+    import ctypes as C
+
+    lib = _native.load()
+    dom = (C.c_double * 3)(1.0, 1.0, 1.0)
+    mesh = (C.c_int * 3)(8, 8, 8)
+
+    def create(opts):
+        h = C.c_void_p()
+        rc = lib.pmf_create(C.cast(dom, C.c_void_p), C.cast(mesh, C.c_void_p), opts.encode(), C.byref(h))
+        if rc == 0:
+            lib.pmf_destroy(h)
+        return rc
+
+    bad = ["-eg_op 7", "-pmf_precision half", "-ksp_constant_null_space maybe", "-pmf_eig_rel_floor 1.5",
+           "-pmf_eig_rel_floor -0.1", "-pmf_learned"]
+    for opts in bad:
+        assert create("-sd 2 " + opts) == 62, opts
+    good = ["", "-ksp_constant_null_space", "-ksp_constant_null_space false", "-pmf_eig_rel_floor 1e-4",
+            "-pmf_eig_init 1 -pmf_precision mixed", "-use_2level -no_shift_A_cc"]
+    for opts in good:
+        assert create("-sd 2 " + opts) in (0, 76), opts
