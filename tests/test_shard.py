@@ -41,7 +41,7 @@ def _free_port():
 
 def _local_preconditioner(pc, op, slab, halo):
     """The oracle's PC_apply_vec restricted to one slab, with the exchanges."""
-    lay, plane = pc.lay, slab.plane
+    lay = pc.lay
     lo, hi = slab.first_cell, slab.first_cell + slab.ncell
     elo, ehi = slab.ext_cells
     A_loc = op.A[lo:hi][:, elo:ehi].tocsr()
