@@ -111,6 +111,56 @@ class Halo:
         return torch.cat([t for t in (lo, v, hi) if t is not None])
 
 
+class ShardedCycle:
+    """PC_apply_vec (src/PreMixFEM_3D.c:1840-1936) on one slab: y = 0, then for
+    each visit of ``schedule`` r = x - A y and y += B_level r.
+
+    The local mathematics comes in as callables on this process's part:
+    ``residual(x, y_ext)`` (x - A y with y extended by its halo planes),
+    ``level1(r)`` (the subdomain solves), ``restrict(r)`` (Phi^T r on the local
+    coarse dofs), ``prolong(z)`` (Phi z), ``level2(c)`` (the virtual ranks'
+    coarse solves), ``level3_rhs(c)`` (the n3-vector with this process's
+    entries of Psi^T r, zeros elsewhere), ``level3_solve(d)`` (the replicated
+    level-3 solve), ``level3_back(w)`` (V w on the local coarse dofs), and for
+    the 2-level schedule ``coarse_rhs(c)`` / ``coarse_solve(cg)`` (the global
+    coarse vector with the local entries, and its solve restricted to the local
+    dofs).  The cycle owns the exchanges: the halo of y before every residual
+    after the first visit, and the sum over processes of the level-3 (or global
+    coarse) right-hand side.  Schedule entries: 1, 2, 3, or "2g".
+    """
+
+    def __init__(self, schedule, halo, **pieces):
+        self.schedule = list(schedule)
+        self.halo = halo
+        self.p = pieces
+        self.sums = 0  # coarse right-hand sides summed over the processes
+
+    def _sum(self, v):
+        dist.all_reduce(v)
+        self.sums += 1
+        return v
+
+    def apply(self, x):
+        p = self.p
+        y = torch.zeros_like(x)
+        for v, lvl in enumerate(self.schedule):
+            r = x.clone() if v == 0 else p["residual"](x, self.halo.extend(y))
+            if lvl == 1:
+                y += p["level1"](r)
+                continue
+            c = p["restrict"](r)
+            if lvl == 2:
+                z = p["level2"](c)
+            elif lvl == 3:
+                z = p["level3_back"](p["level3_solve"](self._sum(p["level3_rhs"](c))))
+            elif lvl == "2g":
+                z = p["coarse_solve"](self._sum(p["coarse_rhs"](c)))
+            else:
+                raise ValueError(f"unknown cycle level {lvl!r}")
+            y += p["prolong"](z)
+        return y
+
+
 def global_sum(*values, like=None):
     """Sums of host scalars (or 0-d tensors) over every process, in one all-reduce."""
     t = torch.tensor([float(v) for v in values], dtype=torch.float64,

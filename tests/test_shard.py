@@ -4,11 +4,12 @@ Each process owns a z-slab of whole virtual-rank layers.  Its local operator
 and the local pieces of the oracle's three-level preconditioner (level-1
 solvers of its subdomains, its part of Phi, the level-2 factors of its virtual
 ranks, its level-3 V blocks and the replicated level-3 factor) stand in for
-the device kernels; the exchanges are the library's: halo planes before every
-stencil product, the level-3 right-hand side (and the 2-level coarse
-right-hand side) summed over the processes, and the CG dots.  The assembled
-solution and the iteration count must match the single-process oracle (the
-sums of the dot products are only reordered: iterations +-1, solution 1e-10).
+the device kernels as shard.ShardedCycle's callables; the exchanges are the
+module's own: halo planes before every stencil product, the level-3 right-hand
+side (and the 2-level coarse right-hand side) summed over the processes, and
+the CG dots.  The assembled solution and the iteration count must match the
+single-process oracle (the sums of the dot products are only reordered:
+iterations +-1, solution 1e-10).
 """
 import socket
 
@@ -39,8 +40,8 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _local_preconditioner(pc, op, slab, halo):
-    """The oracle's PC_apply_vec restricted to one slab, with the exchanges."""
+def _local_pieces(pc, op, slab):
+    """The oracle's local mathematics on one slab, as ShardedCycle's callables."""
     lay = pc.lay
     lo, hi = slab.first_cell, slab.first_cell + slab.ncell
     elo, ehi = slab.ext_cells
@@ -49,57 +50,52 @@ def _local_preconditioner(pc, op, slab, halo):
     d0, d1 = int(pc.dof_idx[subs[0]]), int(pc.dof_idx[subs[-1] + 1])
     Phi = pc.Phi[lo:hi][:, d0:d1].tocsr()
     nc = int(pc.dof_idx[-1])
-    two_level = pc.opts.use_2level
-    if not two_level:
+    t, n = torch.from_numpy, lambda v: v.numpy()
+
+    def level1(r):
+        y = np.zeros(r.shape[0])
+        for s in subs:
+            idx = pc.sub_idx[s] - lo
+            y[idx] += pc.lv1[s].solve(n(r)[idx])
+        return t(y)
+
+    def level2(c):
+        z = np.zeros(c.shape[0])
+        for vr in slab.vranks:
+            d, f = pc.lv2[vr]
+            z[d - d0] = O.chol_semidef_solve(f, n(c)[d - d0])
+        return t(z)
+
+    pieces = dict(residual=lambda x, y_ext: t(n(x) - A_loc @ n(y_ext)), level1=level1,
+                  restrict=lambda r: t(Phi.T @ n(r)), prolong=lambda z: t(Phi @ n(z)), level2=level2)
+    if pc.opts.use_2level:
+        def coarse_rhs(c):
+            cg = np.zeros(nc)
+            cg[d0:d1] = n(c)
+            return t(cg)
+
+        pieces.update(coarse_rhs=coarse_rhs,
+                      coarse_solve=lambda cg: t(O.chol_semidef_solve(pc.lv2c, n(cg))[d0:d1]))
+    else:
         off3 = np.concatenate([[0], np.cumsum([V.shape[1] for _, V in pc.V3])])
-        n3 = int(off3[-1])
 
-    def residual(x, y, first):
-        if first:
-            return x.copy()
-        y_ext = halo.extend(torch.from_numpy(y)).numpy()
-        return x - A_loc @ y_ext
+        def level3_rhs(c):
+            d3 = np.zeros(int(off3[-1]))
+            for vr in slab.vranks:
+                d, V = pc.V3[vr]
+                d3[off3[vr]:off3[vr + 1]] = V.T @ n(c)[d - d0]
+            return t(d3)
 
-    def apply(r_t):
-        x = r_t.numpy()
-        y = np.zeros_like(x)
-        for v, lvl in enumerate(pc.schedule()):
-            r = residual(x, y, v == 0)
-            if lvl == 1:
-                for s in subs:
-                    idx = pc.sub_idx[s] - lo
-                    y[idx] += pc.lv1[s].solve(r[idx])
-                continue
-            c = Phi.T @ r
-            z = np.zeros_like(c)
-            if lvl == 2:
-                for vr in slab.vranks:
-                    d, f = pc.lv2[vr]
-                    z[d - d0] = O.chol_semidef_solve(f, c[d - d0])
-            elif lvl == 3:
-                d3 = np.zeros(n3)
-                for vr in slab.vranks:
-                    d, V = pc.V3[vr]
-                    d3[off3[vr]:off3[vr + 1]] = V.T @ c[d - d0]
-                d3 = torch.from_numpy(d3)
-                dist.all_reduce(d3)
-                w = O.chol_semidef_solve(pc.lv3, d3.numpy())
-                for vr in slab.vranks:
-                    d, V = pc.V3[vr]
-                    z[d - d0] = V @ w[off3[vr]:off3[vr + 1]]
-            else:  # "2g": the global coarse right-hand side, summed over the processes
-                cg = np.zeros(nc)
-                cg[d0:d1] = c
-                cg = torch.from_numpy(cg)
-                dist.all_reduce(cg)
-                z = O.chol_semidef_solve(pc.lv2c, cg.numpy())[d0:d1]
-            y += Phi @ z
-        return torch.from_numpy(y)
+        def level3_back(w):
+            z = np.zeros(d1 - d0)
+            for vr in slab.vranks:
+                d, V = pc.V3[vr]
+                z[d - d0] = V @ n(w)[off3[vr]:off3[vr + 1]]
+            return t(z)
 
-    def matvec(p):
-        return torch.from_numpy(A_loc @ halo.extend(p).numpy())
-
-    return matvec, apply
+        pieces.update(level3_rhs=level3_rhs, level3_back=level3_back,
+                      level3_solve=lambda d3: t(O.chol_semidef_solve(pc.lv3, n(d3))))
+    return pieces, lambda p: t(A_loc @ n(p))
 
 
 def _worker(rank, world, port, name, out):
@@ -113,10 +109,15 @@ def _worker(rank, world, port, name, out):
         pc = O.Preconditioner(op, o)
         slab = shard.plan_slabs(prob["mesh"], o.vranks, world)[rank]
         halo = shard.Halo(slab)
-        matvec, apply = _local_preconditioner(pc, op, slab, halo)
+        pieces, stencil = _local_pieces(pc, op, slab)
+        cycle = shard.ShardedCycle(pc.schedule(), halo, **pieces)
+
+        def matvec(p):
+            return stencil(halo.extend(p))
+
         b = op.rhs()
         lo, hi = slab.first_cell, slab.first_cell + slab.ncell
-        x, its, hist, reason = shard.pcg(torch.from_numpy(b[lo:hi].copy()), matvec, apply, op.n,
+        x, its, hist, reason = shard.pcg(torch.from_numpy(b[lo:hi].copy()), matvec, cycle.apply, op.n,
                                          rtol=pc.opts.rtol, null_space=o.constant_null_space)
         xg = torch.zeros(op.n, dtype=torch.float64)
         xg[lo:hi] = x
@@ -124,7 +125,7 @@ def _worker(rank, world, port, name, out):
         if rank == 0:
             np.save(out, xg.numpy())
             with open(out + ".txt", "w") as f:
-                f.write(f"{its} {reason} {halo.exchanges}\n")
+                f.write(f"{its} {reason} {halo.exchanges} {cycle.sums}\n")
     finally:
         dist.destroy_process_group()
 
@@ -138,7 +139,7 @@ def test_sharded_solve_matches_single_process(name, tmp_path, monkeypatch):
         monkeypatch.setenv(v, "1")
     mp.spawn(_worker, args=(world, _free_port(), name, out), nprocs=world, join=True)
     x = np.load(out)
-    its, reason, exchanges = open(out + ".txt").read().split()
+    its, reason, exchanges, sums = open(out + ".txt").read().split()
     prob = make()
     ref = O.solve(prob, O.Options(**opts))
     assert reason == ref["reason"] == "converged_rtol"
@@ -149,8 +150,10 @@ def test_sharded_solve_matches_single_process(name, tmp_path, monkeypatch):
     assert np.linalg.norm(b - a) <= 1e-10 * np.linalg.norm(a)
     # one halo exchange per A p of the CG step and per residual of the cycle
     # after its first visit: its preconditioner applications and its A p
-    visits = len(ref["pc"].schedule())
-    assert int(exchanges) == int(its) * visits
+    sched = ref["pc"].schedule()
+    assert int(exchanges) == int(its) * len(sched)
+    # one coarse right-hand side summed per level-3 (or 2-level) visit of each application
+    assert int(sums) == int(its) * sum(1 for lvl in sched if lvl in (3, "2g"))
 
 
 def test_slab_plan():
