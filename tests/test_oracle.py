@@ -189,3 +189,19 @@ def test_fp32_stored_basis_keeps_the_channel_iterations(contrast, mesh, sd, its)
     r32 = O.solve(prob, O.Options(**opts, phi_fp32=True))
     assert r64["reason"] == r32["reason"] == "converged_rtol"
     assert r64["its"] == its and abs(r32["its"] - r64["its"]) <= 1
+
+
+def test_channel_subdomains_hold_near_zero_clusters():
+    # The mechanism behind the channel-field stalls of a loose eigen stopping
+    # test: every separate channel piece in a subdomain gives a near-zero local
+    # mode, so many subdomains hold clusters of eigenvalues far below lscale
+    # (max diag(A_N) / M), and the en_lv1 cut falls inside some of them.
+    prob = fields.layered(seed=2, M=30, N=20, P=15, smooth_layers=6)
+    o = O.Options(sd=(3, 2, 3), en_lv1=8, en_lv2=4)
+    op = O.Operator(prob)
+    pc = O.Preconditioner(op, o)
+    ev = np.stack(pc.eigvals_lv1)
+    lscale = np.array([(np.diag(op.neumann(s).toarray()) / op.mass_diag(s, o.eg_op)).max() for s in pc.lay.subs])
+    near_zero = (ev / lscale[:, None] < 1e-4).sum(axis=1)
+    assert (near_zero >= 2).sum() >= 5
+    assert near_zero.max() > 4  # a cluster straddling en_lv1 = 4
