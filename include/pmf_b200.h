@@ -51,8 +51,8 @@ typedef struct pmf_solver pmf_solver;
  * -pmf_eig_init 0|1 (set-up phase as batched kernels, off by default),
  * -pmf_eig_rel_floor f (0 <= f < 1; > 0: the local eigensolves stop when
  * ||r_j||_{M^-1} <= tol x max(|lambda_j|, f x lscale), an eigenvalue-relative
- * test, instead of tol x lscale with lscale = max diag(A_N)/M; for the FP64
- * form, off by default),
+ * test, instead of tol x lscale with lscale = max diag(A_N)/M; experimental,
+ * off by default),
  * -pmf_eig_profile 1 (per-phase timing, pmf_get_eig_phases), -pmf_pcg_graph
  * 0|1 (PCG iterations replayed as CUDA graphs, on by default), -pmf_autotune
  * 0|1 (launch-shape tuning, on by default; pmf_tune_report). */
