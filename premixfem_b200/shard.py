@@ -86,29 +86,35 @@ def plan_slabs(mesh, vranks, world):
 
 class Halo:
     """z-halo exchange: extend(v) returns [plane z0 - 1 | v | plane z1], the
-    ghost planes received from the neighbouring processes."""
+    ghost planes received from the neighbouring processes straight into a
+    buffer kept by the exchange (one copy of v per call; the returned tensor
+    is that buffer and is overwritten by the next call)."""
 
     def __init__(self, slab: Slab):
         self.s = slab
         self.exchanges = 0  # count of extend() calls that exchanged planes
+        self.buf = None
 
     def extend(self, v):
         s = self.s
-        lo = hi = None
+        lo = s.plane if s.below is not None else 0
+        n_ext = lo + s.ncell + (s.plane if s.above is not None else 0)
+        if self.buf is None or self.buf.dtype != v.dtype or self.buf.device != v.device:
+            self.buf = torch.empty(n_ext, dtype=v.dtype, device=v.device)
+        buf = self.buf
+        buf[lo:lo + s.ncell].copy_(v)
         reqs = []
         if s.below is not None:
-            lo = torch.empty(s.plane, dtype=v.dtype, device=v.device)
-            reqs.append(dist.isend(v[: s.plane].contiguous(), s.below))
-            reqs.append(dist.irecv(lo, s.below))
+            reqs.append(dist.isend(buf[lo:lo + s.plane], s.below))
+            reqs.append(dist.irecv(buf[:lo], s.below))
         if s.above is not None:
-            hi = torch.empty(s.plane, dtype=v.dtype, device=v.device)
-            reqs.append(dist.isend(v[-s.plane:].contiguous(), s.above))
-            reqs.append(dist.irecv(hi, s.above))
+            reqs.append(dist.isend(buf[lo + s.ncell - s.plane:lo + s.ncell], s.above))
+            reqs.append(dist.irecv(buf[lo + s.ncell:], s.above))
         for r in reqs:
             r.wait()
         if reqs:
             self.exchanges += 1
-        return torch.cat([t for t in (lo, v, hi) if t is not None])
+        return buf
 
 
 class ShardedCycle:
