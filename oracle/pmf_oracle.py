@@ -11,7 +11,9 @@ and it cannot be compiled here (it needs PETSc, SLEPc, MPI, MUMPS and
 SuperLU_dist, none of which are installed).  This oracle is therefore pinned
 only to mathematics: tests/test_oracle.py checks it against closed-form
 eigenvalues of constant-coefficient operators, exact Cholesky on chains, the
-textbook IC(0) definition and direct sparse solves.
+textbook IC(0) definition and direct sparse solves.  tests/golden/ holds its
+own results on the reference's test.c and cross-field problems: they pin the
+oracle against its own changes, not against the reference.
 
 Third-party arithmetic restated here (pinned versions from the reference's
 build notes, Compiling_optimized_PETSc_for_AMD_CPUs.md:76-83):
