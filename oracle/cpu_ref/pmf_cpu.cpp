@@ -715,16 +715,19 @@ extern "C" {
 //   mesh[3] M N P; dom[3] domain lengths; kx, ky, kz cell permeabilities (ky / kz may be
 //   null: isotropic); source per cell; dir_on[6] / dir_val[6] Dirichlet faces
 //   x- x+ y- y+ z- z+ and their pressures.
-//   iopt[19]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
+//   iopt[20]: sd[3], vranks[3], en_lv1, en_lv2, si_lv1, si_lv2, use_W_cycle, max_it,
 //             eig_max_it, eg_op, threads (<= 0: the OpenMP default), constant null
 //             space (-ksp_constant_null_space: every preconditioned residual loses its
-//             mean), no_shift_A_cc, use_2level, use_full_Cholesky_lv1
+//             mean), no_shift_A_cc, use_2level, use_full_Cholesky_lv1, nrhs
 //   dopt[6]:  rtol, eig_tol, eig_sigma (IC(0) shift of the eigensolver, x max A_ii/M_ii),
 //             eig_rel_floor (> 0: eigen residual test relative to max(|lambda|, floor x
 //             lscale)), eb_lv1, eb_lv2 (< 0: 1 / NIL, every subdomain keeps en_lv1 and
 //             every rank en_lv2 vectors)
-//   x_out[n]: solution; info[10]: its, setup_s, solve_s, threads, eig_its_mean,
-//             eig_its_max, eig_unconverged, ||r_final||, ||r_0||, level-3 size
+//   x_out[nrhs n]: solutions; info[12]: its, setup_s, solve_s (all right-hand
+//             sides), threads, eig_its_mean, eig_its_max, eig_unconverged,
+//             ||r_final||, ||r_0|| (its, ||r|| of the first right-hand side), level-3
+//             size, its summed and the largest over the right-hand sides
+//   source[nrhs n]: nrhs = iopt[19] right-hand sides solved after one set-up
 // Returns 0, -1 for invalid arguments, -2 when a subdomain block of
 // -use_full_Cholesky_lv1 is not positive definite.
 int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const double* ky, const double* kz,
@@ -737,11 +740,12 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   const int wcycle = iopt[10], max_it = iopt[11], eig_max_it = iopt[12], eg_op = iopt[13], threads = iopt[14];
   const bool null_space = iopt[15] != 0, no_shift = iopt[16] != 0, two_level = iopt[17] != 0,
              full_chol = iopt[18] != 0;
+  const int nrhs = iopt[19];
   const double rtol = dopt[0], eig_tol = dopt[1], eig_sigma = dopt[2], eig_rel_floor = dopt[3];
   const double eb1 = dopt[4] < 0.0 ? 1.0 / NIL : dopt[4], eb2 = dopt[5] < 0.0 ? 1.0 / NIL : dopt[5];
   for (int i = 0; i < 3; ++i)
     if (mesh[i] < 1 || sd[i] < 1 || vr[i] < 1 || mesh[i] < vr[i] * sd[i]) return -1;
-  if (k < 1 || k > 64 || en2_in < 1 || eg_op < 0 || eg_op > 2) return -1;
+  if (k < 1 || k > 64 || en2_in < 1 || eg_op < 0 || eg_op > 2 || nrhs < 1) return -1;
   if (threads > 0) omp_set_num_threads(threads);
 
   const auto t0 = clk::now();
@@ -1126,13 +1130,9 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     }
   };
 
-  // ---- PETSc KSPSolve_CG, unpreconditioned norm, zero initial guess
+  // ---- PETSc KSPSolve_CG, unpreconditioned norm, zero initial guess, for each
+  // right-hand side after the one set-up
   Vec r(n), z(n), pp(n), w(n);
-#pragma omp parallel for schedule(static)
-  for (long long i = 0; i < n; ++i) {
-    r[i] = source[i] + p.bval[i];
-    x_out[i] = 0.0;
-  }
   auto dot = [&](const double* a, const double* c) {
     double s = 0.0;
 #pragma omp parallel for reduction(+ : s) schedule(static)
@@ -1149,8 +1149,14 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < n; ++i) v[i] += s;
   };
-  double dp = std::sqrt(dot(r.data(), r.data()));
-  const double r0 = dp;
+  auto cg = [&](const double* src, double* x_out, double& dp, double& r0) {
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < n; ++i) {
+    r[i] = src[i] + p.bval[i];
+    x_out[i] = 0.0;
+  }
+  dp = std::sqrt(dot(r.data(), r.data()));
+  r0 = dp;
   const double ttol = std::max(rtol * dp, 1e-50);
   int its = 0;
   if (dp > ttol) {
@@ -1185,6 +1191,19 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
       beta = dot(z.data(), r.data());
     }
   }
+  return its;
+  };
+  double dp = 0.0, r0 = 0.0;
+  int its = 0, its_sum = 0, its_max = 0;
+  for (int q = nrhs - 1; q >= 0; --q) {  // the first right-hand side last: info[] reports it
+    double dq, r0q;
+    const int iq = cg(source + (size_t)q * n, x_out + (size_t)q * n, dq, r0q);
+    its_sum += iq;
+    its_max = std::max(its_max, iq);
+    its = iq;
+    dp = dq;
+    r0 = r0q;
+  }
   const auto t2 = clk::now();
   if (info) {
     double eit = 0.0;
@@ -1204,6 +1223,8 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     info[7] = dp;
     info[8] = r0;
     info[9] = two_level ? 0 : n3_kept;
+    info[10] = its_sum;
+    info[11] = its_max;
   }
   return 0;
 }
