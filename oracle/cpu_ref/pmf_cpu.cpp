@@ -82,6 +82,7 @@ void chol_semidef(Vec& A, int n, std::vector<char>& null, double rel_tol = 1e-14
     }
     const double l = std::sqrt(d);
     rj[j] = l;
+#pragma omp parallel for schedule(static) if (n - j > 256)
     for (int i = j + 1; i < n; ++i) {
       double* ri = &A[(size_t)i * n];
       double v = ri[j];
@@ -205,6 +206,93 @@ void sym_eig(Vec A, int n, Vec& w, Vec& Q) {
     for (int i = 0; i < n; ++i) Q2[(size_t)i * n + j] = Q[(size_t)i * n + ord[j]];
   }
   Q.swap(Q2);
+}
+
+// The k smallest eigenpairs of a symmetric positive semidefinite A (n x n, row-major)
+// by inverse subspace iteration: block p = min(n, k + 4), Y = (A + s I)^-1 X with a
+// Cholesky factor (s = 1e-10 max diag, so that null directions stay solvable), an
+// orthonormal basis of Y, Rayleigh-Ritz on it, until the k wanted residuals
+// ||A v - t v|| fall below 1e-12 max diag.  w: k ascending values; V: n x k,
+// eigenvector j in column j (V[i * k + j]).
+void smallest_eig(const Vec& A, int n, int k, Vec& w, Vec& V) {
+  const int p = std::min(n, k + 4);
+  double dmax = 0.0;
+  for (int i = 0; i < n; ++i) dmax = std::max(dmax, A[(size_t)i * n + i]);
+  Vec L = A;
+  for (int i = 0; i < n; ++i) L[(size_t)i * n + i] += 1e-10 * dmax;
+  std::vector<char> nl;
+  chol_semidef(L, n, nl);
+  Vec X((size_t)n * p), Y((size_t)n * p), AY((size_t)n * p), th, Z;
+  unsigned long long st = 0x2545F4914F6CDD1Dull;
+  for (auto& v : X) {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    v = (double)(st >> 11) / 9007199254740992.0 - 0.5;
+  }
+  for (int it = 0; it < 300; ++it) {
+#pragma omp parallel for schedule(static) if (n > 512)
+    for (int c = 0; c < p; ++c) {
+      Vec col(n);
+      for (int i = 0; i < n; ++i) col[i] = X[(size_t)i * p + c];
+      chol_solve(L, nl, n, col.data());
+      for (int i = 0; i < n; ++i) Y[(size_t)i * p + c] = col[i];
+    }
+    for (int pass = 0; pass < 2; ++pass)  // modified Gram-Schmidt, twice
+      for (int c = 0; c < p; ++c) {
+        for (int b = 0; b < c; ++b) {
+          double d = 0.0;
+          for (int i = 0; i < n; ++i) d += Y[(size_t)i * p + b] * Y[(size_t)i * p + c];
+          for (int i = 0; i < n; ++i) Y[(size_t)i * p + c] -= d * Y[(size_t)i * p + b];
+        }
+        double nn = 0.0;
+        for (int i = 0; i < n; ++i) nn += Y[(size_t)i * p + c] * Y[(size_t)i * p + c];
+        nn = nn > 0.0 ? 1.0 / std::sqrt(nn) : 0.0;
+        for (int i = 0; i < n; ++i) Y[(size_t)i * p + c] *= nn;
+      }
+#pragma omp parallel for schedule(static) if (n > 512)
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < p; ++c) {
+        double v = 0.0;
+        for (int q = 0; q < n; ++q) v += A[(size_t)i * n + q] * Y[(size_t)q * p + c];
+        AY[(size_t)i * p + c] = v;
+      }
+    Vec H((size_t)p * p, 0.0);
+    for (int a = 0; a < p; ++a)
+      for (int b = 0; b < p; ++b) {
+        double v = 0.0;
+        for (int i = 0; i < n; ++i) v += Y[(size_t)i * p + a] * AY[(size_t)i * p + b];
+        H[(size_t)a * p + b] = v;
+      }
+    for (int a = 0; a < p; ++a)
+      for (int b = 0; b < a; ++b) H[(size_t)a * p + b] = H[(size_t)b * p + a] = 0.5 * (H[(size_t)a * p + b] + H[(size_t)b * p + a]);
+    sym_eig(H, p, th, Z);
+    double worst = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double xr[64], ar[64];
+      for (int j = 0; j < p; ++j) {
+        double xv = 0.0, av = 0.0;
+        for (int b = 0; b < p; ++b) {
+          xv += Y[(size_t)i * p + b] * Z[(size_t)b * p + j];
+          av += AY[(size_t)i * p + b] * Z[(size_t)b * p + j];
+        }
+        xr[j] = xv;
+        ar[j] = av;
+      }
+      for (int j = 0; j < p; ++j) {
+        X[(size_t)i * p + j] = xr[j];
+        AY[(size_t)i * p + j] = ar[j] - th[j] * xr[j];  // residual, reusing AY
+      }
+    }
+    for (int j = 0; j < k; ++j) {
+      double r2 = 0.0;
+      for (int i = 0; i < n; ++i) r2 += AY[(size_t)i * p + j] * AY[(size_t)i * p + j];
+      worst = std::max(worst, std::sqrt(r2));
+    }
+    if (worst <= 1e-12 * dmax) break;
+  }
+  w.assign(th.begin(), th.begin() + k);
+  V.assign((size_t)n * k, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) V[(size_t)i * k + j] = X[(size_t)i * p + j];
 }
 
 // ---- operator (PC_create_A, :1757-1824) -------------------------------------------------
@@ -897,7 +985,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
   std::vector<Vec> A2L(nrank), V3(nrank);
   std::vector<std::vector<char>> A2null(nrank);
   std::vector<int> num3(nrank, 0);
-#pragma omp parallel for schedule(dynamic)
+#pragma omp parallel for schedule(dynamic) if (nrank > 1)
   for (int r = 0; r < (two_level ? 0 : nrank); ++r) {
     Vec A((size_t)nr * nr, 0.0), AN((size_t)nr * nr, 0.0);
     for (int a = 0; a < spr; ++a) {
@@ -935,8 +1023,14 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     Vec ANc((size_t)na * na), w, V;
     for (int i = 0; i < na; ++i)
       for (int j = 0; j < na; ++j) ANc[(size_t)i * na + j] = AN[(size_t)act[i] * nr + act[j]];
-    sym_eig(ANc, na, w, V);
     const int k3 = std::min(en2_in, na);
+    int ldv = na;
+    if (na > 256 && k3 + 4 <= 64) {  // the k3 smallest only: inverse subspace iteration
+      smallest_eig(ANc, na, k3, w, V);
+      ldv = k3;
+    } else {
+      sym_eig(ANc, na, w, V);
+    }
     int num = k3;
     for (int j = 0; j < k3; ++j)
       if (w[j] >= eb2) {
@@ -946,7 +1040,7 @@ int pmf_cpu_solve(const int* mesh, const double* dom, const double* kx, const do
     num3[r] = num;
     V3[r].assign((size_t)nr * en2, 0.0);
     for (int i = 0; i < na; ++i)
-      for (int j = 0; j < num; ++j) V3[r][(size_t)act[i] * en2 + j] = V[(size_t)i * na + j];
+      for (int j = 0; j < num; ++j) V3[r][(size_t)act[i] * en2 + j] = V[(size_t)i * ldv + j];
   }
 
   // A3 = V^T (Phi^T A Phi) V + NIL I, assembled block by block (each thread owns the

@@ -103,6 +103,19 @@ def test_adaptive_eigenvector_counts_match_oracle():
     assert np.linalg.norm(got["x"] - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
 
 
+def test_large_coarse_level_uses_the_smallest_eigenpairs_only():
+    # 256 subdomains of 4 x 4 x 8 cells, k = 4: 1 024 coarse unknowns on one rank,
+    # so the restatement's level-3 HEP takes the inverse subspace iteration for its
+    # 4 smallest eigenpairs instead of a full dense eigendecomposition
+    prob = fields.unit_cube_grf(32, seed=6)
+    opts = dict(sd=(8, 8, 4), en_lv1=4, en_lv2=4)
+    ref = O.solve(prob, O.Options(**opts))
+    got = CR.solve(prob, **opts)
+    assert got["n3"] == 4
+    assert abs(got["its"] - ref["its"]) <= 1, (got["its"], ref["its"])
+    assert np.linalg.norm(got["x"] - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
+
+
 def test_rejects_too_many_eigenvectors():
     prob = fields.random_box((4, 4, 4), seed=1)
     with pytest.raises(ValueError):
