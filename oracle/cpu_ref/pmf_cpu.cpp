@@ -16,7 +16,9 @@
 // with SVQB orthonormalisation (Stathopoulos & Wu 2002) preconditioned by IC(0)
 // of A^N + sigma M; the level-3 HEP and the Rayleigh-Ritz problems by
 // Householder tridiagonalisation and the implicit symmetric QR step with a
-// Wilkinson shift (Golub & Van Loan, Matrix Computations, Alg. 8.3.1-8.3.3);
+// Wilkinson shift (Golub & Van Loan, Matrix Computations, Alg. 8.3.1-8.3.3),
+// a level-3 HEP of more than 256 coarse unknowns by inverse subspace iteration
+// for its smallest eigenpairs (Alg. 8.2.3 with a Rayleigh-Ritz step);
 // MUMPS / SuperLU by a dense Cholesky factorisation that drops null pivots;
 // CHOLMOD (-use_full_Cholesky_lv1) by a band Cholesky of each subdomain block
 // (Golub & Van Loan, Alg. 4.3.5).  Adaptive eigenvector counts (-eb_lv1,
