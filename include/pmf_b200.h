@@ -10,8 +10,8 @@
  * selects whether array arguments are device (CUDA) or host pointers.
  *
  * This ABI is what a foreign-function binding of the reference's solve path
- * would call (see INTEGRATION.md for the ctypes binding); the PETSc-style
- * drop-in header PreMixFEM_3D.h is implemented on top of it.  Mapping to the
+ * would call (a ctypes binding, for instance); the PETSc-style drop-in header
+ * PreMixFEM_3D.h is implemented on top of it.  Mapping to the
  * reference interface (src/PreMixFEM_3D.h of Laphet/PreMixFEM):
  *   pmf_create        <- PC_init            (src/PreMixFEM_3D.h:47, src/PreMixFEM_3D.c:1650-1741)
  *   pmf_set_kappa     <- caller fills PCCtx.kappa[3] (src/PreMixFEM_3D.h:34; src/Expe_scal.c:11-42)
@@ -68,7 +68,8 @@ int pmf_setup(pmf_solver* s);
 int pmf_rhs(pmf_solver* s, const double* source, double* rhs, int on_device);
 int pmf_apply_A(pmf_solver* s, const double* x, double* y, int on_device);
 int pmf_pc_apply(pmf_solver* s, const double* x, double* y, int on_device);
-/* reason: 1 converged, 2 max_it, 3 indefinite, 4 nan/inf */
+/* reason: 1 converged (residual test), 2 max_it, 3 indefinite, 4 nan/inf, 5 converged because the
+ * preconditioned residual's dot z.r is exactly zero (PETSc's KSP_CONVERGED_ATOL for KSPCG) */
 int pmf_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason);
 
 /* info[0..11] = ncell_lo32, nsub, nrank, subdomains_per_rank, kmax, nr, en_lv2, n3,
@@ -139,8 +140,9 @@ int pmf_get_learned_stats(pmf_solver* s, long long stats[4], double* net_ms);
  *   - the first call on each device resolves and zeroes the scratch (with
  *     cudaGetSymbolAddress and cudaMemset, synchronising the device): make that
  *     first call before any stream capture begins;
- *   - the scratch's ticket counter must be zero when a call starts; set-up
- *     zeroes it and every completed call leaves it at zero;
+ *   - the scratch's ticket counter must be zero when a call starts: it is
+ *     zero when the library's module loads, the first call on each device
+ *     zeroes it again, and every completed call leaves it at zero;
  *   - all calls on one device share the scratch: overlapping calls (two
  *     streams, two threads) race and return wrong results; serialise them.
  */

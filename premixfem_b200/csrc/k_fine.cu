@@ -181,7 +181,8 @@ void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, doub
 }
 
 // beta = z.r (the dot is written per block by the preconditioner's last kernel
-// or by k_dot); a zero beta ends the loop (KSP_CONVERGED_ATOL).
+// or by k_dot); a zero beta ends the loop with done = 5 (KSP_CONVERGED_ATOL,
+// as KSPSolve_CG reports it).
 __global__ void k_pcg_beta_fin(const double* part, int nb, PcgState* s) {
   __shared__ double red[32];
   if (s->done) return;
@@ -190,7 +191,7 @@ __global__ void k_pcg_beta_fin(const double* part, int nb, PcgState* s) {
     s->beta = v;
     if (v == 0.0) {
       s->its += 1;
-      s->done = 1;
+      s->done = 5;
     }
   }
 }

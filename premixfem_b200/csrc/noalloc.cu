@@ -24,8 +24,9 @@
 //     cudaGetSymbolAddress (which may load this module and reserve its static
 //     memory) and zeroes the ticket counter; make that first call, on every
 //     device used, before any stream capture begins;
-//   * the ticket counter must be zero when a call starts: it is zero after
-//     set-up and every completed call returns it to zero.  The partial sums
+//   * the ticket counter must be zero when a call starts: it is zero when
+//     the module loads, the first call on each device zeroes it again, and
+//     every completed call returns it to zero.  The partial sums
 //     need no initial value (each block writes its own slot first);
 //   * calls on the same device share the scratch, so two calls that overlap
 //     in time (different streams, different host threads, or the same solver

@@ -771,14 +771,17 @@ PetscErrorCode KSPSolve(KSP ksp, Vec b, Vec x) {
     ctx->t_stages[STAGE_AV] += s->last_solve_ms * 1e-3 + (s->t_stages[pmf::ST_AV] - av0);
     ksp->its = its;
     ksp->rnorm = rnorm;
+    // pmf::Solver::solve stop codes -> KSPConvergedReason, as cg_host sets them
     if (code == 1)
       ksp->reason = rnorm <= ksp->atol ? KSP_CONVERGED_ATOL : KSP_CONVERGED_RTOL;
-    else if (code == 2)
-      ksp->reason = KSP_DIVERGED_ITS;
+    else if (code == 5)
+      ksp->reason = KSP_CONVERGED_ATOL;  // z.r = 0
     else if (code == 3)
       ksp->reason = KSP_DIVERGED_INDEFINITE_MAT;
-    else
+    else if (code == 4)
       ksp->reason = KSP_DIVERGED_NANORINF;
+    else
+      ksp->reason = KSP_DIVERGED_ITS;  // 2, or a loop stopped by the host guard
   } else {
     PetscCall(cg_host(ksp, b, x));
   }

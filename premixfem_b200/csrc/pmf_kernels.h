@@ -15,7 +15,9 @@ inline void note_launch() { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAX
 // iteration needs no host round trip (PETSc KSPSolve_CG recurrences).
 struct PcgState {
   double dp, ttol, beta, betaold, dpi, dpiold, alpha, rnorm0;
-  int its, max_it, first, done;  // done: 0 running, 1 converged, 2 max_it, 3 indefinite, 4 nan
+  // done: 0 running, 1 converged (residual test), 2 max_it, 3 indefinite, 4 nan/inf,
+  // 5 converged because z.r = 0 (KSP_CONVERGED_ATOL)
+  int its, max_it, first, done;
 };
 
 constexpr int kCellThreads = 256;

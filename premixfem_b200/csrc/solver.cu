@@ -394,46 +394,81 @@ int Solver::build_partition() {
   return 0;
 }
 
-void Solver::alloc_fine() {
+// cudaMalloc with its return code checked: on failure *p is null, err names
+// the array and the PETSc-style code 76 comes back.
+int Solver::dalloc(void** p, size_t bytes, const char* what) {
+  *p = nullptr;
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) return 0;
+  *p = nullptr;
+  cudaGetLastError();  // clear the sticky-free allocation error
+  err = std::string("cudaMalloc ") + what + " (" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e);
+  return 76;  // PETSC_ERR_LIB
+}
+
+// The fine-grid arrays of the operator, the preconditioner and the CG loop.
+// All or nothing: when one allocation fails, every array allocated here is
+// freed and reset to null (so a later call retries from scratch) and the
+// error is returned before any kernel can write through a null pointer.
+int Solver::alloc_fine() {
   const size_t n = (size_t)g.ncell;
-  cudaMalloc(&tx, n * 8);
-  cudaMalloc(&ty, n * 8);
-  cudaMalloc(&tz, n * 8);
-  cudaMalloc(&diag, n * 8);
-  cudaMalloc(&db, n * 8);
-  cudaMalloc(&bval, n * 8);
-  cudaMalloc(&inv64, n * 8);
-  cudaMalloc(&vb, n * 8);
-  cudaMalloc(&vx, n * 8);
-  cudaMalloc(&r, n * 8);
-  cudaMalloc(&z, n * 8);
-  cudaMalloc(&p0, n * 8);
-  cudaMalloc(&p1, n * 8);
-  cudaMalloc(&w, n * 8);
   const size_t pb = opt.precision == 1 ? 4 : 8;
-  cudaMalloc(&y0, n * pb);
-  cudaMalloc(&y1, n * pb);
-  cudaMalloc(&phi, n * kmax * pb);
-  if (opt.precision == 1) {
-    cudaMalloc(&tx32, n * 4);
-    cudaMalloc(&ty32, n * 4);
-    cudaMalloc(&tz32, n * 4);
-    cudaMalloc(&diag32, n * 4);
-    cudaMalloc(&inv32, n * 4);
-  }
   const int nparts = std::max(cell_blocks(g.ncell), nsub) + 64;
-  cudaMalloc(&part, (size_t)(nparts + cell_blocks(g.ncell)) * 8);
+  struct A {
+    void** p;
+    size_t bytes;
+    const char* what;
+  };
+  std::vector<A> list = {{(void**)&tx, n * 8, "tx"},      {(void**)&ty, n * 8, "ty"},
+                         {(void**)&tz, n * 8, "tz"},      {(void**)&diag, n * 8, "diag"},
+                         {(void**)&db, n * 8, "db"},      {(void**)&bval, n * 8, "bval"},
+                         {(void**)&inv64, n * 8, "inv64"}, {(void**)&vb, n * 8, "vb"},
+                         {(void**)&vx, n * 8, "vx"},      {(void**)&r, n * 8, "r"},
+                         {(void**)&z, n * 8, "z"},        {(void**)&p0, n * 8, "p0"},
+                         {(void**)&p1, n * 8, "p1"},      {(void**)&w, n * 8, "w"},
+                         {(void**)&y0, n * pb, "y0"},     {(void**)&y1, n * pb, "y1"},
+                         {(void**)&phi, n * kmax * pb, "phi"},
+                         {(void**)&part, (size_t)(nparts + cell_blocks(g.ncell)) * 8, "part"},
+                         {(void**)&state, sizeof(PcgState), "state"}};
+  if (opt.precision == 1) {
+    list.push_back({(void**)&tx32, n * 4, "tx32"});
+    list.push_back({(void**)&ty32, n * 4, "ty32"});
+    list.push_back({(void**)&tz32, n * 4, "tz32"});
+    list.push_back({(void**)&diag32, n * 4, "diag32"});
+    list.push_back({(void**)&inv32, n * 4, "inv32"});
+  }
+  for (size_t i = 0; i < list.size(); ++i) {
+    if (int e = dalloc(list[i].p, list[i].bytes, list[i].what)) {
+      for (size_t j = 0; j < i; ++j) {
+        cudaFree(*list[j].p);
+        *list[j].p = nullptr;
+      }
+      zpart = nullptr;
+      return e;
+    }
+  }
   zpart = part + nparts;
-  cudaMalloc(&state, sizeof(PcgState));
+  return 0;
 }
 
 int Solver::set_kappa(const double* k0, const double* k1, const double* k2, bool on_device) {
   if (int e = build_partition()) return e;
   const size_t n = (size_t)g.ncell;
-  if (!kx) {
-    if (int e = check(cudaMalloc(&kx, n * 8), "cudaMalloc kappa")) return e;
-    cudaMalloc(&ky, n * 8);
-    cudaMalloc(&kz, n * 8);
+  if (!kx || !ky || !kz) {
+    for (double** p : {&kx, &ky, &kz}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    int e = dalloc((void**)&kx, n * 8, "kappa x");
+    if (!e) e = dalloc((void**)&ky, n * 8, "kappa y");
+    if (!e) e = dalloc((void**)&kz, n * 8, "kappa z");
+    if (e) {
+      for (double** p : {&kx, &ky, &kz}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+      }
+      return e;
+    }
   }
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   cudaMemcpyAsync(kx, k0, n * 8, kind, st);
@@ -497,7 +532,8 @@ int Solver::assemble() {
     err = "kappa not set";
     return 73;
   }
-  if (!tx) alloc_fine();
+  if (!tx)
+    if (int e = alloc_fine()) return e;
   assemble_launch();
   return check(cudaStreamSynchronize(st), "assemble");
 }
@@ -517,11 +553,15 @@ int Solver::alloc_eb(int m, bool mixed) {
   if (int e = check(cudaMalloc(&eb.gpart, ns * eb.nchunk * 2 * 32 * 32 * sizeof(double)), "cudaMalloc Grams"))
     return e;
   if (int e = check(cudaMalloc(&eb.rpart, ns * eb.nchunk * 10 * sizeof(double)), "cudaMalloc residuals")) return e;
-  if (!eb.nactive) cudaMalloc(&eb.nactive, 4 * sizeof(int));
-  if (!eb.colcells) cudaMalloc(&eb.colcells, sizeof(unsigned long long));
+  if (!eb.nactive)
+    if (int e = dalloc((void**)&eb.nactive, 4 * sizeof(int), "eigensolver counters")) return e;
+  if (!eb.colcells)
+    if (int e = dalloc((void**)&eb.colcells, sizeof(unsigned long long), "eigensolver traffic counter")) return e;
   if (eb.alist) cudaFree(eb.alist);
-  cudaMalloc(&eb.alist, ns * sizeof(int));
-  if (!eb.h_nactive) cudaMallocHost(&eb.h_nactive, 4 * sizeof(int));
+  if (int e = dalloc((void**)&eb.alist, ns * sizeof(int), "eigensolver active list")) return e;
+  if (!eb.h_nactive)
+    if (int e = check(cudaMallocHost(&eb.h_nactive, 4 * sizeof(int)), "cudaMallocHost eigensolver counters"))
+      return e;
   return 0;
 }
 
@@ -582,10 +622,10 @@ int Solver::run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1) {
     if (int e = check(cudaMalloc(&net_y, (size_t)nsub * NET_VOX * NET_COUT * sizeof(float)), "cudaMalloc net output"))
       return e;
     if (int e = check(cudaMalloc(&net_x, (size_t)chunk * NET_VOX * NET_CIN * 2), "cudaMalloc net input")) return e;
-    cudaMalloc(&d_fail_list, sizeof(int) * nsub);
-    cudaMalloc(&d_fail_count, sizeof(int));
-    cudaMalloc(&d_iters_learned, sizeof(int) * nsub);
-    cudaMalloc(&d_status_learned, sizeof(int) * nsub);
+    if (int e = dalloc((void**)&d_fail_list, sizeof(int) * nsub, "fallback list")) return e;
+    if (int e = dalloc((void**)&d_fail_count, sizeof(int), "fallback count")) return e;
+    if (int e = dalloc((void**)&d_iters_learned, sizeof(int) * nsub, "learned iterations")) return e;
+    if (int e = dalloc((void**)&d_status_learned, sizeof(int) * nsub, "learned status")) return e;
   }
   int dmask = 0;
   for (int f = 0; f < 6; ++f)
@@ -640,11 +680,22 @@ int Solver::setup() {
     return 73;  // PETSC_ERR_ARG_WRONGSTATE
   }
   if (opt.autotune >= 0) tune_set_enabled(opt.autotune == 1);
-  cudaEvent_t e[8];
-  for (auto& x : e) cudaEventCreate(&x);
+  // stage events, destroyed on every return path
+  struct StageEvents {
+    cudaEvent_t ev[8];
+    StageEvents() {
+      for (auto& x : ev) cudaEventCreate(&x);
+    }
+    ~StageEvents() {
+      for (auto& x : ev) cudaEventDestroy(x);
+    }
+  } evs;
+  cudaEvent_t* e = evs.ev;
   const bool mixed = opt.precision == 1;
-  if (!tx) alloc_fine();
-  if (!d_subs) cudaMalloc(&d_subs, sizeof(SubInfo) * nsub);
+  if (!tx)
+    if (int er = alloc_fine()) return er;
+  if (!d_subs)
+    if (int er = dalloc((void**)&d_subs, sizeof(SubInfo) * nsub, "subdomain table")) return er;
   cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
   cudaEventRecord(e[0], st);
   // operator (PC_create_A) and level 1
@@ -652,7 +703,8 @@ int Solver::setup() {
   int dmask = 0;
   for (int f = 0; f < 6; ++f)
     if (dir_on_[f]) dmask |= 1 << f;
-  if (!d_flag) cudaMalloc(&d_flag, 4 * sizeof(int));
+  if (!d_flag)
+    if (int er = dalloc((void**)&d_flag, 4 * sizeof(int), "pivot flags")) return er;
   cudaMemsetAsync(d_flag, 0, 4 * sizeof(int), st);
   if (opt.use_full_Cholesky_lv1) {
     if (int er = setup_band_cholesky(mixed)) return er;
@@ -668,11 +720,15 @@ int Solver::setup() {
   }
   cudaEventRecord(e[1], st);
   // level-2 local eigenproblems
-  if (!d_eig1) {
-    cudaMalloc(&d_eig1, sizeof(double) * nsub * opt.en_lv1);
-    cudaMalloc(&d_ks, sizeof(int) * nsub);
-    cudaMalloc(&d_iters, sizeof(int) * nsub);
-    cudaMalloc(&d_status, sizeof(int) * nsub);
+  if (!d_eig1 || !d_ks || !d_iters || !d_status) {
+    for (void* q : {(void*)d_eig1, (void*)d_ks, (void*)d_iters, (void*)d_status})
+      if (q) cudaFree(q);
+    d_eig1 = nullptr;
+    d_ks = d_iters = d_status = nullptr;
+    if (int er = dalloc((void**)&d_eig1, sizeof(double) * nsub * opt.en_lv1, "local eigenvalues")) return er;
+    if (int er = dalloc((void**)&d_ks, sizeof(int) * nsub, "local eigen counts")) return er;
+    if (int er = dalloc((void**)&d_iters, sizeof(int) * nsub, "eigensolver iterations")) return er;
+    if (int er = dalloc((void**)&d_status, sizeof(int) * nsub, "eigensolver status")) return er;
   }
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -707,7 +763,8 @@ int Solver::setup() {
   la.xinit_k = 0;
   la.sub_list = nullptr;
   la.nlist = nullptr;
-  if (!d_queue) cudaMalloc(&d_queue, sizeof(int));
+  if (!d_queue)
+    if (int er = dalloc((void**)&d_queue, sizeof(int), "eigensolver queue")) return er;
   la.queue = d_queue;
   la.mode = 0;
   la.rel_floor = opt.eig_rel_floor;
@@ -722,7 +779,7 @@ int Solver::setup() {
   long long* d_prof = nullptr;
   const bool prof_eig = getenv("PMF_PROFILE_EIGEN") != nullptr;
   if (prof_eig) {
-    cudaMalloc(&d_prof, sizeof(long long) * 16 * eig_blocks);
+    if (int er = dalloc((void**)&d_prof, sizeof(long long) * 16 * eig_blocks, "eigensolver probe")) return er;
     cudaMemsetAsync(d_prof, 0, sizeof(long long) * 16 * eig_blocks, st);
     la.prof = d_prof;
   }
@@ -798,22 +855,43 @@ int Solver::setup() {
   for (int s = 0; s < nsub; ++s) subs[s].k = ks[s];
   cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
   // level-2 Galerkin (Phi^T A Phi) and per-rank inverses
-  if (!blk) {
-    cudaMalloc(&blk, sizeof(double) * nsub * 7 * kmax * kmax);
-    cudaMalloc(&gface, sizeof(double) * nsub * 6 * kmax * kmax);
-    cudaMalloc(&A2inv, sizeof(double) * nrank * nr * nr);
-    cudaMalloc(&AN, sizeof(double) * nrank * nr * nr);
-    cudaMalloc(&ANinv, sizeof(double) * nrank * nr * nr);
-    cudaMalloc(&V3, sizeof(double) * nrank * nr * en2);
-    cudaMalloc(&d_eig3, sizeof(double) * nrank * en2);
-    cudaMalloc(&d_l3it, sizeof(int) * nrank);
-    cudaMalloc(&A3inv, sizeof(double) * n3 * n3);
-    cudaMalloc(&c, sizeof(double) * nsub * kmax);
-    cudaMalloc(&dz, sizeof(double) * nsub * kmax);
-    cudaMalloc(&Zacc, sizeof(double) * nsub * kmax);
-    cudaMalloc(&d3, sizeof(double) * n3);
-    cudaMalloc(&w3, sizeof(double) * n3);
-    cudaMalloc(&d_rank_nb, sizeof(int) * nrank * 6);
+  if (!coarse_ok) {
+    // all or nothing, as alloc_fine
+    struct A {
+      void** p;
+      size_t bytes;
+      const char* what;
+    };
+    const A list[] = {{(void**)&blk, sizeof(double) * nsub * 7 * kmax * kmax, "coarse blocks"},
+                      {(void**)&gface, sizeof(double) * nsub * 6 * kmax * kmax, "coarse face blocks"},
+                      {(void**)&A2inv, sizeof(double) * nrank * nr * nr, "level-2 inverses"},
+                      {(void**)&AN, sizeof(double) * nrank * nr * nr, "rank-Neumann matrices"},
+                      {(void**)&ANinv, sizeof(double) * nrank * nr * nr, "rank-Neumann inverses"},
+                      {(void**)&V3, sizeof(double) * nrank * nr * en2, "level-3 eigenvectors"},
+                      {(void**)&d_eig3, sizeof(double) * nrank * en2, "level-3 eigenvalues"},
+                      {(void**)&d_l3it, sizeof(int) * nrank, "level-3 iterations"},
+                      {(void**)&A3inv, sizeof(double) * n3 * n3, "level-3 inverse"},
+                      {(void**)&c, sizeof(double) * nsub * kmax, "coarse residual"},
+                      {(void**)&dz, sizeof(double) * nsub * kmax, "coarse correction"},
+                      {(void**)&Zacc, sizeof(double) * nsub * kmax, "coarse accumulator"},
+                      {(void**)&d3, sizeof(double) * n3, "level-3 right-hand side"},
+                      {(void**)&w3, sizeof(double) * n3, "level-3 solution"},
+                      {(void**)&d_rank_nb, sizeof(int) * nrank * 6, "rank neighbours"}};
+    const int nl = (int)(sizeof(list) / sizeof(list[0]));
+    for (int i = 0; i < nl; ++i) {
+      if (*list[i].p) cudaFree(*list[i].p);
+      *list[i].p = nullptr;
+    }
+    for (int i = 0; i < nl; ++i) {
+      if (int er = dalloc(list[i].p, list[i].bytes, list[i].what)) {
+        for (int j = 0; j < i; ++j) {
+          cudaFree(*list[j].p);
+          *list[j].p = nullptr;
+        }
+        return er;
+      }
+    }
+    coarse_ok = true;
   }
   if (mixed)
     launch_galerkin<float>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const float*)phi, blk, gface, st);
@@ -833,7 +911,6 @@ int Solver::setup() {
     cudaEventElapsedTime(&tot, e[0], e[5]);
     t_stages[ST_SU] += tot * 1e-3;
     last_setup_ms = tot;
-    for (auto& x : e) cudaEventDestroy(x);
     // launch shapes of the preconditioner kernels (first set-up of a shape only)
     if (mixed)
       tune_pc<float>();
@@ -902,7 +979,8 @@ int Solver::setup() {
     rnb[rr * 6 + 4] = at(rx, ry, rz - 1);
     rnb[rr * 6 + 5] = at(rx, ry, rz + 1);
   }
-  if (!d_ks3) cudaMalloc(&d_ks3, sizeof(int) * nrank);
+  if (!d_ks3)
+    if (int er = dalloc((void**)&d_ks3, sizeof(int) * nrank, "level-3 counts")) return er;
   cudaMemcpyAsync(d_ks3, ks3.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_rank_nb, rnb.data(), sizeof(int) * nrank * 6, cudaMemcpyHostToDevice, st);
   { note_launch(); k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3); }
@@ -949,7 +1027,8 @@ int Solver::setup_band_cholesky(bool mixed) {
   }
   if (mixed && !band32)
     if (int er = check(cudaMalloc(&band32, sizeof(float) * len), "cudaMalloc Cholesky factors (FP32)")) return er;
-  if (!d_boff) cudaMalloc(&d_boff, sizeof(long long) * nsub);
+  if (!d_boff)
+    if (int er = dalloc((void**)&d_boff, sizeof(long long) * nsub, "Cholesky offsets")) return er;
   cudaMemcpyAsync(d_boff, off.data(), sizeof(long long) * nsub, cudaMemcpyHostToDevice, st);
   launch_band_chol_factor(g, d_subs, nsub, mb, tx, ty, tz, diag, d_boff, band64, d_flag, st);
   if (mixed) launch_to_f32(band64, band32, len, st);
@@ -1242,7 +1321,9 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   last_its = h_state->its;
   if (its) *its = h_state->its;
   if (rnorm) *rnorm = h_state->dp;
-  if (reason) *reason = h_state->done;
+  // the host guard stopped the loop before the device set a stop code: the
+  // iteration budget is spent (KSP_DIVERGED_ITS)
+  if (reason) *reason = h_state->done ? h_state->done : 2;
   return e;
 }
 

@@ -122,6 +122,7 @@ class Solver {
          *A3inv = nullptr, *d_eig1 = nullptr, *d_eig3 = nullptr;
   int *d_ks = nullptr, *d_iters = nullptr, *d_status = nullptr, *d_l3it = nullptr, *d_flag = nullptr;
   int* d_rank_nb = nullptr;
+  bool coarse_ok = false;  // the level-2/3 arrays above are allocated
   void* eig_work = nullptr;
   size_t eig_work_bytes = 0;
   double *c = nullptr, *dz = nullptr, *Zacc = nullptr, *d3 = nullptr, *w3 = nullptr;
@@ -134,8 +135,9 @@ class Solver {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   int check(cudaError_t e, const char* what);
+  int dalloc(void** p, size_t bytes, const char* what);
   int build_partition();
-  void alloc_fine();
+  int alloc_fine();
   void assemble_launch();
   template <typename T>
   void apply_impl(const double* x, double* out, double* partial, const int* done);

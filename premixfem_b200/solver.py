@@ -20,7 +20,8 @@ from . import _native
 
 FACE_IDS = {"x-": 0, "x+": 1, "y-": 2, "y+": 3, "z-": 4, "z+": 5}
 STAGE_NAMES = ("su_lv1", "su_lv2_1", "su_lv2_2", "su_lv3_1", "su_lv3_2", "av_lv1", "av_lv2", "av_lv3", "su", "av")
-REASONS = {1: "converged", 2: "diverged_its", 3: "diverged_indefinite", 4: "diverged_nanorinf"}
+REASONS = {1: "converged", 2: "diverged_its", 3: "diverged_indefinite", 4: "diverged_nanorinf",
+           5: "converged_atol"}
 
 
 def options_string(opts=None, **kw):
