@@ -12,11 +12,24 @@ One step = one full setup (operator assembly, level-1 IC(0), batched local
 eigensolves, Galerkin level 2, level-3 eigensolve + Galerkin, coarse
 inverses) plus one PCG solve to 1e-8 on the workload's seeded synthetic field.
 
-  value   mixed/learned form, inputs resident in HBM (kappa and rhs on the device)
-  e2e     mixed form through the C ABI with host buffers (host->device copy
-          of kappa and source, device->host copy of the solution, inside the
-          timed region)
-  plain   plain FP64 form, same workload, for the speed-up the metric names
+Forms measured on the headline workload (fracture256):
+  value        mixed form with the learned start, inputs resident in HBM
+  mixed_nonet  the mixed form with random eigensolver starts (the network's own gain)
+  plain_fp64   plain FP64 form (random starts), the comparator the metric names
+  e2e          the mixed/learned form through the C ABI with host buffers
+               (host->device copies of kappa and source, device->host copies
+               of the right-hand side and solution, inside the timed region)
+Accuracy: every form's solution against an FP64 reference solution (the
+device FP64 form solved to relative residual 1e-13), true residuals, the
+local eigensolvers' stop codes; in the CPU-baseline leg, a seeded sample of
+64 subdomains' local eigenvalues against the oracle's exact local GHEPs.
+Roofline: the kernels of one PCG iteration timed by class with CUDA events
+on the solver stream (pmf_profile_iteration); the dominant class is the
+`roofline` object.
+
+Secondary workloads (--extra, default "layered,large512") run after the
+headline with their own 3 warm-up + 3 timed steps per form and are reported
+under "workloads" in the same line.
 
 Multi-GPU (torchrun, N ranks): every rank solves its own seeded replica on
 its own GPU (no data-path collective: replicas only); step time is the max
@@ -32,6 +45,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import statistics
@@ -58,11 +72,28 @@ WORKLOADS = {
         opts={"sd": 4, "pmf_vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
         learned=os.path.join(ROOT, "premixfem_b200", "weights", "fracture16_k6.pmfnet"),
         desc="fracture256: 256^3 unit cells, 200 fractures k=1e4, 5% barriers k=1e-4, p=1|0 on x faces; "
-             "16^3 subdomains of 16^3 cells (virtual rank grid 4x4x4, -sd 4), en_lv1=6, en_lv2=4, V-cycle; "
-             "mixed form with the learned eigensolver start (network trained on seeds 101-110, this field is "
-             "seed 4)",
+             "16^3 subdomains of 16^3 cells (virtual rank grid 4x4x4, -sd 4), en_lv1=6, en_lv2=4, V-cycle, "
+             "rtol 1e-8 (seeded synthetic field, seed 4)",
         sample_n=128, sample_opts={"sd": 4, "vranks": (2, 2, 2), "en_lv1": 6, "en_lv2": 4},
         cpu_opts={"sd": 4, "vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
+    ),
+    # 60 x 220 x 85 layered channel field (pure Neumann, constant null space), k = 4.
+    "layered": dict(
+        make=lambda seed: fields.layered(seed=2),
+        opts={"pmf_sd": (3, 11, 17), "pmf_vranks": (2, 2, 1), "en_lv1": 4, "en_lv2": 4,
+              "ksp_constant_null_space": True},
+        desc="layered: 60x220x85 cells of 20x10x2, 35 lognormal layers (sigma 1.5) over 50 layers of sinuous "
+             "channels (contrast 1e6), +/-1 injector/producer columns, no-flux walls (-ksp_constant_null_space); "
+             "6x22x17 subdomains of 10x10x5 on a 2x2x1 virtual rank grid, en_lv1=4, en_lv2=4",
+        cpu_opts={"sd": (3, 11, 17), "vranks": (2, 2, 1), "en_lv1": 4, "en_lv2": 4, "constant_null_space": True},
+    ),
+    # 512 x 512 x 256 anisotropic GRF with fracture planes, k = 8.
+    "large512": dict(
+        make=lambda seed: fields.large_frac(512, 512, 256, seed=5),
+        opts={"sd": 4, "pmf_vranks": (8, 8, 4), "en_lv1": 8, "en_lv2": 4},
+        desc="large512: 512x512x256 unit-cube cells, exp(GRF sigma 3, correlation (0.1, 0.1, 0.02)) with 400 "
+             "fracture planes of contrast 1e6, p=0 on z=0, unit source; 32x32x16 subdomains of 16^3 (-sd 4 on an "
+             "8x8x4 virtual rank grid), en_lv1=8, en_lv2=4",
     ),
     # 32^3 unit-cube GRF, the small CPU-runnable case.
     "unit_cube_grf32": dict(
@@ -74,9 +105,9 @@ WORKLOADS = {
     ),
 }
 
-# Algorithmic bytes per cell of the FP64 operator kernel k_spmv (y = A x):
-# reads x, tx, ty, tz, diag (5 x 8 B), writes y (8 B).
-SPMV_BYTES_PER_CELL = 6 * 8
+# ncu DRAM traffic of the level-1 kernel with an iterate (k_ic_apply<float,1,1>), bytes per cell, from
+# the capture summarised in profiles/ic_apply_fracture128_mixed.md (None until one exists).
+IC_APPLY_Y_TRAFFIC_PER_CELL = None
 
 
 def _peaks():
@@ -147,6 +178,30 @@ def _dist_env():
     return rank, world, local
 
 
+def class_bytes(n, nsub, nrank, nr, n3, k, w):
+    """Algorithmic bytes per PCG iteration of each kernel class of pmf_profile_iteration
+    (V-cycle, si_lv1 = si_lv2 = 1: one first level-1 visit, one final level-1 visit with
+    the iterate, one residual + restriction, one prolongation, two level-2 and one level-3
+    coarse solve).  n cells, w bytes per preconditioner value, k basis vectors per subdomain."""
+    return {
+        # read r (FP64), tx, ty, tz, 1/d; write y
+        "lv1_first": n * (8 + 5 * w),
+        # read r (FP64), y, tx, ty, tz, diag, 1/d; write the FP64 result
+        "lv1_with_y": n * (16 + 6 * w),
+        # read r (FP64), y, tx, ty, tz, diag, Phi (k values)
+        "resid_restrict": n * (8 + 5 * w + k * w),
+        # dense per-rank level-2 inverses (two visits), the level-3 inverse, the coarse blocks
+        "coarse": 2 * nrank * nr * nr * 8 + n3 * n3 * 8 + nsub * 7 * k * k * 8,
+        # read Phi, y; write y
+        "prolong": n * (k + 2) * w,
+        # read z, p, tx, ty, tz, diag; write p, w
+        "cg_p_update_Ap": n * 64,
+        # read x, r, p, w; write x, r
+        "cg_x_r_update": n * 48,
+        "beta": nsub * 8,
+    }
+
+
 def run_b200(args):
     import torch
 
@@ -162,27 +217,7 @@ def run_b200(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lib = _native.load()
-    wl = WORKLOADS[args.workload]
-    prob = wl["make"](args.seed + rank)
-    M, N, P = prob["mesh"]
-    n = M * N * P
-    kx = torch.from_numpy(np.ascontiguousarray(prob["kappa"][0]).ravel()).cuda()
-    src_h = np.ascontiguousarray(prob["source"]).ravel()
-    src_d = torch.from_numpy(src_h).cuda()
-    kx_host = torch.from_numpy(np.ascontiguousarray(prob["kappa"][0]).ravel()).pin_memory()
-    src_host = torch.from_numpy(src_h).pin_memory()
-    x_host = torch.empty(n, dtype=torch.float64).pin_memory()
-
-    def make_solver(prec):
-        o = dict(wl["opts"], pmf_precision=prec)
-        if prec == "mixed" and wl.get("learned"):
-            o["pmf_learned"] = wl["learned"]
-        if prec == "mixed":
-            o["pmf_eig_profile"] = 1  # per-phase CUDA events of the batched eigensolver (roofline below)
-        s = DarcySolver(prob["dom"], prob["mesh"], options_string(o))
-        for f, v in prob["dirichlet"].items():
-            s.set_dirichlet(f, v)
-        return s
+    hbm, bf16, peak_kind = _peaks()
 
     def barrier():
         torch.cuda.synchronize()
@@ -196,95 +231,166 @@ def run_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def device_step(s):
-        s.set_kappa(kx, kx, kx)
-        s.setup()
-        b = torch.empty_like(src_d)
-        s.rhs(src_d, b)
-        x = torch.empty_like(src_d)
-        _, its, rn, reason = s.solve(b, x)
-        su, so = s.timing()
-        return su, so, its, rn, reason, b, x
+    def measure(name, steps, warmup, headline):
+        wl = WORKLOADS[name]
+        prob = wl["make"](args.seed + rank)
+        M, N, P = prob["mesh"]
+        n = M * N * P
+        kap = [torch.from_numpy(np.ascontiguousarray(k).ravel()).cuda() for k in prob["kappa"][:1]]
+        kx = kap[0]
+        src_h = np.ascontiguousarray(prob["source"]).ravel()
+        src_d = torch.from_numpy(src_h).cuda()
 
-    results = {}
-    for prec in ("mixed", "fp64"):
-        s = make_solver(prec)
-        for _ in range(args.warmup):
-            device_step(s)
-        barrier()
-        steps = []
-        launches0 = lib.pmf_launch_count()
-        with ClockSampler(local) as clk:
-            for _ in range(args.steps):
-                barrier()
-                su, so, its, rn, reason, b, x = device_step(s)
-                barrier()
-                steps.append((su, so, its, rn, reason))
-        launches = lib.pmf_launch_count() - launches0
-        stages = s.stages()
-        ev1, ks, it1, st1 = s.eigen_lv1()
-        lst = (C.c_longlong * 4)()
-        net_ms = C.c_double()
-        _native.check(lib.pmf_get_learned_stats(s.h, lst, C.byref(net_ms)))
-        phases = (C.c_double * 8)()
-        colcells = C.c_ulonglong()
-        _native.check(lib.pmf_get_eig_phases(s.h, phases, C.byref(colcells)))
-        bn = float(torch.linalg.norm(b))
-        res = float(torch.linalg.norm(b - torch.from_numpy(s.apply_A(x.cpu().numpy())).cuda())) / bn
-        results[prec] = dict(steps=steps, launches=launches, clocks=clk.summary(), stages=stages,
-                             eig_iters_mean=float(it1.mean()), eig_iters_max=int(it1.max()),
-                             eig_iters_sum=int(it1.sum()), cells_per_sub=n / len(it1),
-                             eig_unconverged=int((st1 != 0).sum()), rel_residual=res, x=x.cpu().numpy(),
-                             learned=dict(used=int(lst[0]), fallbacks=int(lst[1]), net_ms=round(net_ms.value, 3)),
-                             eig_phases=list(phases), eig_colcells=int(colcells.value))
-        if prec == "mixed":
-            # e2e through the C ABI with host buffers (copies inside the timed region)
-            e2e = []
-            for _ in range(max(1, args.steps)):
-                barrier()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record()
-                s.set_kappa(kx_host.numpy(), kx_host.numpy(), kx_host.numpy())
-                s.setup()
-                bh = s.rhs(src_host.numpy())
-                s.solve(bh, x_host.numpy())
-                e1.record()
-                torch.cuda.synchronize()
-                e2e.append(e0.elapsed_time(e1) / 1e3)
-            results["e2e"] = e2e
-            # live per-kernel timing of the PCG operator kernel for the solve-phase roofline
-            results["spmv_ms"] = time_spmv(s, n)
+        def make_solver(form, extra=None):
+            o = dict(wl["opts"], pmf_precision="fp64" if form.startswith("fp64") else "mixed")
+            if form == "mixed" and wl.get("learned"):
+                o["pmf_learned"] = wl["learned"]
+            if form == "mixed" and headline:
+                o["pmf_eig_profile"] = 1  # per-phase CUDA events of the batched eigensolver
+            o.update(extra or {})
+            s = DarcySolver(prob["dom"], prob["mesh"], options_string(o))
+            for f, v in prob["dirichlet"].items():
+                s.set_dirichlet(f, v)
+            return s
+
+        def device_step(s):
+            s.set_kappa(kx, kx, kx)
+            s.setup()
+            b = torch.empty_like(src_d)
+            s.rhs(src_d, b)
+            x = torch.empty_like(src_d)
+            _, its, rn, reason = s.solve(b, x)
+            su, so = s.timing()
+            return su, so, its, rn, reason, b, x
+
+        def true_residual(s, b, x):
+            ax = torch.empty_like(x)
+            s.apply_A(x, ax)
+            return float(torch.linalg.norm(b - ax) / torch.linalg.norm(b))
+
+        forms = ["mixed"] + (["mixed_nonet"] if wl.get("learned") else []) + ["fp64"]
+        res = {}
+        sol = {}
+        boxes = None
+        for form in forms:
+            s = make_solver(form)
+            for _ in range(warmup):
+                device_step(s)
+            barrier()
+            steps_l = []
+            launches0 = lib.pmf_launch_count()
+            with ClockSampler(local) as clk:
+                for _ in range(steps):
+                    barrier()
+                    su, so, its, rn, reason, b, x = device_step(s)
+                    barrier()
+                    steps_l.append((su, so, its, rn, reason))
+            launches = lib.pmf_launch_count() - launches0
+            ev1, ks, it1, st1 = s.eigen_lv1()
+            lst = (C.c_longlong * 4)()
+            net_ms = C.c_double()
+            _native.check(lib.pmf_get_learned_stats(s.h, lst, C.byref(net_ms)))
+            r = dict(steps=steps_l, launches=launches, clocks=clk.summary(),
+                     setup_s=statistics.mean(v[0] for v in steps_l) / 1e3,
+                     solve_s=statistics.mean(v[1] for v in steps_l) / 1e3,
+                     its=steps_l[-1][2], reason=steps_l[-1][4], rel_residual=true_residual(s, b, x),
+                     eig=dict(iters_mean=float(it1.mean()), iters_max=int(it1.max()),
+                              status={"converged": int((st1 == 0).sum()), "rounding_floor": int((st1 == 2).sum()),
+                                      "max_it": int((st1 == 1).sum())}),
+                     ev1=ev1, learned=dict(used=int(lst[0]), fallbacks=int(lst[1]),
+                                           net_ms=round(net_ms.value, 3)))
+            if boxes is None:
+                boxes = s.subdomains()[0]
+            r["t"] = r["setup_s"] + r["solve_s"]
+            sol[form] = x
+            if form == "mixed" and headline:
+                phases = (C.c_double * 8)()
+                colcells = C.c_ulonglong()
+                _native.check(lib.pmf_get_eig_phases(s.h, phases, C.byref(colcells)))
+                r["eig_phases"] = list(phases)
+                # per-class kernel times of one PCG iteration on this solve's data
+                r["profile"] = s.profile_iteration(reps=5)
+                r["info"] = s.info()
+                # e2e through the C ABI with host buffers (copies inside the timed region)
+                kx_host = torch.from_numpy(np.ascontiguousarray(prob["kappa"][0]).ravel()).pin_memory()
+                src_host = torch.from_numpy(src_h).pin_memory()
+                x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+                e2e = []
+                for _ in range(max(1, steps)):
+                    barrier()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    s.set_kappa(kx_host.numpy(), kx_host.numpy(), kx_host.numpy())
+                    s.setup()
+                    bh = s.rhs(src_host.numpy())
+                    s.solve(bh, x_host.numpy())
+                    e1.record()
+                    torch.cuda.synchronize()
+                    e2e.append(e0.elapsed_time(e1) / 1e3)
+                r["e2e"] = e2e
+            res[form] = r
+            s.close()
+            del s
+            gc.collect()
+        # FP64 reference solution: the device FP64 form solved to relative residual 1e-13
+        s = make_solver("fp64_ref", {"ksp_rtol": "1e-13"})
+        _, _, its_ref, _, reason_ref, b, xref = device_step(s)
         s.close()
+        del s
+        nref = float(torch.linalg.norm(xref))
+        err = {f: float(torch.linalg.norm(sol[f] - xref)) / nref for f in forms}
+        out = dict(wl=wl, prob=prob, n=n, res=res, forms=forms, boxes=boxes, err=err,
+                   ref=dict(its=its_ref, reason=reason_ref))
+        del sol, xref, kx, src_d, kap
+        gc.collect()
+        torch.cuda.empty_cache()
+        return out
 
-    mixed = results["mixed"]["steps"]
-    plain = results["fp64"]["steps"]
-    t_mixed = maxr(statistics.mean(su + so for su, so, *_ in mixed) / 1e3)
-    t_plain = maxr(statistics.mean(su + so for su, so, *_ in plain) / 1e3)
-    t_e2e = maxr(statistics.mean(results["e2e"]))
-    su_m = statistics.mean(x[0] for x in mixed) / 1e3
-    so_m = statistics.mean(x[1] for x in mixed) / 1e3
-    su_p = statistics.mean(x[0] for x in plain) / 1e3
-    so_p = statistics.mean(x[1] for x in plain) / 1e3
-    its_m = mixed[-1][2]
-    its_p = plain[-1][2]
-    xdiff = float(np.linalg.norm(results["mixed"]["x"] - results["fp64"]["x"]) / np.linalg.norm(results["fp64"]["x"]))
-    hbm, bf16, peak_kind = _peaks()
-    # dominant kernel of the step: the batched local eigensolver (stage su_lv2_1)
-    st = results["mixed"]["stages"]
-    eig_s = st["su_lv2_1"] / (args.steps + args.warmup)
-    spmv_ms = results["spmv_ms"]
-    # dominant kernel of the step: the batched eigensolver's basis update k_eb_update<float>
-    # (X <- [X W P] Y, P <- [W P] Y per subdomain).  Algorithmic bytes per subdomain-iteration:
-    # read the nS basis columns and write X and P (2m columns), 4 bytes per FP32 value; the library
-    # counts sum(nS x cells) over subdomain-iterations (colcells) and times the phase with events.
-    m_blk = wl["opts"]["en_lv1"] + 2
-    lob_sub_iters = results["mixed"]["eig_iters_sum"]
-    ph = results["mixed"]["eig_phases"]
-    upd_bytes = 4.0 * (results["mixed"]["eig_colcells"] + 2 * m_blk * results["mixed"]["cells_per_sub"] * lob_sub_iters)
-    upd_s = ph[4] * 1e-3
-    biter = n * (104 + 4 * (25 + 6 * wl["opts"]["en_lv1"]))
-    spmv_gbs = SPMV_BYTES_PER_CELL * n / (spmv_ms * 1e-3) / 1e9
+    def form_summary(r):
+        return {"setup_s": round(r["setup_s"], 6), "solve_s": round(r["solve_s"], 6), "total_s": round(r["t"], 6),
+                "pcg_iters": r["its"], "reason": r["reason"], "rel_residual": r["rel_residual"],
+                "eigensolver": dict(r["eig"], learned_start=r["learned"]), "clocks": r["clocks"]}
+
+    def accuracy(m):
+        return {"error_vs_fp64_ref": {f: m["err"][f] for f in m["forms"]},
+                "fp64_ref": f"device FP64 form, PCG to relative residual 1e-13 ({m['ref']['its']} iterations, "
+                            f"{m['ref']['reason']}); not a direct solve at this size"}
+
+    main_name = args.workload
+    m = measure(main_name, args.steps, args.warmup, headline=True)
+    wl, n, res = m["wl"], m["n"], m["res"]
+    mix, plain = res["mixed"], res["fp64"]
+    t_mixed = maxr(mix["t"])
+    t_plain = maxr(plain["t"])
+    t_e2e = maxr(statistics.mean(mix["e2e"]))
+
+    # roofline: the dominant kernel class of a PCG iteration, timed live
+    info = mix["info"]
+    k = wl["opts"]["en_lv1"]
+    cb = class_bytes(n, info["nsub"], info["nrank"], info["nr"], info["n3"], k, 4)
+    prof = mix["profile"]
+    per_class = {}
+    for c, (ms, nl) in prof.items():
+        if nl == 0:
+            continue
+        per_class[c] = {"ms_per_iteration": round(ms, 4), "launch_groups": nl,
+                        "algorithmic_bytes": int(cb[c]),
+                        "achieved_gbs": round(cb[c] / (ms * 1e-3) / 1e9, 1) if ms > 0 else None}
+        per_class[c]["frac"] = round(per_class[c]["achieved_gbs"] / hbm, 4) if ms > 0 else None
+    dom = max((c for c in per_class if c.startswith("lv1") or c in ("resid_restrict", "prolong", "cg_p_update_Ap",
+                                                                     "cg_x_r_update")),
+              key=lambda c: per_class[c]["ms_per_iteration"])
+    d = per_class[dom]
+    dom_ms_launch = d["ms_per_iteration"] / d["launch_groups"]
+    dom_bytes_launch = cb[dom] / d["launch_groups"]
+    traffic = None
+    if dom == "lv1_with_y" and IC_APPLY_Y_TRAFFIC_PER_CELL:
+        traffic = int(IC_APPLY_Y_TRAFFIC_PER_CELL * n)
+    iter_ms = sum(v[0] for v in prof.values())
+    iter_bytes = sum(cb[c] for c in prof if prof[c][1] > 0)
+    biter = n * (104 + 4 * (25 + 6 * k))
+    its_m = mix["its"]
     line = {
         "metric": METRIC,
         "value": round(t_mixed, 6),
@@ -304,63 +410,70 @@ def run_b200(args):
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "l2": "inputs larger than L2 (kappa 3 x 134 MB, vectors 134 MB each)",
         },
-        "pcg_iters": {"mixed": its_m, "plain_fp64": its_p},
-        "setup_s": {"mixed": round(su_m, 6), "plain_fp64": round(su_p, 6)},
-        "solve_s": {"mixed": round(so_m, 6), "plain_fp64": round(so_p, 6)},
+        "pcg_iters": {"mixed": its_m, "plain_fp64": plain["its"]},
+        "setup_s": {"mixed": round(mix["setup_s"], 6), "plain_fp64": round(plain["setup_s"], 6)},
+        "solve_s": {"mixed": round(mix["solve_s"], 6), "plain_fp64": round(plain["solve_s"], 6)},
         "plain_fp64_value": round(t_plain, 6),
         "speedup_vs_plain_fp64": round(t_plain / t_mixed, 3),
-        "rel_residual": {"mixed": results["mixed"]["rel_residual"], "plain_fp64": results["fp64"]["rel_residual"]},
-        "solution_rel_diff_mixed_vs_fp64": xdiff,
-        "eigensolver": {"iters_mean": results["mixed"]["eig_iters_mean"], "iters_max": results["mixed"]["eig_iters_max"],
-                        "unconverged": results["mixed"]["eig_unconverged"],
-                        "plain_fp64_iters_mean": results["fp64"]["eig_iters_mean"],
-                        "plain_fp64_iters_max": results["fp64"]["eig_iters_max"],
-                        "learned_start": results["mixed"]["learned"]},
+        "forms": {f: form_summary(res[f]) for f in m["forms"]},
+        "accuracy": accuracy(m),
         # host buffers: kappa x3 + source + rhs in (5n doubles); rhs + solution out (2n doubles)
         "e2e": {"value": round(t_e2e, 6), "unit": "s", "h2d_bytes_per_step": int(5 * n * 8),
                 "d2h_bytes_per_step": int(2 * n * 8)},
-        "gpu_launches": int(results["mixed"]["launches"] / max(1, args.steps)),
+        "gpu_launches": int(mix["launches"] / max(1, args.steps)),
         "roofline": {
-            "kernel": "k_eb_update<float> (batched LOBPCG basis update, largest single kernel of the step)",
+            "kernel": {"lv1_with_y": "k_ic_apply<float,1,1> (level-1 IC(0) solve with the iterate, final visit)",
+                       "lv1_first": "k_ic_apply<float,0,0> (level-1 IC(0) solve, first visit)"}.get(dom, dom),
             "bound": "hbm",
-            "achieved": round(upd_bytes / upd_s / 1e9, 1) if upd_s > 0 else None,
+            "achieved": round(dom_bytes_launch / (dom_ms_launch * 1e-3) / 1e9, 1),
             "peak": hbm,
             "unit": "GB/s",
-            "frac": round(upd_bytes / upd_s / 1e9 / hbm, 4) if upd_s > 0 else None,
-            "traffic": None,
-            "bytes_per_step": upd_bytes,
-            "time_s_per_step": round(upd_s, 6),
+            "frac": round(dom_bytes_launch / (dom_ms_launch * 1e-3) / 1e9 / hbm, 4),
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": int(dom_bytes_launch),
+            "ms_per_launch": round(dom_ms_launch, 4),
             "peak_kind": peak_kind,
+            "timing": "CUDA events on the solver stream around each launch group of one PCG iteration, "
+                      "5 repetitions outside the CUDA graph (pmf_profile_iteration)",
         },
-        "lobpcg_phases_ms": {"resid_control": round(ph[0], 2), "precond": round(ph[1], 2), "gram": round(ph[2], 2),
-                             "rayleigh_ritz": round(ph[3], 2), "update": round(ph[4], 2),
-                             "a_images": round(ph[5], 2), "lockstep_iterations": int(ph[6]),
-                             "eigen_stage_s": round(eig_s, 6)},
-        "roofline_solve_model": {
-            "phase": "PCG solve (all kernels), algorithmic bytes B_iter = N*[104 + w*(25+6k)], w=4, k=6",
-            "bound": "hbm",
-            "achieved": round(biter * its_m / so_m / 1e9, 1),
-            "peak": hbm,
-            "unit": "GB/s",
-            "frac": round(biter * its_m / so_m / 1e9 / hbm, 4),
-            "bytes_per_iteration": biter,
+        "solve_phase": {
+            "model": {"bytes_per_iteration": biter, "formula": "N*[104 + w*(25+6k)], w=4",
+                      "achieved_gbs": round(biter * its_m / mix["solve_s"] / 1e9, 1),
+                      "frac": round(biter * its_m / mix["solve_s"] / 1e9 / hbm, 4)},
+            "launched_kernels": {"bytes_per_iteration": int(iter_bytes), "iteration_ms": round(iter_ms, 4),
+                                 "achieved_gbs": round(iter_bytes / (iter_ms * 1e-3) / 1e9, 1),
+                                 "frac": round(iter_bytes / (iter_ms * 1e-3) / 1e9 / hbm, 4),
+                                 "by_class": per_class},
         },
-        "roofline_solve": {
-            "kernel": "k_spmv (7-point FP64 operator, y = A x)",
-            "bound": "hbm",
-            "achieved": round(spmv_gbs, 1),
-            "peak": hbm,
-            "unit": "GB/s",
-            "frac": round(spmv_gbs / hbm, 4),
-            "traffic": None,
-            "bytes_per_cell": SPMV_BYTES_PER_CELL,
-            "peak_kind": peak_kind,
-        },
-        "clocks": results["mixed"]["clocks"],
+        "clocks": mix["clocks"],
         "autotune": _tune_choices(lib),
     }
+    if "eig_phases" in mix:
+        ph = mix["eig_phases"]
+        line["lobpcg_phases_ms"] = {"resid_control": round(ph[0], 2), "precond": round(ph[1], 2),
+                                    "gram": round(ph[2], 2), "rayleigh_ritz": round(ph[3], 2),
+                                    "update": round(ph[4], 2), "a_images": round(ph[5], 2),
+                                    "lockstep_iterations": int(ph[6])}
+    extras = {}
+    for name in [e for e in args.extra.split(",") if e and e != main_name]:
+        try:
+            e = measure(name, 3, 3, headline=False)
+            er = e["res"]
+            extras[name] = {"config": e["wl"]["desc"], "cells": e["n"], "steps": 3, "warmup": 3,
+                            "value": round(maxr(er["mixed"]["t"]), 6),
+                            "plain_fp64_value": round(maxr(er["fp64"]["t"]), 6),
+                            "speedup_vs_plain_fp64": round(er["fp64"]["t"] / er["mixed"]["t"], 3),
+                            "forms": {f: form_summary(er[f]) for f in e["forms"]},
+                            "accuracy": accuracy(e)}
+            del e
+        except Exception as ex:  # a secondary workload never voids the headline line
+            extras[name] = {"error": f"{type(ex).__name__}: {ex}"}
+        gc.collect()
+    if extras:
+        line["workloads"] = extras
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, wl, prob, its_p)
+        line["cpu_baseline"] = cpu_baseline(args, wl, m["prob"], plain["its"])
+        line["accuracy"]["local_eigenvalues_sample"] = eig_sample(m)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -380,23 +493,24 @@ def _tune_choices(lib):
     return {k.rsplit("|", 1)[0]: [v["choice"], v["us"]] for k, v in table.items()}
 
 
-def time_spmv(s, n):
-    """Average duration of the FP64 PCG operator kernel, timed with CUDA events on the solver stream."""
-    import torch
-    x = torch.randn(n, dtype=torch.float64, device="cuda")
-    y = torch.empty_like(x)
-    for _ in range(3):
-        s.apply_A(x, y)
-    torch.cuda.synchronize()
-    reps = 20
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        s.apply_A(x, y)
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+def eig_sample(m, count=64, seed=12):
+    """Checker, CPU-baseline leg: local eigenvalues of a seeded sample of subdomains, every GPU form
+    against the oracle's exact local GHEP (ARPACK shift-and-invert on each subdomain's crop)."""
+    from oracle import pmf_oracle as O
+
+    boxes = m["boxes"]
+    k = m["wl"]["opts"]["en_lv1"]
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(len(boxes), size=min(count, len(boxes)), replace=False))
+    t0 = time.perf_counter()
+    ref = O.local_eigenvalues(m["prob"], boxes[pick], k)
+    out = {"subdomains": int(len(pick)), "of": int(len(boxes)), "seed": seed,
+           "oracle": "exact local GHEP A_N v = lambda M v per subdomain (ARPACK shift-invert, target -1e-12)",
+           "oracle_s": round(time.perf_counter() - t0, 2)}
+    for f, r in m["res"].items():
+        rel, null = O.eigenvalue_errors(r["ev1"][pick], ref)
+        out[f] = {"max_rel_err": rel, "null_mode_abs_err_over_lambda_max": null}
+    return out
 
 
 def _crop(prob, ns):
@@ -419,7 +533,8 @@ def cpu_run(wl, prob, crop=False):
 
     so = wl["sample_opts"] if crop else wl["cpu_opts"]
     sub = _crop(prob, wl["sample_n"]) if crop else prob
-    return CR.solve(sub, sd=so["sd"], vranks=so.get("vranks", (1, 1, 1)), en_lv1=so["en_lv1"], en_lv2=so["en_lv2"])
+    kw = {k: v for k, v in so.items() if k not in ("sd", "vranks")}
+    return CR.solve(sub, sd=so["sd"], vranks=so.get("vranks", (1, 1, 1)), **kw)
 
 
 def cpu_baseline(args, wl, prob, gpu_its):
@@ -437,9 +552,13 @@ def run_reference(args):
     if rank != 0:
         return
     wl = WORKLOADS[args.workload]
+    if "cpu_opts" not in wl:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU restatement run is defined for "
+                                                              f"{args.workload}"}), flush=True)
+        return
     prob = wl["make"](args.seed)
     for _ in range(args.warmup):
-        cpu_run(wl, prob, crop=True)
+        cpu_run(wl, prob, crop="sample_n" in wl)
     vals, r = [], None
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -448,8 +567,8 @@ def run_reference(args):
     wall = time.perf_counter() - t0
     value = statistics.mean(vals)
     cb = {"value": round(value, 3), "unit": "s", "cores": r["threads"], "kind": "port",
-          "sample": f"full workload per timed step (warm-up steps on a {wl['sample_n']}^3 crop): C++/OpenMP FP64 "
-                    f"restatement on {r['threads']} host threads, {r['its']} PCG iterations, last step setup "
+          "sample": f"full workload per timed step (warm-up steps on a {wl.get('sample_n', 'full')}^3 crop): C++/OpenMP "
+                    f"FP64 restatement on {r['threads']} host threads, {r['its']} PCG iterations, last step setup "
                     f"{r['setup_s']:.2f} s + solve {r['solve_s']:.2f} s",
           "wall_s": round(wall, 2)}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -468,6 +587,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="fracture256", choices=sorted(WORKLOADS))
+    ap.add_argument("--extra", default="layered,large512",
+                    help="secondary workloads measured after the headline (comma separated, '' for none)")
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

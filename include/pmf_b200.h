@@ -2,8 +2,8 @@
  * pmf_b200.h -- flat C ABI of the B200 PreMixFEM solver library
  * (libpremixfem_b200.so).  Plain pointers and sizes only; every function
  * returns 0 on success or a PETSc-style error code (62 bad argument, 73 wrong
- * state, 56 unsupported, 71 zero pivot, 76 CUDA/library failure) and leaves a
- * message for pmf_last_error().
+ * state, 56 unsupported, 71 zero pivot, 76 CUDA/library failure, 83 a local
+ * eigensolve did not converge) and leaves a message for pmf_last_error().
  *
  * Arrays are float64, natural order with x fastest (cell id
  * (ez*N + ey)*M + ex), the DMDA ordering the reference uses.  "on_device"
@@ -41,7 +41,9 @@ typedef struct pmf_solver pmf_solver;
  * residual of the CG solve; for operators with no Dirichlet face); B200
  * extensions: -pmf_sd sx,sy,sz (subdomains per
  * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
- * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it, -pmf_learned
+ * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it (a local eigensolve
+ * that spends it makes pmf_setup fail with 83, as the reference's SLEPc check
+ * does, unless -pmf_eig_allow_unconverged keeps its last block), -pmf_learned
  * <weights file> (learned initial blocks for the local eigensolves),
  * -pmf_learned_its N and -pmf_learned_tol t (a subdomain whose LOBPCG from the
  * learned start has not reached relative residual t within N iterations is
@@ -71,6 +73,18 @@ int pmf_pc_apply(pmf_solver* s, const double* x, double* y, int on_device);
 /* reason: 1 converged (residual test), 2 max_it, 3 indefinite, 4 nan/inf, 5 converged because the
  * preconditioned residual's dot z.r is exactly zero (PETSc's KSP_CONVERGED_ATOL for KSPCG) */
 int pmf_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason);
+
+/* Device time of the kernels of one PCG iteration by class, after pmf_setup (and normally a
+ * pmf_solve, whose final residual is the input): the iteration's launches run `reps` times outside
+ * any CUDA graph with an event after each launch group, on scratch vectors (the solver's last
+ * solution and residual are kept; its CG scalars are not).  ms[c] = mean device milliseconds per
+ * iteration, launches[c] = launch groups per iteration, for the classes
+ *   0 level-1 first visit (IC(0) sweeps of the residual), 1 level-1 visits with an iterate
+ *   (r - A y, sweeps, y +=; the last one writes the FP64 result and the z.r partials),
+ *   2 residual + level-2 restriction, 3 coarse solves (levels 2 and 3), 4 prolongation,
+ *   5 CG p-update + A p, 6 CG x/r update + residual norm, 7 beta = z.r.
+ * No counterpart in the reference (PETSc's -log_view plays this role there). */
+int pmf_profile_iteration(pmf_solver* s, int reps, double ms[8], int launches[8]);
 
 /* info[0..11] = ncell_lo32, nsub, nrank, subdomains_per_rank, kmax, nr, en_lv2, n3,
  *               max_cells, max_lines, precision, is_setup */

@@ -694,3 +694,67 @@ def solve(problem, opts: Options):
     x, its, hist, reason = pcg(op.A, b, pc.apply, rtol=pc.opts.rtol, max_it=pc.opts.max_it,
                                null_space=pc.opts.constant_null_space)
     return {"op": op, "pc": pc, "b": b, "x": x, "its": its, "hist": hist, "reason": reason}
+
+
+def crop_around(problem, box):
+    """The problem restricted to ``box`` plus a one-cell halo where the mesh has
+    cells, and the box in the crop's coordinates.
+
+    A subdomain's level-2 GHEP (src/PreMixFEM_3D.c:243-346) reads the
+    permeability of its own cells and of their face neighbours, the global
+    boundary flags of its cells and the Dirichlet faces it touches; the crop
+    keeps all of them (a crop face that is not a global face is never reached
+    from inside the box), so the local matrices are the same as on the full
+    mesh without assembling the whole operator.
+    """
+    M, N, P = problem["mesh"]
+    L, W, H = problem["dom"]
+    h = (L / M, W / N, H / P)
+    x0, nx, y0, ny, z0, nz = (int(v) for v in box[:6])
+    lo = (max(0, x0 - 1), max(0, y0 - 1), max(0, z0 - 1))
+    hi = (min(M, x0 + nx + 1), min(N, y0 + ny + 1), min(P, z0 + nz + 1))
+    sl = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+    mesh = (hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2])
+    kap = tuple(np.ascontiguousarray(np.asarray(k)[sl]) for k in problem["kappa"])
+    on = {"x-": lo[0] == 0, "x+": hi[0] == M, "y-": lo[1] == 0, "y+": hi[1] == N, "z-": lo[2] == 0, "z+": hi[2] == P}
+    dirichlet = {f: v for f, v in problem.get("dirichlet", {}).items() if on[f]}
+    crop = dict(mesh=mesh, dom=(h[0] * mesh[0], h[1] * mesh[1], h[2] * mesh[2]), kappa=kap,
+                source=np.zeros((mesh[2], mesh[1], mesh[0])), dirichlet=dirichlet)
+    return crop, (x0 - lo[0], nx, y0 - lo[1], ny, z0 - lo[2], nz)
+
+
+def local_eigenvalues(problem, boxes, k, eg_op=EIG_OP_MOD, method="arpack"):
+    """The k smallest eigenvalues of each subdomain's GHEP A_i^N v = lambda M_i v
+    (src/PreMixFEM_3D.c:224-390), one row per box: dense ``eigh`` or ARPACK
+    shift-and-invert with SLEPc's target -NIL (:354-365), computed on
+    ``crop_around`` crops."""
+    out = []
+    for box in boxes:
+        crop, cb = crop_around(problem, box)
+        op = Operator(crop)
+        An = op.neumann(cb)
+        Md = op.mass_diag(cb, eg_op)
+        if method == "arpack" and k < An.shape[0] - 1:
+            w = spla.eigsh(sp.csc_matrix(An), k=k, M=sp.diags(Md).tocsc(), sigma=-NIL, which="LM",
+                           return_eigenvectors=False, tol=0.0)
+            w = np.sort(w)
+        else:
+            w = sla.eigh(An.toarray(), np.diag(Md), subset_by_index=[0, k - 1], eigvals_only=True)
+        out.append(w)
+    return np.array(out)
+
+
+def eigenvalue_errors(ev, ref):
+    """Relative errors of computed local eigenvalues ``ev`` against ``ref``
+    (rows: subdomains).  Returns (max relative error over the eigenvalues
+    above 1e-8 x the row's largest, max |error| / row's largest over the
+    others, i.e. the near-zero modes such as the constant of a pure-Neumann
+    subdomain)."""
+    ev = np.asarray(ev, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    big = np.abs(ref) > 1e-8 * scale
+    d = np.abs(ev - ref)
+    rel = float((d / np.where(big, np.abs(ref), 1.0))[big].max()) if big.any() else 0.0
+    null = float((d / scale)[~big].max()) if (~big).any() else 0.0
+    return rel, null

@@ -105,6 +105,12 @@ int pmf_solve(pmf_solver* h, const double* b, double* x, int on_device, int* its
   return wrap(h, h->s->solve(b, x, on_device != 0, its, rnorm, reason));
 }
 
+int pmf_profile_iteration(pmf_solver* h, int reps, double ms[8], int launches[8]) {
+  PMF_CHECK_HANDLE(h);
+  if (!ms || !launches || reps < 1) return fail(62, "pmf_profile_iteration: null output or reps < 1");
+  return wrap(h, h->s->profile_iteration(reps, ms, launches));
+}
+
 int pmf_get_info(pmf_solver* h, int info[12]) {
   PMF_CHECK_HANDLE(h);
   pmf::Solver& s = *h->s;

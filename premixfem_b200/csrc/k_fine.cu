@@ -170,7 +170,8 @@ __global__ void k_pcg_start_fin(const double* part, int nb, PcgState* s, double 
     s->max_it = max_it;
     s->first = 1;
     s->beta = s->betaold = s->dpi = s->dpiold = s->alpha = 0.0;
-    s->done = (dp <= s->ttol) ? 1 : 0;
+    // KSPConvergedDefault tests for NaN/Inf before the tolerance
+    s->done = (!(dp == dp) || isinf(dp)) ? 4 : (dp <= s->ttol) ? 1 : 0;
   }
 }
 void launch_pcg_start(const Grid& g, const double* b, double* x, double* r, double* part, PcgState* s, double rtol,

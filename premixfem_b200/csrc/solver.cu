@@ -139,6 +139,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_final", &o->eig_final);
   db.get_int("pmf_eig_init", &o->eig_init);
   db.get_int("pmf_eig_profile", &o->eig_profile);
+  o->eig_allow_unconverged = db.has("pmf_eig_allow_unconverged");
   db.get_int("pmf_pcg_graph", &o->pcg_graph);
   db.get_int("pmf_autotune", &o->autotune);
   {
@@ -279,6 +280,8 @@ Solver::~Solver() {
   if (h_state) cudaFreeHost(h_state);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  for (auto& e : prof_ev)
+    if (e) cudaEventDestroy(e);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -711,6 +714,21 @@ int Solver::setup() {
   } else {
     launch_ic_factor(g, d_subs, nsub, max_lines, tx, ty, tz, diag, inv64, d_flag, st);
   }
+  {
+    // a non-positive level-1 pivot (a cell with kappa <= 0, for instance)
+    // stops the set-up here, before the eigensolves see the operator, as
+    // PETSc's factorisation fails in KSPSetUp (src/PreMixFEM_3D.c:200-215)
+    if (int er = check(cudaStreamSynchronize(st), "level-1 factorisation")) return er;
+    int bad_pivots = 0;
+    if (int er = check(cudaMemcpy(&bad_pivots, d_flag, sizeof(int), cudaMemcpyDeviceToHost), "pivot flag"))
+      return er;
+    if (bad_pivots) {
+      err = std::to_string(bad_pivots) +
+            (opt.use_full_Cholesky_lv1 ? " non-positive pivot(s) in the level-1 Cholesky factorisations"
+                                       : " non-positive IC(0) pivot(s) in the level-1 factorisations");
+      return 71;  // PETSC_ERR_MAT_LU_ZRPVT
+    }
+  }
   if (mixed) {
     launch_to_f32(tx, tx32, g.ncell, st);
     launch_to_f32(ty, ty32, g.ncell, st);
@@ -845,12 +863,18 @@ int Solver::setup() {
   }
   cudaMemcpy(eig_status.data(), d_status, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
   cudaMemcpy(eig1.data(), d_eig1, sizeof(double) * eig1.size(), cudaMemcpyDeviceToHost);
-  int bad_pivots = 0;
-  cudaMemcpy(&bad_pivots, d_flag, sizeof(int), cudaMemcpyDeviceToHost);
-  if (bad_pivots) {
-    err = opt.use_full_Cholesky_lv1 ? "non-positive pivot in a level-1 Cholesky factorisation"
-                                    : "non-positive IC(0) pivot in a level-1 factorisation";
-    return 71;  // PETSC_ERR_MAT_LU_ZRPVT
+  {
+    // SLEPc "cannot find enough eigenvectors" (src/PreMixFEM_3D.c:367):
+    // a local eigensolve that used its whole iteration budget is an error
+    // unless -pmf_eig_allow_unconverged keeps its last Ritz block
+    int nmax = 0;
+    for (int s_ = 0; s_ < nsub; ++s_) nmax += eig_status[s_] == 1;
+    if (nmax && !opt.eig_allow_unconverged) {
+      err = "local eigensolver did not converge on " + std::to_string(nmax) + " of " + std::to_string(nsub) +
+            " subdomains within -pmf_eig_max_it " + std::to_string(opt.eig_max_it) +
+            " iterations (-pmf_eig_allow_unconverged keeps the unconverged blocks)";
+      return 83;  // PETSC_ERR_USER
+    }
   }
   for (int s = 0; s < nsub; ++s) subs[s].k = ks[s];
   cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
@@ -1120,9 +1144,11 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
     if (v == 1) {
       if (z_pend) {
         launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st, pr_threads);
+        prof_mark(PROF_PROLONG);
         z_pend = false;
       }
       const T* yin = y_zero ? nullptr : yb[cur];
+      const int lv1_slot = y_zero ? PROF_LV1_FIRST : PROF_LV1_Y;
       if (opt.use_full_Cholesky_lv1) {
         const T* tband = f32 ? (const T*)band32 : (const T*)band64;
         if (last)
@@ -1141,16 +1167,19 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
                            nullptr, nullptr, done, st, ic_threads);
         cur = 1 - cur;
       }
+      prof_mark(lv1_slot);
       y_zero = false;
       c_valid = false;
     } else {
       if (!c_valid) {
         if (z_pend) {
           launch_prolong<T>(g, d_subs, nsub, kmax, tphi, Zacc, yb[cur], done, st, pr_threads);
+          prof_mark(PROF_PROLONG);
           z_pend = false;
         }
         launch_resid_restrict<T>(g, d_subs, nsub, kmax, ttx, tty, ttz, tdg, tphi, x, y_zero ? nullptr : yb[cur], c,
                                  done, st, rr_threads);
+        prof_mark(PROF_RESTRICT);
         c_valid = true;
       }
       if (v == 2) {
@@ -1172,8 +1201,73 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
         launch_a2_mult(d_subs, nsub, kmax, blk, dz, c, c, done, st);
       else
         c_valid = false;
+      prof_mark(PROF_COARSE);
     }
   }
+}
+
+void Solver::prof_mark(int slot) {
+  if (!prof_on || prof_n >= 64) return;
+  cudaEventRecord(prof_ev[prof_n], st);
+  prof_slot[prof_n++] = slot;
+}
+
+// One PCG iteration's kernels (CG p-update + A p, x/r update, the whole
+// preconditioner application, beta) run `reps` times outside any graph, with
+// an event after each launch group; ms[c] is the mean device time per
+// iteration of class c, launches[c] its launch groups per iteration.  Runs on
+// scratch: the solution and residual go to the host-staging buffers vx, vb and
+// the CG scalars to the solver's state (reset here, rewritten by every solve).
+int Solver::profile_iteration(int reps, double ms[PROF_SLOTS], int launches[PROF_SLOTS]) {
+  if (!is_setup) {
+    err = "setup not done";
+    return 73;
+  }
+  for (int c_ = 0; c_ < PROF_SLOTS; ++c_) {
+    ms[c_] = 0.0;
+    launches[c_] = 0;
+  }
+  if (!prof_ev[0])
+    for (auto& e : prof_ev)
+      if (int er = check(cudaEventCreate(&e), "profile events")) return er;
+  PcgState hs;
+  memset(&hs, 0, sizeof(hs));
+  hs.beta = hs.betaold = 1.0;
+  hs.max_it = 1 << 30;
+  cudaMemcpyAsync(vb, r, sizeof(double) * g.ncell, cudaMemcpyDeviceToDevice, st);
+  cudaMemsetAsync(vx, 0, sizeof(double) * g.ncell, st);
+  cudaMemsetAsync(p0, 0, sizeof(double) * g.ncell, st);
+  for (int rep = 0; rep < std::max(1, reps); ++rep) {
+    *h_state = hs;
+    cudaMemcpyAsync(state, h_state, sizeof(PcgState), cudaMemcpyHostToDevice, st);
+    prof_n = 0;
+    prof_on = true;
+    prof_mark(-1);
+    launch_pcg_iter_a(g, tx, ty, tz, diag, z, p0, p1, w, part, state, st, pcga_variant);
+    prof_mark(PROF_CG_A);
+    launch_pcg_iter_b(g.ncell, vx, vb, p1, w, part, state, st);
+    prof_mark(PROF_CG_B);
+    apply(vb, z, part, nullptr);
+    if (opt.null_space)
+      launch_pcg_null_beta(z, vb, g.ncell, part, zpart, state, st);
+    else
+      launch_pcg_beta_fin(part, nparts_apply(), state, st);
+    prof_mark(PROF_BETA);
+    prof_on = false;
+    if (int er = check(cudaStreamSynchronize(st), "profile iteration")) return er;
+    if (int er = check(cudaGetLastError(), "profile iteration launch")) return er;
+    for (int i = 1; i < prof_n; ++i) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, prof_ev[i - 1], prof_ev[i]);
+      const int c_ = prof_slot[i];
+      if (c_ >= 0 && c_ < PROF_SLOTS) {
+        ms[c_] += t;
+        if (rep == 0) launches[c_] += 1;
+      }
+    }
+  }
+  for (int c_ = 0; c_ < PROF_SLOTS; ++c_) ms[c_] /= std::max(1, reps);
+  return 0;
 }
 
 void Solver::apply(const double* x, double* out, double* partial, const int* done) {

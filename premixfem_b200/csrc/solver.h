@@ -42,6 +42,7 @@ struct Options {
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
+  bool eig_allow_unconverged = false;  // keep the Ritz blocks of local eigensolves that hit eig_max_it
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
@@ -174,6 +175,17 @@ class Solver {
   double net_ms = 0.0;
   int run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1);
   int nparts_apply() const { return nsub; }
+  // Per-kernel-class device time of one PCG iteration (profile_iteration):
+  // while prof_on, apply_impl records an event after each launch group,
+  // tagged with its class (PROF_* below).
+  enum { PROF_LV1_FIRST = 0, PROF_LV1_Y, PROF_RESTRICT, PROF_COARSE, PROF_PROLONG, PROF_CG_A, PROF_CG_B, PROF_BETA,
+         PROF_SLOTS };
+  bool prof_on = false;
+  int prof_n = 0;
+  cudaEvent_t prof_ev[64] = {};
+  int prof_slot[64] = {};
+  void prof_mark(int slot);
+  int profile_iteration(int reps, double ms[PROF_SLOTS], int launches[PROF_SLOTS]);
 };
 
 }  // namespace pmf

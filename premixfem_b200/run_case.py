@@ -15,8 +15,9 @@ Cases (subdomains of 16^3 cells unless stated):
              en_lv1 = 4, -ksp_constant_null_space; --n is ignored
   large      n x n x n/2 anisotropic GRF (sigma 3) with fracture planes of
              contrast 1e6, p = 0 on z = 0 (512 x 512 x 256 at n = 512):
-             16^3 subdomains, -sd 8 on an (n/128, n/128, n/256) virtual rank
-             grid, en_lv1 = 8, en_lv2 = 4
+             16^3 subdomains, -sd 4 on an (n/64, n/64, n/128) virtual rank
+             grid (64 subdomains, 512 coarse unknowns per rank), en_lv1 = 8,
+             en_lv2 = 4
   batch      --count independent unit-cube GRF problems (per-axis sizes
              U{24..80}, sigma U[1,3], correlation U[0.05,0.2], p = 0 on
              x = 1), ~8^3 ragged subdomains, en_lv1 = 4; one set-up and four
@@ -59,7 +60,7 @@ def make_case(case, n, seed):
         f = n / 512.0
         prob = fields.large_frac(M=n, N=n, P=n // 2, seed=seed, n_frac=max(1, int(400 * f * f)),
                                  frac_lo=max(4, int(32 * f)), frac_hi=int(256 * f))
-        opts = {"sd": 8, "pmf_vranks": (n // 128, n // 128, n // 256), "en_lv1": 8, "en_lv2": 4}
+        opts = {"sd": 4, "pmf_vranks": (n // 64, n // 64, n // 128), "en_lv1": 8, "en_lv2": 4}
     else:
         raise SystemExit(f"unknown case {case}")
     return prob, opts

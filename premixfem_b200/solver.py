@@ -200,6 +200,26 @@ class DarcySolver:
         _native.check(self.lib.pmf_get_timing(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def learned_stats(self):
+        """Learned start of the last set-up: used (0/1), fallbacks, LOBPCG iterations from the
+        learned start, iterations of the fallbacks, network inference ms."""
+        st = (C.c_longlong * 4)()
+        nm = C.c_double()
+        _native.check(self.lib.pmf_get_learned_stats(self.h, st, C.byref(nm)))
+        return {"used": int(st[0]), "fallbacks": int(st[1]), "learned_iters": int(st[2]),
+                "fallback_iters": int(st[3]), "net_ms": float(nm.value)}
+
+    PROFILE_CLASSES = ("lv1_first", "lv1_with_y", "resid_restrict", "coarse", "prolong", "cg_p_update_Ap",
+                       "cg_x_r_update", "beta")
+
+    def profile_iteration(self, reps=5):
+        """Device ms per PCG iteration by kernel class and launch groups per iteration (see pmf_b200.h)."""
+        ms = np.zeros(8)
+        nl = np.zeros(8, dtype=np.int32)
+        _native.check(self.lib.pmf_profile_iteration(self.h, int(reps), ms.ctypes.data_as(C.c_void_p),
+                                                     nl.ctypes.data_as(C.c_void_p)))
+        return {k: (float(m), int(n)) for k, m, n in zip(self.PROFILE_CLASSES, ms, nl)}
+
 
 # ---------------------------------------------------------------------------
 # The reference's interface (src/PreMixFEM_3D.h:32-67), same names and order.
