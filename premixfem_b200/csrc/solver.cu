@@ -140,6 +140,21 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_init", &o->eig_init);
   db.get_int("pmf_eig_profile", &o->eig_profile);
   o->eig_allow_unconverged = db.has("pmf_eig_allow_unconverged");
+  {
+    auto itk = db.kv.find("pmf_lv1_kernel");
+    if (itk != db.kv.end()) {
+      if (itk->second == "auto")
+        o->lv1_kernel = 0;
+      else if (itk->second == "natural")
+        o->lv1_kernel = 1;
+      else if (itk->second == "blocked")
+        o->lv1_kernel = 2;
+      else {
+        *err = "Error in -pmf_lv1_kernel (auto | natural | blocked)";
+        return 62;
+      }
+    }
+  }
   db.get_int("pmf_pcg_graph", &o->pcg_graph);
   db.get_int("pmf_autotune", &o->autotune);
   {
@@ -282,6 +297,8 @@ Solver::~Solver() {
   if (ev1) cudaEventDestroy(ev1);
   for (auto& e : prof_ev)
     if (e) cudaEventDestroy(e);
+  for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr})
+    if (q) cudaFree(q);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -736,6 +753,14 @@ int Solver::setup() {
     launch_to_f32(diag, diag32, g.ncell, st);
     launch_to_f32(inv64, inv32, g.ncell, st);
   }
+  if (!opt.use_full_Cholesky_lv1) {
+    if (int er = setup_ic_blocked(mixed)) return er;
+    if (opt.lv1_kernel == 2 && !ic_blk_ok) {
+      err = "-pmf_lv1_kernel blocked needs every subdomain 16 cells wide in x with x0 % 4 == 0, M % 4 == 0 and "
+            "ny*nz <= 256";
+      return 56;  // PETSC_ERR_SUP
+    }
+  }
   cudaEventRecord(e[1], st);
   // level-2 local eigenproblems
   if (!d_eig1 || !d_ks || !d_iters || !d_status) {
@@ -1060,6 +1085,84 @@ int Solver::setup_band_cholesky(bool mixed) {
   return check(cudaStreamSynchronize(st), "level-1 Cholesky factorisation");
 }
 
+// The subdomain-blocked copy of the IC(0) factor for k_ic_apply_blk, when
+// every subdomain fits that kernel (16 cells wide in x, 16-byte aligned
+// rows, at most 256 x-lines); rebuilt by every set-up.
+int Solver::setup_ic_blocked(bool mixed) {
+  ic_blk_ok = g.M % 4 == 0 && max_lines <= 256;
+  blk_ny = blk_nz = 0;
+  for (const SubInfo& S : subs) {
+    if (S.nx != 16 || S.x0 % 4) ic_blk_ok = false;
+    blk_ny = std::max(blk_ny, S.ny);
+    blk_nz = std::max(blk_nz, S.nz);
+  }
+  const size_t smem = mixed ? ic_blk_smem_bytes<float>(max_cells, blk_ny, blk_nz)
+                            : ic_blk_smem_bytes<double>(max_cells, blk_ny, blk_nz);
+  if (smem > 227 * 1024) ic_blk_ok = false;
+  if (!d_kerr) {
+    if (int e = dalloc((void**)&d_kerr, sizeof(int), "kernel wait flag")) return e;
+    cudaMemsetAsync(d_kerr, 0, sizeof(int), st);
+  }
+  if (!ic_blk_ok) return 0;
+  if (!d_coff) {
+    std::vector<long long> off(nsub);
+    long long acc = 0;
+    for (int s = 0; s < nsub; ++s) {
+      off[s] = acc;
+      acc += (long long)subs[s].nx * subs[s].ny * subs[s].nz;
+    }
+    if (int e = dalloc((void**)&d_coff, sizeof(long long) * nsub, "blocked factor offsets")) return e;
+    if (int e = dalloc(&ic_coef, (size_t)acc * ic_blk_coef_bytes(mixed ? 4 : 8), "blocked IC(0) factor")) {
+      cudaFree(d_coff);
+      d_coff = nullptr;
+      return e;
+    }
+    cudaMemcpyAsync(d_coff, off.data(), sizeof(long long) * nsub, cudaMemcpyHostToDevice, st);
+    // the host vector must outlive the asynchronous copy
+    if (int e = check(cudaStreamSynchronize(st), "blocked factor offsets")) return e;
+  }
+  if (mixed)
+    launch_pack_ic_coef<float>(g, d_subs, nsub, d_coff, tx32, ty32, tz32, inv32, ic_coef, st);
+  else
+    launch_pack_ic_coef<double>(g, d_subs, nsub, d_coff, tx, ty, tz, inv64, ic_coef, st);
+  return 0;
+}
+
+// A bounded wait inside a kernel ran out (the kernel recorded it and returned
+// without computing): report it as a library failure.
+int Solver::check_kernel_flag(const char* what) {
+  if (!d_kerr) return 0;
+  int f = 0;
+  if (int e = check(cudaMemcpy(&f, d_kerr, sizeof(int), cudaMemcpyDeviceToHost), what)) return e;
+  if (f) {
+    cudaMemset(d_kerr, 0, sizeof(int));
+    err = std::string(what) + ": a level-1 kernel's wait for its bulk copy ran out";
+    return 76;
+  }
+  return 0;
+}
+
+// One level-1 visit: out = yin + IC^-1 (x - A yin) with the tuned kernel.
+template <typename T>
+void Solver::launch_lv1(const double* x, const T* yin, T* out_t, double* out_d, double* partial, const int* done) {
+  const bool f32 = sizeof(T) == 4;
+  const T* ttx = f32 ? (const T*)tx32 : (const T*)tx;
+  const T* tty = f32 ? (const T*)ty32 : (const T*)ty;
+  const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
+  const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
+  // the blocked kernel reads and writes 16-byte vectors: a caller's vector at
+  // an odd offset takes the natural-order kernel
+  auto al16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+  if (ic_variant == 1 && ic_blk_ok && al16(x) && al16(yin) && al16(out_t) && al16(out_d)) {
+    launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, blk_ny, blk_nz, d_coff, ic_coef, ttx, tty, ttz, tdg, x, yin,
+                           out_t, out_d, partial, done, d_kerr, st);
+  } else {
+    const T* tinv = f32 ? (const T*)inv32 : (const T*)inv64;
+    launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, out_t, out_d,
+                       partial, done, st, ic_threads);
+  }
+}
+
 // Threads per subdomain of the level-1 solve and of the level-2 restriction /
 // prolongation, chosen by the launch-shape tuner on scratch buffers (the first
 // set-up of a shape times every candidate; later set-ups reuse the choice).
@@ -1077,7 +1180,7 @@ void Solver::tune_pc() {
   cudaMemsetAsync(ya, 0, sizeof(T) * g.ncell, st);
   cudaMemsetAsync(z, 0, sizeof(double) * g.ncell, st);
   cudaMemsetAsync(Zacc, 0, sizeof(double) * nsub * kmax, st);
-  const int old[4] = {ic_threads, rr_threads, pr_threads, pcga_variant};
+  const int old[5] = {ic_threads, rr_threads, pr_threads, pcga_variant, ic_variant};
   char key[192];
   const char* prec = f32 ? "f32" : "f64";
   if (!opt.use_full_Cholesky_lv1) {
@@ -1085,13 +1188,23 @@ void Solver::tune_pc() {
     std::vector<int> cand = {base};
     for (int t : {384, 512, 768, 1024})
       if (t > base) cand.push_back(t);
-    snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d", prec, nsub, max_cells, max_lines);
-    const int ci = tune_choose(key, (int)cand.size(), [&](int i) {
-      launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, ya, yo, nullptr,
-                         nullptr, nullptr, st, cand[i]);
+    // candidates: the natural-order kernel with each thread count, then the
+    // blocked kernel (the last candidate, when every subdomain fits it)
+    const int nnat = (int)cand.size();
+    snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d|b%d", prec, nsub, max_cells, max_lines, ic_blk_ok ? 1 : 0);
+    const int ci = tune_choose(key, nnat + (ic_blk_ok ? 1 : 0), [&](int i) {
+      if (i < nnat)
+        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, ya, yo, nullptr,
+                           nullptr, nullptr, st, cand[i]);
+      else
+        launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, blk_ny, blk_nz, d_coff, ic_coef, ttx, tty, ttz, tdg, z,
+                               ya, yo, nullptr, nullptr, nullptr, d_kerr, st);
       return true;
     }, st);
-    ic_threads = cand[ci];
+    ic_variant = ci >= nnat ? 1 : 0;
+    ic_threads = cand[std::min(ci, nnat - 1)];
+    if (opt.lv1_kernel == 1) ic_variant = 0;
+    if (opt.lv1_kernel == 2) ic_variant = 1;  // eligibility checked by setup()
   }
   const int rcand[3] = {256, 128, 512};
   snprintf(key, sizeof(key), "resid_restrict|%s|n%d|c%d|k%d", prec, nsub, max_cells, kmax);
@@ -1117,7 +1230,8 @@ void Solver::tune_pc() {
       return true;
     }, st);
   }
-  if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads || old[3] != pcga_variant)) {
+  if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads || old[3] != pcga_variant ||
+                   old[4] != ic_variant)) {
     cudaGraphExecDestroy(pcg_exec);  // captured with other launch shapes
     pcg_exec = nullptr;
     pcg_graph_x = nullptr;
@@ -1131,7 +1245,6 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
   const T* tty = f32 ? (const T*)ty32 : (const T*)ty;
   const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
   const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
-  const T* tinv = f32 ? (const T*)inv32 : (const T*)inv64;
   const T* tphi = (const T*)phi;
   T* yb[2] = {(T*)y0, (T*)y1};
   const std::vector<int> sch = schedule();
@@ -1160,11 +1273,9 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
           cur = 1 - cur;
         }
       } else if (last)
-        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, nullptr, out,
-                           partial, done, st, ic_threads);
+        launch_lv1<T>(x, yin, nullptr, out, partial, done);
       else {
-        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, yb[1 - cur],
-                           nullptr, nullptr, done, st, ic_threads);
+        launch_lv1<T>(x, yin, yb[1 - cur], nullptr, nullptr, done);
         cur = 1 - cur;
       }
       prof_mark(lv1_slot);
@@ -1326,6 +1437,7 @@ int Solver::pc_apply(const double* x_in, double* y_out, bool on_device) {
   if (!on_device) cudaMemcpyAsync(y_out, ys, n * 8, cudaMemcpyDeviceToHost, st);
   int e = check(cudaStreamSynchronize(st), "PC_apply_vec");
   if (!e) e = check(cudaGetLastError(), "PC_apply_vec launch");
+  if (!e) e = check_kernel_flag("PC_apply_vec");
   float ms = 0;
   cudaEventElapsedTime(&ms, ev0, ev1);
   t_stages[ST_AV] += ms * 1e-3;
@@ -1409,6 +1521,7 @@ int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, d
   cudaEventRecord(ev1, st);
   if (!on_device) cudaMemcpyAsync(x_out, xs, n * 8, cudaMemcpyDeviceToHost, st);
   int e = check(cudaStreamSynchronize(st), "KSPSolve");
+  if (!e) e = check_kernel_flag("KSPSolve");
   float ms = 0;
   cudaEventElapsedTime(&ms, ev0, ev1);
   last_solve_ms = ms;

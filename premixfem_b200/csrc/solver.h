@@ -43,6 +43,7 @@ struct Options {
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
   bool eig_allow_unconverged = false;  // keep the Ritz blocks of local eigensolves that hit eig_max_it
+  int lv1_kernel = 0;  // level-1 solve kernel: 0 the tuner's choice, 1 natural-order, 2 subdomain-blocked
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
@@ -165,6 +166,17 @@ class Solver {
   template <typename T>
   void tune_pc();
   int ic_threads = 0, rr_threads = 256, pr_threads = 256, pcga_variant = 0;  // tuned launch shapes
+  // level-1 solve with the subdomain-blocked IC(0) factor (k_ic_apply_blk)
+  bool ic_blk_ok = false;  // every subdomain fits the blocked kernel
+  int ic_variant = 0;      // 0 natural-order kernel, 1 blocked kernel (tuner's choice)
+  int blk_ny = 0, blk_nz = 0;
+  long long* d_coff = nullptr;  // per subdomain: first cell in the blocked arrays
+  void* ic_coef = nullptr;      // blocked {tx, ty, tz, 1/D} (precision of the preconditioner)
+  int* d_kerr = nullptr;        // set by a kernel whose bounded wait ran out
+  int check_kernel_flag(const char* what);
+  int setup_ic_blocked(bool mixed);
+  template <typename T>
+  void launch_lv1(const double* x, const T* yin, T* out_t, double* out_d, double* partial, const int* done);
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;
