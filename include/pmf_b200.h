@@ -42,13 +42,16 @@ typedef struct pmf_solver pmf_solver;
  * extensions: -pmf_sd sx,sy,sz (subdomains per
  * rank and axis), -pmf_vranks px,py,pz (virtual DMDA process grid),
  * -pmf_precision fp64|mixed, -pmf_eig_tol, -pmf_eig_max_it (a local eigensolve
- * that spends it makes pmf_setup fail with 83, as the reference's SLEPc check
- * does, unless -pmf_eig_allow_unconverged keeps its last block), -pmf_learned
+ * that spends it keeps its last Ritz block and reports status 1; with
+ * -pmf_eig_require_converged pmf_setup fails with 83 instead, as the
+ * reference's SLEPc check does), -pmf_learned
  * <weights file> (learned initial blocks for the local eigensolves),
  * -pmf_learned_its N and -pmf_learned_tol t (a subdomain whose LOBPCG from the
  * learned start has not reached relative residual t within N iterations is
- * solved again from a random start at the normal tolerance; defaults 30 and
- * 1e-4), -pmf_eig_batched 0|1 and -pmf_eig_final 0|1 (phase-batched
+ * solved again from a random start at the normal tolerance; defaults 60 and
+ * the eigensolver's own tolerance, so a learned start is held to the same
+ * accuracy as a random one; t can only loosen it), -pmf_eig_batched 0|1 and
+ * -pmf_eig_final 0|1 (phase-batched
  * eigensolver and its batched final phase, both on by default),
  * -pmf_eig_init 0|1 (set-up phase as batched kernels, off by default),
  * -pmf_eig_rel_floor f (0 <= f < 1; > 0: the local eigensolves stop when

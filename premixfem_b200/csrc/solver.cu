@@ -139,7 +139,7 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_final", &o->eig_final);
   db.get_int("pmf_eig_init", &o->eig_init);
   db.get_int("pmf_eig_profile", &o->eig_profile);
-  o->eig_allow_unconverged = db.has("pmf_eig_allow_unconverged");
+  o->eig_require_converged = db.has("pmf_eig_require_converged");
   {
     auto itk = db.kv.find("pmf_lv1_kernel");
     if (itk != db.kv.end()) {
@@ -889,15 +889,15 @@ int Solver::setup() {
   cudaMemcpy(eig_status.data(), d_status, sizeof(int) * nsub, cudaMemcpyDeviceToHost);
   cudaMemcpy(eig1.data(), d_eig1, sizeof(double) * eig1.size(), cudaMemcpyDeviceToHost);
   {
-    // SLEPc "cannot find enough eigenvectors" (src/PreMixFEM_3D.c:367):
-    // a local eigensolve that used its whole iteration budget is an error
-    // unless -pmf_eig_allow_unconverged keeps its last Ritz block
+    // A local eigensolve that used its whole iteration budget keeps its last
+    // Ritz block (status 1, counted by pmf_get_eigen_lv1); with
+    // -pmf_eig_require_converged it is an error instead, as SLEPc's "cannot
+    // find enough eigenvectors" is in the reference (src/PreMixFEM_3D.c:367)
     int nmax = 0;
     for (int s_ = 0; s_ < nsub; ++s_) nmax += eig_status[s_] == 1;
-    if (nmax && !opt.eig_allow_unconverged) {
+    if (nmax && opt.eig_require_converged) {
       err = "local eigensolver did not converge on " + std::to_string(nmax) + " of " + std::to_string(nsub) +
-            " subdomains within -pmf_eig_max_it " + std::to_string(opt.eig_max_it) +
-            " iterations (-pmf_eig_allow_unconverged keeps the unconverged blocks)";
+            " subdomains within -pmf_eig_max_it " + std::to_string(opt.eig_max_it) + " iterations";
       return 83;  // PETSC_ERR_USER
     }
   }
@@ -1218,13 +1218,18 @@ void Solver::tune_pc() {
     return true;
   }, st)];
   // the CG step's fused p-update + operator kernel: 2.5-D march or grid-stride
-  // (the main kernel alone is timed; the state says first step, not done)
+  // (the main kernel alone is timed, in the state of a later iteration, whose
+  // p = z + (beta/betaold) p reads the previous p; not done)
   {
     PcgState hs;
     memset(&hs, 0, sizeof(hs));
-    hs.first = 1;
-    cudaMemcpy(state, &hs, sizeof(hs), cudaMemcpyHostToDevice);
-    snprintf(key, sizeof(key), "pcg_iter_a|M%d|N%d|P%d", g.M, g.N, g.P);
+    hs.first = 0;
+    hs.beta = hs.betaold = 1.0;
+    hs.dpi = 1.0;
+    cudaMemsetAsync(p0, 0, sizeof(double) * g.ncell, st);
+    cudaMemcpyAsync(state, &hs, sizeof(hs), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    snprintf(key, sizeof(key), "pcg_iter_a|M%d|N%d|P%d|p", g.M, g.N, g.P);
     pcga_variant = tune_choose(key, 2, [&](int i) {
       launch_pcg_iter_a_main(g, tx, ty, tz, diag, z, p0, p1, w, part, state, st, i);
       return true;
@@ -1344,6 +1349,7 @@ int Solver::profile_iteration(int reps, double ms[PROF_SLOTS], int launches[PROF
   PcgState hs;
   memset(&hs, 0, sizeof(hs));
   hs.beta = hs.betaold = 1.0;
+  hs.dpi = 1.0;  // a positive previous p.Ap: the indefinite test compares signs
   hs.max_it = 1 << 30;
   cudaMemcpyAsync(vb, r, sizeof(double) * g.ncell, cudaMemcpyDeviceToDevice, st);
   cudaMemsetAsync(vx, 0, sizeof(double) * g.ncell, st);

@@ -42,15 +42,15 @@ struct Options {
   int eig_ctas = 0;  // persistent CTAs of the batched eigensolver (0: one per SM)
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
-  bool eig_allow_unconverged = false;  // keep the Ritz blocks of local eigensolves that hit eig_max_it
+  bool eig_require_converged = false;  // a local eigensolve that hits eig_max_it fails the set-up (error 83)
   int lv1_kernel = 0;  // level-1 solve kernel: 0 the tuner's choice, 1 natural-order, 2 subdomain-blocked
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
   // from a random start with the full iteration budget
   std::string learned_path;
-  int learned_its = 30;
-  double learned_tol = 1e-4;  // Ritz-residual gate of the learned start
+  int learned_its = 60;
+  double learned_tol = -1.0;  // Ritz-residual gate of the learned start (< 0: the eigensolver's own tolerance)
 };
 
 // PETSc-style options database ("-name value" pairs); flags carry an empty value.

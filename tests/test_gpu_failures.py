@@ -2,7 +2,9 @@
 
 The reference stops with a PETSc error where its libraries fail:
   * SLEPc finds fewer than en_lv1 local eigenpairs (src/PreMixFEM_3D.c:367,
-    PETSC_ERR_USER; level 3 at :1098);
+    PETSC_ERR_USER; level 3 at :1098) -- here with -pmf_eig_require_converged,
+    since by default a local eigensolve that spends its iterations keeps its
+    last Ritz block;
   * a factorisation meets a zero pivot (the local KSPs are set up with
     KSPSetErrorIfNotConverged, :212, :725, :903, :1376);
   * PETSc's KSPConvergedDefault ends a solve whose residual norm is NaN or Inf
@@ -80,15 +82,15 @@ def test_nonpositive_kappa_gives_zero_pivot_error(native, bad_kappa, precision):
 def test_eigensolver_iteration_budget(native, precision):
     prob = fields.unit_cube_grf(16, seed=3)
     opts = options_string(dict(OPTS, pmf_precision=precision, pmf_eig_max_it=1))
-    s = DarcySolver.from_problem(prob, opts)
+    s = DarcySolver.from_problem(prob, opts + " -pmf_eig_require_converged")
     with pytest.raises(PmfError) as e:
         s.setup()
     assert e.value.code == 83, e.value
     assert "did not converge" in str(e.value)
     s.close()
-    # -pmf_eig_allow_unconverged keeps the one-step Ritz blocks: the set-up
-    # completes, reports status 1 (max_it) and the solve still converges
-    s = DarcySolver.from_problem(prob, opts + " -pmf_eig_allow_unconverged")
+    # by default the one-step Ritz blocks are kept: the set-up completes,
+    # reports status 1 (max_it) and the solve still converges
+    s = DarcySolver.from_problem(prob, opts)
     s.setup()
     ev, ks, iters, status = s.eigen_lv1()
     assert (status == 1).any()
