@@ -408,6 +408,15 @@ def chol_semidef(A, rel_tol=1.0e-14):
     A = np.array(A, dtype=np.float64, copy=True)
     n = A.shape[0]
     scale = max(np.max(np.abs(np.diag(A))), 1e-300)
+    if n > 2048:
+        # large matrices: LAPACK's Cholesky, which is the loop below whenever no
+        # pivot falls to the null threshold (checked on the computed pivots)
+        try:
+            Lf = sla.cholesky(A, lower=True, check_finite=False)
+            if np.all(np.diag(Lf) ** 2 > rel_tol * scale):
+                return Lf, np.zeros(n, dtype=bool)
+        except sla.LinAlgError:
+            pass
     L = np.zeros_like(A)
     null = np.zeros(n, dtype=bool)
     for j in range(n):

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "pmf_common.cuh"
 
 namespace pmf {
@@ -144,6 +146,27 @@ void launch_assemble_dense(const SubInfo* subs, int nsub, int nrank, int spr, in
                            const double* gface, int mode, double* dense, cudaStream_t st);
 // In-place batched SPD inverse by Gauss-Jordan; pivots <= tol*max|diag| are null directions.
 void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st);
+
+// ---- -use_2level: banded Cholesky of the global coarse matrix (k_coarse_band.cu) ----
+struct CBandPlan {
+  long long nc = 0;   // coarse unknowns (nsub x kmax)
+  long long b = 0;    // half-bandwidth in subdomain-grid order
+  int B = 0;          // tile bandwidth (64 x 64 tiles)
+  int NS = 0;         // superblocks of B tiles
+  long long NTp = 0;  // tiles per side, padded to NS x B
+  std::vector<int> perm;  // grid-order dof -> natural coarse dof (s x kmax + j), -1 for padding
+  size_t tile_bytes = 0, T_bytes = 0, X_bytes = 0;
+};
+// grid: subdomains per axis; returns 62 if the boxes do not form that grid
+int cband_plan(const std::vector<SubInfo>& subs, const int grid[3], int kmax, CBandPlan* p);
+// A2 (+ shift on the diagonal) -> tile-band Cholesky factor T and superblock inverses X; nullf
+// (NTp x 64 ints) flags null pivots (<= tol x max|diag|), nnull counts them; scale: one device double
+void launch_cband_factor(const SubInfo* subs, int kmax, const double* blk, const int* d_perm, const CBandPlan& p,
+                         double shift, double tol, double* T, double* X, int* nullf, int* nnull, double* scale,
+                         cudaStream_t st);
+// out = A2^+ c (natural coarse order); v, y, t: work vectors of NTp x 64 doubles
+void launch_cband_solve(const int* d_perm, const CBandPlan& p, const double* T, const double* X, const double* c,
+                        double* out, double* v, double* y, double* t, const int* done, cudaStream_t st);
 
 // ---- eigen solvers -----------------------------------------------------------------
 struct LobpcgArgs {

@@ -288,7 +288,10 @@ Solver::~Solver() {
                   (void*)eb.alist, (void*)eb.colcells})
     if (p) cudaFree(p);
   if (eb.h_nactive) cudaFreeHost(eb.h_nactive);
-  for (void* p : {(void*)A2g, (void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
+  for (void* p : {(void*)cb_T, (void*)cb_X, (void*)cb_v, (void*)cb_y, (void*)cb_t, (void*)cb_perm, (void*)cb_null,
+                  (void*)cb_scale})
+    if (p) cudaFree(p);
+  for (void* p : {(void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
                   (void*)d_status_learned, (void*)d_boff, (void*)band64, (void*)band32})
     if (p) cudaFree(p);
   delete net;
@@ -401,13 +404,7 @@ int Solver::build_partition() {
   nr = spr * kmax;
   en2 = std::min(opt.en_lv2, nr);
   n3 = nrank * en2;
-  if (opt.use_2level) {
-    if ((long long)nsub * kmax > 8192) {
-      err = "-use_2level: the global coarse problem (subdomains * en_lv1) must have <= 8192 unknowns for the "
-            "dense coarse solver";
-      return 56;
-    }
-  } else if (nr > 4096 || n3 > 8192) {
+  if (!opt.use_2level && (nr > 4096 || n3 > 8192)) {
     err = "coarse blocks too large (subdomains per rank * en_lv1 <= 4096, ranks * en_lv2 <= 8192)";
     return 62;
   }
@@ -971,17 +968,9 @@ int Solver::setup() {
   };
   if (opt.use_2level) {
     // _PC_setup_lv2_c (:423-735): the global Galerkin matrix Phi^T A Phi over all
-    // subdomains (+ NIL I unless -no_shift_A_cc), inverted densely
-    const long long nc = (long long)nsub * kmax;
-    if (!A2g) {
-      if (int er = check(cudaMalloc(&A2g, sizeof(double) * nc * nc), "cudaMalloc global coarse matrix")) return er;
-    }
-    launch_assemble_dense(d_subs, nsub, 1, nsub, kmax, blk, gface, 0, A2g, st);
-    if (!opt.no_shift_A_cc) {
-      note_launch();
-      k_add_diag<<<1, 256, 0, st>>>(1, (int)nc, A2g, 1.0e-12, 0);
-    }
-    launch_spd_inverse(1, (int)nc, A2g, 1e-14, d_flag + 1, st);
+    // subdomains (+ NIL I unless -no_shift_A_cc), factorised by the banded
+    // Cholesky in subdomain-grid order (k_coarse_band.cu)
+    if (int er = setup_two_level()) return er;
     cudaEventRecord(e[3], st);
     cudaEventRecord(e[4], st);
     cudaEventRecord(e[5], st);
@@ -1040,6 +1029,51 @@ int Solver::setup() {
   launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
   cudaEventRecord(e[5], st);
   return finish();
+}
+
+// -use_2level: plan, allocate (once per plan) and factorise the banded
+// global coarse matrix.  The factor and the superblock inverses take
+// T_bytes + X_bytes of device memory (about 0.65 GB for 24 576 unknowns,
+// 8.8 GB for 131 072); a device without room for them gets error 55.
+int Solver::setup_two_level() {
+  const int grid[3] = {opt.vranks[0] * opt.sd[0], opt.vranks[1] * opt.sd[1], opt.vranks[2] * opt.sd[2]};
+  CBandPlan p;
+  if (int e = cband_plan(subs, grid, kmax, &p)) {
+    err = "-use_2level: the subdomains do not form a grid";
+    return e;
+  }
+  const size_t vec = (size_t)p.NTp * 64 * sizeof(double);
+  if (!cb_T || p.NTp != cband.NTp || p.B != cband.B) {
+    for (void** q : {(void**)&cb_T, (void**)&cb_X, (void**)&cb_v, (void**)&cb_y, (void**)&cb_t, (void**)&cb_perm,
+                     (void**)&cb_null, (void**)&cb_scale}) {
+      if (*q) cudaFree(*q);
+      *q = nullptr;
+    }
+    size_t freeb = 0, totb = 0;
+    cudaMemGetInfo(&freeb, &totb);
+    const size_t need = p.T_bytes + p.X_bytes + 3 * vec + p.perm.size() * 8 + (256u << 20);
+    if (need > freeb) {
+      err = "-use_2level: not enough device memory for the banded coarse factor (" + std::to_string(need >> 20) +
+            " MiB needed, " + std::to_string(freeb >> 20) + " MiB free)";
+      return 55;  // PETSC_ERR_MEM
+    }
+    int e = dalloc((void**)&cb_T, p.T_bytes, "coarse band factor");
+    if (!e) e = dalloc((void**)&cb_X, p.X_bytes, "coarse superblock inverses");
+    if (!e) e = dalloc((void**)&cb_v, vec, "coarse work");
+    if (!e) e = dalloc((void**)&cb_y, vec, "coarse work");
+    if (!e) e = dalloc((void**)&cb_t, vec, "coarse work");
+    if (!e) e = dalloc((void**)&cb_perm, p.perm.size() * sizeof(int), "coarse ordering");
+    if (!e) e = dalloc((void**)&cb_null, p.perm.size() * sizeof(int), "coarse null flags");
+    if (!e) e = dalloc((void**)&cb_scale, sizeof(double), "coarse scale");
+    if (e) return e;
+    cudaMemcpyAsync(cb_perm, p.perm.data(), p.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    // the plan's host vector must outlive the copy
+    if (int er = check(cudaStreamSynchronize(st), "coarse ordering")) return er;
+  }
+  cband = p;
+  launch_cband_factor(d_subs, kmax, blk, cb_perm, cband, opt.no_shift_A_cc ? 0.0 : 1.0e-12, 1e-14, cb_T, cb_X,
+                      cb_null, d_flag + 1, cb_scale, st);
+  return 0;
 }
 
 // -use_full_Cholesky_lv1 (src/PreMixFEM_3D.c:205-207): banded Cholesky factors
@@ -1301,7 +1335,7 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
       if (v == 2) {
         launch_block_gemv(nrank, nr, A2inv, c, dz, 0, done, st);
       } else if (v == 4) {  // _PC_apply_vec_lv2_2level (:1481-1537)
-        launch_block_gemv(1, (int)ncoarse, A2g, c, dz, 0, done, st);
+        launch_cband_solve(cb_perm, cband, cb_T, cb_X, c, dz, cb_v, cb_y, cb_t, done, st);
       } else {
         launch_lv3_restrict(nrank, nr, en2, V3, c, d3, done, st);
         launch_block_gemv(1, n3, A3inv, d3, w3, 0, done, st);

@@ -180,7 +180,11 @@ class Solver {
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;
-  double* A2g = nullptr;  // -use_2level: inverse of the global coarse matrix
+  // -use_2level: banded Cholesky of the global coarse matrix (k_coarse_band.cu)
+  CBandPlan cband;
+  double *cb_T = nullptr, *cb_X = nullptr, *cb_v = nullptr, *cb_y = nullptr, *cb_t = nullptr, *cb_scale = nullptr;
+  int *cb_perm = nullptr, *cb_null = nullptr;
+  int setup_two_level();
   int *d_fail_list = nullptr, *d_fail_count = nullptr, *d_iters_learned = nullptr, *d_status_learned = nullptr;
   int learned_used = 0, learned_fallbacks = 0;
   long long learned_iters = 0, fallback_iters = 0;
