@@ -1504,8 +1504,9 @@ __global__ void __launch_bounds__(256) k_eb_rr(EbArgs a, double drop) {
 }
 
 // X <- S Y, P <- [W P] Y_WP (and the FP64 A-images in FP64 storage), per chunk.
-// NK / NJ: k-steps and 8-column tiles of the tensor-core update (6 / 1 for m <= 8).
-template <typename T, int NK, int NJ>
+// NK / NJ: k-steps and 8-column tiles of the tensor-core update (6 / 1 for m <= 8);
+// ST: groups of 8 cells each warp has loading while it multiplies one (1 or 2).
+template <typename T, int NK, int NJ, int ST>
 __global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
   __shared__ double Ys[LB_LD * LB_LD];
   const int s = eb_sub(a, blockIdx.y);
@@ -1521,9 +1522,9 @@ __global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
   __syncthreads();
   EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
   const int m = a.m;
-  cta_update_mma<T, NK, NJ, 1>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+  cta_update_mma<T, NK, NJ, ST>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
   if (sizeof(T) == 8)
-    cta_update_mma<double, NK, NJ, 1>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+    cta_update_mma<double, NK, NJ, ST>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
 }
 
 // ---- final phase (k_lobpcg mode 2 as phase kernels over every subdomain of
@@ -1984,8 +1985,9 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   const size_t gram_smem = (size_t)8 * 32 * 32 * sizeof(double);
   const size_t rr_smem = sizeof(LbSmall) + sizeof(LbMats);
   cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem_max);
-  // basis update tiles: <6,1> (3 CTAs per SM) is the built-in for m <= 8, <8,2> the alternative
-  const int nupd = a.m <= 8 ? 2 : 1;
+  // basis update tiles: <6,1> (3 CTAs per SM) is the built-in for m <= 8, <8,2> the alternative;
+  // candidates 2 / 3 are the same tiles with two groups of cells loading ahead per warp
+  const int nupd = a.m <= 8 ? 4 : 2;
   char kpre[96], kupd[96];
   snprintf(kpre, sizeof(kpre), "eb_precond|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
   snprintf(kupd, sizeof(kupd), "eb_update|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
@@ -2052,9 +2054,13 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     note_launch();
     cudaEventRecord(tev[2], st);
     if (a.m <= 8 && uc == 0)
-      k_eb_update<T, 6, 1><<<gchunk, 256, 0, st>>>(e);
+      k_eb_update<T, 6, 1, 1><<<gchunk, 256, 0, st>>>(e);
+    else if (a.m <= 8 && uc == 2)
+      k_eb_update<T, 6, 1, 2><<<gchunk, 256, 0, st>>>(e);
+    else if (uc == 3 || (a.m > 8 && uc == 1))
+      k_eb_update<T, 8, 2, 2><<<gchunk, 256, 0, st>>>(e);
     else
-      k_eb_update<T, 8, 2><<<gchunk, 256, 0, st>>>(e);
+      k_eb_update<T, 8, 2, 1><<<gchunk, 256, 0, st>>>(e);
     cudaEventRecord(tev[3], st);
     prev_pc = pc;
     prev_uc = uc;
