@@ -526,11 +526,97 @@ static bool spd_inverse_cl(int nb, int n, double* a, double tol, int* nnull, cud
   return true;
 }
 
+// The same Gauss-Jordan inverse spread over the whole GPU, for matrices too
+// large for one cluster: per pivot k, k_gj_pivot (one CTA per matrix) takes
+// column k and the scaled pivot row into scratch, and k_gj_update applies the
+// rank-1 update to every element of every matrix in parallel, with
+// k_spd_inverse's arithmetic per element (so the results agree bit for bit).
+__global__ void k_gj_scale(int n, const double* a_all, double* scale) {
+  const double* a = a_all + (long long)blockIdx.x * n * n;
+  __shared__ double red[32];
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(a[(long long)i * n + i]));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) red[wid] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) m = fmax(m, red[w]);
+    scale[blockIdx.x] = m > 0 ? m : 1.0;
+  }
+}
+__global__ void k_gj_pivot(int n, const double* a_all, int k, double tol, const double* scale, double* colk,
+                           double* rowk, int* nullk, int* nnull) {
+  const long long b = blockIdx.x;
+  const double* a = a_all + b * n * n;
+  const double piv = a[(long long)k * n + k];
+  const bool isnull = !(piv > tol * scale[b]);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    colk[b * n + i] = a[(long long)i * n + k];
+    rowk[b * n + i] = isnull ? 0.0 : (i == k ? 1.0 : a[(long long)k * n + i]) / piv;
+  }
+  if (threadIdx.x == 0) {
+    nullk[b] = isnull ? 1 : 0;
+    if (isnull && nnull) atomicAdd(nnull, 1);
+  }
+}
+__global__ void k_gj_update(int n, double* a_all, int k, const double* colk, const double* rowk, const int* nullk) {
+  const long long b = blockIdx.y;
+  double* a = a_all + b * n * n;
+  const long long nn = (long long)n * n;
+  const bool isnull = nullk[b] != 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    if (isnull) {
+      if (i == k || j == k) a[e] = 0.0;
+    } else if (i == k) {
+      a[e] = rowk[b * n + j];
+    } else {
+      a[e] = (j == k ? 0.0 : a[e]) - colk[b * n + i] * rowk[b * n + j];
+    }
+  }
+}
+__global__ void k_gj_sym(int n, double* a_all) {
+  double* a = a_all + (long long)blockIdx.y * n * n;
+  const long long nn = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    if (j > i) {
+      const double v = 0.5 * (a[e] + a[(long long)j * n + i]);
+      a[e] = v;
+      a[(long long)j * n + i] = v;
+    }
+  }
+}
+
 void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
   const int R = (n + kSpdCl - 1) / kSpdCl;
   if (n <= 128 && R <= kSpdWarps && spd_inverse_cl<4, 1>(nb, n, a, tol, nnull, st)) return;
   if (n > 128 && n <= 256 && R <= 2 * kSpdWarps && spd_inverse_cl<8, 2>(nb, n, a, tol, nnull, st)) return;
   if (n > 256 && n <= 384 && R <= 3 * kSpdWarps && spd_inverse_cl<12, 3>(nb, n, a, tol, nnull, st)) return;
+  if (n > 384) {
+    // scratch: per matrix the scale, column k, the scaled row k and the null flag
+    double* scr = nullptr;
+    const size_t bytes = sizeof(double) * (size_t)nb * (2 * (size_t)n + 2);
+    if (cudaMallocAsync((void**)&scr, bytes, st) == cudaSuccess) {
+      double* scale = scr;
+      double* colk = scr + nb;
+      double* rowk = colk + (size_t)nb * n;
+      int* nullk = reinterpret_cast<int*>(rowk + (size_t)nb * n);
+      { note_launch(); k_gj_scale<<<nb, 256, 0, st>>>(n, a, scale); }
+      const long long nn = (long long)n * n;
+      const int gx = (int)std::max<long long>(1, std::min<long long>((nn + 255) / 256, (148 * 8 + nb - 1) / nb));
+      for (int k = 0; k < n; ++k) {
+        { note_launch(); k_gj_pivot<<<nb, 256, 0, st>>>(n, a, k, tol, scale, colk, rowk, nullk, nnull); }
+        { note_launch(); k_gj_update<<<dim3(gx, nb), 256, 0, st>>>(n, a, k, colk, rowk, nullk); }
+      }
+      { note_launch(); k_gj_sym<<<dim3(gx, nb), 256, 0, st>>>(n, a); }
+      cudaFreeAsync(scr, st);
+      return;
+    }
+    (void)cudaGetLastError();  // no scratch: the one-CTA kernel below
+  }
   const int smem = 2 * n * sizeof(double);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   { note_launch(); k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull); }

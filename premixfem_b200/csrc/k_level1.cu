@@ -12,19 +12,18 @@
 //   1. thread 0 starts a cp.async.bulk copy of the subdomain's coefficient
 //      block (64 KB for 16^3 FP32 cells) into shared memory, completed on an
 //      mbarrier;
-//   2. meanwhile every thread (one per x-line (j, k)) loads its line of the
-//      residual x (FP64) and, when the visit has an iterate y, its line of y
-//      and of the diagonal with 16-byte vector loads, and the threads on the
-//      subdomain's faces load the neighbouring cells of y and the couplings
-//      of the upper faces;
-//   3. r = x - A y on the subdomain (the same operations in the same order as
-//      the natural-order kernel, so the result is bit-identical), then the
-//      forward and backward hyperplane sweeps in shared memory, and the line
-//      is written out (y + IC^-1 r, as the preconditioner's FP32 iterate or
-//      the FP64 result with the z.r partial).
+//   2. meanwhile the threads stage the subdomain's residual x (and, when the
+//      visit has an iterate, y) in shared memory with coalesced loads;
+//   3. r = x - A y on the subdomain (the natural-order kernel's operations in
+//      its order; the two kernels differ only where the compiler contracts a
+//      multiply-add differently), then the forward and backward hyperplane
+//      sweeps in shared memory, and the result is written out (y + IC^-1 r,
+//      as the preconditioner's FP32 iterate or the FP64 result with the z.r
+//      partial).
 //
-// With 16^3 FP32 subdomains a CTA uses 89 KB of shared memory, so two CTAs
-// share an SM and one's copy overlaps the other's sweeps.  The only wait is
+// With 16^3 FP32 subdomains a CTA uses 81 KB of shared memory (97 KB with an
+// iterate), so two CTAs share an SM and one's copy overlaps the other's
+// sweeps.  The only wait is
 // thread 0's on the mbarrier, bounded by an iteration limit: if the copy had
 // not landed by then the CTA records the failure in *err and returns without
 // touching the data (the host turns the flag into an error code).
@@ -83,55 +82,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
   return ok != 0;
 }
 
-// 16 consecutive values with 16-byte loads / stores (16-byte aligned address)
-__device__ __forceinline__ void load16(const float* p, float (&r)[kNX]) {
-  const float4* q = reinterpret_cast<const float4*>(p);
-#pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    const float4 a = q[v];
-    r[4 * v] = a.x;
-    r[4 * v + 1] = a.y;
-    r[4 * v + 2] = a.z;
-    r[4 * v + 3] = a.w;
-  }
-}
-__device__ __forceinline__ void load16(const double* p, double (&r)[kNX]) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    const double2 a = q[v];
-    r[2 * v] = a.x;
-    r[2 * v + 1] = a.y;
-  }
-}
-__device__ __forceinline__ void store16(float* p, const float (&r)[kNX]) {
-  float4* q = reinterpret_cast<float4*>(p);
-#pragma unroll
-  for (int v = 0; v < 4; ++v) q[v] = make_float4(r[4 * v], r[4 * v + 1], r[4 * v + 2], r[4 * v + 3]);
-}
-__device__ __forceinline__ void store16(double* p, const double (&r)[kNX]) {
-  double2* q = reinterpret_cast<double2*>(p);
-#pragma unroll
-  for (int v = 0; v < 8; ++v) q[v] = make_double2(r[2 * v], r[2 * v + 1]);
-}
-
 }  // namespace
 
 // Shared-memory layout of k_ic_apply_blk (bytes): header (mbarrier, flag,
 // reduction scratch) 512, coefficients ldc x sizeof(V4), u ldc x sizeof(T),
-// y faces 2 x 16 x (max_nz + max_ny) x sizeof(T), upper-face couplings
-// 16 x (max_nz + max_ny) x sizeof(T).
+// and, for visits with an iterate, the subdomain's y: ldc x sizeof(T).
 template <typename T>
-static size_t ic_blk_smem(int ldc, int max_ny, int max_nz) {
+static size_t ic_blk_smem(int ldc, bool has_y) {
   typedef typename Coef4<T>::type V4;
-  return 512 + (size_t)ldc * sizeof(V4) + (size_t)ldc * sizeof(T) + (size_t)3 * kNX * (max_nz + max_ny) * sizeof(T);
+  return 512 + (size_t)ldc * sizeof(V4) + (size_t)ldc * sizeof(T) * (has_y ? 2 : 1);
 }
 
+// Work is cell-parallel except in the sweeps: thread t handles the cells
+// cl = t + n * blockDim.x, consecutive threads on consecutive cells, so the
+// shared-memory reads of the coefficients and of y are free of bank
+// conflicts; blockDim.x is a multiple of 16, so a thread keeps its position i
+// in the x-line and only steps through lines.  In the sweeps thread (j, k)
+// owns the x-line (., j, k) and handles its cell i = d - j - k on hyperplane d.
 template <typename T, bool HAS_Y, bool FINAL>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1))
+__global__ void __launch_bounds__(512, 2)
     k_ic_apply_blk(Grid g, const SubInfo* subs, const long long* coff, const typename Coef4<T>::type* coef,
                    const T* tx, const T* ty, const T* tz, const T* diag, const double* x, const T* yin, T* out_t,
-                   double* out_d, double* part, const int* done, int* err, int ldc, int fny, int fnz) {
+                   double* out_d, double* part, const int* done, int* err, int ldc) {
   typedef typename Coef4<T>::type V4;
   if (done && *done) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -140,14 +112,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1))
   double* red = reinterpret_cast<double*>(smem_raw + 256);
   V4* cs = reinterpret_cast<V4*>(smem_raw + 512);
   T* u = reinterpret_cast<T*>(cs + ldc);
-  T* yf = u + ldc;                   // y of the neighbouring cells: [face 0 y-][nz][16], [1 y+][nz][16],
-                                     // [2 z-][ny][16], [3 z+][ny][16]
-  T* tf = yf + 2 * kNX * (fnz + fny);  // couplings of the upper faces: [y+][nz][16], [z+][ny][16]
+  T* ys = u + ldc;  // HAS_Y only
   const SubInfo S = subs[blockIdx.x];
   const int ny = S.ny, nz = S.nz, nxny = kNX * ny, ncells = nxny * nz, nlines = ny * nz;
-  const int t = threadIdx.x;
-  const int j = t % ny, k = t / ny;
-  const bool line = t < nlines;
+  const int t = threadIdx.x, bd = blockDim.x, lstep = bd / kNX;
   if (t == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
@@ -156,48 +124,18 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1))
     bulk_g2s(cs, coef + coff[blockIdx.x], bytes, bar);
   }
   const long long MN = (long long)g.M * g.N;
-  const long long cg0 = ((long long)(S.z0 + k) * g.N + (S.y0 + j)) * g.M + S.x0;
-  double xr[kNX];
-  T yr[kNX], dr[kNX];
-  T yl = (T)0, yh = (T)0, txh = (T)0;
-  if (line) {
-    load16(x + cg0, xr);
-    if (HAS_Y) {
-      load16(yin + cg0, yr);
-      load16(diag + cg0, dr);
-      if (S.x0 > 0) yl = yin[cg0 - 1];
-      if (S.x0 + kNX < g.M) {
-        yh = yin[cg0 + kNX];
-        txh = tx[cg0 + kNX];
-      }
-      T tmp[kNX], tmp2[kNX];
-      if (j == 0 && S.y0 > 0) {
-        load16(yin + cg0 - g.M, tmp);
-#pragma unroll
-        for (int i = 0; i < kNX; ++i) yf[k * kNX + i] = tmp[i];
-      }
-      if (j == ny - 1 && S.y0 + ny < g.N) {
-        load16(yin + cg0 + g.M, tmp);
-        load16(ty + cg0 + g.M, tmp2);
-#pragma unroll
-        for (int i = 0; i < kNX; ++i) {
-          yf[(fnz + k) * kNX + i] = tmp[i];
-          tf[k * kNX + i] = tmp2[i];
-        }
-      }
-      if (k == 0 && S.z0 > 0) {
-        load16(yin + cg0 - MN, tmp);
-#pragma unroll
-        for (int i = 0; i < kNX; ++i) yf[(2 * fnz + j) * kNX + i] = tmp[i];
-      }
-      if (k == nz - 1 && S.z0 + nz < g.P) {
-        load16(yin + cg0 + MN, tmp);
-        load16(tz + cg0 + MN, tmp2);
-#pragma unroll
-        for (int i = 0; i < kNX; ++i) {
-          yf[(2 * fnz + fny + j) * kNX + i] = tmp[i];
-          tf[(fnz + j) * kNX + i] = tmp2[i];
-        }
+  const int i0 = t & (kNX - 1);
+  // the subdomain's x (and y) into shared memory while the coefficients land
+  {
+    int line = t >> 4, j = line % ny, k = line / ny;
+    for (int cl = t; cl < ncells; cl += bd) {
+      const long long cg = ((long long)(S.z0 + k) * g.N + (S.y0 + j)) * g.M + S.x0 + i0;
+      u[cl] = (T)x[cg];
+      if (HAS_Y) ys[cl] = yin[cg];
+      j += lstep;
+      while (j >= ny) {
+        j -= ny;
+        ++k;
       }
     }
   }
@@ -220,104 +158,101 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 2 : 1))
   }
   __syncthreads();
   if (*flag) return;
-  const int base = (k * ny + j) * kNX;  // local index of the line's first cell
   if (HAS_Y) {
-    // r = x - A y in the natural-order kernel's order of operations (apply_A):
-    // diagonal, x-, x+, y-, y+, z-, z+
-    if (line) store16(u + base, yr);
+    // r = x - A y in apply_A's order of operations: diagonal, x-, x+, y-, y+, z-, z+
+    int line = t >> 4, j = line % ny, k = line / ny;
+    const int i = i0;
+    for (int cl = t; cl < ncells; cl += bd) {
+      const long long cg = ((long long)(S.z0 + k) * g.N + (S.y0 + j)) * g.M + S.x0 + i;
+      const V4 c = cs[cl];
+      const T yc = ys[cl];
+      T v = diag[cg] * yc;
+      if (i > 0)
+        v -= c.x * ys[cl - 1];
+      else if (S.x0 > 0)
+        v -= c.x * yin[cg - 1];
+      if (i < kNX - 1)
+        v -= cs[cl + 1].x * ys[cl + 1];
+      else if (S.x0 + kNX < g.M)
+        v -= tx[cg + 1] * yin[cg + 1];
+      if (j > 0)
+        v -= c.y * ys[cl - kNX];
+      else if (S.y0 > 0)
+        v -= c.y * yin[cg - g.M];
+      if (j < ny - 1)
+        v -= cs[cl + kNX].y * ys[cl + kNX];
+      else if (S.y0 + ny < g.N)
+        v -= ty[cg + g.M] * yin[cg + g.M];
+      if (k > 0)
+        v -= c.z * ys[cl - nxny];
+      else if (S.z0 > 0)
+        v -= c.z * yin[cg - MN];
+      if (k < nz - 1)
+        v -= cs[cl + nxny].z * ys[cl + nxny];
+      else if (S.z0 + nz < g.P)
+        v -= tz[cg + MN] * yin[cg + MN];
+      u[cl] = u[cl] - v;
+      j += lstep;
+      while (j >= ny) {
+        j -= ny;
+        ++k;
+      }
+    }
     __syncthreads();
-    T rr[kNX];
-    if (line) {
-#pragma unroll
-      for (int i = 0; i < kNX; ++i) {
+  }
+  // forward sweep (D + L) w = r: w_i = (r_i + sum_{lower j} t_ij w_j) / D_i, hyperplane i + j + k = d
+  {
+    const int j = t % ny, k = t / ny;
+    const bool line = t < nlines;
+    const int base = (k * ny + j) * kNX;
+    const int nplanes = kNX + ny + nz - 2;
+    const int jk = j + k;
+    for (int d = 0; d < nplanes; ++d) {
+      const int i = d - jk;
+      if (line && i >= 0 && i < kNX) {
         const int cl = base + i;
         const V4 c = cs[cl];
-        T v = dr[i] * yr[i];
-        if (i > 0)
-          v -= c.x * yr[i - 1];
-        else if (S.x0 > 0)
-          v -= c.x * yl;
-        if (i < kNX - 1)
-          v -= cs[cl + 1].x * yr[i + 1];
-        else if (S.x0 + kNX < g.M)
-          v -= txh * yh;
-        if (j > 0)
-          v -= c.y * u[cl - kNX];
-        else if (S.y0 > 0)
-          v -= c.y * yf[k * kNX + i];
-        if (j < ny - 1)
-          v -= cs[cl + kNX].y * u[cl + kNX];
-        else if (S.y0 + ny < g.N)
-          v -= tf[k * kNX + i] * yf[(fnz + k) * kNX + i];
-        if (k > 0)
-          v -= c.z * u[cl - nxny];
-        else if (S.z0 > 0)
-          v -= c.z * yf[(2 * fnz + j) * kNX + i];
-        if (k < nz - 1)
-          v -= cs[cl + nxny].z * u[cl + nxny];
-        else if (S.z0 + nz < g.P)
-          v -= tf[(fnz + j) * kNX + i] * yf[(2 * fnz + fny + j) * kNX + i];
-        rr[i] = (T)xr[i] - v;
+        T s = u[cl];
+        if (k > 0) s += c.z * u[cl - nxny];
+        if (j > 0) s += c.y * u[cl - kNX];
+        if (i > 0) s += c.x * u[cl - 1];
+        u[cl] = s * c.w;
       }
+      __syncthreads();
     }
-    __syncthreads();
-    if (line) store16(u + base, rr);
-  } else {
-    if (line) {
-      T rr[kNX];
-#pragma unroll
-      for (int i = 0; i < kNX; ++i) rr[i] = (T)xr[i];
-      store16(u + base, rr);
+    // backward sweep (D + L^T) z = D w: z_i = w_i + (sum_{upper j} t_ij z_j) / D_i
+    for (int d = nplanes - 1; d >= 0; --d) {
+      const int i = d - jk;
+      if (line && i >= 0 && i < kNX) {
+        const int cl = base + i;
+        T s = (T)0;
+        if (i < kNX - 1) s += cs[cl + 1].x * u[cl + 1];
+        if (j < ny - 1) s += cs[cl + kNX].y * u[cl + kNX];
+        if (k < nz - 1) s += cs[cl + nxny].z * u[cl + nxny];
+        u[cl] = u[cl] + s * cs[cl].w;
+      }
+      __syncthreads();
     }
-  }
-  __syncthreads();
-  // forward sweep (D + L) w = r: w_i = (r_i + sum_{lower j} t_ij w_j) / D_i, hyperplane i + j + k = d
-  const int nplanes = kNX + ny + nz - 2;
-  const int jk = j + k;
-  for (int d = 0; d < nplanes; ++d) {
-    const int i = d - jk;
-    if (line && i >= 0 && i < kNX) {
-      const int cl = base + i;
-      const V4 c = cs[cl];
-      T s = u[cl];
-      if (k > 0) s += c.z * u[cl - nxny];
-      if (j > 0) s += c.y * u[cl - kNX];
-      if (i > 0) s += c.x * u[cl - 1];
-      u[cl] = s * c.w;
-    }
-    __syncthreads();
-  }
-  // backward sweep (D + L^T) z = D w: z_i = w_i + (sum_{upper j} t_ij z_j) / D_i
-  for (int d = nplanes - 1; d >= 0; --d) {
-    const int i = d - jk;
-    if (line && i >= 0 && i < kNX) {
-      const int cl = base + i;
-      T s = (T)0;
-      if (i < kNX - 1) s += cs[cl + 1].x * u[cl + 1];
-      if (j < ny - 1) s += cs[cl + kNX].y * u[cl + kNX];
-      if (k < nz - 1) s += cs[cl + nxny].z * u[cl + nxny];
-      u[cl] = u[cl] + s * cs[cl].w;
-    }
-    __syncthreads();
   }
   double dot = 0.0;
-  if (line) {
-    T o[kNX];
-#pragma unroll
-    for (int i = 0; i < kNX; ++i) {
-      o[i] = u[base + i];
-      if (HAS_Y) o[i] += yr[i];
-    }
-    if (FINAL) {
-      double od[kNX];
-#pragma unroll
-      for (int i = 0; i < kNX; ++i) {
-        od[i] = (double)o[i];
-        dot += xr[i] * od[i];
+  {
+    int line = t >> 4, j = line % ny, k = line / ny;
+    for (int cl = t; cl < ncells; cl += bd) {
+      const long long cg = ((long long)(S.z0 + k) * g.N + (S.y0 + j)) * g.M + S.x0 + i0;
+      T o = u[cl];
+      if (HAS_Y) o += ys[cl];
+      if (FINAL) {
+        const double od = (double)o;
+        out_d[cg] = od;
+        dot += x[cg] * od;
+      } else {
+        out_t[cg] = o;
       }
-      store16(out_d + cg0, od);
-    } else {
-      store16(out_t + cg0, o);
+      j += lstep;
+      while (j >= ny) {
+        j -= ny;
+        ++k;
+      }
     }
   }
   if (FINAL) {
@@ -356,26 +291,27 @@ void launch_pack_ic_coef(const Grid& g, const SubInfo* subs, int nsub, const lon
 size_t ic_blk_coef_bytes(int prec_bytes) { return prec_bytes == 4 ? sizeof(float4) : sizeof(double4); }
 
 template <typename T>
-size_t ic_blk_smem_bytes(int max_cells, int max_ny, int max_nz) {
-  return ic_blk_smem<T>(max_cells, max_ny, max_nz);
+size_t ic_blk_smem_bytes(int max_cells) {
+  return ic_blk_smem<T>(max_cells, true);
 }
 
 template <typename T>
-void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_cells, int max_ny, int max_nz,
-                         const long long* coff, const void* coef, const T* tx, const T* ty, const T* tz,
-                         const T* diag, const double* x, const T* yin, T* out_t, double* out_d, double* part,
-                         const int* done, int* err, cudaStream_t st) {
+void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_cells, const long long* coff,
+                         const void* coef, const T* tx, const T* ty, const T* tz, const T* diag, const double* x,
+                         const T* yin, T* out_t, double* out_d, double* part, const int* done, int* err,
+                         cudaStream_t st, int threads) {
   typedef typename Coef4<T>::type V4;
   const int ldc = max_cells;
-  const size_t smem = ic_blk_smem<T>(ldc, max_ny, max_nz);
+  const size_t smem = ic_blk_smem<T>(ldc, yin != nullptr);
   const bool fin = out_d != nullptr;
   const V4* c4 = reinterpret_cast<const V4*>(coef);
+  threads = (threads == 256 || threads == 512) ? threads : 512;
 #define PMF_BLK(HY, FN)                                                                                              \
   {                                                                                                                  \
     cudaFuncSetAttribute(k_ic_apply_blk<T, HY, FN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);        \
     note_launch();                                                                                                   \
-    k_ic_apply_blk<T, HY, FN><<<nsub, 256, smem, st>>>(g, subs, coff, c4, tx, ty, tz, diag, x, yin, out_t, out_d,  \
-                                                       part, done, err, ldc, max_ny, max_nz);                        \
+    k_ic_apply_blk<T, HY, FN><<<nsub, threads, smem, st>>>(g, subs, coff, c4, tx, ty, tz, diag, x, yin, out_t,      \
+                                                           out_d, part, done, err, ldc);                             \
   }
   if (yin) {
     if (fin) PMF_BLK(true, true) else PMF_BLK(true, false)
@@ -388,10 +324,10 @@ void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_c
 #define PMF_INST(T)                                                                                                \
   template void launch_pack_ic_coef<T>(const Grid&, const SubInfo*, int, const long long*, const T*, const T*,   \
                                        const T*, const T*, void*, cudaStream_t);                                 \
-  template size_t ic_blk_smem_bytes<T>(int, int, int);                                                           \
-  template void launch_ic_apply_blk<T>(const Grid&, const SubInfo*, int, int, int, int, const long long*,        \
-                                       const void*, const T*, const T*, const T*, const T*, const double*,       \
-                                       const T*, T*, double*, double*, const int*, int*, cudaStream_t);
+  template size_t ic_blk_smem_bytes<T>(int);                                                                     \
+  template void launch_ic_apply_blk<T>(const Grid&, const SubInfo*, int, int, const long long*, const void*,     \
+                                       const T*, const T*, const T*, const T*, const double*, const T*, T*,      \
+                                       double*, double*, const int*, int*, cudaStream_t, int);
 PMF_INST(float)
 PMF_INST(double)
 #undef PMF_INST

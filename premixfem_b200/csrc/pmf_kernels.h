@@ -80,20 +80,20 @@ void launch_ic_apply(const Grid& g, const SubInfo* subs, int nsub, int max_lines
 // The same solve with the IC(0) factor in a subdomain-blocked copy,
 // coef[coff[s] + cl] = {tx, ty, tz, 1/D} of the cells of s in local order
 // (float4 / double4), staged by one TMA bulk copy per subdomain.  Needs every
-// subdomain 16 cells wide with x0 % 4 == 0, M % 4 == 0 and ny*nz <= 256; the
-// result is bit-identical to launch_ic_apply.  *err is set if a CTA's copy did
-// not complete within its wait limit.
+// subdomain 16 cells wide with ny*nz <= 256; the result equals launch_ic_apply's
+// up to the rounding of contracted multiply-adds.  *err is set if a CTA's copy
+// did not complete within its wait limit.  threads: 256 or 512.
 template <typename T>
 void launch_pack_ic_coef(const Grid& g, const SubInfo* subs, int nsub, const long long* coff, const T* tx,
                          const T* ty, const T* tz, const T* inv, void* coef, cudaStream_t st);
 size_t ic_blk_coef_bytes(int prec_bytes);
 template <typename T>
-size_t ic_blk_smem_bytes(int max_cells, int max_ny, int max_nz);
+size_t ic_blk_smem_bytes(int max_cells);
 template <typename T>
-void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_cells, int max_ny, int max_nz,
-                         const long long* coff, const void* coef, const T* tx, const T* ty, const T* tz,
-                         const T* diag, const double* x, const T* yin, T* out_t, double* out_d, double* part,
-                         const int* done, int* err, cudaStream_t st);
+void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_cells, const long long* coff,
+                         const void* coef, const T* tx, const T* ty, const T* tz, const T* diag, const double* x,
+                         const T* yin, T* out_t, double* out_d, double* part, const int* done, int* err,
+                         cudaStream_t st, int threads);
 
 // Exact level-1 solves (-use_full_Cholesky_lv1): banded Cholesky of every
 // subdomain block in natural order, column j of L at band[boff[s] + j*band_ld(b)],

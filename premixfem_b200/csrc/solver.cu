@@ -1123,15 +1123,10 @@ int Solver::setup_band_cholesky(bool mixed) {
 // every subdomain fits that kernel (16 cells wide in x, 16-byte aligned
 // rows, at most 256 x-lines); rebuilt by every set-up.
 int Solver::setup_ic_blocked(bool mixed) {
-  ic_blk_ok = g.M % 4 == 0 && max_lines <= 256;
-  blk_ny = blk_nz = 0;
-  for (const SubInfo& S : subs) {
-    if (S.nx != 16 || S.x0 % 4) ic_blk_ok = false;
-    blk_ny = std::max(blk_ny, S.ny);
-    blk_nz = std::max(blk_nz, S.nz);
-  }
-  const size_t smem = mixed ? ic_blk_smem_bytes<float>(max_cells, blk_ny, blk_nz)
-                            : ic_blk_smem_bytes<double>(max_cells, blk_ny, blk_nz);
+  ic_blk_ok = max_lines <= 256;
+  for (const SubInfo& S : subs)
+    if (S.nx != 16) ic_blk_ok = false;
+  const size_t smem = mixed ? ic_blk_smem_bytes<float>(max_cells) : ic_blk_smem_bytes<double>(max_cells);
   if (smem > 227 * 1024) ic_blk_ok = false;
   if (!d_kerr) {
     if (int e = dalloc((void**)&d_kerr, sizeof(int), "kernel wait flag")) return e;
@@ -1184,12 +1179,10 @@ void Solver::launch_lv1(const double* x, const T* yin, T* out_t, double* out_d, 
   const T* tty = f32 ? (const T*)ty32 : (const T*)ty;
   const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
   const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
-  // the blocked kernel reads and writes 16-byte vectors: a caller's vector at
-  // an odd offset takes the natural-order kernel
-  auto al16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
-  if (ic_variant == 1 && ic_blk_ok && al16(x) && al16(yin) && al16(out_t) && al16(out_d)) {
-    launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, blk_ny, blk_nz, d_coff, ic_coef, ttx, tty, ttz, tdg, x, yin,
-                           out_t, out_d, partial, done, d_kerr, st);
+  const int kind = yin ? 1 : 0;
+  if (ic_variant[kind] == 1 && ic_blk_ok) {
+    launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, x, yin, out_t, out_d,
+                           partial, done, d_kerr, st, ic_blk_threads[kind]);
   } else {
     const T* tinv = f32 ? (const T*)inv32 : (const T*)inv64;
     launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, x, yin, out_t, out_d,
@@ -1214,7 +1207,8 @@ void Solver::tune_pc() {
   cudaMemsetAsync(ya, 0, sizeof(T) * g.ncell, st);
   cudaMemsetAsync(z, 0, sizeof(double) * g.ncell, st);
   cudaMemsetAsync(Zacc, 0, sizeof(double) * nsub * kmax, st);
-  const int old[5] = {ic_threads, rr_threads, pr_threads, pcga_variant, ic_variant};
+  const int old[8] = {ic_threads,    rr_threads,    pr_threads,        pcga_variant,
+                      ic_variant[0], ic_variant[1], ic_blk_threads[0], ic_blk_threads[1]};
   char key[192];
   const char* prec = f32 ? "f32" : "f64";
   if (!opt.use_full_Cholesky_lv1) {
@@ -1222,23 +1216,34 @@ void Solver::tune_pc() {
     std::vector<int> cand = {base};
     for (int t : {384, 512, 768, 1024})
       if (t > base) cand.push_back(t);
-    // candidates: the natural-order kernel with each thread count, then the
-    // blocked kernel (the last candidate, when every subdomain fits it)
+    // candidates per visit kind (first visit: no iterate; later visits: with
+    // one): the natural-order kernel with each thread count, then the blocked
+    // kernel with 512 and 256 threads (when every subdomain fits it).  The
+    // natural kernel's thread count is tuned on the visits with an iterate.
     const int nnat = (int)cand.size();
-    snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d|b%d", prec, nsub, max_cells, max_lines, ic_blk_ok ? 1 : 0);
-    const int ci = tune_choose(key, nnat + (ic_blk_ok ? 1 : 0), [&](int i) {
-      if (i < nnat)
-        launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, ya, yo, nullptr,
-                           nullptr, nullptr, st, cand[i]);
-      else
-        launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, blk_ny, blk_nz, d_coff, ic_coef, ttx, tty, ttz, tdg, z,
-                               ya, yo, nullptr, nullptr, nullptr, d_kerr, st);
-      return true;
-    }, st);
-    ic_variant = ci >= nnat ? 1 : 0;
-    ic_threads = cand[std::min(ci, nnat - 1)];
-    if (opt.lv1_kernel == 1) ic_variant = 0;
-    if (opt.lv1_kernel == 2) ic_variant = 1;  // eligibility checked by setup()
+    const int nblk = ic_blk_ok ? 2 : 0;
+    const int blk_threads[2] = {512, 256};
+    for (int kind = 1; kind >= 0; --kind) {
+      snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d|b%d|y%d", prec, nsub, max_cells, max_lines, nblk, kind);
+      const int ncand = kind == 1 ? nnat + nblk : 1 + nblk;
+      const int ci = tune_choose(key, ncand, [&](int i) {
+        const int nn = kind == 1 ? nnat : 1;
+        if (i < nn)
+          launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, kind ? ya : nullptr,
+                             yo, nullptr, nullptr, nullptr, st, kind ? cand[i] : ic_threads);
+        else
+          launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, z,
+                                 kind ? ya : nullptr, yo, nullptr, nullptr, nullptr, d_kerr, st,
+                                 blk_threads[i - nn]);
+        return true;
+      }, st);
+      const int nn = kind == 1 ? nnat : 1;
+      ic_variant[kind] = ci >= nn ? 1 : 0;
+      if (ci >= nn) ic_blk_threads[kind] = blk_threads[ci - nn];
+      if (kind == 1) ic_threads = cand[std::min(ci, nnat - 1)];
+      if (opt.lv1_kernel == 1) ic_variant[kind] = 0;
+      if (opt.lv1_kernel == 2) ic_variant[kind] = 1;  // eligibility checked by setup()
+    }
   }
   const int rcand[3] = {256, 128, 512};
   snprintf(key, sizeof(key), "resid_restrict|%s|n%d|c%d|k%d", prec, nsub, max_cells, kmax);
@@ -1270,7 +1275,8 @@ void Solver::tune_pc() {
     }, st);
   }
   if (pcg_exec && (old[0] != ic_threads || old[1] != rr_threads || old[2] != pr_threads || old[3] != pcga_variant ||
-                   old[4] != ic_variant)) {
+                   old[4] != ic_variant[0] || old[5] != ic_variant[1] || old[6] != ic_blk_threads[0] ||
+                   old[7] != ic_blk_threads[1])) {
     cudaGraphExecDestroy(pcg_exec);  // captured with other launch shapes
     pcg_exec = nullptr;
     pcg_graph_x = nullptr;

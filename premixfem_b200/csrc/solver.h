@@ -168,8 +168,9 @@ class Solver {
   int ic_threads = 0, rr_threads = 256, pr_threads = 256, pcga_variant = 0;  // tuned launch shapes
   // level-1 solve with the subdomain-blocked IC(0) factor (k_ic_apply_blk)
   bool ic_blk_ok = false;  // every subdomain fits the blocked kernel
-  int ic_variant = 0;      // 0 natural-order kernel, 1 blocked kernel (tuner's choice)
-  int blk_ny = 0, blk_nz = 0;
+  // per visit kind (0: first visit, no iterate; 1: visits with an iterate):
+  // 0 natural-order kernel, 1 blocked kernel (tuner's choice), and its threads
+  int ic_variant[2] = {0, 0}, ic_blk_threads[2] = {512, 512};
   long long* d_coff = nullptr;  // per subdomain: first cell in the blocked arrays
   void* ic_coef = nullptr;      // blocked {tx, ty, tz, 1/D} (precision of the preconditioner)
   int* d_kerr = nullptr;        // set by a kernel whose bounded wait ran out

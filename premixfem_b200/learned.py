@@ -227,7 +227,7 @@ def train(out, seeds, val_seed, n=256, epochs=20, batch=64, lr=2e-3, seed=1, log
     return hist
 
 
-def evaluate(weights, n=128, seed=77, precision="mixed", learned_its=30, eig_tol=None):
+def evaluate(weights, n=128, seed=77, precision="mixed", learned_its=60, eig_tol=None):
     """Set-up and solve with and without the learned start on one held-out field."""
     import torch
     res = {}

@@ -138,12 +138,15 @@ def test_learned_start_keeps_results(native, torch, tmp_path):
 
 def test_trained_network_reduces_eigensolver_iterations(native, torch):
     """What the trained network gains over the randomly started eigensolve, on a
-    field it was not trained on (seed 77; training used seeds 101-110): fewer
-    LOBPCG iterations at the same PCG iteration count (+-1) and solution."""
+    field it was not trained on (seed 77; training used seeds 101-110), with the
+    learned start held to the random start's own eigensolver tolerance: fewer
+    LOBPCG iterations (about 20 % on this field) and a shorter set-up, at the
+    same PCG iteration count (+-1) and solution."""
     assert os.path.exists(learned.DEFAULT_WEIGHTS)
     res = learned.evaluate(learned.DEFAULT_WEIGHTS, n=128, seed=77)
     r, l = res["random"], res["learned"]
-    assert l["eig_iters_mean"] <= 0.7 * r["eig_iters_mean"], res
+    assert l["eig_iters_mean"] <= 0.9 * r["eig_iters_mean"], res
+    assert l["setup_ms"] < r["setup_ms"], res
     assert l["fallbacks"] <= 0.05 * 512, res
     assert abs(l["pcg_iters"] - r["pcg_iters"]) <= 1, res
     assert res["solution_rel_diff"] < 1e-6, res
