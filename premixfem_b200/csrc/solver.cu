@@ -141,6 +141,19 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
   db.get_int("pmf_eig_profile", &o->eig_profile);
   o->eig_require_converged = db.has("pmf_eig_require_converged");
   {
+    auto ite = db.kv.find("pmf_eig_precision");
+    if (ite != db.kv.end()) {
+      if (ite->second == "fp64" || ite->second == "double")
+        o->eig_precision = 0;
+      else if (ite->second == "fp32" || ite->second == "mixed")
+        o->eig_precision = 1;
+      else {
+        *err = "Error in -pmf_eig_precision (fp64 | fp32)";
+        return 62;
+      }
+    }
+  }
+  {
     auto itk = db.kv.find("pmf_lv1_kernel");
     if (itk != db.kv.end()) {
       if (itk->second == "auto")
@@ -300,7 +313,7 @@ Solver::~Solver() {
   if (ev1) cudaEventDestroy(ev1);
   for (auto& e : prof_ev)
     if (e) cudaEventDestroy(e);
-  for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr})
+  for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr, (void*)phi64})
     if (q) cudaFree(q);
   if (st) cudaStreamDestroy(st);
 }
@@ -585,29 +598,31 @@ int Solver::alloc_eb(int m, bool mixed) {
 // The batched local eigensolves over `list` (nullptr: every subdomain), with
 // the phase-batched solver or the single persistent launch.
 int Solver::run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1) {
-  const bool mixed = opt.precision == 1;
+  const bool e32 = eig32();
+  // FP64 eigenvectors go to phi, or to phi64 when the preconditioner is FP32
+  double* out64 = opt.precision == 1 ? phi64 : (double*)phi;
   if (!opt.eig_batched) {
     if (list) {
       la.sub_list = list;
       la.nlist = d_fail_count;
     }
-    if (mixed)
+    if (e32)
       launch_lobpcg<float>(la, eig_blocks, eig_work, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
                            max_lines, st);
     else
-      launch_lobpcg<double>(la, eig_blocks, eig_work, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
-                            max_cells, max_lines, st);
+      launch_lobpcg<double>(la, eig_blocks, eig_work, out64, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                            max_lines, st);
     return 0;
   }
-  if (int e = alloc_eb(la.m, mixed)) return e;
+  if (int e = alloc_eb(la.m, e32)) return e;
   eb.phase_ms = opt.eig_profile ? eig_phase_ms : nullptr;
   int r;
-  if (mixed)
+  if (e32)
     r = launch_lobpcg_batched<float>(la, eb, list, nlist, (float*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
                                      max_cells, max_lines, st);
   else
-    r = launch_lobpcg_batched<double>(la, eb, list, nlist, (double*)phi, d_eig1, d_iters, d_status, d_ks, eb1,
-                                      max_cells, max_lines, st);
+    r = launch_lobpcg_batched<double>(la, eb, list, nlist, out64, d_eig1, d_iters, d_status, d_ks, eb1, max_cells,
+                                      max_lines, st);
   if (r) {
     err = "batched eigensolve: a CUDA call failed";
     return r;
@@ -783,7 +798,9 @@ int Solver::setup() {
   la.kmax = kmax;
   la.eg_op = opt.eg_op;
   la.max_it = opt.eig_max_it;
-  la.tol = opt.eig_tol > 0 ? opt.eig_tol : (mixed ? 1e-6 : 1e-8);
+  la.tol = opt.eig_tol > 0 ? opt.eig_tol : (eig32() ? 1e-6 : 1e-8);
+  if (mixed && !eig32() && !phi64)
+    if (int er = dalloc((void**)&phi64, sizeof(double) * (size_t)g.ncell * kmax, "FP64 eigenvectors")) return er;
   la.sigma_rel = opt.eig_sigma;
   la.seed = opt.seed;
   la.tx = tx;
@@ -823,7 +840,7 @@ int Solver::setup() {
     cudaMemsetAsync(d_prof, 0, sizeof(long long) * 16 * eig_blocks, st);
     la.prof = d_prof;
   }
-  const size_t need = ((lobpcg_work_bytes(max_cells, la.m, mixed ? 4 : 8) + 255) & ~(size_t)255) * eig_blocks;
+  const size_t need = ((lobpcg_work_bytes(max_cells, la.m, eig32() ? 4 : 8) + 255) & ~(size_t)255) * eig_blocks;
   if (eig_work_bytes < need) {
     if (eig_work) cudaFree(eig_work);
     if (int er = check(cudaMalloc(&eig_work, need), "cudaMalloc eigen work")) return er;
@@ -939,6 +956,7 @@ int Solver::setup() {
     }
     coarse_ok = true;
   }
+  if (mixed && !eig32()) launch_to_f32(phi64, (float*)phi, g.ncell * kmax, st);  // the basis the FP32 cycle uses
   if (mixed)
     launch_galerkin<float>(g, d_subs, nsub, kmax, tx, ty, tz, diag, (const float*)phi, blk, gface, st);
   else

@@ -44,6 +44,7 @@ struct Options {
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
   bool eig_require_converged = false;  // a local eigensolve that hits eig_max_it fails the set-up (error 83)
   int lv1_kernel = 0;  // level-1 solve kernel: 0 the tuner's choice, 1 natural-order, 2 subdomain-blocked
+  int eig_precision = -1;  // local eigensolver vectors: -1 as the preconditioner, 0 FP64, 1 FP32 (mixed only)
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
   // iterations; subdomains that have not converged by then are solved again
@@ -179,6 +180,9 @@ class Solver {
   template <typename T>
   void launch_lv1(const double* x, const T* yin, T* out_t, double* out_d, double* partial, const int* done);
   int run_eigen(LobpcgArgs& la, const int* list, int nlist, int eig_blocks, double eb1);
+  // the local eigensolves run on FP32 vectors (the mixed form's default)
+  bool eig32() const { return opt.precision == 1 && opt.eig_precision != 0; }
+  double* phi64 = nullptr;  // FP64 eigensolver output of the mixed form with -pmf_eig_precision fp64
   double* l3work = nullptr;  // level-3 subspace-iteration blocks
   int* d_ks3 = nullptr;
   // -use_2level: banded Cholesky of the global coarse matrix (k_coarse_band.cu)
