@@ -105,9 +105,10 @@ WORKLOADS = {
     ),
 }
 
-# ncu DRAM traffic of the level-1 kernel with an iterate (k_ic_apply<float,1,1>), bytes per cell, from
-# the capture summarised in profiles/ic_apply_fracture128_mixed.md (None until one exists).
-IC_APPLY_Y_TRAFFIC_PER_CELL = None
+# ncu DRAM traffic of the level-1 kernel with an iterate (k_ic_apply<float,1,1>), bytes per cell:
+# 67 167 488 B read / 2 097 152 cells at 128^3 (profiles/ic_apply_fracture128_mixed.md) plus the
+# 8 B/cell FP64 result, which stays in L2 at that size; scaled by the cell count.
+IC_APPLY_Y_TRAFFIC_PER_CELL = 67167488 / 2097152 + 8
 
 
 def _peaks():

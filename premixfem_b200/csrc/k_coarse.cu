@@ -98,6 +98,81 @@ void launch_lv3_prolong(int nrank, int nr, int en2, const double* V, const doubl
   { note_launch(); k_lv3_prolong<<<(int)((n + 255) / 256), 256, 0, st>>>(nrank, nr, en2, V, w, dz, done); }
 }
 
+// ---- the same products over ranks of different sizes (RankLayout) ----------
+__device__ __forceinline__ int rank_nr(const RankLayout& L, int r) { return (L.first[r + 1] - L.first[r]) * L.kmax; }
+__device__ __forceinline__ long long rank_dof0(const RankLayout& L, int r) { return (long long)L.first[r] * L.kmax; }
+// the rank whose range [off[r], off[r+1]) holds e (binary search)
+__device__ __forceinline__ int rank_of(const long long* off, int nrank, long long e) {
+  int lo = 0, hi = nrank - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= e)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// out[g] = sum_j inv_r[i][j] in[dof0_r + j] for coarse dof g = dof0_r + i, one warp per dof
+__global__ void k_block_gemv_r(RankLayout L, long long ncoarse, const double* inv, const double* in, double* out,
+                               const int* done) {
+  if (done && *done) return;
+  const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= ncoarse) return;
+  const int r = L.dof_rank[g];
+  const int nr = rank_nr(L, r);
+  const long long d0 = rank_dof0(L, r);
+  const double* A = inv + L.off2[r] + (g - d0) * nr;
+  const double* x = in + d0;
+  double acc = 0.0;
+  for (int j = lane; j < nr; j += 32) acc += A[j] * x[j];
+  acc = warp_sum(acc);
+  if (lane == 0) out[g] = acc;
+}
+void launch_block_gemv_r(const RankLayout& L, long long ncoarse, const double* inv, const double* in, double* out,
+                         const int* done, cudaStream_t st) {
+  const long long threads = ncoarse * 32;
+  { note_launch(); k_block_gemv_r<<<(int)((threads + 255) / 256), 256, 0, st>>>(L, ncoarse, inv, in, out, done); }
+}
+__global__ void k_lv3_restrict_r(RankLayout L, int nrank, int en2, const double* V, const double* c, double* d,
+                                 const int* done) {
+  if (done && *done) return;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= (long long)nrank * en2) return;
+  const int r = (int)(row / en2), j = (int)(row % en2);
+  const int nr = rank_nr(L, r);
+  const double* Vr = V + L.offv[r];
+  const double* cr = c + rank_dof0(L, r);
+  double acc = 0.0;
+  for (int i = lane; i < nr; i += 32) acc += Vr[(long long)i * en2 + j] * cr[i];
+  acc = warp_sum(acc);
+  if (lane == 0) d[row] = acc;
+}
+void launch_lv3_restrict_r(const RankLayout& L, int nrank, int en2, const double* V, const double* c, double* d,
+                           const int* done, cudaStream_t st) {
+  const long long threads = (long long)nrank * en2 * 32;
+  { note_launch(); k_lv3_restrict_r<<<(int)((threads + 255) / 256), 256, 0, st>>>(L, nrank, en2, V, c, d, done); }
+}
+__global__ void k_lv3_prolong_r(RankLayout L, long long ncoarse, int en2, const double* V, const double* w, double* dz,
+                                const int* done) {
+  if (done && *done) return;
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= ncoarse) return;
+  const int r = L.dof_rank[g];
+  const double* Vi = V + L.offv[r] + (g - rank_dof0(L, r)) * en2;
+  const double* wr = w + (long long)r * en2;
+  double acc = 0.0;
+  for (int j = 0; j < en2; ++j) acc += Vi[j] * wr[j];
+  dz[g] = acc;
+}
+void launch_lv3_prolong_r(const RankLayout& L, long long ncoarse, int en2, const double* V, const double* w,
+                          double* dz, const int* done, cudaStream_t st) {
+  { note_launch(); k_lv3_prolong_r<<<(int)((ncoarse + 255) / 256), 256, 0, st>>>(L, ncoarse, en2, V, w, dz, done); }
+}
+
 __global__ void k_axpy(long long n, double a, const double* x, double* y, const int* done) {
   if (done && *done) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -277,6 +352,55 @@ __global__ void k_assemble_dense(const SubInfo* subs, int nrank, int spr, int km
     dense[e] = v;
   }
 }
+__global__ void k_assemble_dense_r(const SubInfo* subs, int nrank, RankLayout L, long long total, const double* blk,
+                                   const double* gface, int mode, double* dense) {
+  const int kmax = L.kmax;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = rank_of(L.off2, nrank, e);
+    const long long nr = rank_nr(L, r);
+    const long long rem = e - L.off2[r];
+    const int row = (int)(rem / nr), col = (int)(rem % nr);
+    const int a = row / kmax, i = row % kmax, b = col / kmax, j = col % kmax;
+    const int s = L.first[r] + a, s2 = L.first[r] + b;
+    const SubInfo& S = subs[s];
+    double v = 0.0;
+    if (i >= S.k || j >= subs[s2].k) {
+      v = (row == col) ? 1.0 : 0.0;
+    } else if (a == b) {
+      v = blk[(((long long)s * 7) * kmax + i) * kmax + j];
+      if (mode == 1)
+        for (int f = 0; f < 6; ++f)
+          if (S.nb[f] >= 0 && subs[S.nb[f]].rank != r) v -= gface[(((long long)s * 6 + f) * kmax + i) * kmax + j];
+    } else {
+      for (int f = 0; f < 6; ++f)
+        if (S.nb[f] == s2) v = blk[(((long long)s * 7 + 1 + f) * kmax + i) * kmax + j];
+    }
+    dense[e] = v;
+  }
+}
+void launch_assemble_dense_r(const SubInfo* subs, int nrank, const RankLayout& L, long long total, const double* blk,
+                             const double* gface, int mode, double* dense, cudaStream_t st) {
+  const int nb = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+  { note_launch(); k_assemble_dense_r<<<nb, 256, 0, st>>>(subs, nrank, L, total, blk, gface, mode, dense); }
+}
+__global__ void k_add_diag_r(RankLayout L, double* dense, double mu, int relative) {
+  const int r = blockIdx.x;
+  const int n = rank_nr(L, r);
+  double* A = dense + L.off2[r];
+  __shared__ double mx;
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) m = fmax(m, fabs(A[(long long)i * n + i]));
+    mx = relative ? m * mu : mu;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) A[(long long)i * n + i] += mx;
+}
+void launch_add_diag_r(const RankLayout& L, int nrank, double* dense, double mu, int relative, cudaStream_t st) {
+  { note_launch(); k_add_diag_r<<<nrank, 256, 0, st>>>(L, dense, mu, relative); }
+}
+
 void launch_assemble_dense(const SubInfo* subs, int nsub, int nrank, int spr, int kmax, const double* blk,
                            const double* gface, int mode, double* dense, cudaStream_t st) {
   (void)nsub;
@@ -531,11 +655,21 @@ static bool spd_inverse_cl(int nb, int n, double* a, double tol, int* nnull, cud
 // column k and the scaled pivot row into scratch, and k_gj_update applies the
 // rank-1 update to every element of every matrix in parallel, with
 // k_spd_inverse's arithmetic per element (so the results agree bit for bit).
-__global__ void k_gj_scale(int n, const double* a_all, double* scale) {
-  const double* a = a_all + (long long)blockIdx.x * n * n;
+// Matrix b has order nv[b] (or n) and starts at off[b] (or b n^2); pivots past
+// a matrix's order leave it alone.
+struct GjShape {
+  const int* nv;         // per matrix order, or null (all n)
+  const long long* off;  // per matrix offset, or null (b n^2)
+  int n;
+  __device__ int ord(int b) const { return nv ? nv[b] : n; }
+  __device__ long long at(int b) const { return off ? off[b] : (long long)b * n * n; }
+};
+__global__ void k_gj_scale(GjShape sh, const double* a_all, double* scale) {
+  const int nb = sh.ord(blockIdx.x);
+  const double* a = a_all + sh.at(blockIdx.x);
   __shared__ double red[32];
   double mx = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(a[(long long)i * n + i]));
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) mx = fmax(mx, fabs(a[(long long)i * nb + i]));
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (lane == 0) red[wid] = mx;
@@ -546,39 +680,47 @@ __global__ void k_gj_scale(int n, const double* a_all, double* scale) {
     scale[blockIdx.x] = m > 0 ? m : 1.0;
   }
 }
-__global__ void k_gj_pivot(int n, const double* a_all, int k, double tol, const double* scale, double* colk,
+__global__ void k_gj_pivot(GjShape sh, const double* a_all, int k, double tol, const double* scale, double* colk,
                            double* rowk, int* nullk, int* nnull) {
-  const long long b = blockIdx.x;
-  const double* a = a_all + b * n * n;
+  const int b = blockIdx.x;
+  const int n = sh.ord(b);
+  if (k >= n) return;
+  const double* a = a_all + sh.at(b);
+  const long long base = (long long)b * sh.n;
   const double piv = a[(long long)k * n + k];
   const bool isnull = !(piv > tol * scale[b]);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    colk[b * n + i] = a[(long long)i * n + k];
-    rowk[b * n + i] = isnull ? 0.0 : (i == k ? 1.0 : a[(long long)k * n + i]) / piv;
+    colk[base + i] = a[(long long)i * n + k];
+    rowk[base + i] = isnull ? 0.0 : (i == k ? 1.0 : a[(long long)k * n + i]) / piv;
   }
   if (threadIdx.x == 0) {
     nullk[b] = isnull ? 1 : 0;
     if (isnull && nnull) atomicAdd(nnull, 1);
   }
 }
-__global__ void k_gj_update(int n, double* a_all, int k, const double* colk, const double* rowk, const int* nullk) {
-  const long long b = blockIdx.y;
-  double* a = a_all + b * n * n;
-  const long long nn = (long long)n * n;
+__global__ void k_gj_update(GjShape sh, double* a_all, int k, const double* colk, const double* rowk,
+                            const int* nullk) {
+  const int b = blockIdx.y;
+  const int n = sh.ord(b);
+  if (k >= n) return;
+  double* a = a_all + sh.at(b);
+  const long long nn = (long long)n * n, base = (long long)b * sh.n;
   const bool isnull = nullk[b] != 0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / n), j = (int)(e % n);
     if (isnull) {
       if (i == k || j == k) a[e] = 0.0;
     } else if (i == k) {
-      a[e] = rowk[b * n + j];
+      a[e] = rowk[base + j];
     } else {
-      a[e] = (j == k ? 0.0 : a[e]) - colk[b * n + i] * rowk[b * n + j];
+      a[e] = (j == k ? 0.0 : a[e]) - colk[base + i] * rowk[base + j];
     }
   }
 }
-__global__ void k_gj_sym(int n, double* a_all) {
-  double* a = a_all + (long long)blockIdx.y * n * n;
+__global__ void k_gj_sym(GjShape sh, double* a_all) {
+  const int b = blockIdx.y;
+  const int n = sh.ord(b);
+  double* a = a_all + sh.at(b);
   const long long nn = (long long)n * n;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / n), j = (int)(e % n);
@@ -589,34 +731,56 @@ __global__ void k_gj_sym(int n, double* a_all) {
     }
   }
 }
+// nb matrices of orders <= n; returns false when the scratch could not be allocated
+static bool gj_inverse(int nb, GjShape sh, double* a, double tol, int* nnull, cudaStream_t st) {
+  const int n = sh.n;
+  double* scr = nullptr;
+  const size_t bytes = sizeof(double) * (size_t)nb * (2 * (size_t)n + 2);
+  if (cudaMallocAsync((void**)&scr, bytes, st) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  double* scale = scr;
+  double* colk = scr + nb;
+  double* rowk = colk + (size_t)nb * n;
+  int* nullk = reinterpret_cast<int*>(rowk + (size_t)nb * n);
+  { note_launch(); k_gj_scale<<<nb, 256, 0, st>>>(sh, a, scale); }
+  const long long nn = (long long)n * n;
+  const int gx = (int)std::max<long long>(1, std::min<long long>((nn + 255) / 256, (148 * 8 + nb - 1) / nb));
+  for (int k = 0; k < n; ++k) {
+    { note_launch(); k_gj_pivot<<<nb, 256, 0, st>>>(sh, a, k, tol, scale, colk, rowk, nullk, nnull); }
+    { note_launch(); k_gj_update<<<dim3(gx, nb), 256, 0, st>>>(sh, a, k, colk, rowk, nullk); }
+  }
+  { note_launch(); k_gj_sym<<<dim3(gx, nb), 256, 0, st>>>(sh, a); }
+  cudaFreeAsync(scr, st);
+  return true;
+}
+
+void launch_spd_inverse_r(const RankLayout& L, int nrank, int nr_max, double* dense, double tol, int* nnull,
+                          cudaStream_t st) {
+  // the per-rank orders as an int array next to the layout: nr_r = (first[r+1] - first[r]) x kmax
+  int* nv = nullptr;
+  if (cudaMallocAsync((void**)&nv, sizeof(int) * nrank, st) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  std::vector<int> h_first(nrank + 1), h_nv(nrank);
+  cudaMemcpyAsync(h_first.data(), L.first, sizeof(int) * (nrank + 1), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (int r = 0; r < nrank; ++r) h_nv[r] = (h_first[r + 1] - h_first[r]) * L.kmax;
+  cudaMemcpyAsync(nv, h_nv.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
+  GjShape sh{nv, L.off2, nr_max};
+  gj_inverse(nrank, sh, dense, tol, nnull, st);
+  cudaFreeAsync(nv, st);
+  cudaStreamSynchronize(st);  // the host vector must outlive the copy
+}
 
 void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
   const int R = (n + kSpdCl - 1) / kSpdCl;
   if (n <= 128 && R <= kSpdWarps && spd_inverse_cl<4, 1>(nb, n, a, tol, nnull, st)) return;
   if (n > 128 && n <= 256 && R <= 2 * kSpdWarps && spd_inverse_cl<8, 2>(nb, n, a, tol, nnull, st)) return;
   if (n > 256 && n <= 384 && R <= 3 * kSpdWarps && spd_inverse_cl<12, 3>(nb, n, a, tol, nnull, st)) return;
-  if (n > 384) {
-    // scratch: per matrix the scale, column k, the scaled row k and the null flag
-    double* scr = nullptr;
-    const size_t bytes = sizeof(double) * (size_t)nb * (2 * (size_t)n + 2);
-    if (cudaMallocAsync((void**)&scr, bytes, st) == cudaSuccess) {
-      double* scale = scr;
-      double* colk = scr + nb;
-      double* rowk = colk + (size_t)nb * n;
-      int* nullk = reinterpret_cast<int*>(rowk + (size_t)nb * n);
-      { note_launch(); k_gj_scale<<<nb, 256, 0, st>>>(n, a, scale); }
-      const long long nn = (long long)n * n;
-      const int gx = (int)std::max<long long>(1, std::min<long long>((nn + 255) / 256, (148 * 8 + nb - 1) / nb));
-      for (int k = 0; k < n; ++k) {
-        { note_launch(); k_gj_pivot<<<nb, 256, 0, st>>>(n, a, k, tol, scale, colk, rowk, nullk, nnull); }
-        { note_launch(); k_gj_update<<<dim3(gx, nb), 256, 0, st>>>(n, a, k, colk, rowk, nullk); }
-      }
-      { note_launch(); k_gj_sym<<<dim3(gx, nb), 256, 0, st>>>(n, a); }
-      cudaFreeAsync(scr, st);
-      return;
-    }
-    (void)cudaGetLastError();  // no scratch: the one-CTA kernel below
-  }
+  if (n > 384 && gj_inverse(nb, GjShape{nullptr, nullptr, n}, a, tol, nnull, st)) return;
   const int smem = 2 * n * sizeof(double);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   { note_launch(); k_spd_inverse<<<nb, 1024, smem, st>>>(n, a, tol, nnull); }
@@ -669,14 +833,16 @@ __device__ __forceinline__ void cta_stage_block(const double* X, int nr, int p, 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int p, const double* A_all, const double* inv_all,
-                                     double* V_all, double* evals_all, int* iters, double tol, int max_it,
-                                     double* work_all, int ldx) {
+__global__ void __launch_bounds__(512) k_dense_smallest_eig(RankLayout L, int en2, int p, const double* A_all,
+                                                             const double* inv_all, double* V_all, double* evals_all,
+                                                             int* iters, double tol, int max_it, double* work_all,
+                                                             int ldx) {
   extern __shared__ double xs[];  // nr x ldx staging block when ldx > 0
   const int r = blockIdx.x;
-  const double* A = A_all + (long long)r * nr * nr;
-  const double* inv = inv_all + (long long)r * nr * nr;
-  double* X = work_all + (long long)r * 3 * nr * p;
+  const int nr = rank_nr(L, r);
+  const double* A = A_all + L.off2[r];
+  const double* inv = inv_all + L.off2[r];
+  double* X = work_all + L.offw[r];
   double* Y = X + (long long)nr * p;
   double* AY = Y + (long long)nr * p;
   __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP],
@@ -824,7 +990,7 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
     __syncthreads();
     if (conv) break;
   }
-  double* V = V_all + (long long)r * nr * en2;
+  double* V = V_all + L.offv[r];
   for (long long e = tid; e < (long long)nr * en2; e += nt) {
     const int i = (int)(e / en2), j = (int)(e % en2);
     V[e] = X[(long long)i * p + j];
@@ -833,8 +999,9 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(int nr, int en2, int
   if (tid == 0) iters[r] = it + 1;
 }
 
-void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
-                               double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st) {
+void launch_dense_smallest_eig(const RankLayout& L, int nrank, int nr, int en2, int p, const double* A,
+                               const double* inv, double* V, double* evals, int* iters, double tol, int max_it,
+                               double* work, cudaStream_t st) {
   // stage the iteration block in shared memory (odd leading dimension: no bank conflicts) when it fits
   int ldx = p | 1;
   size_t smem = (size_t)nr * ldx * sizeof(double);
@@ -844,7 +1011,7 @@ void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* 
   } else {  // the kernel also holds ~26 KB of static shared memory
     cudaFuncSetAttribute(k_dense_smallest_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
-  { note_launch(); k_dense_smallest_eig<<<nrank, 512, smem, st>>>(nr, en2, p, A, inv, V, evals, iters, tol, max_it, work, ldx); }
+  { note_launch(); k_dense_smallest_eig<<<nrank, 512, smem, st>>>(L, en2, p, A, inv, V, evals, iters, tol, max_it, work, ldx); }
 }
 
 }  // namespace pmf

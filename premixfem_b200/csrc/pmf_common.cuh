@@ -29,7 +29,21 @@ struct SubInfo {
   int k;                       // eigen vectors kept (eigen_num_lv1)
   int local;                   // index inside its rank
   int nb[6];                   // neighbour subdomain across x-, x+, y-, y+, z-, z+ (-1: none)
-  int pad;
+  int prob;                    // problem of a batch (0 for a single problem)
+};
+
+// One problem of a batch.  The problems of a batch share one mesh: problem q
+// occupies the cells x < M, y < N of the layers z0 .. z0 + P - 1 of a mesh
+// max(M) x max(N) x sum(P + 1); the other cells and one layer between
+// consecutive problems hold zero permeability, which decouples them.
+struct ProbInfo {
+  int M, N, P, z0;              // the problem's mesh and first layer in the shared mesh
+  double Hx, Hy, Hz, meas;      // cell size and volume
+  double cx, cy, cz;            // |face|^2 / |cell| per direction
+  int dmask;                    // Dirichlet faces (bit f: x-, x+, y-, y+, z-, z+)
+  double dval[6];               // Dirichlet values
+  long long c0, c1;             // cell range [c0, c1) of its layers in the shared mesh
+  int s0, s1;                   // its subdomains [s0, s1)
 };
 
 struct Grid {

@@ -120,6 +120,35 @@ void launch_prolong(const Grid& g, const SubInfo* subs, int nsub, int kmax, cons
                     const int* done, cudaStream_t st, int threads = 256);
 
 // ---- coarse (FP64) -------------------------------------------------------------
+// Where each virtual rank's coarse data live: rank r owns subdomains
+// first[r] .. first[r+1]-1 (contiguous), so nr_r = (first[r+1] - first[r]) x kmax
+// coarse dofs starting at first[r] x kmax; its dense nr_r x nr_r blocks start
+// at off2[r], its level-3 vectors (nr_r x en2) at offv[r], its level-3 work
+// (3 x nr_r x p) at offw[r].  A grid of ranks of equal size is the special case
+// first[r] = r spr, off2[r] = r nr^2 ...; a batch of problems has one rank per
+// problem and ragged sizes.  All arrays are device arrays of nrank + 1 entries;
+// dof_rank (nsub x kmax) maps a coarse dof to its rank.
+struct RankLayout {
+  const int* first = nullptr;
+  const long long* off2 = nullptr;
+  const long long* offv = nullptr;
+  const long long* offw = nullptr;
+  const int* dof_rank = nullptr;
+  int kmax = 0;
+};
+void launch_block_gemv_r(const RankLayout& L, long long ncoarse, const double* inv, const double* in, double* out,
+                         const int* done, cudaStream_t st);
+void launch_lv3_restrict_r(const RankLayout& L, int nrank, int en2, const double* V, const double* c, double* d,
+                           const int* done, cudaStream_t st);
+void launch_lv3_prolong_r(const RankLayout& L, long long ncoarse, int en2, const double* V, const double* w,
+                          double* dz, const int* done, cudaStream_t st);
+void launch_assemble_dense_r(const SubInfo* subs, int nrank, const RankLayout& L, long long total, const double* blk,
+                             const double* gface, int mode, double* dense, cudaStream_t st);
+// dense[r] += mu (relative != 0: mu x max |diag| of the block) on the diagonal, one CTA per rank
+void launch_add_diag_r(const RankLayout& L, int nrank, double* dense, double mu, int relative, cudaStream_t st);
+// Gauss-Jordan inverses of the ragged blocks (the multi-CTA form of launch_spd_inverse)
+void launch_spd_inverse_r(const RankLayout& L, int nrank, int nr_max, double* dense, double tol, int* nnull,
+                          cudaStream_t st);
 // out = alpha*v_in_out_base - A2 * v   where A2 is block sparse: blk[s][b][kmax][kmax],
 // b = 0 diagonal, 1..6 couplings to nb[b-1].  If base is null the base term is 0.
 void launch_a2_mult(const SubInfo* subs, int nsub, int kmax, const double* blk, const double* v, const double* base,
@@ -250,7 +279,8 @@ int launch_lobpcg_batched(const LobpcgArgs& a, const EbBuffers& b, const int* li
 
 // Level-3 eigenpairs: smallest en2 of dense symmetric A[r] (nr x nr), via subspace
 // iteration with the inverse of (A + mu I) (given as inv) and Rayleigh-Ritz.
-void launch_dense_smallest_eig(int nrank, int nr, int en2, int p, const double* A, const double* inv, double* V,
-                               double* evals, int* iters, double tol, int max_it, double* work, cudaStream_t st);
+void launch_dense_smallest_eig(const RankLayout& L, int nrank, int nr_max, int en2, int p, const double* A,
+                               const double* inv, double* V, double* evals, int* iters, double tol, int max_it,
+                               double* work, cudaStream_t st);
 
 }  // namespace pmf

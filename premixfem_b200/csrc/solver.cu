@@ -215,18 +215,21 @@ __global__ void k_add_diag(int nb, int n, double* a, double mu_rel, int relative
 
 // A3 = V^T (Phi^T A Phi) V block (r, r2): sum over subdomains s of rank r and the
 // block-sparse coupling to subdomains of rank r2.  Padded level-3 dofs are identity.
-__global__ void k_build_a3(const SubInfo* subs, int spr, int kmax, int en2, const double* blk, const double* V,
+__global__ void k_build_a3(const SubInfo* subs, RankLayout L, int en2, const double* blk, const double* V,
                            const int* rank_nb, const int* ks3, double* A3, int n3, double nil) {
   const int r = blockIdx.x / 7, q = blockIdx.x % 7;
   const int r2 = q == 0 ? r : rank_nb[r * 6 + q - 1];
   if (r2 < 0) return;
-  const int nr = spr * kmax;
+  const int kmax = L.kmax;
+  const int nsr = L.first[r + 1] - L.first[r];
+  const double* Vr = V + L.offv[r];
+  const double* Vr2 = V + L.offv[r2];
   for (int e = threadIdx.x; e < en2 * en2; e += blockDim.x) {
     const int j = e / en2, j2 = e % en2;
     double v = 0.0;
     if (j < ks3[r] && j2 < ks3[r2]) {
-      for (int a = 0; a < spr; ++a) {
-        const int s = r * spr + a;
+      for (int a = 0; a < nsr; ++a) {
+        const int s = L.first[r] + a;
         const SubInfo& S = subs[s];
         for (int b = 0; b < 7; ++b) {
           const int nb = b == 0 ? s : S.nb[b - 1];
@@ -234,10 +237,10 @@ __global__ void k_build_a3(const SubInfo* subs, int spr, int kmax, int en2, cons
           const int la = subs[nb].local;
           const double* B = blk + ((long long)s * 7 + b) * kmax * kmax;
           for (int i = 0; i < kmax; ++i) {
-            const double vi = V[((long long)r * nr + a * kmax + i) * en2 + j];
+            const double vi = Vr[((long long)a * kmax + i) * en2 + j];
             if (vi == 0.0) continue;
             double t = 0.0;
-            for (int i2 = 0; i2 < kmax; ++i2) t += B[i * kmax + i2] * V[((long long)r2 * nr + la * kmax + i2) * en2 + j2];
+            for (int i2 = 0; i2 < kmax; ++i2) t += B[i * kmax + i2] * Vr2[((long long)la * kmax + i2) * en2 + j2];
             v += vi * t;
           }
         }
@@ -250,12 +253,13 @@ __global__ void k_build_a3(const SubInfo* subs, int spr, int kmax, int en2, cons
   }
 }
 
-__global__ void k_zero_v_cols(int nrank, int nr, int en2, double* V, const int* ks3) {
-  const long long n = (long long)nrank * nr * en2;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const int r = (int)(e / ((long long)nr * en2));
-    const int j = (int)(e % en2);
-    if (j >= ks3[r]) V[e] = 0.0;
+// level-3 eigenvector columns beyond a rank's adaptive count are zero
+__global__ void k_zero_v_cols(int nrank, RankLayout L, int en2, double* V, const int* ks3) {
+  for (int r = blockIdx.x; r < nrank; r += gridDim.x) {
+    const long long n = L.offv[r + 1] - L.offv[r];
+    double* Vr = V + L.offv[r];
+    for (long long e = threadIdx.x; e < n; e += blockDim.x)
+      if ((int)(e % en2) >= ks3[r]) Vr[e] = 0.0;
   }
 }
 
@@ -313,7 +317,8 @@ Solver::~Solver() {
   if (ev1) cudaEventDestroy(ev1);
   for (auto& e : prof_ev)
     if (e) cudaEventDestroy(e);
-  for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr, (void*)phi64})
+  for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr, (void*)phi64, (void*)d_rl_first, (void*)d_rl_off,
+                  (void*)d_rl_dof_rank})
     if (q) cudaFree(q);
   if (st) cudaStreamDestroy(st);
 }
@@ -363,7 +368,7 @@ int Solver::build_partition() {
               S.rank = rr;
               S.local = loc;
               S.k = opt.en_lv1;
-              S.pad = 0;
+              S.prob = 0;
               if (S.nx < 1 || S.ny < 1 || S.nz < 1) {
                 err = "empty subdomain: too many subdomains or ranks for the mesh";
                 return 62;
@@ -414,14 +419,68 @@ int Solver::build_partition() {
     err = "en_lv1 larger than a subdomain";
     return 62;
   }
-  nr = spr * kmax;
-  en2 = std::min(opt.en_lv2, nr);
-  n3 = nrank * en2;
+  rank_first.assign(nrank + 1, 0);
+  for (int r = 0; r <= nrank; ++r) rank_first[r] = r * spr;
+  ragged = false;
+  rank_sizes();
   if (!opt.use_2level && (nr > 4096 || n3 > 8192)) {
     err = "coarse blocks too large (subdomains per rank * en_lv1 <= 4096, ranks * en_lv2 <= 8192)";
     return 62;
   }
   return 0;
+}
+
+// Sizes of the per-rank coarse data from rank_first: nr is the largest rank's
+// coarse order, en2 = min(en_lv2, the smallest rank's order), and the prefix
+// sums of the dense blocks (nr_r^2), level-3 vectors (nr_r en2) and level-3
+// work (3 nr_r p).
+void Solver::rank_sizes() {
+  nr = 0;
+  nr_min = 1 << 30;
+  for (int r = 0; r < nrank; ++r) {
+    const int n = (rank_first[r + 1] - rank_first[r]) * kmax;
+    nr = std::max(nr, n);
+    nr_min = std::min(nr_min, n);
+  }
+  en2 = std::min(opt.en_lv2, nr_min);
+  n3 = nrank * en2;
+  l3p = std::min(nr_min, std::min(32, 2 * en2 + 4));
+  tot2 = totv = totw = 0;
+  for (int r = 0; r < nrank; ++r) {
+    const long long n = (long long)(rank_first[r + 1] - rank_first[r]) * kmax;
+    tot2 += n * n;
+    totv += n * en2;
+    totw += 3 * n * l3p;
+  }
+}
+
+int Solver::rank_layout() {
+  if (d_rl_first) return 0;
+  std::vector<long long> off(3 * (size_t)(nrank + 1), 0);
+  for (int r = 0; r < nrank; ++r) {
+    const long long n = (long long)(rank_first[r + 1] - rank_first[r]) * kmax;
+    off[r + 1] = off[r] + n * n;
+    off[(nrank + 1) + r + 1] = off[(nrank + 1) + r] + n * en2;
+    off[2 * (nrank + 1) + r + 1] = off[2 * (nrank + 1) + r] + 3 * n * l3p;
+  }
+  std::vector<int> dof_rank((size_t)nsub * kmax);
+  for (int r = 0; r < nrank; ++r)
+    for (long long g = (long long)rank_first[r] * kmax; g < (long long)rank_first[r + 1] * kmax; ++g) dof_rank[g] = r;
+  int e = dalloc((void**)&d_rl_first, sizeof(int) * (nrank + 1), "rank layout");
+  if (!e) e = dalloc((void**)&d_rl_off, sizeof(long long) * off.size(), "rank layout");
+  if (!e) e = dalloc((void**)&d_rl_dof_rank, sizeof(int) * dof_rank.size(), "rank layout");
+  if (e) return e;
+  cudaMemcpyAsync(d_rl_first, rank_first.data(), sizeof(int) * (nrank + 1), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_rl_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_rl_dof_rank, dof_rank.data(), sizeof(int) * dof_rank.size(), cudaMemcpyHostToDevice, st);
+  rl.first = d_rl_first;
+  rl.off2 = d_rl_off;
+  rl.offv = d_rl_off + (nrank + 1);
+  rl.offw = d_rl_off + 2 * (nrank + 1);
+  rl.dof_rank = d_rl_dof_rank;
+  rl.kmax = kmax;
+  // the host vectors must outlive the copies
+  return check(cudaStreamSynchronize(st), "rank layout");
 }
 
 // cudaMalloc with its return code checked: on failure *p is null, err names
@@ -918,6 +977,7 @@ int Solver::setup() {
   for (int s = 0; s < nsub; ++s) subs[s].k = ks[s];
   cudaMemcpyAsync(d_subs, subs.data(), sizeof(SubInfo) * nsub, cudaMemcpyHostToDevice, st);
   // level-2 Galerkin (Phi^T A Phi) and per-rank inverses
+  if (int er = rank_layout()) return er;
   if (!coarse_ok) {
     // all or nothing, as alloc_fine
     struct A {
@@ -927,10 +987,10 @@ int Solver::setup() {
     };
     const A list[] = {{(void**)&blk, sizeof(double) * nsub * 7 * kmax * kmax, "coarse blocks"},
                       {(void**)&gface, sizeof(double) * nsub * 6 * kmax * kmax, "coarse face blocks"},
-                      {(void**)&A2inv, sizeof(double) * nrank * nr * nr, "level-2 inverses"},
-                      {(void**)&AN, sizeof(double) * nrank * nr * nr, "rank-Neumann matrices"},
-                      {(void**)&ANinv, sizeof(double) * nrank * nr * nr, "rank-Neumann inverses"},
-                      {(void**)&V3, sizeof(double) * nrank * nr * en2, "level-3 eigenvectors"},
+                      {(void**)&A2inv, sizeof(double) * tot2, "level-2 inverses"},
+                      {(void**)&AN, sizeof(double) * tot2, "rank-Neumann matrices"},
+                      {(void**)&ANinv, sizeof(double) * tot2, "rank-Neumann inverses"},
+                      {(void**)&V3, sizeof(double) * totv, "level-3 eigenvectors"},
                       {(void**)&d_eig3, sizeof(double) * nrank * en2, "level-3 eigenvalues"},
                       {(void**)&d_l3it, sizeof(int) * nrank, "level-3 iterations"},
                       {(void**)&A3inv, sizeof(double) * n3 * n3, "level-3 inverse"},
@@ -997,19 +1057,25 @@ int Solver::setup() {
     l3_iters.clear();
     return finish();
   }
-  launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 0, A2inv, st);
-  launch_spd_inverse(nrank, nr, A2inv, 1e-14, d_flag + 1, st);
+  launch_assemble_dense_r(d_subs, nrank, rl, tot2, blk, gface, 0, A2inv, st);
+  if (ragged)
+    launch_spd_inverse_r(rl, nrank, nr, A2inv, 1e-14, d_flag + 1, st);
+  else
+    launch_spd_inverse(nrank, nr, A2inv, 1e-14, d_flag + 1, st);
   cudaEventRecord(e[3], st);
   // level 3: rank-Neumann HEP
-  launch_assemble_dense(d_subs, nsub, nrank, spr, kmax, blk, gface, 1, AN, st);
-  cudaMemcpyAsync(ANinv, AN, sizeof(double) * nrank * nr * nr, cudaMemcpyDeviceToDevice, st);
-  { note_launch(); k_add_diag<<<nrank, 256, 0, st>>>(nrank, nr, ANinv, 1e-8, 1); }
-  launch_spd_inverse(nrank, nr, ANinv, 1e-14, d_flag + 2, st);
-  const int p = std::min(nr, std::min(32, 2 * en2 + 4));
+  launch_assemble_dense_r(d_subs, nrank, rl, tot2, blk, gface, 1, AN, st);
+  cudaMemcpyAsync(ANinv, AN, sizeof(double) * tot2, cudaMemcpyDeviceToDevice, st);
+  launch_add_diag_r(rl, nrank, ANinv, 1e-8, 1, st);
+  if (ragged)
+    launch_spd_inverse_r(rl, nrank, nr, ANinv, 1e-14, d_flag + 2, st);
+  else
+    launch_spd_inverse(nrank, nr, ANinv, 1e-14, d_flag + 2, st);
   if (!l3work) {
-    if (int er = check(cudaMalloc(&l3work, sizeof(double) * nrank * 3 * nr * p), "cudaMalloc l3 work")) return er;
+    if (int er = check(cudaMalloc(&l3work, sizeof(double) * totw), "cudaMalloc l3 work")) return er;
   }
-  launch_dense_smallest_eig(nrank, nr, en2, p, AN, ANinv, V3, d_eig3, d_l3it, opt.l3_tol, opt.l3_max_it, l3work, st);
+  launch_dense_smallest_eig(rl, nrank, nr, en2, l3p, AN, ANinv, V3, d_eig3, d_l3it, opt.l3_tol, opt.l3_max_it, l3work,
+                            st);
   if (int er = check(cudaStreamSynchronize(st), "level-3 eigensolve")) return er;
   eig3.resize((size_t)nrank * en2);
   l3_iters.resize(nrank);
@@ -1039,10 +1105,10 @@ int Solver::setup() {
     if (int er = dalloc((void**)&d_ks3, sizeof(int) * nrank, "level-3 counts")) return er;
   cudaMemcpyAsync(d_ks3, ks3.data(), sizeof(int) * nrank, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_rank_nb, rnb.data(), sizeof(int) * nrank * 6, cudaMemcpyHostToDevice, st);
-  { note_launch(); k_zero_v_cols<<<256, 256, 0, st>>>(nrank, nr, en2, V3, d_ks3); }
+  { note_launch(); k_zero_v_cols<<<std::min(nrank, 1024), 256, 0, st>>>(nrank, rl, en2, V3, d_ks3); }
   cudaEventRecord(e[4], st);
   { note_launch(); k_zero_d<<<256, 256, 0, st>>>(A3inv, (long long)n3 * n3); }
-  { note_launch(); k_build_a3<<<nrank * 7, 64, 0, st>>>(d_subs, spr, kmax, en2, blk, V3, d_rank_nb, d_ks3, A3inv, n3,
+  { note_launch(); k_build_a3<<<nrank * 7, 64, 0, st>>>(d_subs, rl, en2, blk, V3, d_rank_nb, d_ks3, A3inv, n3,
                                        opt.no_shift_A_cc ? 0.0 : 1.0e-12); }
   launch_spd_inverse(1, n3, A3inv, 1e-14, d_flag + 3, st);
   cudaEventRecord(e[5], st);
@@ -1357,13 +1423,13 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
         c_valid = true;
       }
       if (v == 2) {
-        launch_block_gemv(nrank, nr, A2inv, c, dz, 0, done, st);
+        launch_block_gemv_r(rl, ncoarse, A2inv, c, dz, done, st);
       } else if (v == 4) {  // _PC_apply_vec_lv2_2level (:1481-1537)
         launch_cband_solve(cb_perm, cband, cb_T, cb_X, c, dz, cb_v, cb_y, cb_t, done, st);
       } else {
-        launch_lv3_restrict(nrank, nr, en2, V3, c, d3, done, st);
+        launch_lv3_restrict_r(rl, nrank, en2, V3, c, d3, done, st);
         launch_block_gemv(1, n3, A3inv, d3, w3, 0, done, st);
-        launch_lv3_prolong(nrank, nr, en2, V3, w3, dz, done, st);
+        launch_lv3_prolong_r(rl, ncoarse, en2, V3, w3, dz, done, st);
       }
       if (z_pend)
         launch_axpy(ncoarse, 1.0, dz, Zacc, done, st);

@@ -126,6 +126,18 @@ class Solver {
   int *d_ks = nullptr, *d_iters = nullptr, *d_status = nullptr, *d_l3it = nullptr, *d_flag = nullptr;
   int* d_rank_nb = nullptr;
   bool coarse_ok = false;  // the level-2/3 arrays above are allocated
+  // where each virtual rank's coarse data live (pmf_kernels.h RankLayout);
+  // rank_first is filled by the partition, the rest by rank_layout()
+  std::vector<int> rank_first;  // nrank + 1
+  bool ragged = false;          // ranks of different sizes (a batch of problems)
+  long long tot2 = 0, totv = 0, totw = 0;
+  int nr_min = 0, l3p = 0;
+  RankLayout rl;
+  int* d_rl_first = nullptr;
+  long long* d_rl_off = nullptr;  // off2, offv, offw: 3 x (nrank + 1)
+  int* d_rl_dof_rank = nullptr;
+  void rank_sizes();   // host: nr, nr_min, en2, n3, l3p, tot2, totv, totw from rank_first
+  int rank_layout();   // device copies of the layout
   void* eig_work = nullptr;
   size_t eig_work_bytes = 0;
   double *c = nullptr, *dz = nullptr, *Zacc = nullptr, *d3 = nullptr, *w3 = nullptr;
