@@ -93,6 +93,27 @@ int pmf_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its
  * No counterpart in the reference (PETSc's -log_view plays this role there). */
 int pmf_profile_iteration(pmf_solver* s, int reps, double ms[8], int launches[8]);
 
+/*
+ * A batch of independent problems solved together (BASELINE's batching
+ * configuration; the reference solves one problem per run).  Problem q has
+ * dom[3q..3q+2], mesh[3q..3q+2] and sd[3q..3q+2] subdomains per axis (one
+ * virtual rank per problem: its level 2 is its whole coarse space).  The
+ * problems share one mesh (pmf_batch_info: max M x max N x sum(P + 1) cells;
+ * problem q fills x < M_q, y < N_q of the layers z0[q] .. z0[q] + P_q - 1,
+ * the rest is zero-permeability padding); pmf_set_kappa, pmf_setup, pmf_rhs
+ * and the pmf_get_* queries work on that shared layout.  Every set-up phase
+ * runs one launch over the subdomains of all problems.  pmf_batch_solve runs
+ * one PCG per problem (its, rnorm, reason: nprob entries each), all of them
+ * in one set of launches per iteration.  -pmf_learned, -use_2level and
+ * -ksp_constant_null_space are not available for batches (56); pmf_solve and
+ * pmf_set_dirichlet return 73 on a batch.
+ */
+int pmf_batch_create(int nprob, const double* dom, const int* mesh, const int* sd, const char* options,
+                     pmf_solver** out);
+int pmf_batch_info(pmf_solver* s, int shared_mesh[3], int* z0);
+int pmf_batch_set_dirichlet(pmf_solver* s, int q, int face, double value);
+int pmf_batch_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason);
+
 /* info[0..11] = ncell_lo32, nsub, nrank, subdomains_per_rank, kmax, nr, en_lv2, n3,
  *               max_cells, max_lines, precision, is_setup */
 int pmf_get_info(pmf_solver* s, int info[12]);

@@ -52,6 +52,10 @@ SIGNATURES = {
     "pmf_get_learned_stats": (C.c_int, [_vp, _vp, _dp]),
     "pmf_get_eig_phases": (C.c_int, [_vp, _vp, C.POINTER(C.c_ulonglong)]),
     "pmf_profile_iteration": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "pmf_batch_create": (C.c_int, [C.c_int, _vp, _vp, _vp, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "pmf_batch_info": (C.c_int, [_vp, _vp, _vp]),
+    "pmf_batch_set_dirichlet": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double]),
+    "pmf_batch_solve": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, _vp]),
     "pmf_residual_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pmf_tune_report": (C.c_int, [C.c_char_p, C.c_int]),
     "pmf_launch_count": (C.c_ulonglong, []),

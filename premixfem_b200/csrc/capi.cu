@@ -58,6 +58,57 @@ int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_
   return 0;
 }
 
+int pmf_batch_create(int nprob, const double* dom, const int* mesh, const int* sd, const char* options,
+                     pmf_solver** out) {
+  if (nprob < 1 || !dom || !mesh || !sd || !out) return fail(62, "pmf_batch_create: bad argument");
+  for (int q = 0; q < nprob; ++q) {
+    if (!(dom[3 * q] > 0.0 && dom[3 * q + 1] > 0.0 && dom[3 * q + 2] > 0.0))
+      return fail(62, "Errors in dom(L, W, H) of problem " + std::to_string(q));
+    if (!(mesh[3 * q] > 0 && mesh[3 * q + 1] > 0 && mesh[3 * q + 2] > 0))
+      return fail(62, "Errors in mesh(M, N, P) of problem " + std::to_string(q));
+  }
+  pmf::OptionDB db;
+  db.parse(options ? options : "");
+  pmf::Options o;
+  std::string err;
+  if (int e = pmf::options_from_db(db, &o, &err)) return fail(e, err);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(76, "no CUDA device available");
+  try {
+    pmf_solver* h = new pmf_solver;
+    h->s = new pmf::Solver(nprob, dom, mesh, sd, o);
+    *out = h;
+  } catch (const std::exception& ex) {
+    return fail(76, ex.what());
+  }
+  return 0;
+}
+
+int pmf_batch_info(pmf_solver* h, int shared_mesh[3], int* z0) {
+  PMF_CHECK_HANDLE(h);
+  pmf::Solver& s = *h->s;
+  if (!s.nprob) return fail(73, "not a batch of problems");
+  if (shared_mesh) {
+    shared_mesh[0] = s.g.M;
+    shared_mesh[1] = s.g.N;
+    shared_mesh[2] = s.g.P;
+  }
+  if (z0)
+    for (int q = 0; q < s.nprob; ++q) z0[q] = s.probs[q].z0;
+  return 0;
+}
+
+int pmf_batch_set_dirichlet(pmf_solver* h, int q, int face, double value) {
+  PMF_CHECK_HANDLE(h);
+  return wrap(h, h->s->set_dirichlet_prob(q, face, value));
+}
+
+int pmf_batch_solve(pmf_solver* h, const double* b, double* x, int on_device, int* its, double* rnorm, int* reason) {
+  PMF_CHECK_HANDLE(h);
+  if (!b || !x) return fail(62, "null vector");
+  return wrap(h, h->s->solve_batch(b, x, on_device != 0, its, rnorm, reason));
+}
+
 int pmf_destroy(pmf_solver* h) {
   if (!h) return 0;
   delete h->s;

@@ -634,6 +634,45 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
   return q;
 }
 
+// Cell size, Dirichlet faces and the box of the subdomain's problem: the
+// solver's own for a single problem, the problem table's for a batch.
+struct EigGeom {
+  double Hx, Hy, Hz, meas;
+  int dmask, M, N, z0, z1;
+};
+__device__ __forceinline__ EigGeom eig_geom(const ProbInfo* probs, const Grid& g, double Hx, double Hy, double Hz,
+                                            double meas, int dmask, const SubInfo& S) {
+  EigGeom e;
+  if (probs) {
+    const ProbInfo& p = probs[S.prob];
+    e.Hx = p.Hx;
+    e.Hy = p.Hy;
+    e.Hz = p.Hz;
+    e.meas = p.meas;
+    e.dmask = p.dmask;
+    e.M = p.M;
+    e.N = p.N;
+    e.z0 = p.z0;
+    e.z1 = p.z0 + p.P;
+  } else {
+    e.Hx = Hx;
+    e.Hy = Hy;
+    e.Hz = Hz;
+    e.meas = meas;
+    e.dmask = dmask;
+    e.M = g.M;
+    e.N = g.N;
+    e.z0 = 0;
+    e.z1 = g.P;
+  }
+  return e;
+}
+__device__ __forceinline__ bool touches_dirichlet(const EigGeom& e, const SubInfo& S) {
+  const int dm = e.dmask;
+  return ((dm & 1) && S.x0 == 0) || ((dm & 2) && S.x0 + S.nx == e.M) || ((dm & 4) && S.y0 == 0) ||
+         ((dm & 8) && S.y0 + S.ny == e.N) || ((dm & 16) && S.z0 == e.z0) || ((dm & 32) && S.z0 + S.nz == e.z1);
+}
+
 // out = A^N v on the subdomain (FP64 arithmetic, stored as TO).
 template <typename TI, typename TO>
 __device__ __forceinline__ void neumann_apply_col(const Grid& g, const SubInfo& S, const double* tx, const double* ty,
@@ -695,6 +734,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     if (idx >= count) break;
     const int s = a.sub_list ? a.sub_list[idx] : idx;
     const SubInfo S = a.subs[s];
+    const EigGeom eg = eig_geom(a.probs, g, a.Hx, a.Hy, a.Hz, a.meas, a.dirichlet_mask, S);
     const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
     unsigned char* wbs = a.mode ? a.slab + (size_t)s * a.slab_stride : wb;
     T* X = reinterpret_cast<T*>(wbs);
@@ -737,21 +777,21 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
         mv = dn;
       } else {  // EIG_OP_MOD with the reference's x-direction accumulation (:258-320)
         mv = 0.0;
-        if (i == 0 && ex >= 1) mv += 2.0 * avg_k(a.kx[cg - 1], a.kx[cg]) / a.Hx / a.Hx;
-        if (ex + 1 != g.M) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
-        if (ey >= 1) mv += 2.0 * avg_k(a.ky[cg - g.M], a.ky[cg]) / a.Hy / a.Hy;
-        if (ey + 1 != g.N) mv += 2.0 * avg_k(a.ky[cg], a.ky[cg + g.M]) / a.Hy / a.Hy;
-        if (ez >= 1) mv += 2.0 * avg_k(a.kz[cg - g.MN], a.kz[cg]) / a.Hz / a.Hz;
-        if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / a.Hz / a.Hz;
-        if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
+        if (i == 0 && ex >= 1) mv += 2.0 * avg_k(a.kx[cg - 1], a.kx[cg]) / eg.Hx / eg.Hx;
+        if (ex + 1 != g.M) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / eg.Hx / eg.Hx;
+        if (ey >= 1) mv += 2.0 * avg_k(a.ky[cg - g.M], a.ky[cg]) / eg.Hy / eg.Hy;
+        if (ey + 1 != g.N) mv += 2.0 * avg_k(a.ky[cg], a.ky[cg + g.M]) / eg.Hy / eg.Hy;
+        if (ez >= 1) mv += 2.0 * avg_k(a.kz[cg - g.MN], a.kz[cg]) / eg.Hz / eg.Hz;
+        if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / eg.Hz / eg.Hz;
+        if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / eg.Hx / eg.Hx;
         // Dirichlet extension: 2 t_b per boundary face
-        if (a.dirichlet_mask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-        if (a.dirichlet_mask & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-        if (a.dirichlet_mask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-        if (a.dirichlet_mask & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-        if (a.dirichlet_mask & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-        if (a.dirichlet_mask & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-        mv = mv * a.meas;
+        if (eg.dmask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / eg.Hx / eg.Hx;
+        if (eg.dmask & 2 && ex == eg.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / eg.Hx / eg.Hx;
+        if (eg.dmask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / eg.Hy / eg.Hy;
+        if (eg.dmask & 8 && ey == eg.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / eg.Hy / eg.Hy;
+        if (eg.dmask & 16 && ez == eg.z0) mv += 2.0 * (2.0 * a.kz[cg]) / eg.Hz / eg.Hz;
+        if (eg.dmask & 32 && ez == eg.z1 - 1) mv += 2.0 * (2.0 * a.kz[cg]) / eg.Hz / eg.Hz;
+        mv = mv * eg.meas;
       }
       Md[cl] = mv;
       dN[cl] = dn;
@@ -1115,9 +1155,7 @@ __global__ void __launch_bounds__(LB_THREADS) k_lobpcg(LobpcgArgs a, unsigned ch
     bool snap = false;
     double cval = 0.0;
     if (sizeof(T) == 4 && num >= 1) {
-      const int dm = a.dirichlet_mask;
-      const bool touches = ((dm & 1) && S.x0 == 0) || ((dm & 2) && S.x0 + nx == g.M) || ((dm & 4) && S.y0 == 0) ||
-                           ((dm & 8) && S.y0 + ny == g.N) || ((dm & 16) && S.z0 == 0) || ((dm & 32) && S.z0 + nz == g.P);
+      const bool touches = touches_dirichlet(eg, S);
       if (!touches) {
         double msum = 0.0, vsum = 0.0;
         for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
@@ -1233,6 +1271,7 @@ struct EbArgs {
   int* alist;  // subdomains still iterating, compacted by k_eb_control
   unsigned long long* colcells;  // sum over active subdomain-iterations of (basis columns x cells)
   const double *tx, *ty, *tz;
+  const ProbInfo* probs;  // a batch's problem table, or null
 };
 
 // Phase kernels index the compacted active list; the control kernel the full list.
@@ -1614,9 +1653,7 @@ __global__ void __launch_bounds__(256) k_eb_fin_rr(EbArgs a, double eb, int dmas
   bool snap = false;
   double cval = 0.0;
   if (sizeof(T) == 4 && num >= 1) {
-    const bool touches = ((dmask & 1) && S.x0 == 0) || ((dmask & 2) && S.x0 + S.nx == a.g.M) ||
-                         ((dmask & 4) && S.y0 == 0) || ((dmask & 8) && S.y0 + S.ny == a.g.N) ||
-                         ((dmask & 16) && S.z0 == 0) || ((dmask & 32) && S.z0 + S.nz == a.g.P);
+    const bool touches = touches_dirichlet(eig_geom(a.probs, a.g, 0.0, 0.0, 0.0, 0.0, dmask, S), S);
     if (!touches) {
       EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
       double msum = 0.0, vsum = 0.0;
@@ -1693,6 +1730,7 @@ __global__ void __launch_bounds__(256) k_eb_init_a(EbArgs e, LobpcgArgs a) {
   EbState& es = e.state[s];
   const SubInfo S = e.subs[s];
   const Grid g = e.g;
+  const EigGeom eg = eig_geom(a.probs, g, a.Hx, a.Hy, a.Hz, a.meas, a.dirichlet_mask, S);
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
   const int m = e.m, ld = e.ld;
   EbSlab<T> sl(e.slab + (size_t)s * e.slab_stride, m, ld);
@@ -1715,20 +1753,20 @@ __global__ void __launch_bounds__(256) k_eb_init_a(EbArgs e, LobpcgArgs a) {
       mv = dn;
     } else {  // EIG_OP_MOD with the reference's x-direction accumulation (:258-320)
       mv = 0.0;
-      if (i == 0 && ex >= 1) mv += 2.0 * avg_k(a.kx[cg - 1], a.kx[cg]) / a.Hx / a.Hx;
-      if (ex + 1 != g.M) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
-      if (ey >= 1) mv += 2.0 * avg_k(a.ky[cg - g.M], a.ky[cg]) / a.Hy / a.Hy;
-      if (ey + 1 != g.N) mv += 2.0 * avg_k(a.ky[cg], a.ky[cg + g.M]) / a.Hy / a.Hy;
-      if (ez >= 1) mv += 2.0 * avg_k(a.kz[cg - g.MN], a.kz[cg]) / a.Hz / a.Hz;
-      if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / a.Hz / a.Hz;
-      if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / a.Hx / a.Hx;
-      if (a.dirichlet_mask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-      if (a.dirichlet_mask & 2 && ex == g.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / a.Hx / a.Hx;
-      if (a.dirichlet_mask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-      if (a.dirichlet_mask & 8 && ey == g.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / a.Hy / a.Hy;
-      if (a.dirichlet_mask & 16 && ez == 0) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-      if (a.dirichlet_mask & 32 && ez == g.P - 1) mv += 2.0 * (2.0 * a.kz[cg]) / a.Hz / a.Hz;
-      mv = mv * a.meas;
+      if (i == 0 && ex >= 1) mv += 2.0 * avg_k(a.kx[cg - 1], a.kx[cg]) / eg.Hx / eg.Hx;
+      if (ex + 1 != g.M) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / eg.Hx / eg.Hx;
+      if (ey >= 1) mv += 2.0 * avg_k(a.ky[cg - g.M], a.ky[cg]) / eg.Hy / eg.Hy;
+      if (ey + 1 != g.N) mv += 2.0 * avg_k(a.ky[cg], a.ky[cg + g.M]) / eg.Hy / eg.Hy;
+      if (ez >= 1) mv += 2.0 * avg_k(a.kz[cg - g.MN], a.kz[cg]) / eg.Hz / eg.Hz;
+      if (ez + 1 != g.P) mv += 2.0 * avg_k(a.kz[cg], a.kz[cg + g.MN]) / eg.Hz / eg.Hz;
+      if (i + 1 < nx) mv += 2.0 * avg_k(a.kx[cg], a.kx[cg + 1]) / eg.Hx / eg.Hx;
+      if (eg.dmask & 1 && ex == 0) mv += 2.0 * (2.0 * a.kx[cg]) / eg.Hx / eg.Hx;
+      if (eg.dmask & 2 && ex == eg.M - 1) mv += 2.0 * (2.0 * a.kx[cg]) / eg.Hx / eg.Hx;
+      if (eg.dmask & 4 && ey == 0) mv += 2.0 * (2.0 * a.ky[cg]) / eg.Hy / eg.Hy;
+      if (eg.dmask & 8 && ey == eg.N - 1) mv += 2.0 * (2.0 * a.ky[cg]) / eg.Hy / eg.Hy;
+      if (eg.dmask & 16 && ez == eg.z0) mv += 2.0 * (2.0 * a.kz[cg]) / eg.Hz / eg.Hz;
+      if (eg.dmask & 32 && ez == eg.z1 - 1) mv += 2.0 * (2.0 * a.kz[cg]) / eg.Hz / eg.Hz;
+      mv = mv * eg.meas;
     }
     sl.Md[cl] = mv;
     sl.dN[cl] = dn;
@@ -1955,6 +1993,7 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   e.tx = a.tx;
   e.ty = a.ty;
   e.tz = a.tz;
+  e.probs = a.probs;
   if (a.init_batched) {
     const size_t init_smem = (size_t)20 * e.ldc;  // FP64 pivots + three FP32 coupling arrays
     const size_t rr_smem0 = sizeof(LbSmall) + sizeof(LbMats);

@@ -33,22 +33,52 @@ __global__ void k_assemble(AssembleArgs a, double* tx, double* ty, double* tz, d
        c += (long long)gridDim.x * blockDim.x) {
     int ex, ey, ez;
     decode(c, g, ex, ey, ez);
-    const double txc = ex > 0 ? a.cx * hmean(a.kx[c - 1], a.kx[c]) : 0.0;
-    const double tyc = ey > 0 ? a.cy * hmean(a.ky[c - g.M], a.ky[c]) : 0.0;
-    const double tzc = ez > 0 ? a.cz * hmean(a.kz[c - g.MN], a.kz[c]) : 0.0;
-    const double txn = ex < g.M - 1 ? a.cx * hmean(a.kx[c], a.kx[c + 1]) : 0.0;
-    const double tyn = ey < g.N - 1 ? a.cy * hmean(a.ky[c], a.ky[c + g.M]) : 0.0;
-    const double tzn = ez < g.P - 1 ? a.cz * hmean(a.kz[c], a.kz[c + g.MN]) : 0.0;
+    // the cell's problem: its face coefficients, faces and Dirichlet data
+    double cx = a.cx, cy = a.cy, cz = a.cz;
+    int lo[3] = {0, 0, 0}, hi[3] = {g.M, g.N, g.P};
+    bool dir_on[6];
+    double dir_val[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      dir_on[f] = a.dir_on[f] != 0;
+      dir_val[f] = a.dir_val[f];
+    }
+    if (a.probs) {
+      const int q = a.layer_prob[ez];
+      if (q < 0 || ex >= a.probs[q].M || ey >= a.probs[q].N) {  // no problem: decoupled, zero row
+        tx[c] = ty[c] = tz[c] = diag[c] = db[c] = bval[c] = 0.0;
+        continue;
+      }
+      const ProbInfo& p = a.probs[q];
+      cx = p.cx;
+      cy = p.cy;
+      cz = p.cz;
+      hi[0] = p.M;
+      hi[1] = p.N;
+      lo[2] = p.z0;
+      hi[2] = p.z0 + p.P;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        dir_on[f] = (p.dmask >> f) & 1;
+        dir_val[f] = p.dval[f];
+      }
+    }
+    const double txc = ex > lo[0] ? cx * hmean(a.kx[c - 1], a.kx[c]) : 0.0;
+    const double tyc = ey > lo[1] ? cy * hmean(a.ky[c - g.M], a.ky[c]) : 0.0;
+    const double tzc = ez > lo[2] ? cz * hmean(a.kz[c - g.MN], a.kz[c]) : 0.0;
+    const double txn = ex < hi[0] - 1 ? cx * hmean(a.kx[c], a.kx[c + 1]) : 0.0;
+    const double tyn = ey < hi[1] - 1 ? cy * hmean(a.ky[c], a.ky[c + g.M]) : 0.0;
+    const double tzn = ez < hi[2] - 1 ? cz * hmean(a.kz[c], a.kz[c + g.MN]) : 0.0;
     double dbc = 0.0, bv = 0.0;
-    const bool on[6] = {ex == 0, ex == g.M - 1, ey == 0, ey == g.N - 1, ez == 0, ez == g.P - 1};
-    const double cf[6] = {a.cx, a.cx, a.cy, a.cy, a.cz, a.cz};
+    const bool on[6] = {ex == lo[0], ex == hi[0] - 1, ey == lo[1], ey == hi[1] - 1, ez == lo[2], ez == hi[2] - 1};
+    const double cf[6] = {cx, cx, cy, cy, cz, cz};
     const double kk[6] = {a.kx[c], a.kx[c], a.ky[c], a.ky[c], a.kz[c], a.kz[c]};
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      if (a.dir_on[f] && on[f]) {
+      if (dir_on[f] && on[f]) {
         const double tb = cf[f] * (2.0 * kk[f]);
         dbc += tb;
-        bv += tb * a.dir_val[f];
+        bv += tb * dir_val[f];
       }
     }
     tx[c] = txc;
@@ -64,6 +94,21 @@ __global__ void k_assemble(AssembleArgs a, double* tx, double* ty, double* tz, d
     db[c] = dbc;
     bval[c] = bv;
   }
+}
+
+__global__ void k_zero_padding(Grid g, const ProbInfo* probs, const int* layer_prob, double* kx, double* ky,
+                               double* kz) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    int ex, ey, ez;
+    decode(c, g, ex, ey, ez);
+    const int q = layer_prob[ez];
+    if (q < 0 || ex >= probs[q].M || ey >= probs[q].N) kx[c] = ky[c] = kz[c] = 0.0;
+  }
+}
+void launch_zero_padding(const Grid& g, const ProbInfo* probs, const int* layer_prob, double* kx, double* ky,
+                         double* kz, cudaStream_t st) {
+  { note_launch(); k_zero_padding<<<cell_blocks(g.ncell), kCellThreads, 0, st>>>(g, probs, layer_prob, kx, ky, kz); }
 }
 
 void launch_assemble(const AssembleArgs& a, double* tx, double* ty, double* tz, double* diag, double* db,

@@ -32,7 +32,13 @@ struct AssembleArgs {
   double cx, cy, cz;           // |face|^2/|cell| per direction
   double dir_val[6];           // Dirichlet value per face (x-,x+,y-,y+,z-,z+)
   int dir_on[6];
+  // a batch of problems: the problem table and the problem of each layer (-1: separator)
+  const ProbInfo* probs = nullptr;
+  const int* layer_prob = nullptr;
 };
+// a batch: zero permeability in the cells that belong to no problem
+void launch_zero_padding(const Grid& g, const ProbInfo* probs, const int* layer_prob, double* kx, double* ky,
+                         double* kz, cudaStream_t st);
 void launch_assemble(const AssembleArgs& a, double* tx, double* ty, double* tz, double* diag, double* db,
                      double* bval, cudaStream_t st);
 void launch_to_f32(const double* in, float* out, long long n, cudaStream_t st);
@@ -64,6 +70,17 @@ int launch_pcg_iter_a_main(const Grid& g, const double* tx, const double* ty, co
 void launch_pcg_iter_b(long long n, double* x, double* r, const double* p, const double* w, double* part,
                        PcgState* s, cudaStream_t st);
 void launch_dot(const double* a, const double* b, long long n, double* part, double* out, cudaStream_t st);
+
+// ---- CG over a batch of problems (k_batch.cu): per-problem scalars, 2-D grids
+// (blocks x problems); all_done is set when every problem has stopped
+void launch_bpcg_start(const ProbInfo* probs, int nprob, const double* b, double* x, double* r, double* part,
+                       PcgState* st, double rtol, double atol, int max_it, int* all_done, int nblk, cudaStream_t s);
+void launch_bpcg_beta(const ProbInfo* probs, int nprob, const double* part, PcgState* st, cudaStream_t s);
+void launch_bpcg_iter_a(const Grid& g, const ProbInfo* probs, int nprob, const double* tx, const double* ty,
+                        const double* tz, const double* diag, const double* z, const double* pin, double* pout,
+                        double* w, double* part, PcgState* st, int nblk, cudaStream_t s);
+void launch_bpcg_iter_b(const ProbInfo* probs, int nprob, double* x, double* r, const double* p, const double* w,
+                        double* part, PcgState* st, int* all_done, int nblk, cudaStream_t s);
 
 // ---- level 1 (IC(0) block solves) -------------------------------------------
 void launch_ic_factor(const Grid& g, const SubInfo* subs, int nsub, int max_lines, const double* tx, const double* ty,
@@ -235,6 +252,7 @@ struct LobpcgArgs {
   size_t slab_stride;
   void* state;          // per-subdomain EbState array (modes 1, 2)
   int dirichlet_mask;   // bit f set: face f (x-,x+,y-,y+,z-,z+) is a Dirichlet face
+  const ProbInfo* probs = nullptr;  // a batch: per-problem cell size and Dirichlet faces (SubInfo::prob)
   int ld;               // column stride of the work block vectors (set by the launcher)
   int ldc;              // stride of the shared-memory sweep arrays (set by the launcher)
   int mb;               // vectors per shared-memory sweep (set by the launcher)

@@ -291,6 +291,80 @@ Solver::Solver(const double d[3], const int mesh[3], const Options& o) : opt(o) 
   cudaMallocHost(&h_state, sizeof(PcgState));
 }
 
+// A batch of nprob problems (dom, mesh, sd: 3 values per problem) on one
+// shared mesh: problem q's cells x < M_q, y < N_q of the layers
+// z0_q .. z0_q + P_q - 1, one layer of zero permeability between problems.
+Solver::Solver(int np, const double* doms, const int* meshes, const int* sds, const Options& o) : opt(o) {
+  nprob = np;
+  probs.assign(np, ProbInfo());
+  bsd.assign(sds, sds + 3 * np);
+  int M = 0, N = 0, P = 0;
+  for (int q = 0; q < np; ++q) {
+    ProbInfo& p = probs[q];
+    p.M = meshes[3 * q];
+    p.N = meshes[3 * q + 1];
+    p.P = meshes[3 * q + 2];
+    p.z0 = P;
+    P += p.P + (q + 1 < np ? 1 : 0);
+    M = std::max(M, p.M);
+    N = std::max(N, p.N);
+    p.Hx = doms[3 * q] / (double)p.M;  // :1707-1709
+    p.Hy = doms[3 * q + 1] / (double)p.N;
+    p.Hz = doms[3 * q + 2] / (double)p.P;
+    p.meas = p.Hx * p.Hy * p.Hz;
+    const double fyz = p.Hy * p.Hz, fzx = p.Hz * p.Hx, fxy = p.Hx * p.Hy;
+    p.cx = fyz * fyz / p.meas;
+    p.cy = fzx * fzx / p.meas;
+    p.cz = fxy * fxy / p.meas;
+    p.dmask = 0;
+    for (double& v : p.dval) v = 0.0;
+  }
+  g.M = M;
+  g.N = N;
+  g.P = P;
+  g.MN = M * N;
+  g.ncell = (long long)M * N * P;
+  for (ProbInfo& p : probs) {
+    p.c0 = (long long)p.z0 * g.MN;
+    p.c1 = (long long)(p.z0 + p.P) * g.MN;
+  }
+  for (int i = 0; i < 3; ++i) {
+    dom[i] = doms[i];
+    H[i] = probs[0].Hx;
+  }
+  H[1] = probs[0].Hy;
+  H[2] = probs[0].Hz;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaMallocHost(&h_state, sizeof(PcgState));
+}
+
+int Solver::set_dirichlet_prob(int q, int face, double value) {
+  if (q < 0 || q >= nprob || face < 0 || face > 5) {
+    err = "batch Dirichlet face: problem index or face (0..5) out of range";
+    return 62;
+  }
+  probs[q].dmask |= 1 << face;
+  probs[q].dval[face] = value;
+  return 0;
+}
+
+// Device copies of the problem table and of the layer -> problem map.
+int Solver::upload_probs() {
+  if (!nprob) return 0;
+  if (!d_probs) {
+    if (int e = dalloc((void**)&d_probs, sizeof(ProbInfo) * nprob, "batch problem table")) return e;
+    if (int e = dalloc((void**)&d_layer_prob, sizeof(int) * g.P, "batch layer map")) return e;
+  }
+  layer_prob.assign(g.P, -1);
+  for (int q = 0; q < nprob; ++q)
+    for (int z = probs[q].z0; z < probs[q].z0 + probs[q].P; ++z) layer_prob[z] = q;
+  cudaMemcpyAsync(d_probs, probs.data(), sizeof(ProbInfo) * nprob, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_layer_prob, layer_prob.data(), sizeof(int) * g.P, cudaMemcpyHostToDevice, st);
+  return check(cudaStreamSynchronize(st), "batch problem table");
+}
+
 Solver::~Solver() {
   if (st) cudaStreamSynchronize(st);
   void* ptrs[] = {d_subs, kx,    ky,    kz,    tx,     ty,    tz,     diag,     db,       bval,    tx32,  ty32,
@@ -301,6 +375,11 @@ Solver::~Solver() {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
+  if (bpcg_exec) cudaGraphExecDestroy(bpcg_exec);
+  for (void* p : {(void*)bstate, (void*)d_all_done})
+    if (p) cudaFree(p);
+  if (h_bstate) cudaFreeHost(h_bstate);
+  if (h_all_done) cudaFreeHost(h_all_done);
   for (void* p : {(void*)eb.slab, eb.state, (void*)eb.Ybuf, (void*)eb.gpart, (void*)eb.rpart, (void*)eb.nactive,
                   (void*)eb.alist, (void*)eb.colcells})
     if (p) cudaFree(p);
@@ -318,12 +397,13 @@ Solver::~Solver() {
   for (auto& e : prof_ev)
     if (e) cudaEventDestroy(e);
   for (void* q : {(void*)d_coff, ic_coef, (void*)d_kerr, (void*)phi64, (void*)d_rl_first, (void*)d_rl_off,
-                  (void*)d_rl_dof_rank})
+                  (void*)d_rl_dof_rank, (void*)d_probs, (void*)d_layer_prob})
     if (q) cudaFree(q);
   if (st) cudaStreamDestroy(st);
 }
 
 int Solver::build_partition() {
+  if (nprob) return build_partition_batch();
   const int px = opt.vranks[0], py = opt.vranks[1], pz = opt.vranks[2];
   const int sx = opt.sd[0], sy = opt.sd[1], sz = opt.sd[2];
   if (px < 1 || py < 1 || pz < 1 || sx < 1 || sy < 1 || sz < 1) {
@@ -395,6 +475,79 @@ int Solver::build_partition() {
     S.nb[4] = at(gx, gy, gz - 1);
     S.nb[5] = at(gx, gy, gz + 1);
   }
+  rank_first.assign(nrank + 1, 0);
+  for (int r = 0; r <= nrank; ++r) rank_first[r] = r * spr;
+  ragged = false;
+  return partition_checks();
+}
+
+// A batch of problems: each problem is one virtual rank, split into its own
+// subdomain grid (near-equal, as :47-78) inside its box of the shared mesh;
+// subdomains only neighbour subdomains of their own problem.
+int Solver::build_partition_batch() {
+  nrank = nprob;
+  rank_grid[0] = nprob;
+  rank_grid[1] = rank_grid[2] = 1;
+  subs.clear();
+  rank_first.assign(nprob + 1, 0);
+  max_cells = max_lines = 0;
+  spr = 0;
+  for (int q = 0; q < nprob; ++q) {
+    ProbInfo& pq = probs[q];
+    const int sx = bsd[3 * q], sy = bsd[3 * q + 1], sz = bsd[3 * q + 2];
+    if (sx < 1 || sy < 1 || sz < 1 || sx > pq.M || sy > pq.N || sz > pq.P) {
+      err = "batch problem " + std::to_string(q) + ": subdomain counts must be between 1 and the cells per axis";
+      return 62;
+    }
+    std::vector<int> xs, xl, ys, yl, zs, zl;
+    split(pq.M, sx, xs, xl);
+    split(pq.N, sy, ys, yl);
+    split(pq.P, sz, zs, zl);
+    const int s0 = (int)subs.size();
+    rank_first[q] = s0;
+    pq.s0 = s0;
+    for (int cz = 0; cz < sz; ++cz)
+      for (int cy = 0; cy < sy; ++cy)
+        for (int cx = 0; cx < sx; ++cx) {
+          SubInfo S;
+          S.x0 = xs[cx];
+          S.nx = xl[cx];
+          S.y0 = ys[cy];
+          S.ny = yl[cy];
+          S.z0 = pq.z0 + zs[cz];
+          S.nz = zl[cz];
+          S.rank = q;
+          S.local = (cz * sy + cy) * sx + cx;
+          S.k = opt.en_lv1;
+          S.prob = q;
+          auto at = [&](int x, int y, int z) {
+            return (x < 0 || y < 0 || z < 0 || x >= sx || y >= sy || z >= sz) ? -1 : s0 + (z * sy + y) * sx + x;
+          };
+          S.nb[0] = at(cx - 1, cy, cz);
+          S.nb[1] = at(cx + 1, cy, cz);
+          S.nb[2] = at(cx, cy - 1, cz);
+          S.nb[3] = at(cx, cy + 1, cz);
+          S.nb[4] = at(cx, cy, cz - 1);
+          S.nb[5] = at(cx, cy, cz + 1);
+          max_cells = std::max(max_cells, S.nx * S.ny * S.nz);
+          max_lines = std::max(max_lines, S.ny * S.nz);
+          subs.push_back(S);
+        }
+    pq.s1 = (int)subs.size();
+    spr = std::max(spr, pq.s1 - s0);
+  }
+  nsub = (int)subs.size();
+  rank_first[nprob] = nsub;
+  ragged = true;
+  if (!opt.learned_path.empty() || opt.use_2level) {
+    err = "a batch of problems runs neither -pmf_learned nor -use_2level";
+    return 56;
+  }
+  return partition_checks();
+}
+
+// Limits every partition must meet, then the coarse sizes.
+int Solver::partition_checks() {
   if (max_cells > PMF_MAX_SUB_CELLS || max_lines > 256) {
     err = "subdomain too large for the shared-memory sweeps (cells <= 8192, ny*nz <= 256)";
     return 62;
@@ -415,13 +568,11 @@ int Solver::build_partition() {
     err = "en_lv1 must be <= 8 (block size en_lv1 + guard <= 10)";
     return 62;
   }
-  if (kmax > max_cells) {
-    err = "en_lv1 larger than a subdomain";
-    return 62;
-  }
-  rank_first.assign(nrank + 1, 0);
-  for (int r = 0; r <= nrank; ++r) rank_first[r] = r * spr;
-  ragged = false;
+  for (const SubInfo& S : subs)
+    if (kmax > S.nx * S.ny * S.nz) {
+      err = "en_lv1 larger than a subdomain";
+      return 62;
+    }
   rank_sizes();
   if (!opt.use_2level && (nr > 4096 || n3 > 8192)) {
     err = "coarse blocks too large (subdomains per rank * en_lv1 <= 4096, ranks * en_lv2 <= 8192)";
@@ -563,10 +714,18 @@ int Solver::set_kappa(const double* k0, const double* k1, const double* k2, bool
   cudaMemcpyAsync(kx, k0, n * 8, kind, st);
   cudaMemcpyAsync(ky, k1 ? k1 : k0, n * 8, kind, st);
   cudaMemcpyAsync(kz, k2 ? k2 : k0, n * 8, kind, st);
+  if (nprob) {  // cells of no problem hold zero permeability, whatever the caller passed there
+    if (int e = upload_probs()) return e;
+    launch_zero_padding(g, d_probs, d_layer_prob, kx, ky, kz, st);
+  }
   return check(cudaStreamSynchronize(st), "set_kappa");
 }
 
 int Solver::set_dirichlet(int face, double value) {
+  if (nprob) {
+    err = "a batch takes its Dirichlet faces per problem (pmf_batch_set_dirichlet)";
+    return 73;
+  }
   if (face < 0 || face > 5) {
     err = "Dirichlet face must be 0..5 (x-,x+,y-,y+,z-,z+)";
     return 62;
@@ -613,6 +772,8 @@ void Solver::assemble_launch() {
     aa.dir_on[f] = dir_on_[f];
     aa.dir_val[f] = dir_val_[f];
   }
+  aa.probs = d_probs;
+  aa.layer_prob = d_layer_prob;
   launch_assemble(aa, tx, ty, tz, diag, db, bval, st);
 }
 
@@ -771,6 +932,7 @@ int Solver::setup() {
     return 73;  // PETSC_ERR_ARG_WRONGSTATE
   }
   if (opt.autotune >= 0) tune_set_enabled(opt.autotune == 1);
+  if (int er = upload_probs()) return er;
   // stage events, destroyed on every return path
   struct StageEvents {
     cudaEvent_t ev[8];
@@ -890,6 +1052,7 @@ int Solver::setup() {
   la.slab_stride = 0;
   la.state = nullptr;
   la.dirichlet_mask = dmask;
+  la.probs = d_probs;
   la.ld = 0;
   la.prof = nullptr;
   long long* d_prof = nullptr;
@@ -1090,7 +1253,7 @@ int Solver::setup() {
         break;
       }
   std::vector<int> rnb((size_t)nrank * 6, -1);
-  for (int rr = 0; rr < nrank; ++rr) {
+  for (int rr = 0; rr < nrank && !nprob; ++rr) {
     const int px = rank_grid[0], py = rank_grid[1], pz = rank_grid[2];
     const int rx = rr % px, ry = (rr / px) % py, rz = rr / (px * py);
     auto at = [&](int x, int y, int zz) { return (x < 0 || y < 0 || zz < 0 || x >= px || y >= py || zz >= pz) ? -1 : (zz * py + y) * px + x; };
@@ -1446,6 +1609,106 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
   }
 }
 
+// PCG of every problem of the batch at once (KSPCG per problem, as Solver::solve
+// for one): the CG steps are per-problem kernels over 2-D grids, the
+// preconditioner the shared cycle, skipped once every problem has stopped.
+// its, rnorm, reason: one entry per problem.
+int Solver::solve_batch(const double* b_in, double* x_out, bool on_device, int* its, double* rnorm, int* reason) {
+  if (!nprob) {
+    err = "not a batch of problems";
+    return 73;
+  }
+  if (!is_setup) {
+    err = "setup not done";
+    return 73;
+  }
+  if (opt.null_space) {
+    err = "a batch solve has no constant null space option";
+    return 56;
+  }
+  if (!bstate) {
+    int e = dalloc((void**)&bstate, sizeof(PcgState) * nprob, "batch CG states");
+    if (!e) e = dalloc((void**)&d_all_done, sizeof(int), "batch CG flag");
+    if (!e) e = check(cudaMallocHost(&h_bstate, sizeof(PcgState) * nprob), "pinned batch CG states");
+    if (!e) e = check(cudaMallocHost(&h_all_done, sizeof(int)), "pinned batch CG flag");
+    if (e) return e;
+  }
+  const size_t n = (size_t)g.ncell;
+  const double* bs = b_in;
+  double* xs = x_out;
+  if (!on_device) {
+    cudaMemcpyAsync(vb, b_in, n * 8, cudaMemcpyHostToDevice, st);
+    bs = vb;
+    xs = vx;
+  }
+  // entries outside every problem stay zero in every CG vector
+  for (double* v : {z, p0, p1, w, r, xs}) cudaMemsetAsync(v, 0, n * 8, st);
+  const int nblk = bpcg_blocks();
+  cudaEventRecord(ev0, st);
+  launch_bpcg_start(d_probs, nprob, bs, xs, r, part, bstate, opt.rtol, opt.atol, opt.max_it, d_all_done, nblk, st);
+  apply(r, z, part, d_all_done);
+  launch_bpcg_beta(d_probs, nprob, part, bstate, st);
+  double* pin = p0;
+  double* pout = p1;
+  const int chunk = std::max(2, opt.pcg_chunk & ~1);  // even: the p buffers return to their roles
+  auto enqueue_chunk = [&]() {
+    for (int c_ = 0; c_ < chunk; ++c_) {
+      launch_bpcg_iter_a(g, d_probs, nprob, tx, ty, tz, diag, z, pin, pout, w, part, bstate, nblk, st);
+      launch_bpcg_iter_b(d_probs, nprob, xs, r, pout, w, part, bstate, d_all_done, nblk, st);
+      apply(r, z, part, d_all_done);
+      launch_bpcg_beta(d_probs, nprob, part, bstate, st);
+      std::swap(pin, pout);
+    }
+  };
+  const bool use_graph = opt.pcg_graph != 0;
+  if (use_graph && (!bpcg_exec || bpcg_graph_x != xs)) {
+    if (bpcg_exec) cudaGraphExecDestroy(bpcg_exec);
+    bpcg_exec = nullptr;
+    const unsigned long long l0 = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+    cudaGraph_t graph = nullptr;
+    if (int e = check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture")) return e;
+    enqueue_chunk();
+    if (int e = check(cudaStreamEndCapture(st, &graph), "graph capture")) return e;
+    bpcg_graph_kernels = __atomic_load_n(&g_launches, __ATOMIC_RELAXED) - l0;
+    __atomic_fetch_sub(&g_launches, bpcg_graph_kernels, __ATOMIC_RELAXED);  // captured, not launched
+    const cudaError_t ie = cudaGraphInstantiate(&bpcg_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (int e = check(ie, "graph instantiate")) return e;
+    bpcg_graph_x = xs;
+  }
+  int guard = 0;
+  for (;;) {
+    if (use_graph) {
+      if (int e = check(cudaGraphLaunch(bpcg_exec, st), "graph launch")) return e;
+      __atomic_fetch_add(&g_launches, bpcg_graph_kernels, __ATOMIC_RELAXED);
+    } else {
+      enqueue_chunk();
+    }
+    cudaMemcpyAsync(h_all_done, d_all_done, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int e = check(cudaStreamSynchronize(st), "batch KSPSolve")) return e;
+    if (int e = check(cudaGetLastError(), "batch KSPSolve launch")) return e;
+    if (*h_all_done) break;
+    if (++guard * chunk > opt.max_it + 8) break;
+  }
+  cudaEventRecord(ev1, st);
+  cudaMemcpyAsync(h_bstate, bstate, sizeof(PcgState) * nprob, cudaMemcpyDeviceToHost, st);
+  if (!on_device) cudaMemcpyAsync(x_out, xs, n * 8, cudaMemcpyDeviceToHost, st);
+  int e = check(cudaStreamSynchronize(st), "batch KSPSolve");
+  if (!e) e = check_kernel_flag("batch KSPSolve");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  last_solve_ms = ms;
+  last_its = 0;
+  for (int q = 0; q < nprob; ++q) {
+    const PcgState& s = h_bstate[q];
+    if (its) its[q] = s.its;
+    if (rnorm) rnorm[q] = s.dp;
+    if (reason) reason[q] = s.done ? s.done : 2;
+    last_its = std::max(last_its, s.its);
+  }
+  return e;
+}
+
 void Solver::prof_mark(int slot) {
   if (!prof_on || prof_n >= 64) return;
   cudaEventRecord(prof_ev[prof_n], st);
@@ -1575,6 +1838,10 @@ int Solver::pc_apply(const double* x_in, double* y_out, bool on_device) {
 }
 
 int Solver::solve(const double* b_in, double* x_out, bool on_device, int* its, double* rnorm, int* reason) {
+  if (nprob) {
+    err = "a batch of problems is solved by pmf_batch_solve (one CG per problem)";
+    return 73;
+  }
   if (!is_setup) {
     err = "setup not done";
     return 73;

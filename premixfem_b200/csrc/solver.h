@@ -84,6 +84,8 @@ class Net;
 class Solver {
  public:
   Solver(const double dom[3], const int mesh[3], const Options& o);
+  // a batch of problems on one shared mesh (pmf_batch_create)
+  Solver(int nprob, const double* doms, const int* meshes, const int* sds, const Options& o);
   ~Solver();
 
   int set_kappa(const double* kx, const double* ky, const double* kz, bool on_device);
@@ -138,6 +140,26 @@ class Solver {
   int* d_rl_dof_rank = nullptr;
   void rank_sizes();   // host: nr, nr_min, en2, n3, l3p, tot2, totv, totw from rank_first
   int rank_layout();   // device copies of the layout
+  // a batch of problems (0: one problem)
+  int nprob = 0;
+  std::vector<ProbInfo> probs;
+  std::vector<int> bsd, layer_prob;
+  ProbInfo* d_probs = nullptr;
+  int* d_layer_prob = nullptr;
+  int build_partition_batch();
+  int partition_checks();
+  int set_dirichlet_prob(int q, int face, double value);
+  int upload_probs();
+  // CG over the batch: one PCG per problem, one set of launches for all
+  int solve_batch(const double* b, double* x, bool on_device, int* its, double* rnorm, int* reason);
+  PcgState* bstate = nullptr;    // device, per problem
+  PcgState* h_bstate = nullptr;  // pinned copy
+  int* d_all_done = nullptr;
+  int* h_all_done = nullptr;     // pinned
+  cudaGraphExec_t bpcg_exec = nullptr;
+  const double* bpcg_graph_x = nullptr;
+  unsigned long long bpcg_graph_kernels = 0;
+  int bpcg_blocks() const { return 32; }
   void* eig_work = nullptr;
   size_t eig_work_bytes = 0;
   double *c = nullptr, *dz = nullptr, *Zacc = nullptr, *d3 = nullptr, *w3 = nullptr;

@@ -67,35 +67,36 @@ def make_case(case, n, seed):
 
 
 def run_batch(args):
-    """The batching workload: per problem one set-up and four solves; one JSON
-    line per problem, then the totals."""
+    """The batching workload through one BatchSolver: one batched set-up (every
+    phase one launch over all problems' subdomains) and four batched solves
+    (one CG per problem); per problem the iteration counts, then the totals."""
     import torch
 
-    tot_setup = tot_solve = 0.0
-    its_all = []
-    for q, (prob, sources) in enumerate(fields.grf_batch(count=args.count, seed=args.seed)):
-        opts = {"pmf_sd": fields.tiles(prob["mesh"]), "en_lv1": 4, "en_lv2": 4, "pmf_precision": args.precision}
-        s = DarcySolver.from_problem(prob, options_string(opts) + " " + args.opts)
+    from premixfem_b200.solver import BatchSolver
+
+    batch = fields.grf_batch(count=args.count, seed=args.seed)
+    problems = [p for p, _ in batch]
+    s = BatchSolver(problems, [fields.tiles(p["mesh"]) for p in problems],
+                    options_string({"en_lv1": 4, "en_lv2": 4, "pmf_precision": args.precision}) + " " + args.opts)
+    for rep in range(args.repeat):
+        s.set_kappa_problems(problems)
         s.setup()
         su, _ = s.timing()
-        its, solve_ms = [], 0.0
-        for src in sources:
-            b = s.rhs(torch.from_numpy(np.ascontiguousarray(src).ravel()).cuda())
+        its_all, solve_ms = [], 0.0
+        for j in range(4):
+            b = s.rhs(torch.from_numpy(s.pack([srcs[j] for _, srcs in batch])).cuda())
             x = torch.empty_like(b)
-            _, it, _, reason = s.solve(b, x)
-            if reason != "converged":
-                raise SystemExit(f"problem {q} {prob['mesh']}: {reason}")
-            its.append(it)
+            _, its, _, reasons = s.solve(b, x)
+            bad = [q for q, r in enumerate(reasons) if r != "converged"]
+            if bad:
+                raise SystemExit(f"right-hand side {j}: problems {bad} did not converge ({reasons[bad[0]]})")
+            its_all.append([int(v) for v in its])
             solve_ms += s.timing()[1]
-        s.close()
-        tot_setup += su
-        tot_solve += solve_ms
-        its_all += its
-        print(json.dumps({"case": "batch", "problem": q, "mesh": prob["mesh"], "precision": args.precision,
-                          "setup_ms": round(su, 3), "solve_ms": round(solve_ms, 3), "pcg_iters": its}), flush=True)
-    print(json.dumps({"case": "batch", "problems": args.count, "rhs": 4 * args.count, "precision": args.precision,
-                      "setup_ms_total": round(tot_setup, 3), "solve_ms_total": round(tot_solve, 3),
-                      "pcg_iters_mean": float(np.mean(its_all)), "pcg_iters_max": int(np.max(its_all))}), flush=True)
+        print(json.dumps({"case": "batch", "problems": args.count, "rhs": 4 * args.count, "precision": args.precision,
+                          "rep": rep, "setup_ms": round(su, 3), "solve_ms": round(solve_ms, 3),
+                          "pcg_iters_mean": float(np.mean(its_all)), "pcg_iters_max": int(np.max(its_all)),
+                          "pcg_iters_per_problem": [list(v) for v in zip(*its_all)]}), flush=True)
+    s.close()
 
 
 def main():

@@ -221,6 +221,80 @@ class DarcySolver:
         return {k: (float(m), int(n)) for k, m, n in zip(self.PROFILE_CLASSES, ms, nl)}
 
 
+class BatchSolver(DarcySolver):
+    """Independent problems set up and solved together (pmf_batch_*).
+
+    ``problems``: problem dicts as made by ``premixfem_b200.fields`` (dom, mesh,
+    kappa, dirichlet); ``sds``: subdomains per axis of each problem (one virtual
+    rank per problem).  Vectors of the batch live on the shared mesh the
+    library lays the problems out on; ``pack`` / ``unpack`` convert between it
+    and per-problem arrays."""
+
+    def __init__(self, problems, sds, options=""):
+        self.lib = _native.load()
+        self.nprob = len(problems)
+        if isinstance(options, dict):
+            options = options_string(options)
+        self.options = options
+        dom = np.ascontiguousarray([p["dom"] for p in problems], dtype=np.float64).ravel()
+        mesh = np.ascontiguousarray([p["mesh"] for p in problems], dtype=np.int32).ravel()
+        sd = np.ascontiguousarray(sds, dtype=np.int32).ravel()
+        h = C.c_void_p()
+        _native.check(self.lib.pmf_batch_create(self.nprob, dom.ctypes.data_as(C.c_void_p),
+                                                mesh.ctypes.data_as(C.c_void_p), sd.ctypes.data_as(C.c_void_p),
+                                                options.encode(), C.byref(h)))
+        self.h = h
+        shared = np.zeros(3, dtype=np.int32)
+        z0 = np.zeros(self.nprob, dtype=np.int32)
+        _native.check(self.lib.pmf_batch_info(self.h, shared.ctypes.data_as(C.c_void_p), z0.ctypes.data_as(C.c_void_p)))
+        self.mesh = tuple(int(v) for v in shared)
+        self.z0 = [int(v) for v in z0]
+        self.meshes = [tuple(int(v) for v in p["mesh"]) for p in problems]
+        self.n = self.mesh[0] * self.mesh[1] * self.mesh[2]
+        for q, p in enumerate(problems):
+            for face, v in p.get("dirichlet", {}).items():
+                _native.check(self.lib.pmf_batch_set_dirichlet(self.h, q, FACE_IDS[face], float(v)))
+
+    def pack(self, arrays):
+        """Per-problem arrays (natural order, x fastest) -> one shared-mesh vector (float64, zero padding)."""
+        M, N, P = self.mesh
+        out = np.zeros((P, N, M))
+        for q, a in enumerate(arrays):
+            Mq, Nq, Pq = self.meshes[q]
+            out[self.z0[q]:self.z0[q] + Pq, :Nq, :Mq] = np.asarray(a, dtype=np.float64).reshape(Pq, Nq, Mq)
+        return out.ravel()
+
+    def unpack(self, v):
+        """One shared-mesh vector -> the per-problem arrays (flat, natural order)."""
+        M, N, P = self.mesh
+        v = np.asarray(v).reshape(P, N, M)
+        return [np.ascontiguousarray(v[self.z0[q]:self.z0[q] + Pq, :Nq, :Mq]).ravel()
+                for q, (Mq, Nq, Pq) in enumerate(self.meshes)]
+
+    def set_kappa_problems(self, problems):
+        self.set_kappa(*(self.pack([p["kappa"][d] for p in problems]) for d in range(3)))
+
+    def set_dirichlet(self, face, value):
+        raise ValueError("a batch takes its Dirichlet faces per problem (from the problem dicts)")
+
+    def solve(self, b, out=None):
+        """One PCG per problem; returns (x, its, rnorm, reasons), the last three one entry per problem."""
+        pb, dev, keep = _ptr(b)
+        if out is None:
+            if dev:
+                import torch
+                out = torch.empty_like(b)
+            else:
+                out = np.empty(self.n)
+        px, dev2, keep2 = _ptr(out, writable=True)
+        its = np.zeros(self.nprob, dtype=np.int32)
+        rn = np.zeros(self.nprob)
+        reason = np.zeros(self.nprob, dtype=np.int32)
+        _native.check(self.lib.pmf_batch_solve(self.h, pb, px, dev, its.ctypes.data_as(C.c_void_p),
+                                               rn.ctypes.data_as(C.c_void_p), reason.ctypes.data_as(C.c_void_p)))
+        return out, its, rn, [REASONS.get(int(r), str(int(r))) for r in reason]
+
+
 # ---------------------------------------------------------------------------
 # The reference's interface (src/PreMixFEM_3D.h:32-67), same names and order.
 class PCCtx:

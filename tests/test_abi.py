@@ -72,3 +72,36 @@ def test_option_errors_come_before_the_device():
             "-pmf_eig_init 1 -pmf_precision mixed", "-use_2level -no_shift_A_cc"]
     for opts in good:
         assert create("-sd 2 " + opts) in (0, 76), opts
+
+
+def test_batch_layout_and_argument_checks():
+    """Host side of pmf_batch_create: argument errors come before the device
+    (62 with or without a GPU), and the shared-mesh packing round-trips."""
+    import ctypes as C
+
+    import numpy as np
+
+    from premixfem_b200 import _native
+    from premixfem_b200.solver import BatchSolver
+
+    lib = _native.load()
+    dom = np.ones(6)
+    mesh = np.array([8, 8, 8, 0, 8, 8], dtype=np.int32)
+    sd = np.full(6, 2, dtype=np.int32)
+    h = C.c_void_p()
+    assert lib.pmf_batch_create(2, dom.ctypes.data_as(C.c_void_p), mesh.ctypes.data_as(C.c_void_p),
+                                sd.ctypes.data_as(C.c_void_p), b"", C.byref(h)) == 62
+    assert lib.pmf_batch_create(0, None, None, None, b"", C.byref(h)) == 62
+    mesh[3] = 8
+    assert lib.pmf_batch_create(2, dom.ctypes.data_as(C.c_void_p), mesh.ctypes.data_as(C.c_void_p),
+                                sd.ctypes.data_as(C.c_void_p), b"-eg_op 9", C.byref(h)) == 62
+    # packing on the shared mesh (no device needed): the layout the library reports
+    s = BatchSolver.__new__(BatchSolver)
+    s.meshes = [(3, 4, 2), (5, 2, 3)]
+    s.mesh = (5, 4, 2 + 1 + 3)
+    s.z0 = [0, 3]
+    a = [np.arange(24.0), 100 + np.arange(30.0)]
+    v = s.pack(a)
+    assert v.size == 5 * 4 * 6 and np.count_nonzero(v) == 24 + 30 - 1
+    back = s.unpack(v)
+    assert all(np.array_equal(x, y) for x, y in zip(a, back))
