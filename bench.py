@@ -20,7 +20,8 @@ Forms measured on the headline workload (fracture256):
                (host->device copies of kappa and source, device->host copies
                of the right-hand side and solution, inside the timed region)
 Accuracy: every form's solution against an FP64 reference solution (the
-device FP64 form solved to relative residual 1e-13), true residuals, the
+device FP64 form solved to relative residual 1e-13; 1e-11 and modulo
+constants for the pure-Neumann layered field), true residuals, the
 local eigensolvers' stop codes; in the CPU-baseline leg, a seeded sample of
 64 subdomains' local eigenvalues against the oracle's exact local GHEPs.
 Roofline: the kernels of one PCG iteration timed by class with CUDA events
@@ -88,6 +89,8 @@ WORKLOADS = {
              "computes the local basis in FP64 (-pmf_eig_precision fp64: with the FP32 eigensolver's 1e-6 "
              "residual the near-zero channel modes are too inexact and CG stalls)",
         mixed_opts={"pmf_eig_precision": "fp64"},
+        # the pure-Neumann operator's FP64 CG levels off near 1e-12; solutions are compared modulo constants
+        ref_rtol="1e-11", null_space=True,
         cpu_opts={"sd": (3, 11, 17), "vranks": (2, 2, 1), "en_lv1": 4, "en_lv2": 4, "constant_null_space": True},
     ),
     # 512 x 512 x 256 anisotropic GRF with fracture planes, k = 8.
@@ -354,15 +357,19 @@ def run_b200(args):
             s.close()
             del s
             gc.collect()
-        # FP64 reference solution: the device FP64 form solved to relative residual 1e-13
-        s = make_solver("fp64_ref", {"ksp_rtol": "1e-13"})
+        # FP64 reference solution: the device FP64 form solved to a tight relative residual
+        ref_rtol = wl.get("ref_rtol", "1e-13")
+        s = make_solver("fp64_ref", {"ksp_rtol": ref_rtol, "ksp_max_it": 20000})
         _, _, its_ref, _, reason_ref, b, xref = device_step(s)
         s.close()
         del s
+        if wl.get("null_space"):  # compare modulo constants
+            xref = xref - xref.mean()
+            sol = {f: v - v.mean() for f, v in sol.items()}
         nref = float(torch.linalg.norm(xref))
         err = {f: float(torch.linalg.norm(sol[f] - xref)) / nref for f in forms}
         out = dict(wl=wl, prob=prob, n=n, res=res, forms=forms, boxes=boxes, err=err,
-                   ref=dict(its=its_ref, reason=reason_ref))
+                   ref=dict(its=its_ref, reason=reason_ref, rtol=ref_rtol, null_space=bool(wl.get("null_space"))))
         del sol, xref, kx, src_d, kap
         gc.collect()
         torch.cuda.empty_cache()
@@ -375,8 +382,9 @@ def run_b200(args):
 
     def accuracy(m):
         return {"error_vs_fp64_ref": {f: m["err"][f] for f in m["forms"]},
-                "fp64_ref": f"device FP64 form, PCG to relative residual 1e-13 ({m['ref']['its']} iterations, "
-                            f"{m['ref']['reason']}); not a direct solve at this size"}
+                "fp64_ref": f"device FP64 form, PCG to relative residual {m['ref']['rtol']} ({m['ref']['its']} "
+                            f"iterations, {m['ref']['reason']}); not a direct solve at this size"
+                            + ("; solutions compared modulo constants (pure Neumann)" if m["ref"]["null_space"] else "")}
 
     main_name = args.workload
     m = measure(main_name, args.steps, args.warmup, headline=True)

@@ -94,6 +94,7 @@ def run_batch(args):
             solve_ms += s.timing()[1]
         print(json.dumps({"case": "batch", "problems": args.count, "rhs": 4 * args.count, "precision": args.precision,
                           "rep": rep, "setup_ms": round(su, 3), "solve_ms": round(solve_ms, 3),
+                          "stages_ms": {k: round(v, 3) for k, v in s.stages().items()},
                           "pcg_iters_mean": float(np.mean(its_all)), "pcg_iters_max": int(np.max(its_all)),
                           "pcg_iters_per_problem": [list(v) for v in zip(*its_all)]}), flush=True)
     s.close()
