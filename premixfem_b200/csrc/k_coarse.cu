@@ -651,12 +651,19 @@ static bool spd_inverse_cl(int nb, int n, double* a, double tol, int* nnull, cud
 }
 
 // The same Gauss-Jordan inverse spread over the whole GPU, for matrices too
-// large for one cluster: per pivot k, k_gj_pivot (one CTA per matrix) takes
-// column k and the scaled pivot row into scratch, and k_gj_update applies the
-// rank-1 update to every element of every matrix in parallel, with
-// k_spd_inverse's arithmetic per element (so the results agree bit for bit).
-// Matrix b has order nv[b] (or n) and starts at off[b] (or b n^2); pivots past
-// a matrix's order leave it alone.
+// large for one cluster, in panels of kGjPB pivots.  Eliminating the pivots P
+// of a panel turns [A_PP A_PR; A_RP A_RR] into
+//   A_PP <- Z = A_PP^-1,  A_PR <- Z A_PR,  A_RP <- -A_RP Z,  A_RR <- A_RR - A_RP Z A_PR,
+// which is what the pivots one at a time give in exact arithmetic; Z comes
+// from the pivot-by-pivot Gauss-Jordan of the diagonal block with
+// k_spd_inverse's arithmetic and null-pivot rule (a pivot at or below
+// tol x max|diag| drops its row and column), so a null pivot zeroes its row
+// and column of the result as before.  Per panel: k_gjb_diag (one CTA per
+// matrix), k_gjb_rows (R = Z A_PR), k_gjb_update (the rank-kGjPB update of
+// every element outside the panel: 64 x 64 tiles, 2 n^2 kGjPB flops per
+// panel), k_gjb_cols (A_RP) and k_gjb_prow (A_PR, A_PP).  Matrix b has order
+// nv[b] (or n) and starts at off[b] (or b n^2); panels past a matrix's order
+// leave it alone.
 struct GjShape {
   const int* nv;         // per matrix order, or null (all n)
   const long long* off;  // per matrix offset, or null (b n^2)
@@ -664,6 +671,10 @@ struct GjShape {
   __device__ int ord(int b) const { return nv ? nv[b] : n; }
   __device__ long long at(int b) const { return off ? off[b] : (long long)b * n * n; }
 };
+constexpr int kGjPB = 64;  // pivots per panel
+constexpr int kGjT = 64;   // tile edge of the update
+constexpr int kGjLd = kGjPB + 1;
+
 __global__ void k_gj_scale(GjShape sh, const double* a_all, double* scale) {
   const int nb = sh.ord(blockIdx.x);
   const double* a = a_all + sh.at(blockIdx.x);
@@ -680,43 +691,195 @@ __global__ void k_gj_scale(GjShape sh, const double* a_all, double* scale) {
     scale[blockIdx.x] = m > 0 ? m : 1.0;
   }
 }
-__global__ void k_gj_pivot(GjShape sh, const double* a_all, int k, double tol, const double* scale, double* colk,
-                           double* rowk, int* nullk, int* nnull) {
+
+// Z = inverse of the panel's diagonal block, pivot by pivot in shared memory.
+__global__ void __launch_bounds__(256) k_gjb_diag(GjShape sh, const double* a_all, int k0, double tol,
+                                                  const double* scale, double* zbuf, int* nnull) {
   const int b = blockIdx.x;
   const int n = sh.ord(b);
-  if (k >= n) return;
+  if (k0 >= n) return;
+  const int pb = min(kGjPB, n - k0);
   const double* a = a_all + sh.at(b);
-  const long long base = (long long)b * sh.n;
-  const double piv = a[(long long)k * n + k];
-  const bool isnull = !(piv > tol * scale[b]);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    colk[base + i] = a[(long long)i * n + k];
-    rowk[base + i] = isnull ? 0.0 : (i == k ? 1.0 : a[(long long)k * n + i]) / piv;
+  __shared__ double z[kGjPB][kGjLd];
+  __shared__ double colk[kGjPB], rowk[kGjPB];
+  const int tid = threadIdx.x, bd = blockDim.x;
+  for (int e = tid; e < pb * pb; e += bd) {
+    const int i = e / pb, j = e % pb;
+    z[i][j] = a[(long long)(k0 + i) * n + k0 + j];
   }
-  if (threadIdx.x == 0) {
-    nullk[b] = isnull ? 1 : 0;
-    if (isnull && nnull) atomicAdd(nnull, 1);
+  __syncthreads();
+  const double thr = tol * scale[b];
+  int nul = 0;
+  for (int kk = 0; kk < pb; ++kk) {
+    const double piv = z[kk][kk];
+    const bool isnull = !(piv > thr);
+    for (int i = tid; i < pb; i += bd) {
+      colk[i] = z[i][kk];
+      rowk[i] = isnull ? 0.0 : (i == kk ? 1.0 : z[kk][i]) / piv;
+    }
+    __syncthreads();
+    for (int e = tid; e < pb * pb; e += bd) {
+      const int i = e / pb, j = e % pb;
+      if (isnull) {
+        if (i == kk || j == kk) z[i][j] = 0.0;
+      } else if (i == kk) {
+        z[i][j] = rowk[j];
+      } else {
+        z[i][j] = (j == kk ? 0.0 : z[i][j]) - colk[i] * rowk[j];
+      }
+    }
+    __syncthreads();
+    nul += isnull ? 1 : 0;
   }
+  double* zb = zbuf + (long long)b * kGjPB * kGjPB;
+  for (int e = tid; e < pb * pb; e += bd) zb[(e / pb) * kGjPB + e % pb] = z[e / pb][e % pb];
+  if (tid == 0 && nnull && nul) atomicAdd(nnull, nul);
 }
-__global__ void k_gj_update(GjShape sh, double* a_all, int k, const double* colk, const double* rowk,
-                            const int* nullk) {
+
+// R[c][j] = sum_c' Z[c][c'] A[k0 + c'][j] for the columns j outside the panel; 64 columns per CTA.
+__global__ void __launch_bounds__(256) k_gjb_rows(GjShape sh, const double* a_all, int k0, const double* zbuf,
+                                                  double* rbuf) {
   const int b = blockIdx.y;
   const int n = sh.ord(b);
-  if (k >= n) return;
-  double* a = a_all + sh.at(b);
-  const long long nn = (long long)n * n, base = (long long)b * sh.n;
-  const bool isnull = nullk[b] != 0;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e / n), j = (int)(e % n);
-    if (isnull) {
-      if (i == k || j == k) a[e] = 0.0;
-    } else if (i == k) {
-      a[e] = rowk[base + j];
-    } else {
-      a[e] = (j == k ? 0.0 : a[e]) - colk[base + i] * rowk[base + j];
+  const int j0 = blockIdx.x * kGjT;
+  if (k0 >= n || j0 >= n) return;
+  const int pb = min(kGjPB, n - k0);
+  const double* a = a_all + sh.at(b);
+  extern __shared__ double gj_sm[];
+  double* zs = gj_sm;                 // [kGjPB][kGjLd]
+  double* as = gj_sm + kGjPB * kGjLd;  // [kGjPB][kGjT + 1]
+  const double* zb = zbuf + (long long)b * kGjPB * kGjPB;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < pb * pb; e += blockDim.x) zs[(e / pb) * kGjLd + e % pb] = zb[(e / pb) * kGjPB + e % pb];
+  for (int e = tid; e < pb * kGjT; e += blockDim.x) {
+    const int c = e / kGjT, jj = e % kGjT, j = j0 + jj;
+    as[c * (kGjT + 1) + jj] = j < n ? a[(long long)(k0 + c) * n + j] : 0.0;
+  }
+  __syncthreads();
+  double* rb = rbuf + (long long)b * kGjPB * sh.n;
+  const int tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int c = ty + 16 * r;
+    if (c >= pb) continue;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int q = 0; q < pb; ++q) {
+      const double zv = zs[c * kGjLd + q];
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2) acc[s2] += zv * as[q * (kGjT + 1) + tx + 16 * s2];
+    }
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) {
+      const int j = j0 + tx + 16 * s2;
+      if (j < n && (j < k0 || j >= k0 + pb)) rb[(long long)c * sh.n + j] = acc[s2];
     }
   }
 }
+
+// A[i][j] -= sum_c A[i][k0 + c] R[c][j] for i, j outside the panel; one 64 x 64 tile per CTA.
+__global__ void __launch_bounds__(256) k_gjb_update(GjShape sh, double* a_all, int k0, const double* rbuf,
+                                                    int ntile) {
+  const int b = blockIdx.y;
+  const int n = sh.ord(b);
+  const int i0 = (blockIdx.x / ntile) * kGjT, j0 = (blockIdx.x % ntile) * kGjT;
+  if (k0 >= n || i0 >= n || j0 >= n) return;
+  const int pb = min(kGjPB, n - k0);
+  double* a = a_all + sh.at(b);
+  extern __shared__ double gj_sm[];
+  double* ls = gj_sm;                 // [kGjT][kGjLd]: A[i0 + ii][k0 + c]
+  double* rs = gj_sm + kGjT * kGjLd;  // [kGjPB][kGjT + 1]: R[c][j0 + jj]
+  const double* rb = rbuf + (long long)b * kGjPB * sh.n;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kGjT * pb; e += blockDim.x) {
+    const int ii = e / pb, c = e % pb, i = i0 + ii;
+    ls[ii * kGjLd + c] = i < n ? a[(long long)i * n + k0 + c] : 0.0;
+  }
+  for (int e = tid; e < pb * kGjT; e += blockDim.x) {
+    const int c = e / kGjT, jj = e % kGjT, j = j0 + jj;
+    rs[c * (kGjT + 1) + jj] = (j < n && (j < k0 || j >= k0 + pb)) ? rb[(long long)c * sh.n + j] : 0.0;
+  }
+  __syncthreads();
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) acc[r][s2] = 0.0;
+  for (int c = 0; c < pb; ++c) {
+    double lv[4], rv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) lv[r] = ls[(ty + 16 * r) * kGjLd + c];
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) rv[s2] = rs[c * (kGjT + 1) + tx + 16 * s2];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2) acc[r][s2] += lv[r] * rv[s2];
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = i0 + ty + 16 * r;
+    if (i >= n || (i >= k0 && i < k0 + pb)) continue;
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) {
+      const int j = j0 + tx + 16 * s2;
+      if (j < n && (j < k0 || j >= k0 + pb)) a[(long long)i * n + j] -= acc[r][s2];
+    }
+  }
+}
+
+// A[i][k0 + c] = -sum_c' A[i][k0 + c'] Z[c'][c] for the rows i outside the panel; 64 rows per CTA.
+__global__ void __launch_bounds__(256) k_gjb_cols(GjShape sh, double* a_all, int k0, const double* zbuf) {
+  const int b = blockIdx.y;
+  const int n = sh.ord(b);
+  const int i0 = blockIdx.x * kGjT;
+  if (k0 >= n || i0 >= n) return;
+  const int pb = min(kGjPB, n - k0);
+  double* a = a_all + sh.at(b);
+  extern __shared__ double gj_sm[];
+  double* zs = gj_sm;                 // [kGjPB][kGjLd]
+  double* ls = gj_sm + kGjPB * kGjLd;  // [kGjT][kGjLd]
+  const double* zb = zbuf + (long long)b * kGjPB * kGjPB;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < pb * pb; e += blockDim.x) zs[(e / pb) * kGjLd + e % pb] = zb[(e / pb) * kGjPB + e % pb];
+  for (int e = tid; e < kGjT * pb; e += blockDim.x) {
+    const int ii = e / pb, c = e % pb, i = i0 + ii;
+    ls[ii * kGjLd + c] = i < n ? a[(long long)i * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  const int tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = i0 + ty + 16 * r;
+    if (i >= n || (i >= k0 && i < k0 + pb)) continue;
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) {
+      const int c = tx + 16 * s2;
+      if (c >= pb) continue;
+      double acc = 0.0;
+      for (int q = 0; q < pb; ++q) acc += ls[(ty + 16 * r) * kGjLd + q] * zs[q * kGjLd + c];
+      a[(long long)i * n + k0 + c] = -acc;
+    }
+  }
+}
+
+// the panel's rows: A[k0 + c][j] = R[c][j] outside the panel, Z[c][j - k0] inside
+__global__ void k_gjb_prow(GjShape sh, double* a_all, int k0, const double* zbuf, const double* rbuf) {
+  const int b = blockIdx.y;
+  const int n = sh.ord(b);
+  if (k0 >= n) return;
+  const int pb = min(kGjPB, n - k0);
+  double* a = a_all + sh.at(b);
+  const double* zb = zbuf + (long long)b * kGjPB * kGjPB;
+  const double* rb = rbuf + (long long)b * kGjPB * sh.n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)pb * n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), j = (int)(e % n);
+    a[(long long)(k0 + c) * n + j] =
+        (j >= k0 && j < k0 + pb) ? zb[c * kGjPB + (j - k0)] : rb[(long long)c * sh.n + j];
+  }
+}
+
 __global__ void k_gj_sym(GjShape sh, double* a_all) {
   const int b = blockIdx.y;
   const int n = sh.ord(b);
@@ -735,22 +898,32 @@ __global__ void k_gj_sym(GjShape sh, double* a_all) {
 static bool gj_inverse(int nb, GjShape sh, double* a, double tol, int* nnull, cudaStream_t st) {
   const int n = sh.n;
   double* scr = nullptr;
-  const size_t bytes = sizeof(double) * (size_t)nb * (2 * (size_t)n + 2);
+  const size_t bytes = sizeof(double) * (size_t)nb * (1 + (size_t)kGjPB * kGjPB + (size_t)kGjPB * n);
   if (cudaMallocAsync((void**)&scr, bytes, st) != cudaSuccess) {
     (void)cudaGetLastError();
     return false;
   }
   double* scale = scr;
-  double* colk = scr + nb;
-  double* rowk = colk + (size_t)nb * n;
-  int* nullk = reinterpret_cast<int*>(rowk + (size_t)nb * n);
+  double* zbuf = scr + nb;
+  double* rbuf = zbuf + (size_t)nb * kGjPB * kGjPB;
+  const int sm_rows = (int)(sizeof(double) * (kGjPB * kGjLd + kGjPB * (kGjT + 1)));
+  const int sm_upd = (int)(sizeof(double) * (kGjT * kGjLd + kGjPB * (kGjT + 1)));
+  const int sm_cols = (int)(sizeof(double) * (kGjPB * kGjLd + kGjT * kGjLd));
+  cudaFuncSetAttribute(k_gjb_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_rows);
+  cudaFuncSetAttribute(k_gjb_update, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_upd);
+  cudaFuncSetAttribute(k_gjb_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_cols);
   { note_launch(); k_gj_scale<<<nb, 256, 0, st>>>(sh, a, scale); }
+  const int nt = (n + kGjT - 1) / kGjT;
+  const int gp = (int)std::max<long long>(1, std::min<long long>(((long long)kGjPB * n + 255) / 256, 64));
+  for (int k0 = 0; k0 < n; k0 += kGjPB) {
+    { note_launch(); k_gjb_diag<<<nb, 256, 0, st>>>(sh, a, k0, tol, scale, zbuf, nnull); }
+    { note_launch(); k_gjb_rows<<<dim3(nt, nb), 256, sm_rows, st>>>(sh, a, k0, zbuf, rbuf); }
+    { note_launch(); k_gjb_update<<<dim3(nt * nt, nb), 256, sm_upd, st>>>(sh, a, k0, rbuf, nt); }
+    { note_launch(); k_gjb_cols<<<dim3(nt, nb), 256, sm_cols, st>>>(sh, a, k0, zbuf); }
+    { note_launch(); k_gjb_prow<<<dim3(gp, nb), 256, 0, st>>>(sh, a, k0, zbuf, rbuf); }
+  }
   const long long nn = (long long)n * n;
   const int gx = (int)std::max<long long>(1, std::min<long long>((nn + 255) / 256, (148 * 8 + nb - 1) / nb));
-  for (int k = 0; k < n; ++k) {
-    { note_launch(); k_gj_pivot<<<nb, 256, 0, st>>>(sh, a, k, tol, scale, colk, rowk, nullk, nnull); }
-    { note_launch(); k_gj_update<<<dim3(gx, nb), 256, 0, st>>>(sh, a, k, colk, rowk, nullk); }
-  }
   { note_launch(); k_gj_sym<<<dim3(gx, nb), 256, 0, st>>>(sh, a); }
   cudaFreeAsync(scr, st);
   return true;

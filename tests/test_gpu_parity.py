@@ -55,6 +55,10 @@ CASES = {
                     {"sd": 2, "pmf_vranks": (1, 2, 2), "en_lv1": 4, "en_lv2": 4}),
     "aniso_wcycle": (lambda: dict(fields.aniso_const(8, 8, 8), dirichlet={"z+": 1.0}),
                      {"sd": 2, "en_lv1": 3, "en_lv2": 2, "use_W_cycle": True}),
+    # one virtual rank of 144 subdomains: 576 coarse unknowns, past the cluster
+    # inverse (384), so the rank's level-2 and rank-Neumann inverses take the
+    # panel Gauss-Jordan over nine 64-pivot panels
+    "grf24_rank576": (lambda: fields.unit_cube_grf(24, seed=5), {"pmf_sd": (6, 6, 4), "en_lv1": 4, "en_lv2": 4}),
 }
 
 
