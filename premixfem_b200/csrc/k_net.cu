@@ -274,6 +274,219 @@ __global__ void __launch_bounds__(ROWS * 2 / MT) k_net_fwd(FwdArgs a) {
   }
 }
 
+// ---- 3x3x3 convolutions of 16^3 patches on the tcgen05 tensor cores ---------------------------
+// One CTA (four warps) per patch marches through the 16 output z-planes.  The
+// input planes z-1, z, z+1 sit with a one-voxel zero halo in a ring of four
+// shared-memory slots ([slot][cin/8][18][18][8 channels] BF16) while plane
+// z+2 is copied in with cp.async; all 27 taps' weights stay resident in the
+// UMMA K-major layout ([tap][k-step][2][cout/8][8][8]).  An output plane is
+// two 128-row tiles (rows y x 8 x-positions, one per x half), and for tap
+// (dx, dy, dz) a tile's A operand is just a window of the haloed plane: a
+// no-swizzle K-major descriptor whose 8-row groups step by one haloed row
+// (288 B) and whose two 8-channel groups step by one channel plane, so the
+// im2col gather costs nothing.  One thread issues the 27 x cin/16 x 2
+// tcgen05.mma (kind::f16, BF16 in, FP32 accumulation in TMEM, M = 128,
+// N = cout) and commits them to the plane's mbarrier; the accumulators are
+// double-buffered across planes so that the epilogue of plane z-1
+// (tcgen05.ld, bias, ReLU, BF16 store) overlaps the MMAs of plane z.  Every
+// wait is bounded; a wait that runs out sets *err and skips the stores.
+// TMA multicast is not used (single-GPU code).
+namespace {
+constexpr int kTcPl = 18 * 18;                 // positions of one haloed plane
+constexpr long long kTcSpin = 1LL << 24;      // mbarrier polls before giving up
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool tc_mbar_try(uint64_t* b, uint32_t ph) {
+  uint32_t ok;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok)
+               : "r"(smem_u32(b)), "r"(ph)
+               : "memory");
+  return ok != 0;
+}
+// shared-memory matrix descriptor: no swizzle, K-major, sm_100 version bit
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M x N
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+template <int CIN, int COUT>
+constexpr size_t tc_conv_smem() {
+  return (size_t)27 * CIN * COUT * 2 + 4 * (CIN / 8) * kTcPl * 16 + 64;
+}
+}  // namespace
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128, 1) k_net_conv_tc(const __nv_bfloat16* in, const __nv_bfloat16* wpk,
+                                                       const float* bias, __nv_bfloat16* out, int* err) {
+  constexpr int VIN = CIN / 8, KS = CIN / 16;
+  constexpr int WBYTES = 27 * CIN * COUT * 2;
+  constexpr int SLOT = VIN * kTcPl * 16;
+  constexpr int NCOL = 4 * COUT <= 32 ? 32 : (4 * COUT <= 64 ? 64 : (4 * COUT <= 128 ? 128 : 256));
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && 4 * COUT <= 256, "tile shape");
+  extern __shared__ __align__(1024) unsigned char tc_sm[];
+  unsigned char* slab = tc_sm + WBYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(slab + 4 * SLOT);
+  uint32_t* taddr_s = reinterpret_cast<uint32_t*>(mbar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.x;
+  const __nv_bfloat16* inb = in + (size_t)b * 4096 * CIN;
+  const uint32_t wsa = smem_u32(tc_sm), sla = smem_u32(slab);
+  for (int c = tid; c < WBYTES / 16; c += 128)
+    cp_async16(tc_sm + c * 16, reinterpret_cast<const char*>(wpk) + c * 16, true);
+  auto load_plane = [&](int zi) {
+    unsigned char* base = slab + ((zi + 1) & 3) * SLOT;
+    for (int e = tid; e < VIN * kTcPl; e += 128) {
+      const int cg = e / kTcPl, pp = e % kTcPl, y = pp / 18 - 1, x = pp % 18 - 1;
+      const bool ok = zi >= 0 && zi < 16 && y >= 0 && y < 16 && x >= 0 && x < 16;
+      const __nv_bfloat16* src = ok ? inb + ((size_t)((zi * 16 + y) * 16 + x) * CIN + cg * 8) : inb;
+      cp_async16(base + (cg * kTcPl + pp) * 16, src, ok);
+    }
+  };
+  load_plane(-1);
+  load_plane(0);
+  cp_async_commit();
+  load_plane(1);
+  cp_async_commit();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
+                 "r"(NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    tc_mbar_init(mbar);
+    tc_mbar_init(mbar + 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *taddr_s;
+  constexpr uint32_t idesc = tc_idesc(128, COUT);
+  bool ok = true;
+  auto wait_mma = [&](int zz) {
+    for (long long s = 0; !tc_mbar_try(mbar + (zz & 1), (uint32_t)((zz >> 1) & 1)); ++s)
+      if (s > kTcSpin) {
+        ok = false;
+        break;
+      }
+  };
+  auto epilogue = [&](int zz) {
+    const uint32_t buf = (uint32_t)((zz & 1) * 2 * COUT);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int m = 32 * warp + lane, y = m >> 3, x = 8 * h + (m & 7);
+      __nv_bfloat16* op = out + ((size_t)b * 4096 + (zz * 16 + y) * 16 + x) * COUT;
+#pragma unroll
+      for (int c0 = 0; c0 < COUT; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + buf + (uint32_t)(h * COUT + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(ta));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        uint32_t pk[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float v0 = fmaxf(__uint_as_float(r[2 * q]) + bias[c0 + 2 * q], 0.f);
+          const float v1 = fmaxf(__uint_as_float(r[2 * q + 1]) + bias[c0 + 2 * q + 1], 0.f);
+          __nv_bfloat162 bb = __floats2bfloat162_rn(v0, v1);
+          pk[q] = *reinterpret_cast<uint32_t*>(&bb);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(op + c0);
+        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+      }
+    }
+  };
+  for (int z = 0; z < 16; ++z) {
+    cp_async_wait<0>();  // the weights and the planes up to z + 1 have landed
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t dbuf = tmem + (uint32_t)((z & 1) * 2 * COUT);
+      int cnt = 0;
+      for (int t = 0; t < 27; ++t) {
+        const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+        const uint32_t pbase = sla + (uint32_t)(((z + dz + 1) & 3) * SLOT);
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          const uint64_t bd = tc_desc(wsa + (uint32_t)((t * KS + ks) * 16 * COUT * 2), (COUT / 8) * 128, 128);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t a0 = pbase + (uint32_t)(((2 * ks) * kTcPl + (1 + dy) * 18 + (1 + dx + 8 * h)) * 16);
+            const uint64_t ad = tc_desc(a0, kTcPl * 16, 18 * 16);
+            const uint32_t acc = cnt >= 2 ? 1u : 0u;  // each half's first MMA starts from zero
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                    dbuf + (uint32_t)(h * COUT)),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            ++cnt;
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(mbar + (z & 1)))
+                   : "memory");
+    }
+    // plane z + 2 replaces plane z - 2, which the MMAs of plane z - 1 read last
+    if (z >= 1) wait_mma(z - 1);
+    if (z + 2 <= 16) load_plane(z + 2);
+    cp_async_commit();
+    if (z >= 1 && ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(z - 1);
+    }
+  }
+  wait_mma(15);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) epilogue(15);
+  if (!ok) atomicOr(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL));
+}
+
+// W[tap][cin][cout] (BF16) -> [tap][cin/16][2][cout/8][8 n][8 k], the B operand of k_net_conv_tc
+__global__ void k_net_pack_tc(int cin, int cout, const __nv_bfloat16* w16, __nv_bfloat16* wpk) {
+  const int n = 27 * cin * cout;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int co = i % cout, ci = (i / cout) % cin, t = i / (cin * cout);
+    const int ks = ci / 16, k = ci % 16;
+    const size_t blk = (size_t)(t * (cin / 16) + ks) * 16 * cout;
+    wpk[blk + ((k / 8) * (cout / 8) + co / 8) * 64 + (co % 8) * 8 + k % 8] = w16[i];
+  }
+}
+
+// layers k_net_conv_tc takes: 3x3x3 on 16^3 with ReLU, no skip, BF16 output
+static bool conv_tc_layer(const NetLayer& L) {
+  return L.type == NL_CONV3 && L.s_in == 16 && L.s_out == 16 && L.relu && L.skip < 0 &&
+         ((L.cin == 16 && L.cout == 32) || (L.cin == 32 && L.cout == 32));
+}
+
+static void conv_tc_launch(const NetLayer& L, const __nv_bfloat16* in, const __nv_bfloat16* wpk, const float* bias,
+                           __nv_bfloat16* out, int B, int* err, cudaStream_t st) {
+  if (L.cin == 16) {
+    constexpr size_t sm = tc_conv_smem<16, 32>();
+    cudaFuncSetAttribute(k_net_conv_tc<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_net_conv_tc<16, 32><<<B, 128, sm, st>>>(in, wpk, bias, out, err);
+  } else {
+    constexpr size_t sm = tc_conv_smem<32, 32>();
+    cudaFuncSetAttribute(k_net_conv_tc<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_net_conv_tc<32, 32><<<B, 128, sm, st>>>(in, wpk, bias, out, err);
+  }
+}
+
 // ---- backward -------------------------------------------------------------------------------
 struct DgradArgs {
   int type, cin, cout, s_in, s_out, B;
@@ -637,7 +850,7 @@ Net::Net() {}
 
 Net::~Net() {
   for (int l = 0; l < NET_LAYERS; ++l) {
-    void* p[] = {w32_[l], b32_[l], w16_[l], wt_[l], gw_[l], gb_[l], mw_[l], vw_[l], mb_[l], vb_[l]};
+    void* p[] = {w32_[l], b32_[l], w16_[l], wt_[l], wtc_[l], gw_[l], gb_[l], mw_[l], vw_[l], mb_[l], vb_[l]};
     for (void* q : p)
       if (q) cudaFree(q);
   }
@@ -645,6 +858,20 @@ Net::~Net() {
     if (a > 0 && act_[a]) cudaFree(act_[a]);
     if (dact_[a]) cudaFree(dact_[a]);
   }
+  if (d_err_) cudaFree(d_err_);
+}
+
+int Net::take_error() {
+  if (!d_err_) return 0;
+  int f = 0;
+  if (cudaMemcpy(&f, d_err_, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    err = "reading the network's kernel flag failed";
+    return 76;
+  }
+  if (!f) return 0;
+  cudaMemset(d_err_, 0, sizeof(int));
+  err = "a tensor-core convolution's wait for its MMAs ran out";
+  return 76;
 }
 
 int Net::params() const {
@@ -662,6 +889,7 @@ int Net::alloc_params() {
               cudaMalloc(&gw_[l], nw * 4) == cudaSuccess && cudaMalloc(&gb_[l], nb * 4) == cudaSuccess &&
               cudaMalloc(&mw_[l], nw * 4) == cudaSuccess && cudaMalloc(&vw_[l], nw * 4) == cudaSuccess &&
               cudaMalloc(&mb_[l], nb * 4) == cudaSuccess && cudaMalloc(&vb_[l], nb * 4) == cudaSuccess;
+    if (ok && conv_tc_layer(kNetLayers[l])) ok = cudaMalloc(&wtc_[l], nw * 2) == cudaSuccess;
     if (!ok) {
       err = "cudaMalloc of the network parameters failed";
       return 76;
@@ -671,6 +899,11 @@ int Net::alloc_params() {
     cudaMemset(mb_[l], 0, nb * 4);
     cudaMemset(vb_[l], 0, nb * 4);
   }
+  if (cudaMalloc(&d_err_, sizeof(int)) != cudaSuccess) {
+    err = "cudaMalloc of the network parameters failed";
+    return 76;
+  }
+  cudaMemset(d_err_, 0, sizeof(int));
   return 0;
 }
 
@@ -678,6 +911,7 @@ void Net::refresh(int l, cudaStream_t st) {
   const NetLayer& L = kNetLayers[l];
   const long long n = (long long)wcount(L);
   { note_launch(); k_net_refresh<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(net_taps(L.type), L.cin, L.cout, w32_[l], w16_[l], wt_[l]); }
+  if (wtc_[l]) { note_launch(); k_net_pack_tc<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(L.cin, L.cout, w16_[l], wtc_[l]); }
 }
 
 int Net::set_weights(int l, const float* w, const float* b) {
@@ -860,7 +1094,7 @@ int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_
     // is the built-in choice, the tuner may pick another for this layer and batch
     const int per = L.type == NL_UP2 ? L.s_in * L.s_in * L.s_in : L.s_out * L.s_out * L.s_out;
     static const int kTiles[4][2] = {{256, 2}, {128, 1}, {128, 2}, {64, 1}};
-    int cand[4], nc = 0;
+    int cand[5], nc = 0;
     const int def = per % 256 == 0 ? 0 : 3;
     cand[nc++] = def;
     for (int t = 0; t < 4; ++t)
@@ -870,9 +1104,18 @@ int Net::forward(const __nv_bfloat16* x, int B, float* y, bool keep, cudaStream_
       err = "unsupported layer width";
       return 56;
     }
-    auto launch = [&](int c) -> bool { return fwd_launch(ntv, kTiles[cand[c]][0], kTiles[cand[c]][1], a, rows, st); };
+    // the tensor-core convolution (candidate index 4) where the layer fits it
+    const bool tc = wtc_[l] && conv_tc_layer(L) && !a.outf;
+    if (tc) cand[nc++] = 4;
+    auto launch = [&](int c) -> bool {
+      if (cand[c] == 4) {
+        conv_tc_launch(L, a.in, wtc_[l], a.bias, a.out, B, d_err_, st);
+        return true;
+      }
+      return fwd_launch(ntv, kTiles[cand[c]][0], kTiles[cand[c]][1], a, rows, st);
+    };
     char key[96];
-    snprintf(key, sizeof(key), "net_fwd|L%d|B%d", l, B);
+    snprintf(key, sizeof(key), tc ? "net_fwd|L%d|B%d|tc" : "net_fwd|L%d|B%d", l, B);
     const int c = tune_choose(key, nc, launch, st);
     note_launch();
     launch(c);

@@ -79,7 +79,9 @@ int pmf_net_layer_info(int layer, int info[6]) {
 int pmf_net_forward(pmf_net* h, const void* x, int B, float* y) {
   if (!h || !x || !y || B < 1) return pmf_internal_fail(62, "bad argument to pmf_net_forward");
   if (int e = h->n.forward((const __nv_bfloat16*)x, B, y, true, 0)) return net_fail(h, e);
-  return launch_check("pmf_net_forward");
+  if (int e = launch_check("pmf_net_forward")) return e;
+  if (int e = h->n.take_error()) return net_fail(h, e);
+  return 0;
 }
 
 int pmf_net_backward(pmf_net* h, const float* dy, int B) {

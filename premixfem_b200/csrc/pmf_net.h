@@ -76,6 +76,8 @@ class Net {
   int get_weights(int layer, float* w, float* b) const;
   int set_weights(int layer, const float* w, const float* b);
   int get_grads(int layer, float* gw, float* gb) const;
+  // 76 (and err) when a tensor-core convolution's bounded wait ran out since the last call
+  int take_error();
 
   std::string err;
 
@@ -84,6 +86,8 @@ class Net {
   float* b32_[NET_LAYERS] = {};
   __nv_bfloat16* w16_[NET_LAYERS] = {};
   float* wt_[NET_LAYERS] = {};  // FP32 W[tap][cout][cin] for the input-gradient kernel
+  __nv_bfloat16* wtc_[NET_LAYERS] = {};  // UMMA B-operand layout for k_net_conv_tc (its layers only)
+  int* d_err_ = nullptr;                 // wait-ran-out flag of k_net_conv_tc
   float* gw_[NET_LAYERS] = {};
   float* gb_[NET_LAYERS] = {};
   float* mw_[NET_LAYERS] = {};

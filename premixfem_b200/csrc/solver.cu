@@ -921,6 +921,12 @@ int Solver::run_learned_eigen(LobpcgArgs& la, int eig_blocks, double eb1) {
   cudaEventSynchronize(n1);
   cudaEventElapsedTime(&ms, n0, n1);
   net_ms = ms;
+  if (int e = net->take_error()) {
+    err = net->err;
+    cudaEventDestroy(n0);
+    cudaEventDestroy(n1);
+    return e;
+  }
   cudaEventDestroy(n0);
   cudaEventDestroy(n1);
   return 0;

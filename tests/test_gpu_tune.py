@@ -2,8 +2,9 @@
 
 The tuner chooses by speed alone, so each candidate launch shape is checked
 here by forcing it (PMF_TUNE_FORCE=c): the network forward pass of each row
-tile against the CPU oracle (2e-2, the forward-pass tolerance of
-test_gpu_net.py), and the preconditioner application with each thread count
+tile, and of the tcgen05 convolution (candidate 4, the 3x3x3 layers on 16^3
+patches; the other layers clamp to their last tile), against the CPU oracle
+(2e-2, the forward-pass tolerance of test_gpu_net.py), and the preconditioner application with each thread count
 of the level-1 solve and the level-2 restriction / prolongation against the
 built-in shape (1e-12 in FP64, 1e-5 in mixed precision: only the order of the
 block reductions changes).  The report of a tuned set-up lists its choices.
@@ -25,7 +26,7 @@ def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
 
 
-@pytest.mark.parametrize("cand", [0, 1, 2, 3])
+@pytest.mark.parametrize("cand", [0, 1, 2, 3, 4])
 def test_net_forward_every_tile(native, monkeypatch, cand):
     torch = pytest.importorskip("torch")
     monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
