@@ -28,9 +28,9 @@ Roofline: the kernels of one PCG iteration timed by class with CUDA events
 on the solver stream (pmf_profile_iteration); the dominant class is the
 `roofline` object.
 
-Secondary workloads (--extra, default "layered,large512,batch64") run after the
-headline with their own 3 warm-up + 3 timed steps per form and are reported
-under "workloads" in the same line.
+Secondary workloads (--extra, default "fracture256_2level,layered,large512,
+batch64") run after the headline with their own 3 warm-up + 3 timed steps per
+form and are reported under "workloads" in the same line.
 
 Multi-GPU (torchrun, N ranks): every rank solves its own seeded replica on
 its own GPU (no data-path collective: replicas only); step time is the max
@@ -77,6 +77,14 @@ WORKLOADS = {
              "rtol 1e-8 (seeded synthetic field, seed 4)",
         sample_n=128, sample_opts={"sd": 4, "vranks": (2, 2, 2), "en_lv1": 6, "en_lv2": 4},
         cpu_opts={"sd": 4, "vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4},
+    ),
+    # the same field through the reference's -use_2level branch: one global coarse problem
+    # (24 576 unknowns, banded Cholesky) in place of levels 2 and 3
+    "fracture256_2level": dict(
+        make=lambda seed: fields.fracture256(256, seed=seed),
+        opts={"sd": 4, "pmf_vranks": (4, 4, 4), "en_lv1": 6, "en_lv2": 4, "use_2level": True},
+        desc="fracture256 with -use_2level: the global Phi^T A Phi (24 576 unknowns) by the tiled banded "
+             "Cholesky, random eigensolver starts",
     ),
     # 60 x 220 x 85 layered channel field (pure Neumann, constant null space), k = 4.
     "layered": dict(
@@ -681,7 +689,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="fracture256",
                     choices=sorted(k for k, v in WORKLOADS.items() if not v.get("batch")))
-    ap.add_argument("--extra", default="layered,large512,batch64",
+    ap.add_argument("--extra", default="fracture256_2level,layered,large512,batch64",
                     help="secondary workloads measured after the headline (comma separated, '' for none)")
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -130,6 +130,82 @@ __global__ void k_bpcg_iter_a_fin(const double* part, int nblk, PcgState* st) {
   }
 }
 
+// The same step one cell per thread: a (32 x 4)-thread CTA covers 32 x 4 cells of
+// one layer of the shared mesh, whose problem is layer_prob[z] (separator
+// layers: none); partial (z gy + y) gx + x, so problem q's partials are the
+// contiguous range of its layers.
+__global__ void __launch_bounds__(128) k_bpcg_iter_a1(Grid g, const int* layer_prob, const double* __restrict__ tx,
+                                                     const double* __restrict__ ty, const double* __restrict__ tz,
+                                                     const double* __restrict__ diag, const double* __restrict__ z,
+                                                     const double* __restrict__ pin, double* pout, double* w,
+                                                     double* part, const PcgState* st) {
+  __shared__ double red[4];
+  const int ez = blockIdx.z;
+  const int q = layer_prob[ez];
+  if (q < 0) return;
+  const PcgState& s = st[q];
+  if (s.done) return;
+  const bool first = s.first != 0;
+  const double b = first ? 0.0 : s.beta / s.betaold;
+  const int ex = blockIdx.x * 32 + threadIdx.x, ey = blockIdx.y * 4 + threadIdx.y;
+  double v = 0.0;
+  if (ex < g.M && ey < g.N) {
+    const long long c = ((long long)ez * g.N + ey) * g.M + ex;
+#define PNEW(i) (first ? z[i] : z[i] + b * pin[i])
+    const double pcv = PNEW(c);
+    double a = diag[c] * pcv;
+    if (ex > 0) a -= tx[c] * PNEW(c - 1);
+    if (ex < g.M - 1) a -= tx[c + 1] * PNEW(c + 1);
+    if (ey > 0) a -= ty[c] * PNEW(c - g.M);
+    if (ey < g.N - 1) a -= ty[c + g.M] * PNEW(c + g.M);
+    if (ez > 0) a -= tz[c] * PNEW(c - g.MN);
+    if (ez < g.P - 1) a -= tz[c + g.MN] * PNEW(c + g.MN);
+#undef PNEW
+    pout[c] = pcv;
+    w[c] = a;
+    v = pcv * a;
+  }
+  v = warp_sum(v);
+  if (threadIdx.x == 0) red[threadIdx.y] = v;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    part[((long long)ez * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = ((red[0] + red[1]) + red[2]) + red[3];
+}
+__global__ void __launch_bounds__(1024) k_bpcg_iter_a1_fin(const ProbInfo* probs, const double* part, int per_layer,
+                                                           PcgState* st) {
+  __shared__ double red[32];
+  const int q = blockIdx.x;
+  PcgState& s = st[q];
+  if (s.done) return;
+  const ProbInfo pq = probs[q];
+  const double* pp = part + (long long)pq.z0 * per_layer;
+  const int n = pq.P * per_layer;
+  double a8[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) a8[u] = 0.0;
+  for (int i0 = threadIdx.x; i0 < n; i0 += 8 * blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) a8[u] += pp[i];
+    }
+  }
+  const double dpi = block_sum(((a8[0] + a8[1]) + (a8[2] + a8[3])) + ((a8[4] + a8[5]) + (a8[6] + a8[7])), red);
+  if (threadIdx.x == 0) {
+    s.dpiold = s.dpi;
+    s.dpi = dpi;
+    s.betaold = s.beta;
+    const bool flip = !s.first && ((dpi > 0) != (s.dpiold > 0));
+    s.first = 0;
+    if (dpi == 0.0 || flip) {
+      s.its += 1;
+      s.done = 3;  // KSP_DIVERGED_INDEFINITE_MAT
+    } else {
+      s.alpha = s.beta / dpi;
+    }
+  }
+}
+
 // x += alpha p, r -= alpha w, partial r.r
 __global__ void k_bpcg_iter_b(const ProbInfo* probs, double* x, double* r, const double* p, const double* w,
                               double* part, const PcgState* st, int nblk) {
@@ -188,9 +264,16 @@ void launch_bpcg_start(const ProbInfo* probs, int nprob, const double* b, double
 void launch_bpcg_beta(const ProbInfo* probs, int nprob, const double* part, PcgState* st, cudaStream_t s) {
   { note_launch(); k_bpcg_beta_fin<<<nprob, 256, 0, s>>>(probs, part, st); }
 }
-void launch_bpcg_iter_a(const Grid& g, const ProbInfo* probs, int nprob, const double* tx, const double* ty,
-                        const double* tz, const double* diag, const double* z, const double* pin, double* pout,
-                        double* w, double* part, PcgState* st, int nblk, cudaStream_t s) {
+void launch_bpcg_iter_a(const Grid& g, const ProbInfo* probs, const int* layer_prob, int nprob, const double* tx,
+                        const double* ty, const double* tz, const double* diag, const double* z, const double* pin,
+                        double* pout, double* w, double* part, PcgState* st, int nblk, cudaStream_t s) {
+  // one cell per thread (pcg_part_capacity(g) partials) where the grid fits, else the grid-stride form
+  const dim3 grid((g.M + 31) / 32, (g.N + 3) / 4, g.P);
+  if (layer_prob && grid.y <= 65535 && grid.z <= 65535) {
+    { note_launch(); k_bpcg_iter_a1<<<grid, dim3(32, 4), 0, s>>>(g, layer_prob, tx, ty, tz, diag, z, pin, pout, w, part, st); }
+    { note_launch(); k_bpcg_iter_a1_fin<<<nprob, 1024, 0, s>>>(probs, part, (int)(grid.x * grid.y), st); }
+    return;
+  }
   { note_launch(); k_bpcg_iter_a<<<dim3(nblk, nprob), kBT, 0, s>>>(g, probs, tx, ty, tz, diag, z, pin, pout, w, part, st, nblk); }
   { note_launch(); k_bpcg_iter_a_fin<<<nprob, 256, 0, s>>>(part, nblk, st); }
 }

@@ -1172,19 +1172,295 @@ __global__ void __launch_bounds__(512) k_dense_smallest_eig(RankLayout L, int en
   if (tid == 0) iters[r] = it + 1;
 }
 
+// The same iteration for ranks whose block does not fit in shared memory, in
+// phases over all ranks: the two dense products of an iteration (Y = inv X
+// and AY = A X) spread over CTAs of 32 rows each, the projected problems
+// (SVQB of Y, Rayleigh-Ritz on A) one CTA per rank.  The Ritz vectors' images
+// are rotated with the vectors (A (X U) = (A X) U) instead of recomputed, so an
+// iteration streams each rank's two matrices once.  A converged rank's
+// kernels return at once; the host checks every 8 iterations whether all
+// ranks have converged.
+struct L3Rank {
+  double anorm;
+  double w[PMF_L3_MAXP];
+  int q, conv, it;
+};
+constexpr int kL3Rows = 32;    // rows per CTA of the products
+constexpr int kL3Tile = 256;   // l-values per shared-memory tile of the block
+constexpr int kL3Cols = 16;    // columns the product kernel holds in registers
+
+__global__ void k_l3_init(RankLayout L, int p, const double* A_all, double* work_all, L3Rank* st) {
+  const int r = blockIdx.x;
+  const int nr = rank_nr(L, r);
+  const double* A = A_all + L.off2[r];
+  double* X = work_all + L.offw[r];
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < nr; i += blockDim.x) m = fmax(m, fabs(A[(long long)i * nr + i]));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmax(v, red[w]);
+    st[r].anorm = v > 0 ? v : 1.0;
+    for (int c = 0; c < PMF_L3_MAXP; ++c) st[r].w[c] = 0.0;
+    st[r].q = p;
+    st[r].conv = 0;
+    st[r].it = 0;
+  }
+  for (long long e = threadIdx.x; e < (long long)nr * p; e += blockDim.x)
+    X[e] = hash_uniform(((unsigned long long)r << 40) ^ (unsigned long long)e);
+}
+
+// Out = M In for the rank's first `cols` columns (cols = p, or the kept count q): block src/dst of the
+// rank's workspace (0 X, 1 Y, 2 AY), 32 rows per CTA, 8 warps x 4 rows, lanes along the row.
+__global__ void __launch_bounds__(256) k_l3_mm(RankLayout L, int p, const double* M_all, double* work_all, int src,
+                                               int dst, int use_q, const L3Rank* st) {
+  const int r = blockIdx.y;
+  if (st[r].conv) return;
+  const int nr = rank_nr(L, r);
+  const int i0 = blockIdx.x * kL3Rows;
+  if (i0 >= nr) return;
+  const int cols = use_q ? st[r].q : p;
+  const double* M = M_all + L.off2[r];
+  const double* In = work_all + L.offw[r] + (long long)src * nr * p;
+  double* Out = work_all + L.offw[r] + (long long)dst * nr * p;
+  __shared__ double xs[kL3Tile][kL3Cols + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double acc[4][kL3Cols];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < kL3Cols; ++c) acc[a][c] = 0.0;
+  for (int l0 = 0; l0 < nr; l0 += kL3Tile) {
+    for (int e = threadIdx.x; e < kL3Tile * kL3Cols; e += blockDim.x) {
+      const int l = e / kL3Cols, c = e % kL3Cols;
+      xs[l][c] = (l0 + l < nr && c < cols) ? In[(long long)(l0 + l) * p + c] : 0.0;
+    }
+    __syncthreads();
+    const int lend = min(kL3Tile, nr - l0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = i0 + wid * 4 + a;
+      if (i >= nr) continue;
+      const double* row = M + (long long)i * nr + l0;
+      for (int l = lane; l < lend; l += 32) {
+        const double mv = row[l];
+#pragma unroll
+        for (int c = 0; c < kL3Cols; ++c) acc[a][c] += mv * xs[l][c];
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + wid * 4 + a;
+#pragma unroll
+    for (int c = 0; c < kL3Cols; ++c) {
+      const double v = warp_sum(acc[a][c]);
+      if (lane == 0 && i < nr && c < cols) Out[(long long)i * p + c] = v;
+    }
+  }
+}
+
+// SVQB of Y: G = Y^T Y, D^-1/2 G D^-1/2 = U w U^T, X = Y D^-1/2 U w^-1/2 on the kept columns (q).
+__global__ void __launch_bounds__(512) k_l3_svqb(RankLayout L, int p, double* work_all, L3Rank* st) {
+  const int r = blockIdx.x;
+  if (st[r].conv) return;
+  const int nr = rank_nr(L, r);
+  double* X = work_all + L.offw[r];
+  const double* Y = X + (long long)nr * p;
+  __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP],
+      C[PMF_L3_MAXP * PMF_L3_MAXP], dsc[PMF_L3_MAXP], jac[64];
+  __shared__ int ijac[32];
+  __shared__ int keep;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < p * p; e += nt) {
+    const int a = e / p, b = e % p;
+    double acc = 0.0;
+    for (int l = 0; l < nr; ++l) acc += Y[(long long)l * p + a] * Y[(long long)l * p + b];
+    G[a * PMF_L3_MAXP + b] = acc;
+  }
+  __syncthreads();
+  if (tid < p) dsc[tid] = 1.0 / sqrt(fmax(G[tid * PMF_L3_MAXP + tid], 1e-300));
+  __syncthreads();
+  for (int e = tid; e < p * p; e += nt) {
+    const int a = e / p, b = e % p;
+    G[a * PMF_L3_MAXP + b] *= dsc[a] * dsc[b];
+  }
+  __syncthreads();
+  cta_jacobi_eigh(G, U, w, p, PMF_L3_MAXP, ijac, jac);
+  if (tid == 0) {
+    int kk = 0;
+    const double wmax = w[p - 1];
+    for (int c = p - 1; c >= 0; --c)
+      if (w[c] > 1e-12 * wmax) ++kk;
+    keep = kk;
+    st[r].q = kk;
+  }
+  __syncthreads();
+  const int q = keep;  // kept columns are the last q (largest w)
+  for (int e = tid; e < p * q; e += nt) {
+    const int a = e / q, c = e % q;
+    const int cc = p - q + c;
+    C[a * PMF_L3_MAXP + c] = dsc[a] * U[a * PMF_L3_MAXP + cc] / sqrt(w[cc]);
+  }
+  __syncthreads();
+  for (long long e = tid; e < (long long)nr * q; e += nt) {
+    const int i = (int)(e / q), c = (int)(e % q);
+    double acc = 0.0;
+    for (int a = 0; a < p; ++a) acc += Y[(long long)i * p + a] * C[a * PMF_L3_MAXP + c];
+    X[(long long)i * p + c] = acc;
+  }
+}
+
+// Rayleigh-Ritz on A: H = X^T AY, H = U w U^T, X <- X U, AY <- AY U, residual test of the wanted pairs;
+// columns dropped by the SVQB get fresh random directions for the next iteration.
+__global__ void __launch_bounds__(512) k_l3_rr(RankLayout L, int en2, int p, double* work_all, L3Rank* st,
+                                               double tol, int it) {
+  const int r = blockIdx.x;
+  if (st[r].conv) return;
+  const int nr = rank_nr(L, r);
+  double* X = work_all + L.offw[r];
+  double* Y = X + (long long)nr * p;
+  double* AY = Y + (long long)nr * p;
+  __shared__ double G[PMF_L3_MAXP * PMF_L3_MAXP], U[PMF_L3_MAXP * PMF_L3_MAXP], w[PMF_L3_MAXP], jac[64];
+  __shared__ int ijac[32];
+  __shared__ int conv;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int q = st[r].q;
+  for (int e = tid; e < q * q; e += nt) {
+    const int a = e / q, b = e % q;
+    double acc = 0.0;
+    for (int l = 0; l < nr; ++l) acc += X[(long long)l * p + a] * AY[(long long)l * p + b];
+    G[a * PMF_L3_MAXP + b] = acc;
+  }
+  __syncthreads();
+  for (int e = tid; e < q * q; e += nt) {  // symmetrise
+    const int a = e / q, b = e % q;
+    if (a < b) {
+      const double v = 0.5 * (G[a * PMF_L3_MAXP + b] + G[b * PMF_L3_MAXP + a]);
+      G[a * PMF_L3_MAXP + b] = v;
+      G[b * PMF_L3_MAXP + a] = v;
+    }
+  }
+  __syncthreads();
+  cta_jacobi_eigh(G, U, w, q, PMF_L3_MAXP, ijac, jac);
+  // X <- X U and AY <- AY U, through Y
+  for (long long e = tid; e < (long long)nr * q; e += nt) {
+    const int i = (int)(e / q), c = (int)(e % q);
+    double ax = 0.0;
+    for (int a = 0; a < q; ++a) ax += X[(long long)i * p + a] * U[a * PMF_L3_MAXP + c];
+    Y[(long long)i * p + c] = ax;
+  }
+  __syncthreads();
+  for (long long e = tid; e < (long long)nr * q; e += nt) {
+    const int i = (int)(e / q), c = (int)(e % q);
+    X[(long long)i * p + c] = Y[(long long)i * p + c];
+  }
+  __syncthreads();
+  for (long long e = tid; e < (long long)nr * q; e += nt) {
+    const int i = (int)(e / q), c = (int)(e % q);
+    double ay = 0.0;
+    for (int a = 0; a < q; ++a) ay += AY[(long long)i * p + a] * U[a * PMF_L3_MAXP + c];
+    Y[(long long)i * p + c] = ay;
+  }
+  __syncthreads();
+  for (long long e = tid; e < (long long)nr * q; e += nt) {
+    const int i = (int)(e / q), c = (int)(e % q);
+    AY[(long long)i * p + c] = Y[(long long)i * p + c];
+  }
+  if (tid == 0) conv = q >= en2 ? 1 : 0;
+  __syncthreads();
+  const double thr = tol * st[r].anorm;
+  for (int c = tid; c < min(en2, q); c += nt) {
+    double rr = 0.0;
+    for (int l = 0; l < nr; ++l) {
+      const double v = AY[(long long)l * p + c] - w[c] * X[(long long)l * p + c];
+      rr += v * v;
+    }
+    if (sqrt(rr) > thr) conv = 0;
+  }
+  __syncthreads();
+  if (tid < q) st[r].w[tid] = w[tid];
+  if (tid == 0) {
+    st[r].it = it + 1;
+    st[r].conv = conv;
+  }
+  if (!conv)
+    for (long long e = tid; e < (long long)nr * (p - q); e += nt) {
+      const int i = (int)(e / (p - q)), c = q + (int)(e % (p - q));
+      X[(long long)i * p + c] = hash_uniform(((unsigned long long)(r + 7) << 44) ^ ((unsigned long long)it << 32) ^
+                                             (unsigned long long)e);
+    }
+}
+
+__global__ void k_l3_count(const L3Rank* st, int nrank, int* left) {
+  __shared__ int n;
+  if (threadIdx.x == 0) n = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < nrank; r += blockDim.x)
+    if (!st[r].conv) atomicAdd(&n, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) *left = n;
+}
+
+__global__ void k_l3_out(RankLayout L, int en2, int p, const double* work_all, const L3Rank* st, double* V_all,
+                         double* evals_all, int* iters) {
+  const int r = blockIdx.x;
+  const int nr = rank_nr(L, r);
+  const double* X = work_all + L.offw[r];
+  double* V = V_all + L.offv[r];
+  for (long long e = threadIdx.x; e < (long long)nr * en2; e += blockDim.x) {
+    const int i = (int)(e / en2), j = (int)(e % en2);
+    V[e] = X[(long long)i * p + j];
+  }
+  if (threadIdx.x < en2) evals_all[(long long)r * en2 + threadIdx.x] = st[r].w[threadIdx.x];
+  if (threadIdx.x == 0) iters[r] = st[r].it;
+}
+
 void launch_dense_smallest_eig(const RankLayout& L, int nrank, int nr, int en2, int p, const double* A,
                                const double* inv, double* V, double* evals, int* iters, double tol, int max_it,
                                double* work, cudaStream_t st) {
   // stage the iteration block in shared memory (odd leading dimension: no bank conflicts) when it fits
-  int ldx = p | 1;
-  size_t smem = (size_t)nr * ldx * sizeof(double);
-  if (smem > 160 * 1024) {
-    ldx = 0;
-    smem = 0;
-  } else {  // the kernel also holds ~26 KB of static shared memory
-    cudaFuncSetAttribute(k_dense_smallest_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int ldx = p | 1;
+  const size_t smem = (size_t)nr * ldx * sizeof(double);
+  L3Rank* rs = nullptr;
+  int* left = nullptr;
+  if (smem > 160 * 1024 && p <= kL3Cols && cudaMallocAsync((void**)&rs, sizeof(L3Rank) * nrank + 16, st) == cudaSuccess) {
+    left = reinterpret_cast<int*>(rs + nrank);
+    const int gx = (nr + kL3Rows - 1) / kL3Rows;
+    { note_launch(); k_l3_init<<<nrank, 256, 0, st>>>(L, p, A, work, rs); }
+    for (int it = 0; it < max_it; ++it) {
+      { note_launch(); k_l3_mm<<<dim3(gx, nrank), 256, 0, st>>>(L, p, inv, work, 0, 1, 0, rs); }
+      { note_launch(); k_l3_svqb<<<nrank, 512, 0, st>>>(L, p, work, rs); }
+      { note_launch(); k_l3_mm<<<dim3(gx, nrank), 256, 0, st>>>(L, p, A, work, 0, 2, 1, rs); }
+      { note_launch(); k_l3_rr<<<nrank, 512, 0, st>>>(L, en2, p, work, rs, tol, it); }
+      if ((it + 1) % 8 == 0 || it + 1 == max_it) {
+        int h = 1;
+        { note_launch(); k_l3_count<<<1, 256, 0, st>>>(rs, nrank, left); }
+        if (cudaMemcpyAsync(&h, left, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+          break;  // the caller's stream check reports the error
+        if (h == 0) break;
+      }
+    }
+    { note_launch(); k_l3_out<<<nrank, 256, 0, st>>>(L, en2, p, work, rs, V, evals, iters); }
+    cudaFreeAsync(rs, st);
+    return;
   }
-  { note_launch(); k_dense_smallest_eig<<<nrank, 512, smem, st>>>(L, en2, p, A, inv, V, evals, iters, tol, max_it, work, ldx); }
+  (void)cudaGetLastError();
+  int ld = ldx;
+  size_t sm = smem;
+  if (sm > 160 * 1024) {
+    ld = 0;
+    sm = 0;
+  } else {  // the kernel also holds ~26 KB of static shared memory
+    cudaFuncSetAttribute(k_dense_smallest_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  }
+  { note_launch(); k_dense_smallest_eig<<<nrank, 512, sm, st>>>(L, en2, p, A, inv, V, evals, iters, tol, max_it, work, ld); }
 }
 
 }  // namespace pmf

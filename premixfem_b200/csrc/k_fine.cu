@@ -169,6 +169,23 @@ __device__ __forceinline__ double fixed_sum(const double* part, int n, double* s
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
   return block_sum(v, scratch);
 }
+// The same for long partial lists (the one-cell-per-thread CG step writes one
+// per 128 cells): eight independent accumulators per thread keep eight loads
+// in flight, summed in a fixed order.
+__device__ __forceinline__ double fixed_sum_wide(const double* part, int n, double* scratch) {
+  double a[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) a[u] = 0.0;
+  for (int i0 = threadIdx.x; i0 < n; i0 += 8 * blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) a[u] += part[i];
+    }
+  }
+  const double v = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+  return block_sum(v, scratch);
+}
 
 __global__ void k_dot(const double* a, const double* b, long long n, double* part) {
   __shared__ double red[32];
@@ -321,10 +338,10 @@ __global__ void k_pcg_iter_a(Grid g, const double* tx, const double* ty, const d
   v = block_sum(v, red);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
-__global__ void k_pcg_iter_a_fin(const double* part, int nb, PcgState* s) {
+__global__ void __launch_bounds__(1024) k_pcg_iter_a_fin(const double* part, int nb, PcgState* s) {
   __shared__ double red[32];
   if (s->done) return;
-  const double dpi = fixed_sum(part, nb, red);
+  const double dpi = fixed_sum_wide(part, nb, red);
   if (threadIdx.x == 0) {
     s->dpiold = s->dpi;
     s->dpi = dpi;
@@ -344,6 +361,56 @@ __global__ void k_pcg_iter_a_fin(const double* part, int nb, PcgState* s) {
 // with a one-cell halo, the planes below and above in registers, so z and p
 // are read once per cell (plus the tile halo) instead of at all seven stencil
 // points.  The operator is evaluated in apply_A's order (same w bit for bit).
+// One cell per thread: a (32 x 4)-thread CTA covers 32 x 4 cells of one z-plane,
+// the grid covers the mesh, so no thread decodes a linear index and every load
+// has the whole GPU's parallelism behind it; the seven-point stencil reads its
+// neighbours through L1/L2.  Same arithmetic as k_pcg_iter_a, in the same
+// order.  One partial of p.w per CTA.
+constexpr int kP1X = 32, kP1Y = 4;
+__global__ void __launch_bounds__(kP1X * kP1Y) k_pcg_iter_a1(Grid g, const double* __restrict__ tx,
+                                                            const double* __restrict__ ty,
+                                                            const double* __restrict__ tz,
+                                                            const double* __restrict__ diag,
+                                                            const double* __restrict__ z,
+                                                            const double* __restrict__ pin, double* pout, double* w,
+                                                            double* part, const PcgState* s) {
+  __shared__ double red[kP1Y];
+  if (s->done) return;
+  const bool first = s->first != 0;
+  const double b = first ? 0.0 : s->beta / s->betaold;
+  const int ex = blockIdx.x * kP1X + threadIdx.x, ey = blockIdx.y * kP1Y + threadIdx.y, ez = blockIdx.z;
+  double v = 0.0;
+  if (ex < g.M && ey < g.N) {
+    const long long c = ((long long)ez * g.N + ey) * g.M + ex;
+#define PNEW(i) (first ? z[i] : z[i] + b * pin[i])
+    const double pc = PNEW(c);
+    double a = diag[c] * pc;
+    if (ex > 0) a -= tx[c] * PNEW(c - 1);
+    if (ex < g.M - 1) a -= tx[c + 1] * PNEW(c + 1);
+    if (ey > 0) a -= ty[c] * PNEW(c - g.M);
+    if (ey < g.N - 1) a -= ty[c + g.M] * PNEW(c + g.M);
+    if (ez > 0) a -= tz[c] * PNEW(c - g.MN);
+    if (ez < g.P - 1) a -= tz[c + g.MN] * PNEW(c + g.MN);
+#undef PNEW
+    pout[c] = pc;
+    w[c] = a;
+    v = pc * a;
+  }
+  v = warp_sum(v);
+  if (threadIdx.x == 0) red[threadIdx.y] = v;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    double t = 0.0;
+    for (int i = 0; i < kP1Y; ++i) t += red[i];
+    part[((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+int pcg_part_capacity(const Grid& g) {
+  const long long n1 = (long long)((g.M + kP1X - 1) / kP1X) * ((g.N + kP1Y - 1) / kP1Y) * g.P;
+  return (int)std::max<long long>(cell_blocks(g.ncell), n1);
+}
+
 constexpr int kPaX = 32, kPaY = 16;
 __global__ void __launch_bounds__(kPaX * kPaY) k_pcg_iter_a25(Grid g, const double* __restrict__ tx,
                                                              const double* __restrict__ ty,
@@ -401,14 +468,23 @@ __global__ void __launch_bounds__(kPaX * kPaY) k_pcg_iter_a25(Grid g, const doub
 int launch_pcg_iter_a_main(const Grid& g, const double* tx, const double* ty, const double* tz, const double* diag,
                            const double* z, const double* pin, double* pout, double* w, double* part,
                            const PcgState* s, cudaStream_t st, int variant) {
-  // partials: at most cell_blocks(ncell) blocks (the size the caller's buffer is guaranteed to hold)
+  // variant 0: one cell per thread (pcg_part_capacity(g) partials, the size the caller's buffer holds);
+  // 1: the 2.5-D march; 2: grid-stride.  Variants 1 and 2 use at most cell_blocks(ncell) partials.
+  if (variant == 0) {
+    const dim3 grid((g.M + kP1X - 1) / kP1X, (g.N + kP1Y - 1) / kP1Y, g.P);
+    if (grid.y <= 65535 && grid.z <= 65535) {
+      { note_launch(); k_pcg_iter_a1<<<grid, dim3(kP1X, kP1Y), 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s); }
+      return (int)(grid.x * grid.y * grid.z);
+    }
+    variant = 1;
+  }
   const int cap = cell_blocks(g.ncell);
   const int bx = (g.M + kPaX - 1) / kPaX, by = (g.N + kPaY - 1) / kPaY;
   const int per_z = std::max(1, cap / std::max(1, bx * by));
   const int zc = std::max(16, (g.P + per_z - 1) / per_z);
   const int bz = (g.P + zc - 1) / zc;
   const long long nb25 = (long long)bx * by * bz;
-  if (variant == 0 && nb25 <= cap && by <= 65535 && bz <= 65535) {
+  if (variant == 1 && nb25 <= cap && by <= 65535 && bz <= 65535) {
     { note_launch(); k_pcg_iter_a25<<<dim3(bx, by, bz), kPaX * kPaY, 0, st>>>(g, tx, ty, tz, diag, z, pin, pout, w, part, s, zc); }
     return (int)nb25;
   }
@@ -420,7 +496,7 @@ void launch_pcg_iter_a(const Grid& g, const double* tx, const double* ty, const 
                        const double* z, const double* pin, double* pout, double* w, double* part, PcgState* s,
                        cudaStream_t st, int variant) {
   const int nb = launch_pcg_iter_a_main(g, tx, ty, tz, diag, z, pin, pout, w, part, s, st, variant);
-  { note_launch(); k_pcg_iter_a_fin<<<1, 256, 0, st>>>(part, nb, s); }
+  { note_launch(); k_pcg_iter_a_fin<<<1, 1024, 0, st>>>(part, nb, s); }
 }
 
 // x += alpha p; r -= alpha w; partial r.r; then dp, its and the convergence test.

@@ -24,6 +24,7 @@ struct PcgState {
 
 constexpr int kCellThreads = 256;
 int cell_blocks(long long n);  // grid size for grid-stride cell loops (fixed per n)
+int pcg_part_capacity(const Grid& g);  // partial slots the PCG step kernels may write (>= cell_blocks)
 
 // ---- operator ----------------------------------------------------------------
 struct AssembleArgs {
@@ -76,9 +77,9 @@ void launch_dot(const double* a, const double* b, long long n, double* part, dou
 void launch_bpcg_start(const ProbInfo* probs, int nprob, const double* b, double* x, double* r, double* part,
                        PcgState* st, double rtol, double atol, int max_it, int* all_done, int nblk, cudaStream_t s);
 void launch_bpcg_beta(const ProbInfo* probs, int nprob, const double* part, PcgState* st, cudaStream_t s);
-void launch_bpcg_iter_a(const Grid& g, const ProbInfo* probs, int nprob, const double* tx, const double* ty,
-                        const double* tz, const double* diag, const double* z, const double* pin, double* pout,
-                        double* w, double* part, PcgState* st, int nblk, cudaStream_t s);
+void launch_bpcg_iter_a(const Grid& g, const ProbInfo* probs, const int* layer_prob, int nprob, const double* tx,
+                        const double* ty, const double* tz, const double* diag, const double* z, const double* pin,
+                        double* pout, double* w, double* part, PcgState* st, int nblk, cudaStream_t s);
 void launch_bpcg_iter_b(const ProbInfo* probs, int nprob, double* x, double* r, const double* p, const double* w,
                         double* part, PcgState* st, int* all_done, int nblk, cudaStream_t s);
 

@@ -653,7 +653,7 @@ int Solver::dalloc(void** p, size_t bytes, const char* what) {
 int Solver::alloc_fine() {
   const size_t n = (size_t)g.ncell;
   const size_t pb = opt.precision == 1 ? 4 : 8;
-  const int nparts = std::max(cell_blocks(g.ncell), nsub) + 64;
+  const int nparts = std::max(pcg_part_capacity(g), nsub) + 64;  // partial slots of the CG and level-1 kernels
   struct A {
     void** p;
     size_t bytes;
@@ -1521,8 +1521,8 @@ void Solver::tune_pc() {
     cudaMemsetAsync(p0, 0, sizeof(double) * g.ncell, st);
     cudaMemcpyAsync(state, &hs, sizeof(hs), cudaMemcpyHostToDevice, st);
     cudaStreamSynchronize(st);
-    snprintf(key, sizeof(key), "pcg_iter_a|M%d|N%d|P%d|p", g.M, g.N, g.P);
-    pcga_variant = tune_choose(key, 2, [&](int i) {
+    snprintf(key, sizeof(key), "pcg_iter_a|M%d|N%d|P%d|p3", g.M, g.N, g.P);
+    pcga_variant = tune_choose(key, 3, [&](int i) {
       launch_pcg_iter_a_main(g, tx, ty, tz, diag, z, p0, p1, w, part, state, st, i);
       return true;
     }, st);
@@ -1659,7 +1659,7 @@ int Solver::solve_batch(const double* b_in, double* x_out, bool on_device, int* 
   const int chunk = std::max(2, opt.pcg_chunk & ~1);  // even: the p buffers return to their roles
   auto enqueue_chunk = [&]() {
     for (int c_ = 0; c_ < chunk; ++c_) {
-      launch_bpcg_iter_a(g, d_probs, nprob, tx, ty, tz, diag, z, pin, pout, w, part, bstate, nblk, st);
+      launch_bpcg_iter_a(g, d_probs, d_layer_prob, nprob, tx, ty, tz, diag, z, pin, pout, w, part, bstate, nblk, st);
       launch_bpcg_iter_b(d_probs, nprob, xs, r, pout, w, part, bstate, d_all_done, nblk, st);
       apply(r, z, part, d_all_done);
       launch_bpcg_beta(d_probs, nprob, part, bstate, st);

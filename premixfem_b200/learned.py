@@ -259,6 +259,27 @@ def evaluate(weights, n=128, seed=77, precision="mixed", learned_its=60, eig_tol
     return res
 
 
+def time_forward(weights, batch, reps):
+    """Forward passes of the network on `batch` random 16^3 patches: ms per pass
+    (CUDA events after one untimed pass)."""
+    import torch
+
+    net = Net(path=weights)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((batch, 4096, 16), device="cuda", generator=g).to(torch.bfloat16)
+    y = torch.empty((batch, 4096, 16), dtype=torch.float32, device="cuda")
+    net.forward(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    net.close()
+    return {"batch": batch, "reps": reps, "ms_per_forward": e0.elapsed_time(e1) / reps}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -276,9 +297,16 @@ def main():
     e.add_argument("--n", type=int, default=128)
     e.add_argument("--seed", type=int, default=77)
     e.add_argument("--precision", default="mixed")
-    e.add_argument("--learned-its", type=int, default=30)
+    e.add_argument("--learned-its", type=int, default=60)
     e.add_argument("--eig-tol", type=float, default=None)
+    f = sub.add_parser("forward", help="time the forward pass on random patches (CUDA events)")
+    f.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    f.add_argument("--batch", type=int, default=512)
+    f.add_argument("--reps", type=int, default=3)
     a = ap.parse_args()
+    if a.cmd == "forward":
+        print(json.dumps(time_forward(a.weights, a.batch, a.reps)))
+        return
     if a.cmd == "train":
         fh = open(a.log, "w") if a.log else None
 

@@ -59,6 +59,9 @@ CASES = {
     # inverse (384), so the rank's level-2 and rank-Neumann inverses take the
     # panel Gauss-Jordan over nine 64-pivot panels
     "grf24_rank576": (lambda: fields.unit_cube_grf(24, seed=5), {"pmf_sd": (6, 6, 4), "en_lv1": 4, "en_lv2": 4}),
+    # 1 000 subdomains in one rank, 2 000 coarse unknowns: the level-3 eigensolver's
+    # block no longer fits in shared memory and runs as multi-CTA phases
+    "grf40_rank2000": (lambda: fields.unit_cube_grf(40, seed=6), {"pmf_sd": (10, 10, 10), "en_lv1": 2, "en_lv2": 4}),
 }
 
 

@@ -114,15 +114,15 @@ def test_eigensolver_every_online_shape(native, monkeypatch, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_solve_every_pcg_kernel(native, monkeypatch, precision):
-    """Both candidates of the CG step's fused p-update + operator kernel (the
-    2.5-D march and the grid-stride kernel; forced together with the other
-    shapes' candidates 0 / 1) converge in the same number of iterations (+-1)
-    to the same solution (1e-7 relative: only the order of the dot-product
-    partial sums differs)."""
+    """The three candidates of the CG step's fused p-update + operator kernel
+    (one cell per thread, the 2.5-D march, the grid-stride kernel; forced
+    together with the other shapes' candidates 0 / 1 / 2) converge in the same
+    number of iterations (+-1) to the same solution (1e-7 relative: only the
+    order of the dot-product partial sums differs)."""
     prob = fields.fracture256(64, seed=3)
     opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
     res = []
-    for cand in (0, 1):
+    for cand in (0, 1, 2):
         monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
         s = DarcySolver.from_problem(prob, opts)
         s.setup()
@@ -131,5 +131,6 @@ def test_solve_every_pcg_kernel(native, monkeypatch, precision):
         assert reason == "converged"
         res.append((x.copy(), its))
         s.close()
-    assert abs(res[1][1] - res[0][1]) <= 1, (res[0][1], res[1][1])
-    assert _rel(res[1][0], res[0][0]) <= 1e-7, _rel(res[1][0], res[0][0])
+    for cand in (1, 2):
+        assert abs(res[cand][1] - res[0][1]) <= 1, (cand, res[0][1], res[cand][1])
+        assert _rel(res[cand][0], res[0][0]) <= 1e-7, (cand, _rel(res[cand][0], res[0][0]))
