@@ -20,7 +20,7 @@ Forms measured on the headline workload (fracture256):
                (host->device copies of kappa and source, device->host copies
                of the right-hand side and solution, inside the timed region)
 Accuracy: every form's solution against an FP64 reference solution (the
-device FP64 form solved to relative residual 1e-13; 1e-11 and modulo
+device FP64 form solved to relative residual 1e-13; 1e-10 and modulo
 constants for the pure-Neumann layered field), true residuals, the
 local eigensolvers' stop codes; in the CPU-baseline leg, a seeded sample of
 64 subdomains' local eigenvalues against the oracle's exact local GHEPs.
@@ -97,8 +97,9 @@ WORKLOADS = {
              "computes the local basis in FP64 (-pmf_eig_precision fp64: with the FP32 eigensolver's 1e-6 "
              "residual the near-zero channel modes are too inexact and CG stalls)",
         mixed_opts={"pmf_eig_precision": "fp64"},
-        # the pure-Neumann operator's FP64 CG levels off near 1e-12; solutions are compared modulo constants
-        ref_rtol="1e-11", null_space=True,
+        # the pure-Neumann operator's FP64 CG levels off between 1e-11 and 1e-10 (1e-11 was not reached in
+        # 20 000 iterations); solutions are compared modulo constants
+        ref_rtol="1e-10", null_space=True,
         cpu_opts={"sd": (3, 11, 17), "vranks": (2, 2, 1), "en_lv1": 4, "en_lv2": 4, "constant_null_space": True},
     ),
     # 512 x 512 x 256 anisotropic GRF with fracture planes, k = 8.
@@ -310,6 +311,7 @@ def run_b200(args):
                 device_step(s)
             barrier()
             steps_l = []
+            stages0 = s.stages()
             launches0 = lib.pmf_launch_count()
             with ClockSampler(local) as clk:
                 for _ in range(steps):
@@ -318,6 +320,7 @@ def run_b200(args):
                     barrier()
                     steps_l.append((su, so, its, rn, reason))
             launches = lib.pmf_launch_count() - launches0
+            stages1 = s.stages()
             ev1, ks, it1, st1 = s.eigen_lv1()
             lst = (C.c_longlong * 4)()
             net_ms = C.c_double()
@@ -330,7 +333,11 @@ def run_b200(args):
                               status={"converged": int((st1 == 0).sum()), "rounding_floor": int((st1 == 2).sum()),
                                       "max_it": int((st1 == 1).sum())}),
                      ev1=ev1, learned=dict(used=int(lst[0]), fallbacks=int(lst[1]),
-                                           net_ms=round(net_ms.value, 3)))
+                                           net_ms=round(net_ms.value, 3)),
+                     # set-up stages per step (ms): local eigensolves, level-2 Galerkin + inverses,
+                     # level-3 eigensolve, level-3 Galerkin; the stage timers accumulate over set-ups
+                     stages_ms={k: round((stages1[k] - stages0[k]) * 1e3 / max(1, steps), 2)
+                                for k in ("su_lv1", "su_lv2_1", "su_lv2_2", "su_lv3_1", "su_lv3_2", "su")})
             if boxes is None:
                 boxes = s.subdomains()[0]
             r["t"] = r["setup_s"] + r["solve_s"]
@@ -386,7 +393,8 @@ def run_b200(args):
     def form_summary(r):
         return {"setup_s": round(r["setup_s"], 6), "solve_s": round(r["solve_s"], 6), "total_s": round(r["t"], 6),
                 "pcg_iters": r["its"], "reason": r["reason"], "rel_residual": r["rel_residual"],
-                "eigensolver": dict(r["eig"], learned_start=r["learned"]), "clocks": r["clocks"]}
+                "eigensolver": dict(r["eig"], learned_start=r["learned"]), "setup_stages_ms": r["stages_ms"],
+                "clocks": r["clocks"]}
 
     def accuracy(m):
         return {"error_vs_fp64_ref": {f: m["err"][f] for f in m["forms"]},
