@@ -4,9 +4,11 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdio>
 
 #include "pmf_dense.cuh"
 #include "pmf_kernels.h"
+#include "tune.h"
 
 namespace pmf {
 
@@ -948,11 +950,39 @@ void launch_spd_inverse_r(const RankLayout& L, int nrank, int nr_max, double* de
   cudaStreamSynchronize(st);  // the host vector must outlive the copy
 }
 
-void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
+// The cluster inverse for one of its three widths (false: the shape does not fit it, or the launch was refused).
+static bool spd_inverse_cluster(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
   const int R = (n + kSpdCl - 1) / kSpdCl;
-  if (n <= 128 && R <= kSpdWarps && spd_inverse_cl<4, 1>(nb, n, a, tol, nnull, st)) return;
-  if (n > 128 && n <= 256 && R <= 2 * kSpdWarps && spd_inverse_cl<8, 2>(nb, n, a, tol, nnull, st)) return;
-  if (n > 256 && n <= 384 && R <= 3 * kSpdWarps && spd_inverse_cl<12, 3>(nb, n, a, tol, nnull, st)) return;
+  if (n <= 128 && R <= kSpdWarps) return spd_inverse_cl<4, 1>(nb, n, a, tol, nnull, st);
+  if (n > 128 && n <= 256 && R <= 2 * kSpdWarps) return spd_inverse_cl<8, 2>(nb, n, a, tol, nnull, st);
+  if (n > 256 && n <= 384 && R <= 3 * kSpdWarps) return spd_inverse_cl<12, 3>(nb, n, a, tol, nnull, st);
+  return false;
+}
+
+void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaStream_t st) {
+  if (n <= 384) {
+    // up to 384 unknowns both the cluster inverse and the panel Gauss-Jordan apply: the tuner times
+    // them on a scratch copy of the matrices (the inverse works in place; no null counts while tuning)
+    int choice = 0;
+    if (n > 64 && tune_enabled()) {
+      double* scr = nullptr;
+      const size_t bytes = sizeof(double) * (size_t)nb * n * n;
+      if (cudaMallocAsync((void**)&scr, bytes, st) == cudaSuccess) {
+        char key[64];
+        snprintf(key, sizeof(key), "spd_inverse|n%d|b%d", n, nb);
+        choice = tune_choose(key, 2, [&](int c) {
+          cudaMemcpyAsync(scr, a, bytes, cudaMemcpyDeviceToDevice, st);
+          return c == 0 ? spd_inverse_cluster(nb, n, scr, tol, nullptr, st)
+                        : gj_inverse(nb, GjShape{nullptr, nullptr, n}, scr, tol, nullptr, st);
+        }, st);
+        cudaFreeAsync(scr, st);
+      } else {
+        (void)cudaGetLastError();
+      }
+    }
+    if (choice == 1 && gj_inverse(nb, GjShape{nullptr, nullptr, n}, a, tol, nnull, st)) return;
+    if (spd_inverse_cluster(nb, n, a, tol, nnull, st)) return;
+  }
   if (n > 384 && gj_inverse(nb, GjShape{nullptr, nullptr, n}, a, tol, nnull, st)) return;
   const int smem = 2 * n * sizeof(double);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_spd_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
