@@ -965,20 +965,21 @@ void launch_spd_inverse(int nb, int n, double* a, double tol, int* nnull, cudaSt
     // them on a scratch copy of the matrices (the inverse works in place; no null counts while tuning)
     int choice = 0;
     if (n > 64 && tune_enabled()) {
-      double* scr = nullptr;
+      double* scr = nullptr;  // allocated only when the key is tuned (the candidates run on it)
       const size_t bytes = sizeof(double) * (size_t)nb * n * n;
-      if (cudaMallocAsync((void**)&scr, bytes, st) == cudaSuccess) {
-        char key[64];
-        snprintf(key, sizeof(key), "spd_inverse|n%d|b%d", n, nb);
-        choice = tune_choose(key, 2, [&](int c) {
-          cudaMemcpyAsync(scr, a, bytes, cudaMemcpyDeviceToDevice, st);
-          return c == 0 ? spd_inverse_cluster(nb, n, scr, tol, nullptr, st)
-                        : gj_inverse(nb, GjShape{nullptr, nullptr, n}, scr, tol, nullptr, st);
-        }, st);
-        cudaFreeAsync(scr, st);
-      } else {
-        (void)cudaGetLastError();
-      }
+      char key[64];
+      snprintf(key, sizeof(key), "spd_inverse|n%d|b%d", n, nb);
+      choice = tune_choose(key, 2, [&](int c) {
+        if (!scr && cudaMallocAsync((void**)&scr, bytes, st) != cudaSuccess) {
+          (void)cudaGetLastError();
+          scr = nullptr;
+          return false;
+        }
+        cudaMemcpyAsync(scr, a, bytes, cudaMemcpyDeviceToDevice, st);
+        return c == 0 ? spd_inverse_cluster(nb, n, scr, tol, nullptr, st)
+                      : gj_inverse(nb, GjShape{nullptr, nullptr, n}, scr, tol, nullptr, st);
+      }, st);
+      if (scr) cudaFreeAsync(scr, st);
     }
     if (choice == 1 && gj_inverse(nb, GjShape{nullptr, nullptr, n}, a, tol, nnull, st)) return;
     if (spd_inverse_cluster(nb, n, a, tol, nnull, st)) return;

@@ -24,8 +24,9 @@
 // inverses X_m of the diagonal superblocks (computed once, null rows zeroed)
 //   forward   y_m = X_m (c_m - L_{m,m-1} y_{m-1}),
 //   backward  x_m = X_m^T (y_m - L_{m+1,m}^T x_{m+1}),
-// 4 NS launches of dense matrix-vector products per application, each
-// streaming its superblocks once.
+// dense matrix-vector products streaming each superblock once: a warp per row
+// forward; backward (transposed products) one CTA per 64 x 64 tile writing
+// column partial sums, added per column in a fixed order by a second launch.
 #include <algorithm>
 #include <vector>
 
@@ -343,36 +344,65 @@ __global__ void k_cband_fwd_diag(const double* X, int B, int m, const double* t,
   s = warp_sum(s);
   if (lane == 0) y[(long long)m * B * W + row] = s;
 }
-// backward, part 1: t_m = y_m - L_{m+1,m}^T x_{m+1}: column sums over the tiles (I, J), J in m, I in m+1
-__global__ void k_cband_bwd_off(const double* T, int B, int m, int NS, const double* y, const double* x, double* t,
-                                const int* done) {
+// backward, part 1: t_m = y_m - L_{m+1,m}^T x_{m+1}.  One CTA per tile (I, J) of
+// L_{m+1,m} (J in superblock m, I in m+1, inside the band): 64 columns x 4 groups
+// of 16 rows, the tile's column sums into part[(I - (m+1)B) B + (J - mB)];
+// k_cband_bwd_off_sum adds them per column in a fixed order.
+__global__ void __launch_bounds__(256) k_cband_bwd_off_part(const double* T, int B, int m, int NS, const double* x,
+                                                           double* part, const int* done) {
+  if (done && *done) return;
+  if (m + 1 >= NS) return;
+  const int il = blockIdx.x / B, jl = blockIdx.x % B;
+  const int I = (m + 1) * B + il, J = m * B + jl;
+  const int c = threadIdx.x & (W - 1), rg = threadIdx.x >> 6;
+  __shared__ double red[4][W];
+  double s = 0.0;
+  if (I - J <= B) {
+    const double* tl = tile_ptr(T, B, I, I - J);
+    const double* xx = x + (long long)I * W;
+    for (int r = rg * 16; r < rg * 16 + 16; ++r) s += tl[r * W + c] * xx[r];
+  }
+  red[rg][c] = s;
+  __syncthreads();
+  if (rg == 0) part[((long long)il * B + jl) * W + c] = ((red[0][c] + red[1][c]) + red[2][c]) + red[3][c];
+}
+__global__ void k_cband_bwd_off_sum(int B, int m, int NS, const double* y, const double* part, double* t,
+                                    const int* done) {
   if (done && *done) return;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per column of superblock m
   if (col >= B * W) return;
   const long long g = (long long)m * B * W + col;
   double s = 0.0;
   if (m + 1 < NS) {
-    const int J = m * B + col / W, c = col % W;
-    for (int I = (m + 1) * B; I <= min(J + B, (m + 2) * B - 1); ++I) {
-      const double* tl = tile_ptr(T, B, I, I - J);
-      const double* xx = x + (long long)I * W;
-      for (int r = 0; r < W; ++r) s += tl[r * W + c] * xx[r];
-    }
+    const int jl = col / W, c = col % W, J = m * B + jl;
+    for (int il = 0; il < B; ++il)
+      if ((m + 1) * B + il - J <= B) s += part[((long long)il * B + jl) * W + c];
   }
   t[g] = y[g] - s;
 }
-// backward, part 2: x_m = X_m^T t_m (column sums over the tiles of X_m)
-__global__ void k_cband_bwd_diag(const double* X, int B, int m, const double* t, double* x, const int* done) {
+// backward, part 2: x_m = X_m^T t_m, the same way over the tiles (i, j >= ... i) of X_m
+__global__ void __launch_bounds__(256) k_cband_bwd_diag_part(const double* X, int B, int m, const double* t,
+                                                            double* part, const int* done) {
+  if (done && *done) return;
+  const int i = blockIdx.x / B, j = blockIdx.x % B;
+  if (i < j) return;
+  const int c = threadIdx.x & (W - 1), rg = threadIdx.x >> 6;
+  __shared__ double red[4][W];
+  const double* xt = xtile(X, B, m, i, j);
+  const double* tt = t + (long long)m * B * W + (long long)i * W;
+  double s = 0.0;
+  for (int r = rg * 16; r < rg * 16 + 16; ++r) s += xt[r * W + c] * tt[r];
+  red[rg][c] = s;
+  __syncthreads();
+  if (rg == 0) part[((long long)i * B + j) * W + c] = ((red[0][c] + red[1][c]) + red[2][c]) + red[3][c];
+}
+__global__ void k_cband_bwd_diag_sum(int B, int m, const double* part, double* x, const int* done) {
   if (done && *done) return;
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= B * W) return;
   const int j = col / W, c = col % W;
-  const double* tt = t + (long long)m * B * W;
   double s = 0.0;
-  for (int i = j; i < B; ++i) {
-    const double* xt = xtile(X, B, m, i, j);
-    for (int r = 0; r < W; ++r) s += xt[r * W + c] * tt[i * W + r];
-  }
+  for (int i = j; i < B; ++i) s += part[((long long)i * B + j) * W + c];
   x[(long long)m * B * W + col] = s;
 }
 
@@ -455,7 +485,8 @@ void launch_cband_factor(const SubInfo* subs, int kmax, const double* blk, const
 }
 
 void launch_cband_solve(const int* d_perm, const CBandPlan& p, const double* T, const double* X, const double* c,
-                        double* out, double* v, double* y, double* t, const int* done, cudaStream_t st) {
+                        double* out, double* v, double* y, double* t, double* part, const int* done,
+                        cudaStream_t st) {
   const int B = p.B, NS = p.NS;
   const long long n = p.NTp * W;
   const int rows = B * W;
@@ -466,8 +497,10 @@ void launch_cband_solve(const int* d_perm, const CBandPlan& p, const double* T, 
   }
   // backward into v (the gathered right-hand side is no longer needed)
   for (int m = NS - 1; m >= 0; --m) {
-    { note_launch(); k_cband_bwd_off<<<(rows + 127) / 128, 128, 0, st>>>(T, B, m, NS, y, v, t, done); }
-    { note_launch(); k_cband_bwd_diag<<<(rows + 127) / 128, 128, 0, st>>>(X, B, m, t, v, done); }
+    if (m + 1 < NS) { note_launch(); k_cband_bwd_off_part<<<B * B, 256, 0, st>>>(T, B, m, NS, v, part, done); }
+    { note_launch(); k_cband_bwd_off_sum<<<(rows + 127) / 128, 128, 0, st>>>(B, m, NS, y, part, t, done); }
+    { note_launch(); k_cband_bwd_diag_part<<<B * B, 256, 0, st>>>(X, B, m, t, part, done); }
+    { note_launch(); k_cband_bwd_diag_sum<<<(rows + 127) / 128, 128, 0, st>>>(B, m, part, v, done); }
   }
   { note_launch(); k_cband_scatter<<<256, 256, 0, st>>>(d_perm, n, v, out, done); }
 }

@@ -213,7 +213,8 @@ void launch_cband_factor(const SubInfo* subs, int kmax, const double* blk, const
                          cudaStream_t st);
 // out = A2^+ c (natural coarse order); v, y, t: work vectors of NTp x 64 doubles
 void launch_cband_solve(const int* d_perm, const CBandPlan& p, const double* T, const double* X, const double* c,
-                        double* out, double* v, double* y, double* t, const int* done, cudaStream_t st);
+                        double* out, double* v, double* y, double* t, double* part, const int* done,
+                        cudaStream_t st);
 
 // ---- eigen solvers -----------------------------------------------------------------
 struct LobpcgArgs {

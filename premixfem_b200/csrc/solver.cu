@@ -275,6 +275,22 @@ int Solver::check(cudaError_t e, const char* what) {
   return 76;  // PETSC_ERR_LIB
 }
 
+// The set-up's stream-ordered scratch (cudaMallocAsync / cudaFreeAsync in the
+// coarse inverses and the level-3 eigensolves) comes from the device's default
+// memory pool; by default the pool hands freed memory back to the driver at
+// every synchronisation, so each set-up allocated it afresh, which stalled the
+// set-up for up to half a second at times.  Keeping freed blocks in the pool
+// (a per-process runtime attribute, not a device setting) makes them reusable.
+static void keep_pool_memory() {
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  (void)cudaGetLastError();
+}
+
 Solver::Solver(const double d[3], const int mesh[3], const Options& o) : opt(o) {
   for (int i = 0; i < 3; ++i) dom[i] = d[i];
   g.M = mesh[0];
@@ -285,6 +301,7 @@ Solver::Solver(const double d[3], const int mesh[3], const Options& o) : opt(o) 
   H[0] = dom[0] / (double)g.M;  // :1707-1709
   H[1] = dom[1] / (double)g.N;
   H[2] = dom[2] / (double)g.P;
+  keep_pool_memory();
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
@@ -334,6 +351,7 @@ Solver::Solver(int np, const double* doms, const int* meshes, const int* sds, co
   }
   H[1] = probs[0].Hy;
   H[2] = probs[0].Hz;
+  keep_pool_memory();
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
@@ -384,7 +402,7 @@ Solver::~Solver() {
                   (void*)eb.alist, (void*)eb.colcells})
     if (p) cudaFree(p);
   if (eb.h_nactive) cudaFreeHost(eb.h_nactive);
-  for (void* p : {(void*)cb_T, (void*)cb_X, (void*)cb_v, (void*)cb_y, (void*)cb_t, (void*)cb_perm, (void*)cb_null,
+  for (void* p : {(void*)cb_T, (void*)cb_X, (void*)cb_v, (void*)cb_y, (void*)cb_t, (void*)cb_part, (void*)cb_perm, (void*)cb_null,
                   (void*)cb_scale})
     if (p) cudaFree(p);
   for (void* p : {(void*)d_ks3, (void*)l3work, (void*)d_queue, net_x, (void*)net_y, (void*)d_fail_list, (void*)d_fail_count, (void*)d_iters_learned,
@@ -1297,8 +1315,8 @@ int Solver::setup_two_level() {
   }
   const size_t vec = (size_t)p.NTp * 64 * sizeof(double);
   if (!cb_T || p.NTp != cband.NTp || p.B != cband.B) {
-    for (void** q : {(void**)&cb_T, (void**)&cb_X, (void**)&cb_v, (void**)&cb_y, (void**)&cb_t, (void**)&cb_perm,
-                     (void**)&cb_null, (void**)&cb_scale}) {
+    for (void** q : {(void**)&cb_T, (void**)&cb_X, (void**)&cb_v, (void**)&cb_y, (void**)&cb_t, (void**)&cb_part,
+                     (void**)&cb_perm, (void**)&cb_null, (void**)&cb_scale}) {
       if (*q) cudaFree(*q);
       *q = nullptr;
     }
@@ -1315,6 +1333,7 @@ int Solver::setup_two_level() {
     if (!e) e = dalloc((void**)&cb_v, vec, "coarse work");
     if (!e) e = dalloc((void**)&cb_y, vec, "coarse work");
     if (!e) e = dalloc((void**)&cb_t, vec, "coarse work");
+    if (!e) e = dalloc((void**)&cb_part, (size_t)p.B * p.B * 64 * sizeof(double), "coarse partial sums");
     if (!e) e = dalloc((void**)&cb_perm, p.perm.size() * sizeof(int), "coarse ordering");
     if (!e) e = dalloc((void**)&cb_null, p.perm.size() * sizeof(int), "coarse null flags");
     if (!e) e = dalloc((void**)&cb_scale, sizeof(double), "coarse scale");
@@ -1594,7 +1613,7 @@ void Solver::apply_impl(const double* x, double* out, double* partial, const int
       if (v == 2) {
         launch_block_gemv_r(rl, ncoarse, A2inv, c, dz, done, st);
       } else if (v == 4) {  // _PC_apply_vec_lv2_2level (:1481-1537)
-        launch_cband_solve(cb_perm, cband, cb_T, cb_X, c, dz, cb_v, cb_y, cb_t, done, st);
+        launch_cband_solve(cb_perm, cband, cb_T, cb_X, c, dz, cb_v, cb_y, cb_t, cb_part, done, st);
       } else {
         launch_lv3_restrict_r(rl, nrank, en2, V3, c, d3, done, st);
         launch_block_gemv(1, n3, A3inv, d3, w3, 0, done, st);

@@ -222,6 +222,7 @@ class Solver {
   // -use_2level: banded Cholesky of the global coarse matrix (k_coarse_band.cu)
   CBandPlan cband;
   double *cb_T = nullptr, *cb_X = nullptr, *cb_v = nullptr, *cb_y = nullptr, *cb_t = nullptr, *cb_scale = nullptr;
+  double* cb_part = nullptr;  // column partial sums of the banded backward solve (B x B x 64)
   int *cb_perm = nullptr, *cb_null = nullptr;
   int setup_two_level();
   int *d_fail_list = nullptr, *d_fail_count = nullptr, *d_iters_learned = nullptr, *d_status_learned = nullptr;
