@@ -20,6 +20,7 @@
 // returned eigenvalues and the normalisation v^T M v = 1 (the GHEP
 // normalisation SLEPc returns).
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 
@@ -518,9 +519,12 @@ struct PhaseClock {
   }
 };
 
+// sc: scratch of the tridiagonal eigensolver (>= 2 400 doubles); null: mt.stile and the tiles after it.  The
+// phase-batched Rayleigh-Ritz passes mt.GM: GM, GA and U are dead by then, so its shared memory ends at stile.
 __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop, double jtol,
-                                 PhaseClock* pc = nullptr);
-__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop, double jtol, PhaseClock* pc) {
+                                 PhaseClock* pc = nullptr, double* sc = nullptr);
+__device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double drop, double jtol, PhaseClock* pc,
+                                 double* sc) {
   for (int e = threadIdx.x; e < nS * nS; e += blockDim.x) {
     const int a = e / nS, b = e % nS;
     if (a < b) {
@@ -623,7 +627,7 @@ __device__ int cta_rayleigh_ritz(LbSmall& sm, LbMats& mt, int nS, int m, double 
   __syncthreads();
   if (pc) pc->lap(11);
   // only the lowest min(m, q) eigenpairs of H are needed
-  cta_sym_lowest(mt.H, mt.V, sm.th, q, min(m, q), LB_LD, mt.stile);
+  cta_sym_lowest(mt.H, mt.V, sm.th, q, min(m, q), LB_LD, sc ? sc : mt.stile);
   (void)jtol;
   if (pc) pc->lap(12);
   const int mm = min(m, q);
@@ -1529,7 +1533,7 @@ __global__ void __launch_bounds__(256) k_eb_rr(EbArgs a, double drop) {
   if (threadIdx.x < LB_MM) sm.lam[threadIdx.x] = threadIdx.x < m ? es.lam[threadIdx.x] : 0.0;
   if (threadIdx.x == 0) sm.scal[0] = es.lscale;
   __syncthreads();
-  const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop, 1e-11);
+  const int q = cta_rayleigh_ritz(sm, mt, nS, m, drop, 1e-11, nullptr, mt.GM);
   double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
   for (int e = threadIdx.x; e < nS * m; e += blockDim.x) {
     const int r = e / m, c = e % m;
@@ -2022,7 +2026,7 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   size_t pre_smem_max = 0;
   for (int q = 0; q < nmb; ++q) pre_smem_max = std::max(pre_smem_max, coef + (size_t)4 * e.ldc * mb_c[q]);
   const size_t gram_smem = (size_t)8 * 32 * 32 * sizeof(double);
-  const size_t rr_smem = sizeof(LbSmall) + sizeof(LbMats);
+  const size_t rr_smem = sizeof(LbSmall) + offsetof(LbMats, stile);  // k_eb_rr stops at the tiles: 3 CTAs / SM
   cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem_max);
   // basis update tiles: <6,1> (3 CTAs per SM) is the built-in for m <= 8, <8,2> the alternative;
   // candidates 2 / 3 are the same tiles with two groups of cells loading ahead per warp
