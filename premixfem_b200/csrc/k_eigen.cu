@@ -459,6 +459,53 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
   }
 }
 
+// The same update on the CUDA cores, one cell per thread (FP64 arithmetic):
+// each thread loads the ns values of its cell (independent, coalesced loads:
+// consecutive threads on consecutive cells), then accumulates both outputs
+// with Y broadcast from shared memory, and writes them.  Every value of a
+// cell is read before the cell is written, as in cta_update_mma.
+template <typename T, int MM>
+__device__ __noinline__ void cta_update_cc(T* B0, T* B1, T* B2, int m0, int n1, int n2, int m, const double* Y,
+                                           int ncells, size_t ld) {
+  const int ns = m0 + n1 + n2;
+  for (int cell = threadIdx.x; cell < ncells; cell += blockDim.x) {
+    double sv[3 * MM];
+#pragma unroll
+    for (int b = 0; b < 3 * MM; ++b) {
+      double v = 0.0;
+      if (b < ns) {
+        if (b < m0)
+          v = (double)B0[(size_t)b * ld + cell];
+        else if (b < m0 + n1)
+          v = (double)B1[(size_t)(b - m0) * ld + cell];
+        else
+          v = (double)B2[(size_t)(b - m0 - n1) * ld + cell];
+      }
+      sv[b] = v;
+    }
+    double ax[MM], ap[MM];
+#pragma unroll
+    for (int j = 0; j < MM; ++j) ax[j] = ap[j] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3 * MM; ++b) {
+      if (b < ns) {
+#pragma unroll
+        for (int j = 0; j < MM; ++j) {
+          const double y = Y[b * LB_LD + j];
+          ax[j] += sv[b] * y;
+          if (b >= m0) ap[j] += sv[b] * y;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MM; ++j)
+      if (j < m) {
+        B0[(size_t)j * ld + cell] = (T)ax[j];
+        B2[(size_t)j * ld + cell] = (T)ap[j];
+      }
+  }
+}
+
 // out[b] = A32 u_b for nb vectors staged in shared memory: A32 is the subdomain
 // Neumann operator with its off-diagonal couplings rounded to FP32 (the sweep
 // coefficients), applied in FP64 arithmetic and stored in FP64.  For FP32
@@ -1570,6 +1617,28 @@ __global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
     cta_update_mma<double, NK, NJ, ST>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
 }
 
+// k_eb_update with the CUDA-core update (m <= 8 block columns)
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_eb_update_cc(EbArgs a) {
+  __shared__ double Ys[LB_LD * LB_LD];
+  const int s = eb_sub(a, blockIdx.y);
+  const EbState& es = a.state[s];
+  if (es.done || es.restart) return;
+  const SubInfo S = a.subs[s];
+  const int nc = S.nx * S.ny * S.nz;
+  const int c0 = blockIdx.x * EB_CHUNK;
+  if (c0 >= nc) return;
+  const int cn = min(nc - c0, EB_CHUNK);
+  const double* Y = a.Ybuf + (size_t)s * LB_LD * LB_LD;
+  for (int e = threadIdx.x; e < es.nS * LB_LD; e += blockDim.x) Ys[e] = Y[e];
+  __syncthreads();
+  EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
+  const int m = a.m;
+  cta_update_cc<T, 8>(sl.X + c0, sl.W + c0, sl.P + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+  if (sizeof(T) == 8)
+    cta_update_cc<double, 8>(sl.AX + c0, sl.AW + c0, sl.AP + c0, m, es.nact, es.np, m, Ys, cn, a.ld);
+}
+
 // ---- final phase (k_lobpcg mode 2 as phase kernels over every subdomain of
 // the list): FP64 A-images of X, Grams of X, the FP64 Rayleigh-Ritz with the
 // adaptive count (:369-383) and the output of the k_i wanted vectors.  Run at
@@ -2030,10 +2099,11 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   cudaFuncSetAttribute(k_eb_precond<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pre_smem_max);
   // basis update tiles: <6,1> (3 CTAs per SM) is the built-in for m <= 8, <8,2> the alternative;
   // candidates 2 / 3 are the same tiles with two groups of cells loading ahead per warp
-  const int nupd = a.m <= 8 ? 4 : 2;
+  // candidate 4 (m <= 8): the CUDA-core update, one cell per thread
+  const int nupd = a.m <= 8 ? 5 : 2;
   char kpre[96], kupd[96];
   snprintf(kpre, sizeof(kpre), "eb_precond|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
-  snprintf(kupd, sizeof(kupd), "eb_update|%s|m%d|c%d", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
+  snprintf(kupd, sizeof(kupd), "eb_update|%s|m%d|c%d|cc", sizeof(T) == 4 ? "f32" : "f64", a.m, e.ldc);
   cudaEvent_t tev[4];
   for (auto& x : tev) cudaEventCreate(&x);
   int prev_pc = -1, prev_uc = -1, prev_cols = 0, prev_ns = 0;
@@ -2096,7 +2166,9 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     mark(5);
     note_launch();
     cudaEventRecord(tev[2], st);
-    if (a.m <= 8 && uc == 0)
+    if (a.m <= 8 && uc == 4)
+      k_eb_update_cc<T><<<gchunk, 256, 0, st>>>(e);
+    else if (a.m <= 8 && uc == 0)
       k_eb_update<T, 6, 1, 1><<<gchunk, 256, 0, st>>>(e);
     else if (a.m <= 8 && uc == 2)
       k_eb_update<T, 6, 1, 2><<<gchunk, 256, 0, st>>>(e);

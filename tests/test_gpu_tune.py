@@ -90,12 +90,12 @@ def test_report_lists_the_tuned_shapes(native, monkeypatch):
 def test_eigensolver_every_online_shape(native, monkeypatch, precision):
     """The lock-step eigensolver's online candidates (preconditioner column batch
     3 / 8 / 1, update tiles <6,1> / <8,2>, each with one or two groups of cells
-    loading ahead) give the same local eigenvalues (1e-6 relative) and the same
-    PCG iteration count (+-1)."""
+    loading ahead, and the CUDA-core update) give the same local eigenvalues
+    (1e-6 relative) and the same PCG iteration count (+-1)."""
     prob = fields.fracture256(64, seed=3)
     opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
     res = []
-    for cand in (0, 1, 2, 3):
+    for cand in (0, 1, 2, 3, 4):
         monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
         s = DarcySolver.from_problem(prob, opts)
         s.setup()
@@ -105,7 +105,7 @@ def test_eigensolver_every_online_shape(native, monkeypatch, precision):
         assert reason == "converged"
         res.append((ev, its))
         s.close()
-    for cand in (1, 2, 3):
+    for cand in (1, 2, 3, 4):
         ev0, ev = res[0][0], res[cand][0]
         rel = np.abs(ev - ev0) / np.maximum(np.abs(ev0), 1e-9 * np.abs(ev0).max())
         assert rel.max() <= 1e-6, (cand, rel.max())
