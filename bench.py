@@ -30,7 +30,8 @@ on the solver stream (pmf_profile_iteration); the dominant class is the
 
 Secondary workloads (--extra, default "fracture256_2level,layered,large512,
 batch64") run after the headline with their own 3 warm-up + 3 timed steps per
-form and are reported under "workloads" in the same line.
+form and are reported under "workloads" in the same line; they and the CPU
+baseline run at N = 1 only.
 
 Multi-GPU (torchrun, N ranks): every rank solves its own seeded replica on
 its own GPU (no data-path collective: replicas only); step time is the max
@@ -557,7 +558,9 @@ def run_b200(args):
         return out
 
     extras = {}
-    for name in [e for e in args.extra.split(",") if e and e != main_name]:
+    # secondary workloads and the CPU baseline belong to the 1-GPU line; a multi-rank (scaling) run
+    # measures the headline workload only
+    for name in [e for e in args.extra.split(",") if e and e != main_name and world == 1]:
         if WORKLOADS[name].get("batch"):
             try:
                 extras[name] = measure_batch(name, 3, 3)
@@ -580,7 +583,7 @@ def run_b200(args):
         gc.collect()
     if extras:
         line["workloads"] = extras
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, wl, m["prob"], plain["its"])
         line["accuracy"]["local_eigenvalues_sample"] = eig_sample(m)
     if rank == 0:
