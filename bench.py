@@ -355,6 +355,7 @@ def run_b200(args):
                 kx_host = torch.from_numpy(np.ascontiguousarray(prob["kappa"][0]).ravel()).pin_memory()
                 src_host = torch.from_numpy(src_h).pin_memory()
                 x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+                b_host = torch.empty(n, dtype=torch.float64).pin_memory()  # the right-hand side comes back here
                 e2e = []
                 for _ in range(max(1, steps)):
                     barrier()
@@ -363,8 +364,8 @@ def run_b200(args):
                     e0.record()
                     s.set_kappa(kx_host.numpy(), kx_host.numpy(), kx_host.numpy())
                     s.setup()
-                    bh = s.rhs(src_host.numpy())
-                    s.solve(bh, x_host.numpy())
+                    s.rhs(src_host.numpy(), b_host.numpy())
+                    s.solve(b_host.numpy(), x_host.numpy())
                     e1.record()
                     torch.cuda.synchronize()
                     e2e.append(e0.elapsed_time(e1) / 1e3)
