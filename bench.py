@@ -607,7 +607,7 @@ def _tune_choices(lib):
 
 
 def eig_sample(m, count=64, seed=12):
-    """Checker, CPU-baseline leg: local eigenvalues of a seeded sample of subdomains, every GPU form
+    """CPU-baseline leg: local eigenvalues of a seeded sample of subdomains, every GPU form
     against the oracle's exact local GHEP (ARPACK shift-and-invert on each subdomain's crop)."""
     from oracle import pmf_oracle as O
 

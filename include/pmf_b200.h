@@ -94,8 +94,8 @@ int pmf_solve(pmf_solver* s, const double* b, double* x, int on_device, int* its
 int pmf_profile_iteration(pmf_solver* s, int reps, double ms[8], int launches[8]);
 
 /*
- * A batch of independent problems solved together (BASELINE's batching
- * configuration; the reference solves one problem per run).  Problem q has
+ * A batch of independent problems solved together (many small problems of
+ * different sizes; the reference solves one problem per run).  Problem q has
  * dom[3q..3q+2], mesh[3q..3q+2] and sd[3q..3q+2] subdomains per axis (one
  * virtual rank per problem: its level 2 is its whole coarse space).  The
  * problems share one mesh (pmf_batch_info: max M x max N x sum(P + 1) cells;
