@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(ROWS * 2 / MT) k_net_fwd(FwdArgs a) {
 // double-buffered across planes so that the epilogue of plane z-1
 // (tcgen05.ld, bias, ReLU, BF16 store) overlaps the MMAs of plane z.  Every
 // wait is bounded; a wait that runs out sets *err and skips the stores.
-// TMA multicast is not used (single-GPU code).
+// Every load is a plain per-CTA cp.async (single-GPU code).
 namespace {
 constexpr int kTcPl = 18 * 18;                 // positions of one haloed plane
 constexpr long long kTcSpin = 1LL << 24;      // mbarrier polls before giving up
