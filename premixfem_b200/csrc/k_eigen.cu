@@ -303,11 +303,13 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
     sp[ta] = (ta < nt && a < ns) ? S.col(a) : nullptr;
     ap[ta] = (ta < nt && a < ns) ? AS.col(a) : nullptr;
   }
-  double cm[NT][NT][2], ca[NT][NT][2];
+  // Only the tiles ta <= tb are accumulated (both Grams are symmetric); the
+  // reduction mirrors them.  NT is the exact tile count when nt == NT (the
+  // batched solver dispatches on it); tiles past nt load zeros.
+  constexpr int NP = NT * (NT + 1) / 2;
+  double cm[NP][2], ca[NP][2];
 #pragma unroll
-  for (int i = 0; i < NT; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) cm[i][j][0] = cm[i][j][1] = ca[i][j][0] = ca[i][j][1] = 0.0;
+  for (int p = 0; p < NP; ++p) cm[p][0] = cm[p][1] = ca[p][0] = ca[p][1] = 0.0;
   // Each warp step covers 8 cells (two k-steps of 4): lane l reads cells
   // c0 + l%4 and c0 + 4 + l%4, so a column's two loads fill whole 32-byte
   // sectors, and the next step's 16 loads per lane are in flight during the MMAs.
@@ -339,15 +341,14 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
     if (c0 + 8 * nwarp < ncells) load(c0 + 8 * nwarp);  // next step in flight during the MMAs
 #pragma unroll
     for (int ta = 0; ta < NT; ++ta) {
-      if (ta >= nt) break;
       const double ws = cs[ta] * cw, ws2 = cs2[ta] * cw2;
 #pragma unroll
-      for (int tb = 0; tb < NT; ++tb) {
-        if (tb >= nt) break;
-        dmma884(cm[ta][tb][0], cm[ta][tb][1], ws, cs[tb]);
-        dmma884(ca[ta][tb][0], ca[ta][tb][1], cs[ta], cas[tb]);
-        dmma884(cm[ta][tb][0], cm[ta][tb][1], ws2, cs2[tb]);
-        dmma884(ca[ta][tb][0], ca[ta][tb][1], cs2[ta], cas2[tb]);
+      for (int tb = ta; tb < NT; ++tb) {
+        const int p = ta * NT - ta * (ta - 1) / 2 + (tb - ta);
+        dmma884(cm[p][0], cm[p][1], ws, cs[tb]);
+        dmma884(ca[p][0], ca[p][1], cs[ta], cas[tb]);
+        dmma884(cm[p][0], cm[p][1], ws2, cs2[tb]);
+        dmma884(ca[p][0], ca[p][1], cs2[ta], cas2[tb]);
       }
     }
   }
@@ -358,20 +359,26 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
 #pragma unroll
     for (int ta = 0; ta < NT; ++ta)
 #pragma unroll
-      for (int tb = 0; tb < NT; ++tb) {
-        if (ta < nt && tb < nt) {
+      for (int tb = ta; tb < NT; ++tb) {
+        const int p = ta * NT - ta * (ta - 1) / 2 + (tb - ta);
+        if (tb < nt) {
           const int row = 8 * ta + r, col = 8 * tb + 2 * cq;
-          red[(w * 32 + row) * 32 + col] = which ? ca[ta][tb][0] : cm[ta][tb][0];
-          red[(w * 32 + row) * 32 + col + 1] = which ? ca[ta][tb][1] : cm[ta][tb][1];
+          red[(w * 32 + row) * 32 + col] = which ? ca[p][0] : cm[p][0];
+          red[(w * 32 + row) * 32 + col + 1] = which ? ca[p][1] : cm[p][1];
         }
       }
     __syncthreads();
     double* G = which ? GA : GM;
     for (int e = threadIdx.x; e < ns * ns; e += blockDim.x) {
-      const int a = e / ns, b = e % ns;
+      int a = e / ns, b = e % ns;
+      if ((a >> 3) > (b >> 3)) {  // below the accumulated block triangle: the mirror
+        const int x = a;
+        a = b;
+        b = x;
+      }
       double v = 0.0;
       for (int ww = 0; ww < nwarp; ++ww) v += red[(ww * 32 + a) * 32 + b];
-      G[a * LB_LD + b] = v;
+      G[(e / ns) * LB_LD + (e % ns)] = v;
     }
   }
   __syncthreads();
@@ -380,37 +387,42 @@ __device__ __noinline__ void cta_gram2_mma(const Seg3<TS> S, const Seg3<TA> AS, 
 // In-place basis update on the FP64 tensor cores:
 //   B0[:, j] <- sum_b S_b Y[b][j]            (b < ns, S = [B0 | B1 | B2])
 //   B2[:, j] <- sum_{b >= m0} S_b Y[b][j]    (the new search direction)
-// for j < m (m <= 16).  Warp w handles groups of 8 cells; lane l's A fragment
-// is S_{k0 + l%4} at cell 8g + l/4 and its B fragments come from Y in shared
-// memory.  Every warp reads all ns columns of its 8 cells before writing them.
+// for j < m (m <= 8 NJ).  Warp w handles groups of 8 cells; lane l's A fragment
+// is S_{k0 + l%4} at cell 8g + l/4 and its B fragments come from Y.  Every warp
+// reads all ns columns of its 8 cells before writing them.
+//
+// Each lane resolves its NK column addresses (b = 4 kk + l%4 in [B0 | B1 | B2])
+// once, and for NJ = 1 keeps its Y fragments in registers, so that a group
+// costs NK predicated loads, 2 NK MMAs and the stores: no per-load selection
+// among the three blocks and no loop bounds known only at run time.  Columns
+// b >= ns load as zero and meet zero rows of Y (NK k-steps always run).
 template <typename T, int NK, int NJ, int STAGES>
 __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1, int n2, int m, const double* Y,
                                             int ncells, size_t ld) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int r = lane >> 2, cq = lane & 3;
   const int ns = m0 + n1 + n2;
-  const int nk = (ns + 3) >> 2;
-  const int nj = (m + 7) >> 3;
   const int ngrp = (ncells + 7) >> 3;
+  const T* colp[NK];
+  double yx[NK], yq[NK];  // Y fragments of tile 0 (NJ = 1)
+#pragma unroll
+  for (int kk = 0; kk < NK; ++kk) {
+    const int b = 4 * kk + cq;
+    colp[kk] = b >= ns        ? nullptr
+               : b < m0      ? B0 + (size_t)b * ld
+               : b < m0 + n1 ? B1 + (size_t)(b - m0) * ld
+                             : B2 + (size_t)(b - m0 - n1) * ld;
+    const double y = (NJ == 1 && b < ns && r < m) ? Y[b * LB_LD + r] : 0.0;
+    yx[kk] = y;
+    yq[kk] = b >= m0 ? y : 0.0;
+  }
   // STAGES groups ahead are loading while group gi is multiplied.
   double av[NK], an[NK], an2[NK];
   auto load = [&](int gi, double* dst) {
     const int cell = 8 * gi + r;
     const bool in = cell < ncells;
 #pragma unroll
-    for (int kk = 0; kk < NK; ++kk) {
-      const int b = 4 * kk + cq;
-      double v = 0.0;
-      if (kk < nk && in && b < ns) {
-        if (b < m0)
-          v = (double)B0[(size_t)b * ld + cell];
-        else if (b < m0 + n1)
-          v = (double)B1[(size_t)(b - m0) * ld + cell];
-        else
-          v = (double)B2[(size_t)(b - m0 - n1) * ld + cell];
-      }
-      dst[kk] = v;
-    }
+    for (int kk = 0; kk < NK; ++kk) dst[kk] = (in && colp[kk]) ? (double)colp[kk][cell] : 0.0;
   };
   if (w < ngrp) load(w, an);
   if (STAGES > 1 && w + nwarp < ngrp) load(w + nwarp, an2);
@@ -432,13 +444,14 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
     for (int tj = 0; tj < NJ; ++tj) dx[tj][0] = dx[tj][1] = dp[tj][0] = dp[tj][1] = 0.0;
 #pragma unroll
     for (int kk = 0; kk < NK; ++kk) {
-      if (kk >= nk) break;
 #pragma unroll
       for (int tj = 0; tj < NJ; ++tj) {
-        if (tj >= nj) break;
-        const int bb = 4 * kk + cq, jj = 8 * tj + r;
-        const double y = (bb < ns && jj < m) ? Y[bb * LB_LD + jj] : 0.0;
-        const double yp = bb >= m0 ? y : 0.0;
+        double y = yx[kk], yp = yq[kk];
+        if (NJ > 1) {
+          const int bb = 4 * kk + cq, jj = 8 * tj + r;
+          y = (bb < ns && jj < m) ? Y[bb * LB_LD + jj] : 0.0;
+          yp = bb >= m0 ? y : 0.0;
+        }
         dmma884(dx[tj][0], dx[tj][1], av[kk], y);
         dmma884(dp[tj][0], dp[tj][1], av[kk], yp);
       }
@@ -446,7 +459,6 @@ __device__ __noinline__ void cta_update_mma(T* B0, T* B1, T* B2, int m0, int n1,
     // D fragment: rows = cells 8gi + r, columns j = 8tj + 2cq + {0, 1}
 #pragma unroll
     for (int tj = 0; tj < NJ; ++tj) {
-      if (tj >= nj) break;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int j = 8 * tj + 2 * cq + h;
@@ -1548,7 +1560,9 @@ __global__ void __launch_bounds__(256, 2) k_eb_gram(EbArgs a) {
   double* G = a.gpart + ((size_t)s * a.nchunk + blockIdx.x) * 2 * LB_LD * LB_LD;
   Seg3<T> sS{{sl.X + c0, sl.W + c0, sl.P + c0}, {a.m, es.nact, es.np}, a.ld};
   Seg3<double> sA{{sl.AX + c0, sl.AW + c0, sl.AP + c0}, {a.m, es.nact, es.np}, a.ld};
-  if (es.nS <= 24)
+  if (es.nS <= 16)  // the exact tile count: no zero tiles multiplied
+    cta_gram2_mma<T, double, 2>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+  else if (es.nS <= 24)
     cta_gram2_mma<T, double, 3>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
   else
     cta_gram2_mma<T, double, 4>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
@@ -1597,7 +1611,7 @@ __global__ void __launch_bounds__(256) k_eb_rr(EbArgs a, double drop) {
 // NK / NJ: k-steps and 8-column tiles of the tensor-core update (6 / 1 for m <= 8);
 // ST: groups of 8 cells each warp has loading while it multiplies one (1 or 2).
 template <typename T, int NK, int NJ, int ST>
-__global__ void __launch_bounds__(256, 3) k_eb_update(EbArgs a) {
+__global__ void __launch_bounds__(256, (NJ == 1 && ST == 1) ? 3 : 2) k_eb_update(EbArgs a) {
   __shared__ double Ys[LB_LD * LB_LD];
   const int s = eb_sub(a, blockIdx.y);
   const EbState& es = a.state[s];
@@ -1671,7 +1685,10 @@ __global__ void __launch_bounds__(256, 2) k_eb_fin_gram(EbArgs a) {
   double* G = a.gpart + ((size_t)s * a.nchunk + blockIdx.x) * 2 * LB_LD * LB_LD;
   Seg3<T> sS{{sl.X + c0, sl.X + c0, sl.X + c0}, {a.m, 0, 0}, a.ld};
   Seg3<double> sA{{sl.AX + c0, sl.AX + c0, sl.AX + c0}, {a.m, 0, 0}, a.ld};
-  cta_gram2_mma<T, double, 3>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+  if (a.m <= 8)
+    cta_gram2_mma<T, double, 1>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
+  else
+    cta_gram2_mma<T, double, 2>(sS, sA, sl.Md + c0, cn, G, G + LB_LD * LB_LD, red);
 }
 
 template <typename T>
