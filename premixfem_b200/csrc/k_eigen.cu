@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include "pmf_bulk.cuh"
 #include "pmf_dense.cuh"
 #include "pmf_kernels.h"
 #include "tune.h"
@@ -526,19 +527,25 @@ __device__ __noinline__ void cta_update_cc(T* B0, T* B1, T* B2, int m0, int n1, 
 // uses the true operator.
 __device__ void smem_neumann64(const float* u, int ldc, int nb, int nx, int ny, int nz, const float* ctx,
                                const float* cty, const float* ctz, const double* dN, double* out, size_t ld) {
+  // cell-major: a cell's position, couplings and diagonal are read once for all nb columns
   const int nxny = nx * ny, nc = nxny * nz;
-  for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
-    const int b = e / nc, cl = e % nc;
+  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
     const int i = cl % nx, tt = cl / nx, j = tt % ny, k = tt / ny;
-    const float* ub = u + (size_t)b * ldc;
-    double v = dN[cl] * (double)ub[cl];
-    if (i > 0) v -= (double)ctx[cl] * (double)ub[cl - 1];
-    if (i < nx - 1) v -= (double)ctx[cl + 1] * (double)ub[cl + 1];
-    if (j > 0) v -= (double)cty[cl] * (double)ub[cl - nx];
-    if (j < ny - 1) v -= (double)cty[cl + nx] * (double)ub[cl + nx];
-    if (k > 0) v -= (double)ctz[cl] * (double)ub[cl - nxny];
-    if (k < nz - 1) v -= (double)ctz[cl + nxny] * (double)ub[cl + nxny];
-    out[(size_t)b * ld + cl] = v;
+    const double d = dN[cl];
+    const double cxm = i > 0 ? (double)ctx[cl] : 0.0, cxp = i < nx - 1 ? (double)ctx[cl + 1] : 0.0;
+    const double cym = j > 0 ? (double)cty[cl] : 0.0, cyp = j < ny - 1 ? (double)cty[cl + nx] : 0.0;
+    const double czm = k > 0 ? (double)ctz[cl] : 0.0, czp = k < nz - 1 ? (double)ctz[cl + nxny] : 0.0;
+    for (int b = 0; b < nb; ++b) {
+      const float* ub = u + (size_t)b * ldc;
+      double v = d * (double)ub[cl];
+      if (i > 0) v -= cxm * (double)ub[cl - 1];
+      if (i < nx - 1) v -= cxp * (double)ub[cl + 1];
+      if (j > 0) v -= cym * (double)ub[cl - nx];
+      if (j < ny - 1) v -= cyp * (double)ub[cl + nx];
+      if (k > 0) v -= czm * (double)ub[cl - nxny];
+      if (k < nz - 1) v -= czp * (double)ub[cl + nxny];
+      out[(size_t)b * ld + cl] = v;
+    }
   }
 }
 
@@ -1341,9 +1348,12 @@ struct EbArgs {
 __device__ __forceinline__ int eb_sub(const EbArgs& a, int idx) { return a.alist[idx]; }
 
 // Partial ||AX_j - lambda_j M X_j||^2_{M^-1} over one chunk of cells.
+// All m columns at once: a full chunk gives each thread four consecutive cells
+// (vector loads, every column's loads in flight together); the per-column
+// sums are reduced per warp by shuffles and across the warps in a fixed order.
 template <typename T>
 __global__ void __launch_bounds__(256) k_eb_resid(EbArgs a, int use_alist) {
-  __shared__ double red[32];
+  __shared__ double red[32][LB_MM];
   const int s = use_alist ? a.alist[blockIdx.y] : (a.list ? a.list[blockIdx.y] : (int)blockIdx.y);
   const EbState& es = a.state[s];
   if (es.done) return;
@@ -1352,16 +1362,53 @@ __global__ void __launch_bounds__(256) k_eb_resid(EbArgs a, int use_alist) {
   const int c0 = blockIdx.x * EB_CHUNK, c1 = min(nc, c0 + EB_CHUNK);
   double* out = a.rpart + ((size_t)s * a.nchunk + blockIdx.x) * LB_MM;
   EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, a.ld);
-  for (int j = 0; j < a.m; ++j) {
-    const double lam = es.lam[j];
-    double acc = 0.0;
+  const int m = a.m;
+  double lam[LB_MM], acc[LB_MM];
+#pragma unroll
+  for (int j = 0; j < LB_MM; ++j) {
+    lam[j] = j < m ? es.lam[j] : 0.0;
+    acc[j] = 0.0;
+  }
+  if (c1 - c0 == 4 * (int)blockDim.x) {
+    const int cl = c0 + 4 * threadIdx.x;  // 16-byte aligned: c0 and ld are multiples of 4
+    double md[4];
+    ld4(sl.Md + cl, md);
+#pragma unroll
+    for (int j = 0; j < LB_MM; ++j) {
+      if (j < m) {
+        double ax[4], xv[4];
+        ld4(sl.AX + (size_t)j * a.ld + cl, ax);
+        ld4(sl.X + (size_t)j * a.ld + cl, xv);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double r = ax[q] - lam[j] * md[q] * xv[q];
+          acc[j] += r * r / md[q];
+        }
+      }
+    }
+  } else {
     for (int cl = c0 + threadIdx.x; cl < c1; cl += blockDim.x) {
       const double mv = sl.Md[cl];
-      const double r = sl.AX[(size_t)j * a.ld + cl] - lam * mv * (double)sl.X[(size_t)j * a.ld + cl];
-      acc += r * r / mv;
+#pragma unroll
+      for (int j = 0; j < LB_MM; ++j) {
+        if (j < m) {
+          const double r = sl.AX[(size_t)j * a.ld + cl] - lam[j] * mv * (double)sl.X[(size_t)j * a.ld + cl];
+          acc[j] += r * r / mv;
+        }
+      }
     }
-    acc = block_sum(acc, red);
-    if (threadIdx.x == 0) out[j] = acc;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < LB_MM; ++j) {
+    const double v = warp_sum(acc[j]);
+    if (lane == 0) red[w][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < m) {
+    double v = 0.0;
+    for (int q = 0; q < nw; ++q) v += red[q][threadIdx.x];
+    out[threadIdx.x] = v;
   }
 }
 
@@ -1417,6 +1464,13 @@ __global__ void k_eb_control(EbArgs a, int nlist, int it) {
 // W_c = T (AX_a - lambda_a M X_a) for active columns c (a = act[c]) of one
 // column batch: IC(0) sweeps of A^N + sigma M in shared memory (FP32), and in
 // FP32 storage the FP64 A-image with the FP32-rounded couplings.
+//
+// Shared memory: a 16-byte header (mbarrier, flag), the four coefficient
+// arrays at the slab's pitch ld (one bulk copy of 16 ld bytes, which lands
+// while the threads form the residuals), then the nb columns at pitch ldc.
+// The residuals are formed four cells at a time with vector loads, two groups
+// of four per thread in flight.  Thread 0's wait for the copy is bounded; a
+// copy that does not land sets nactive[3] and the CTA writes nothing.
 template <typename T>
 __global__ void __launch_bounds__(256) k_eb_precond(EbArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -1429,27 +1483,59 @@ __global__ void __launch_bounds__(256) k_eb_precond(EbArgs a) {
   const SubInfo S = a.subs[s];
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxny = nx * ny, nc = nxny * nz;
   const int ldc = a.ldc, ld = a.ld;
-  float* ctx = reinterpret_cast<float*>(smraw);
-  float* cty = ctx + ldc;
-  float* ctz = cty + ldc;
-  float* cinv = ctz + ldc;
-  float* u = cinv + ldc;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
+  int* flag = reinterpret_cast<int*>(smraw + 8);
+  float* ctx = reinterpret_cast<float*>(smraw + 16);
+  float* cty = ctx + ld;
+  float* ctz = cty + ld;
+  float* cinv = ctz + ld;
+  float* u = cinv + ld;
   EbSlab<T> sl(a.slab + (size_t)s * a.slab_stride, a.m, ld);
-  for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-    ctx[cl] = sl.ctx[cl];
-    cty[cl] = sl.cty[cl];
-    ctz[cl] = sl.ctz[cl];
-    cinv[cl] = sl.cinv[cl];
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    const uint32_t bytes = (uint32_t)(16 * (size_t)ld);  // ctx, cty, ctz, cinv: contiguous in the slab
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_g2s(ctx, sl.ctx, bytes, bar);
   }
-  for (int b = 0; b < nb; ++b) {
-    const int col = es.act[c0 + b];
-    const double lam = es.lam[col];
-    for (int cl = threadIdx.x; cl < nc; cl += blockDim.x) {
-      const double r = sl.AX[(size_t)col * ld + cl] - lam * sl.Md[cl] * (double)sl.X[(size_t)col * ld + cl];
+  {
+    const int ng = nc >> 2, tot = nb * ng, bd = blockDim.x;
+    auto resid4 = [&](int e, float4& o) {
+      const int b = e / ng, cl = 4 * (e - b * ng);
+      const int col = es.act[c0 + b];
+      const double lam = es.lam[col];
+      double ax[4], xv[4], md[4];
+      ld4(sl.AX + (size_t)col * ld + cl, ax);
+      ld4(sl.X + (size_t)col * ld + cl, xv);
+      ld4(sl.Md + cl, md);
+      o.x = (float)(T)(ax[0] - lam * md[0] * xv[0]);
+      o.y = (float)(T)(ax[1] - lam * md[1] * xv[1]);
+      o.z = (float)(T)(ax[2] - lam * md[2] * xv[2]);
+      o.w = (float)(T)(ax[3] - lam * md[3] * xv[3]);
+      return b * ldc + cl;
+    };
+    for (int e = threadIdx.x; e < tot; e += 2 * bd) {
+      float4 o0, o1;
+      const int d0 = resid4(e, o0);
+      const int d1 = e + bd < tot ? resid4(e + bd, o1) : -1;
+      *reinterpret_cast<float4*>(u + d0) = o0;
+      if (d1 >= 0) *reinterpret_cast<float4*>(u + d1) = o1;
+    }
+    const int tail = nc - 4 * ng;  // cells past the last group of four
+    for (int e = threadIdx.x; e < nb * tail; e += bd) {
+      const int b = e / tail, cl = 4 * ng + e % tail;
+      const int col = es.act[c0 + b];
+      const double r = sl.AX[(size_t)col * ld + cl] - es.lam[col] * sl.Md[cl] * (double)sl.X[(size_t)col * ld + cl];
       u[(size_t)b * ldc + cl] = (float)(T)r;
     }
   }
+  if (threadIdx.x == 0) {
+    const bool ok = mbar_wait_bounded(bar);
+    *flag = ok ? 0 : 1;
+    if (!ok) atomicOr(a.nactive + 3, 1);
+  }
   __syncthreads();
+  if (*flag) return;
   const int t = threadIdx.x, jj = t % ny, kk = t / ny;
   const bool line = t < ny * nz;
   const int nplanes = nx + ny + nz - 2;
@@ -2102,9 +2188,10 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   }
   // column batch of the preconditioner: the built-in one keeps coefficients + mb
   // vectors within ~113 KB (2 CTAs per SM); the online tuner also tries all m
-  // columns in one CTA (fewer barriers per column, 1 CTA per SM) and one column
-  const size_t coef = (size_t)16 * e.ldc;
-  e.mb = (int)std::max<size_t>(1, std::min<size_t>(a.m, (112 * 1024 - coef) / ((size_t)4 * e.ldc)));
+  // columns in one CTA (fewer barriers per column, 1 CTA per SM) and one column.
+  // coef: the 16-byte header and the four coefficient arrays at pitch ld.
+  const size_t coef = (size_t)16 * e.ld + 16;
+  e.mb = (int)std::max<size_t>(1, std::min<size_t>(a.m, (113 * 1024 - coef) / ((size_t)4 * e.ldc)));
   int mb_c[3], nmb = 0;
   mb_c[nmb++] = e.mb;
   if (a.m != e.mb && coef + (size_t)4 * e.ldc * a.m <= 220 * 1024) mb_c[nmb++] = a.m;
@@ -2149,13 +2236,14 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
   };
   mark(0);
   int nact = nlist, lockstep = 0;
+  cudaMemsetAsync(b.nactive + 3, 0, sizeof(int), st);  // set by a preconditioner copy that never landed
   for (int it = 0; it < a.max_it; ++it) {
     // residual norms of the subdomains still iterating (all of them at it = 0)
     mark(1);
     { note_launch(); k_eb_resid<T><<<dim3(e.nchunk, nact), 256, 0, st>>>(e, it > 0 ? 1 : 0); }
     cudaMemsetAsync(b.nactive, 0, 3 * sizeof(int), st);
     { note_launch(); k_eb_control<<<(nlist + 127) / 128, 128, 0, st>>>(e, nlist, it); }
-    cudaMemcpyAsync(b.h_nactive, b.nactive, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(b.h_nactive, b.nactive, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
     mark(2);
     if (cudaStreamSynchronize(st) != cudaSuccess) return 76;
     report_prev();
@@ -2164,6 +2252,7 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
       cudaEventElapsedTime(&ms, pev[1], pev[2]);
       ptot[0] += ms;
     }
+    if (b.h_nactive[3]) return 76;  // a bounded wait in the preconditioner ran out
     nact = b.h_nactive[0];
     if (nact == 0) break;
     ++lockstep;
@@ -2211,6 +2300,10 @@ int launch_lobpcg_batched(const LobpcgArgs& a_in, const EbBuffers& b, const int*
     }
   }
   if (cudaStreamSynchronize(st) != cudaSuccess) return 76;
+  {
+    int fl = 0;  // the last iteration's preconditioner
+    if (cudaMemcpy(&fl, b.nactive + 3, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || fl) return 76;
+  }
   report_prev();
   for (auto& x : tev) cudaEventDestroy(x);
   if (prof) {

@@ -33,6 +33,7 @@
 // (16-byte aligned rows), ny*nz <= 256 lines.
 #include <stdint.h>
 
+#include "pmf_bulk.cuh"
 #include "pmf_kernels.h"
 
 namespace pmf {
@@ -50,38 +51,7 @@ struct Coef4<double> {
 
 namespace {
 
-constexpr int kNX = 16;                  // cells per x-line of the blocked kernel
-constexpr long long kBulkSpinLimit = 1LL << 22;  // mbarrier polls before the CTA gives up
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-// global -> shared bulk copy (TMA engine); bytes a multiple of 16, both addresses 16-byte aligned
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(b))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
+constexpr int kNX = 16;  // cells per x-line of the blocked kernel
 }  // namespace
 
 // Shared-memory layout of k_ic_apply_blk (bytes): header (mbarrier, flag,
