@@ -431,8 +431,11 @@ def run_b200(args):
     d = per_class[dom]
     dom_ms_launch = d["ms_per_iteration"] / d["launch_groups"]
     dom_bytes_launch = cb[dom] / d["launch_groups"]
+    tune = _tune_choices(lib) or {}
+    lv1_names = {"lv1_with_y": _lv1_kernel(tune, "f32", 1), "lv1_first": _lv1_kernel(tune, "f32", 0)}
     traffic = None
-    if dom == "lv1_with_y" and IC_APPLY_Y_TRAFFIC_PER_CELL:
+    # the ncu capture is of the natural-order kernel's final visit: its traffic is claimed only for that kernel
+    if dom == "lv1_with_y" and IC_APPLY_Y_TRAFFIC_PER_CELL and lv1_names[dom].startswith("k_ic_apply<"):
         traffic = int(IC_APPLY_Y_TRAFFIC_PER_CELL * n)
     iter_ms = sum(v[0] for v in prof.values())
     iter_bytes = sum(cb[c] for c in prof if prof[c][1] > 0)
@@ -469,8 +472,8 @@ def run_b200(args):
                 "d2h_bytes_per_step": int(2 * n * 8)},
         "gpu_launches": int(mix["launches"] / max(1, args.steps)),
         "roofline": {
-            "kernel": {"lv1_with_y": "k_ic_apply<float,1,1> (level-1 IC(0) solve with the iterate, final visit)",
-                       "lv1_first": "k_ic_apply<float,0,0> (level-1 IC(0) solve, first visit)"}.get(dom, dom),
+            "kernel": {"lv1_with_y": lv1_names["lv1_with_y"] + " (level-1 IC(0) solve with the iterate, final visit)",
+                       "lv1_first": lv1_names["lv1_first"] + " (level-1 IC(0) solve, first visit)"}.get(dom, dom),
             "bound": "hbm",
             "achieved": round(dom_bytes_launch / (dom_ms_launch * 1e-3) / 1e9, 1),
             "peak": hbm,
@@ -592,6 +595,25 @@ def run_b200(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _lv1_kernel(tune, prec, kind):
+    """Name of the level-1 kernel the tuner chose for a visit kind (0: first
+    visit, 1: with the iterate, timed in its final-visit form).  Candidates:
+    the natural-order kernel at each thread count, then (b2 / b3 in the key)
+    the blocked kernel at 512 and 256 threads and its staged form."""
+    ty = "float" if prec == "f32" else "double"
+    args = f"<{ty},1,1>" if kind else f"<{ty},0,0>"
+    for key, (choice, us) in tune.items():
+        parts = key.split("|")
+        if parts[0] != "ic_apply" or parts[1] != prec or f"y{kind}" not in parts:
+            continue
+        nblk = int(next((q[1:] for q in parts if q.startswith("b") and q[1:].isdigit()), "0"))
+        nnat = len(us) - nblk
+        if choice < nnat:
+            return "k_ic_apply" + args
+        return ("k_ic_apply_blk" if choice - nnat < 2 else "k_ic_apply_stg") + args
+    return "k_ic_apply" + args
 
 
 def _tune_choices(lib):

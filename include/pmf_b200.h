@@ -61,10 +61,12 @@ typedef struct pmf_solver pmf_solver;
  * -pmf_eig_profile 1 (per-phase timing, pmf_get_eig_phases), -pmf_pcg_graph
  * 0|1 (PCG iterations replayed as CUDA graphs, on by default), -pmf_autotune
  * 0|1 (launch-shape tuning, on by default; pmf_tune_report), -pmf_lv1_kernel
- * auto|natural|blocked (level-1 solve kernel: the tuner's choice, the
- * natural-order kernel, or the kernel that stages each subdomain's IC(0)
- * factor with one TMA bulk copy, which needs every subdomain 16 cells wide in
- * x with x0 and M multiples of 4; both give bit-identical results). */
+ * auto|natural|blocked|staged (level-1 solve kernel: the tuner's choice, the
+ * natural-order kernel, the kernel that stages each subdomain's IC(0) factor
+ * with one TMA bulk copy, which needs every subdomain 16 cells wide in x with
+ * x0 and M multiples of 4, or that kernel with all of its other global loads
+ * issued in one pass up front, which also needs ny <= 16 and nz <= 16; they
+ * agree up to the rounding of contracted multiply-adds). */
 int pmf_create(const double dom[3], const int mesh[3], const char* options, pmf_solver** out);
 int pmf_destroy(pmf_solver* s);
 

@@ -112,6 +112,16 @@ void launch_ic_apply_blk(const Grid& g, const SubInfo* subs, int nsub, int max_c
                          const void* coef, const T* tx, const T* ty, const T* tz, const T* diag, const double* x,
                          const T* yin, T* out_t, double* out_d, double* part, const int* done, int* err,
                          cudaStream_t st, int threads);
+// The same solve with all of a CTA's global loads (x, y, the diagonal and the
+// subdomain's face halo) issued in one unrolled pass before any is used, 512
+// threads.  Needs the blocked kernel's shapes with ny <= 16 and nz <= 16.
+template <typename T>
+size_t ic_stg_smem_bytes(int max_cells);
+template <typename T>
+void launch_ic_apply_stg(const Grid& g, const SubInfo* subs, int nsub, int max_cells, const long long* coff,
+                         const void* coef, const T* tx, const T* ty, const T* tz, const T* diag, const double* x,
+                         const T* yin, T* out_t, double* out_d, double* part, const int* done, int* err,
+                         cudaStream_t st);
 
 // Exact level-1 solves (-use_full_Cholesky_lv1): banded Cholesky of every
 // subdomain block in natural order, column j of L at band[boff[s] + j*band_ld(b)],

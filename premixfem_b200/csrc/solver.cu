@@ -162,8 +162,10 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
         o->lv1_kernel = 1;
       else if (itk->second == "blocked")
         o->lv1_kernel = 2;
+      else if (itk->second == "staged")
+        o->lv1_kernel = 3;
       else {
-        *err = "Error in -pmf_lv1_kernel (auto | natural | blocked)";
+        *err = "Error in -pmf_lv1_kernel (auto | natural | blocked | staged)";
         return 62;
       }
     }
@@ -1017,6 +1019,11 @@ int Solver::setup() {
             "ny*nz <= 256";
       return 56;  // PETSC_ERR_SUP
     }
+    if (opt.lv1_kernel == 3 && !ic_stg_ok) {
+      err = "-pmf_lv1_kernel staged needs every subdomain 16 cells wide in x with x0 % 4 == 0, M % 4 == 0, "
+            "ny <= 16 and nz <= 16";
+      return 56;  // PETSC_ERR_SUP
+    }
   }
   cudaEventRecord(e[1], st);
   // level-2 local eigenproblems
@@ -1396,10 +1403,15 @@ int Solver::setup_band_cholesky(bool mixed) {
 // rows, at most 256 x-lines); rebuilt by every set-up.
 int Solver::setup_ic_blocked(bool mixed) {
   ic_blk_ok = max_lines <= 256;
-  for (const SubInfo& S : subs)
+  ic_stg_ok = true;
+  for (const SubInfo& S : subs) {
     if (S.nx != 16) ic_blk_ok = false;
+    if (S.ny > 16 || S.nz > 16) ic_stg_ok = false;
+  }
   const size_t smem = mixed ? ic_blk_smem_bytes<float>(max_cells) : ic_blk_smem_bytes<double>(max_cells);
   if (smem > 227 * 1024) ic_blk_ok = false;
+  const size_t smem_stg = mixed ? ic_stg_smem_bytes<float>(max_cells) : ic_stg_smem_bytes<double>(max_cells);
+  ic_stg_ok = ic_stg_ok && ic_blk_ok && smem_stg <= 227 * 1024;
   if (!d_kerr) {
     if (int e = dalloc((void**)&d_kerr, sizeof(int), "kernel wait flag")) return e;
     cudaMemsetAsync(d_kerr, 0, sizeof(int), st);
@@ -1452,7 +1464,10 @@ void Solver::launch_lv1(const double* x, const T* yin, T* out_t, double* out_d, 
   const T* ttz = f32 ? (const T*)tz32 : (const T*)tz;
   const T* tdg = f32 ? (const T*)diag32 : (const T*)diag;
   const int kind = yin ? 1 : 0;
-  if (ic_variant[kind] == 1 && ic_blk_ok) {
+  if (ic_variant[kind] == 2 && ic_stg_ok) {
+    launch_ic_apply_stg<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, x, yin, out_t, out_d,
+                           partial, done, d_kerr, st);
+  } else if (ic_variant[kind] >= 1 && ic_blk_ok) {
     launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, x, yin, out_t, out_d,
                            partial, done, d_kerr, st, ic_blk_threads[kind]);
   } else {
@@ -1490,31 +1505,41 @@ void Solver::tune_pc() {
       if (t > base) cand.push_back(t);
     // candidates per visit kind (first visit: no iterate; later visits: with
     // one): the natural-order kernel with each thread count, then the blocked
-    // kernel with 512 and 256 threads (when every subdomain fits it).  The
-    // natural kernel's thread count is tuned on the visits with an iterate.
+    // kernel with 512 and 256 threads (when every subdomain fits it) and its
+    // staged form (when every subdomain also has ny, nz <= 16).  The natural
+    // kernel's thread count is tuned on the visits with an iterate.
     const int nnat = (int)cand.size();
-    const int nblk = ic_blk_ok ? 2 : 0;
+    const int nblk = ic_blk_ok ? (ic_stg_ok ? 3 : 2) : 0;
     const int blk_threads[2] = {512, 256};
+    // The visits with an iterate are timed in the form the V-cycle's last
+    // visit takes (FP64 result and the z.r partials, into p0 and part, which
+    // hold nothing yet); the first visit writes the preconditioner's iterate.
     for (int kind = 1; kind >= 0; --kind) {
-      snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d|b%d|y%d", prec, nsub, max_cells, max_lines, nblk, kind);
+      snprintf(key, sizeof(key), "ic_apply|%s|n%d|c%d|l%d|b%d|y%d|f", prec, nsub, max_cells, max_lines, nblk, kind);
       const int ncand = kind == 1 ? nnat + nblk : 1 + nblk;
+      T* o_t = kind ? nullptr : yo;
+      double* o_d = kind ? p0 : nullptr;
+      double* o_p = kind ? part : nullptr;
       const int ci = tune_choose(key, ncand, [&](int i) {
         const int nn = kind == 1 ? nnat : 1;
         if (i < nn)
           launch_ic_apply<T>(g, d_subs, nsub, max_lines, max_cells, ttx, tty, ttz, tdg, tinv, z, kind ? ya : nullptr,
-                             yo, nullptr, nullptr, nullptr, st, kind ? cand[i] : ic_threads);
-        else
+                             o_t, o_d, o_p, nullptr, st, kind ? cand[i] : ic_threads);
+        else if (i - nn < 2)
           launch_ic_apply_blk<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, z,
-                                 kind ? ya : nullptr, yo, nullptr, nullptr, nullptr, d_kerr, st,
-                                 blk_threads[i - nn]);
+                                 kind ? ya : nullptr, o_t, o_d, o_p, nullptr, d_kerr, st, blk_threads[i - nn]);
+        else
+          launch_ic_apply_stg<T>(g, d_subs, nsub, max_cells, d_coff, ic_coef, ttx, tty, ttz, tdg, z,
+                                 kind ? ya : nullptr, o_t, o_d, o_p, nullptr, d_kerr, st);
         return true;
       }, st);
       const int nn = kind == 1 ? nnat : 1;
-      ic_variant[kind] = ci >= nn ? 1 : 0;
-      if (ci >= nn) ic_blk_threads[kind] = blk_threads[ci - nn];
+      ic_variant[kind] = ci < nn ? 0 : (ci - nn < 2 ? 1 : 2);
+      if (ci >= nn && ci - nn < 2) ic_blk_threads[kind] = blk_threads[ci - nn];
       if (kind == 1) ic_threads = cand[std::min(ci, nnat - 1)];
       if (opt.lv1_kernel == 1) ic_variant[kind] = 0;
       if (opt.lv1_kernel == 2) ic_variant[kind] = 1;  // eligibility checked by setup()
+      if (opt.lv1_kernel == 3) ic_variant[kind] = 2;
     }
   }
   const int rcand[3] = {256, 128, 512};

@@ -43,7 +43,8 @@ struct Options {
   int eig_batched = 1;  // 1: phase-batched LOBPCG (one launch per phase), 0: one persistent launch
   int eig_profile = 0;  // 1: time each phase of the batched eigensolver (pmf_get_eig_phases)
   bool eig_require_converged = false;  // a local eigensolve that hits eig_max_it fails the set-up (error 83)
-  int lv1_kernel = 0;  // level-1 solve kernel: 0 the tuner's choice, 1 natural-order, 2 subdomain-blocked
+  int lv1_kernel = 0;  // level-1 solve kernel: 0 the tuner's choice, 1 natural-order, 2 subdomain-blocked,
+                       // 3 subdomain-blocked with all global loads staged up front
   int eig_precision = -1;  // local eigensolver vectors: -1 as the preconditioner, 0 FP64, 1 FP32 (mixed only)
   // learned initial blocks for the local eigensolves (-pmf_learned <weights>):
   // LOBPCG starts from the network's output and may take learned_its
@@ -203,8 +204,10 @@ class Solver {
   int ic_threads = 0, rr_threads = 256, pr_threads = 256, pcga_variant = 0;  // tuned launch shapes
   // level-1 solve with the subdomain-blocked IC(0) factor (k_ic_apply_blk)
   bool ic_blk_ok = false;  // every subdomain fits the blocked kernel
+  bool ic_stg_ok = false;  // ... and its staged form (k_ic_apply_stg: ny, nz <= 16)
   // per visit kind (0: first visit, no iterate; 1: visits with an iterate):
-  // 0 natural-order kernel, 1 blocked kernel (tuner's choice), and its threads
+  // 0 natural-order kernel, 1 blocked kernel, 2 its staged form (tuner's
+  // choice), and the blocked kernel's threads
   int ic_variant[2] = {0, 0}, ic_blk_threads[2] = {512, 512};
   long long* d_coff = nullptr;  // per subdomain: first cell in the blocked arrays
   void* ic_coef = nullptr;      // blocked {tx, ty, tz, 1/D} (precision of the preconditioner)

@@ -54,14 +54,18 @@ def test_pc_apply_every_thread_shape(native, monkeypatch, precision):
     opts = options_string({"sd": 4, "en_lv1": 6, "en_lv2": 4, "pmf_precision": precision})
     x = np.random.default_rng(5).standard_normal(64 ** 3)
     out = []
-    for cand in (0, 1, 2, 3, 4):  # level 1: 256 / 384 / 512 / 768 / 1024 threads (others clamped)
+    # level 1 with an iterate: the natural kernel at 256 / 384 / 512 / 768 / 1024
+    # threads, the blocked kernel at 512 / 256 and the staged one; the first
+    # visit: natural, blocked 512 / 256, staged (cand 4 and up clamp to it);
+    # the restriction / prolongation's three shapes (others clamped)
+    for cand in range(8):
         monkeypatch.setenv("PMF_TUNE_FORCE", str(cand))
         s = DarcySolver.from_problem(prob, opts)
         s.setup()
         out.append(s.pc_apply(x))
         s.close()
     tol = 1e-12 if precision == "fp64" else 1e-5
-    for cand in (1, 2, 3, 4):
+    for cand in range(1, 8):
         assert _rel(out[cand], out[0]) <= tol, (cand, _rel(out[cand], out[0]))
 
 
