@@ -439,6 +439,60 @@ def chol_semidef_solve(Lnull, b):
     return x
 
 
+def local_basis(op: Operator, box, o: Options):
+    """One subdomain's level-2 basis (_PC_setup_lv2_eigen, :224-421): the
+    en_lv1 smallest pairs of A_i^N v = lambda M_i v and the adaptive count
+    (:369-383).  ``o`` must be normalised.  Returns (w, V, num, vmax)."""
+    k = o.en_lv1
+    An = op.neumann(box)
+    An = An if o.eig_method == "arpack" else An.toarray()
+    Md = op.mass_diag(box, o.eg_op)
+    if k > An.shape[0]:
+        raise ValueError("en_lv1 larger than a subdomain")
+    if o.eig_method == "arpack" and k < An.shape[0] - 1:
+        # SLEPc EPS with STSINVERT and target -NIL (:354-365): Lanczos on (A + NIL M)^-1 M
+        w, V = spla.eigsh(sp.csc_matrix(An), k=k, M=sp.diags(Md).tocsc(), sigma=-NIL, which="LM")
+        order = np.argsort(w)
+        w, V = w[order], V[:, order]
+    else:
+        w, V = sla.eigh(An, np.diag(Md), subset_by_index=[0, k - 1])
+    if o.phi_fp32:
+        V = V.astype(np.float32).astype(np.float64)
+    num, vmax = k, w[k - 1]
+    for j in range(k):
+        if w[j] >= o.eb_lv1:
+            num, vmax = j + 1, w[j]
+            break
+    return w, V, num, vmax
+
+
+def level3_basis(AN, o: Options):
+    """One virtual rank's level-3 vectors (_PC_setup_lv3_eigen, :1086-1115):
+    the en_lv2 smallest eigenpairs of its rank-Neumann coarse matrix and the
+    adaptive count.  Returns (w, V[:, :num], num, vmax)."""
+    AN = AN.toarray() if sp.issparse(AN) else np.asarray(AN)
+    k = min(o.en_lv2, AN.shape[0])
+    w, V = sla.eigh(AN, subset_by_index=[0, k - 1])
+    num, vmax = k, w[k - 1]
+    for j in range(k):
+        if w[j] >= o.eb_lv2:
+            num, vmax = j + 1, w[j]
+            break
+    return w, V[:, :num], num, vmax
+
+
+def cycle_schedule(o: Options):
+    """The visits of PC_apply_vec (:1840-1936) for normalised options: levels
+    1, 2, 3 or "2g" (the 2-level branch's global coarse solve)."""
+    s1 = [1] * o.si_lv1
+    s2 = [2] * o.si_lv2
+    if o.use_W_cycle and not o.use_2level:  # :1857-1894
+        return s1 + s2 + [3] + s2 + [3] + s2 + s1
+    if o.use_2level:  # :1918-1922
+        return s1 + ["2g"] + s1
+    return s1 + s2 + [3] + s2 + s1  # :1896-1928
+
+
 class Preconditioner:
     """The three-level preconditioner: _PC_setup (:1392-1427) + PC_apply_vec (:1840-1936)."""
 
@@ -476,34 +530,14 @@ class Preconditioner:
     # level 2 eigen -----------------------------------------------------
     def _setup_lv2_eigen(self):
         o = self.opts
-        k = o.en_lv1
         self.eig_num_lv1 = []
         self.eig_min_lv1 = []
         self.eig_max_lv1 = []
         self.eigvals_lv1 = []
         self.phi = []  # per subdomain (n_s, en_lv1) M-normalised eigenvectors
         for s in self.lay.subs:
-            An = self.op.neumann(s)
-            An = An if o.eig_method == "arpack" else An.toarray()
-            Md = self.op.mass_diag(s, o.eg_op)
-            if k > An.shape[0]:
-                raise ValueError("en_lv1 larger than a subdomain")
-            if o.eig_method == "arpack" and k < An.shape[0] - 1:
-                # SLEPc EPS with STSINVERT and target -NIL (:354-365): Lanczos on (A + NIL M)^-1 M
-                w, V = spla.eigsh(sp.csc_matrix(An), k=k, M=sp.diags(Md).tocsc(), sigma=-NIL, which="LM")
-                order = np.argsort(w)
-                w, V = w[order], V[:, order]
-            else:
-                w, V = sla.eigh(An, np.diag(Md), subset_by_index=[0, k - 1])
-            if o.phi_fp32:
-                V = V.astype(np.float32).astype(np.float64)
+            w, V, num, vmax = local_basis(self.op, s, o)
             self.eigvals_lv1.append(w)
-            # adaptive count, :369-383
-            num, vmax = k, w[k - 1]
-            for j in range(k):
-                if w[j] >= o.eb_lv1:
-                    num, vmax = j + 1, w[j]
-                    break
             self.eig_num_lv1.append(num)
             self.eig_min_lv1.append(w[0])
             self.eig_max_lv1.append(vmax)
@@ -563,20 +597,12 @@ class Preconditioner:
             d = self.rank_dofs(r)
             cells = box_cells(self.op.mesh, box)
             PhiR = self.Phi[cells][:, d]
-            AN = PhiR.T @ self.op.neumann(box) @ PhiR
-            AN = AN.toarray() if sp.issparse(AN) else np.asarray(AN)
-            k = min(o.en_lv2, AN.shape[0])
-            w, V = sla.eigh(AN, subset_by_index=[0, k - 1])
-            num, vmax = k, w[k - 1]
-            for j in range(k):
-                if w[j] >= o.eb_lv2:
-                    num, vmax = j + 1, w[j]
-                    break
+            w, V, num, vmax = level3_basis(PhiR.T @ self.op.neumann(box) @ PhiR, o)
             self.eigvals_lv2.append(w)
             self.eig_num_lv2.append(num)
             self.eig_min_lv2.append(w[0])
             self.eig_max_lv2.append(vmax)
-            self.V3.append((d, V[:, :num]))
+            self.V3.append((d, V))
             for j in range(num):
                 col = np.zeros(self.Phi.shape[1])
                 col[d] = V[:, j]
@@ -598,14 +624,7 @@ class Preconditioner:
 
     # cycle ------------------------------------------------------------------
     def schedule(self):
-        o = self.opts
-        s1 = [1] * o.si_lv1
-        s2 = [2] * o.si_lv2
-        if o.use_W_cycle and not o.use_2level:  # :1857-1894
-            return s1 + s2 + [3] + s2 + [3] + s2 + s1
-        if o.use_2level:  # :1918-1922
-            return s1 + ["2g"] + s1
-        return s1 + s2 + [3] + s2 + s1  # :1896-1928
+        return cycle_schedule(self.opts)
 
     def apply(self, x):
         """PC_apply_vec: y = 0, then r = x - A y; y += B_l r for each visit."""

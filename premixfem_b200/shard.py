@@ -17,6 +17,19 @@ so its halo is two whole x-y planes, and every subdomain and virtual rank it
 needs lies inside it.  Vectors are torch tensors; the collectives are
 torch.distributed calls on the default process group (NCCL between GPUs,
 gloo on the host).
+
+The set-up splits the same way.  A process reads its slab's permeability and
+the two ghost planes around it; that fixes the transmissibilities of every
+face its cells touch, so the level-1 blocks (:80-222), the local eigenproblems
+(:224-421), the per-rank level-2 blocks (:737-916) and the rank-Neumann
+level-3 eigenproblems (:918-1175) are all local.  Only the global coarse
+matrix couples processes (A_cc of :1177-1390, or Phi^T A Phi of the 2-level
+branch, :423-735): its entries between two slabs come from the faces between
+them, so each process sends its basis (Psi, or Phi) on its two boundary
+planes to its neighbours (``exchange_planes``), computes its own block and
+its coupling to the slab above, and one all-reduce (``sum_coarse``) gives
+every process the whole coarse matrix; the coarse unknowns of each virtual
+rank are counted the same way (``coarse_counts``).
 """
 from __future__ import annotations
 
@@ -165,6 +178,53 @@ class ShardedCycle:
                 raise ValueError(f"unknown cycle level {lvl!r}")
             y += p["prolong"](z)
         return y
+
+
+def exchange_planes(slab: Slab, top, bottom):
+    """The set-up's exchange across the slab faces.
+
+    ``top`` holds this process's values on its top cell plane (z1 - 1), one
+    row per cell of the plane (x fastest) and any number of columns;
+    ``bottom`` the same on its bottom plane (z0).  Each goes to the neighbour
+    on that side, and the neighbours' planes facing this slab come back:
+    returns (from_below, from_above), the values on planes z0 - 1 and z1
+    (None where there is no neighbour).  Column counts may differ between
+    processes, so each message is preceded by its shape.
+    """
+
+    def swap(data, peer):
+        data = data.contiguous()
+        shape = torch.tensor(list(data.shape), dtype=torch.int64, device=data.device)
+        peer_shape = torch.empty(2, dtype=torch.int64, device=data.device)
+        for r in (dist.isend(shape, peer), dist.irecv(peer_shape, peer)):
+            r.wait()
+        buf = torch.empty(tuple(int(v) for v in peer_shape.tolist()), dtype=data.dtype, device=data.device)
+        for r in (dist.isend(data, peer), dist.irecv(buf, peer)):
+            r.wait()
+        return buf
+
+    from_below = swap(bottom, slab.below) if slab.below is not None else None
+    from_above = swap(top, slab.above) if slab.above is not None else None
+    return from_below, from_above
+
+
+def coarse_counts(n_vranks, mine, device="cpu"):
+    """Coarse unknowns per virtual rank, each known only to the process that
+    owns the rank (``mine``: {virtual rank: count}), as one list every
+    process sees (one all-reduce)."""
+    t = torch.zeros(n_vranks, dtype=torch.int64, device=device)
+    for r, c in mine.items():
+        t[r] = int(c)
+    dist.all_reduce(t)
+    return [int(v) for v in t.tolist()]
+
+
+def sum_coarse(m):
+    """The global coarse matrix from every process's contributions (its own
+    block, and its coupling to the slab above with the transpose), summed in
+    place by one all-reduce."""
+    dist.all_reduce(m)
+    return m
 
 
 def global_sum(*values, like=None):

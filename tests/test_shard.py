@@ -1,20 +1,25 @@
 """The solve split over processes (premixfem_b200.shard) on gloo ranks (CPU).
 
-Each process owns a z-slab of whole virtual-rank layers.  Its local operator
-and the local pieces of the oracle's three-level preconditioner (level-1
-solvers of its subdomains, its part of Phi, the level-2 factors of its virtual
-ranks, its level-3 V blocks and the replicated level-3 factor) stand in for
-the device kernels as shard.ShardedCycle's callables; the exchanges are the
-module's own: halo planes before every stencil product, the level-3 right-hand
-side (and the 2-level coarse right-hand side) summed over the processes, and
-the CG dots.  The assembled solution and the iteration count must match the
-single-process oracle (the sums of the dot products are only reordered:
-iterations +-1, solution 1e-10).
+Each process owns a z-slab of whole virtual-rank layers and sets up its part
+of the oracle's three-level preconditioner from its slab and the two ghost
+planes around it only: the level-1 solvers of its subdomains, their local
+bases, the level-2 factors of its virtual ranks and their level-3 vectors.
+The one set-up exchange is the module's own: the basis (Psi, or Phi for the
+2-level branch) on the two boundary planes to the neighbours, from which each
+process adds its coupling to the slab above to the global coarse matrix, and
+one all-reduce of that matrix and of the per-rank coarse counts.  These
+pieces stand in for the device kernels as shard.ShardedCycle's callables; the
+solve's exchanges are the module's too: halo planes before every stencil
+product, the level-3 right-hand side (and the 2-level coarse right-hand side)
+summed over the processes, and the CG dots.  The assembled solution and the
+iteration count must match the single-process oracle (sums and products are
+only reordered: iterations +-1, solution 1e-10).
 """
 import socket
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -40,62 +45,132 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _local_pieces(pc, op, slab):
-    """The oracle's local mathematics on one slab, as ShardedCycle's callables."""
-    lay = pc.lay
-    lo, hi = slab.first_cell, slab.first_cell + slab.ncell
-    elo, ehi = slab.ext_cells
-    A_loc = op.A[lo:hi][:, elo:ehi].tocsr()
-    subs = [i for i, s in enumerate(lay.subs) if s[6] in slab.vranks]
-    d0, d1 = int(pc.dof_idx[subs[0]]), int(pc.dof_idx[subs[-1] + 1])
-    Phi = pc.Phi[lo:hi][:, d0:d1].tocsr()
-    nc = int(pc.dof_idx[-1])
+def _sharded_setup(prob, o, slab, slabs):
+    """This process's part of the three-level preconditioner, built from its
+    slab and the two ghost planes around it only (the problem cropped to
+    planes z0 - 1 .. z1), with the set-up exchanges of premixfem_b200.shard:
+    the basis on the boundary planes to the neighbours, the coarse counts and
+    the global coarse matrix summed over the processes.  Returns
+    ShardedCycle's callables, the local stencil product on halo-extended
+    vectors, this slab's right-hand side and the set-up's exchange count."""
+    M, N, P = prob["mesh"]
+    mn = M * N
+    lay = O.Layout.build(prob["mesh"], o.vranks, o.sd)
+    crop, cbox = O.crop_around(prob, (0, M, 0, N, slab.z0, slab.z1 - slab.z0))
+    opc = O.Operator(crop)
+    zc = slab.z0 - cbox[4]  # first crop plane in global z
+    off, nloc = cbox[4] * mn, slab.ncell  # the slab's cells in the crop's numbering
+    rows = slice(off, off + nloc)
     t, n = torch.from_numpy, lambda v: v.numpy()
+
+    def to_crop(box):
+        return (box[0], box[1], box[2], box[3], box[4] - zc, box[5]) + tuple(box[6:])
+
+    # level 1 and the local bases: subdomain by subdomain, from the crop alone
+    subs = [s_ for s_ in lay.subs if s_[6] in slab.vranks]
+    sub_idx, lv1, phi, nums = [], [], [], []
+    for s_ in subs:
+        bc = to_crop(s_)
+        sub_idx.append(O.box_cells(crop["mesh"], bc) - off)
+        Aloc = opc.principal(bc)
+        lv1.append(O.CholSolver(Aloc) if o.use_full_Cholesky_lv1 else O.IC0Solver(Aloc))
+        w, V, num, _ = O.local_basis(opc, bc, o)
+        phi.append(V)
+        nums.append(num)
+    dof = np.concatenate([[0], np.cumsum(nums)]).astype(int)
+    nd = int(dof[-1])
+    Phi = sp.csr_matrix((np.concatenate([phi[i][:, j] for i in range(len(subs)) for j in range(nums[i])]),
+                         (np.concatenate([sub_idx[i] for i in range(len(subs)) for j in range(nums[i])]),
+                          np.concatenate([np.full(sub_idx[i].size, dof[i] + j)
+                                          for i in range(len(subs)) for j in range(nums[i])]))),
+                        shape=(nloc, nd))
+    A_slab = opc.A[rows][:, rows].tocsr()
+    A2 = (Phi.T @ A_slab @ Phi).toarray()
+    spr = lay.subs_per_rank
+    rdof = {r: np.arange(dof[i * spr], dof[(i + 1) * spr]) for i, r in enumerate(slab.vranks)}
+    lv2 = {r: O.chol_semidef(A2[np.ix_(d, d)]) for r, d in rdof.items()}
+    # the faces between the top plane and the ghost plane above: tz of the ghost plane's cells
+    t_up = opc.tz[slab.z1 - zc].ravel() if slab.above is not None else None
+    exchanges = 0
+
+    def coarse(basis, counts_mine):
+        """The global coarse matrix basis^T A basis from this slab's block and
+        its coupling to the slab above (the neighbours' basis on the facing
+        planes arrives by exchange_planes)."""
+        nonlocal exchanges
+        counts = shard.coarse_counts(len(lay.ranks), counts_mine)
+        offs = np.concatenate([[0], np.cumsum(counts)]).astype(int)
+        lo_, hi_ = offs[slab.vranks[0]], offs[slab.vranks[-1] + 1]
+        m = np.zeros((offs[-1], offs[-1]))
+        m[lo_:hi_, lo_:hi_] = basis.T @ (A_slab @ basis)
+        bt = torch.from_numpy(np.ascontiguousarray(basis[nloc - mn:]))
+        bb = torch.from_numpy(np.ascontiguousarray(basis[:mn]))
+        _, from_above = shard.exchange_planes(slab, bt, bb)
+        exchanges += 1
+        if from_above is not None:
+            up = slabs[slab.rank + 1].vranks
+            ua, ub = offs[up[0]], offs[up[-1] + 1]
+            cpl = basis[nloc - mn:].T @ (-t_up[:, None] * from_above.numpy())
+            m[lo_:hi_, ua:ub] += cpl
+            m[ua:ub, lo_:hi_] += cpl.T
+        mt = shard.sum_coarse(torch.from_numpy(m))
+        return mt.numpy(), offs, lo_, hi_
 
     def level1(r):
         y = np.zeros(r.shape[0])
-        for s in subs:
-            idx = pc.sub_idx[s] - lo
-            y[idx] += pc.lv1[s].solve(n(r)[idx])
+        for idx, sol in zip(sub_idx, lv1):
+            y[idx] += sol.solve(n(r)[idx])
         return t(y)
 
     def level2(c):
         z = np.zeros(c.shape[0])
-        for vr in slab.vranks:
-            d, f = pc.lv2[vr]
-            z[d - d0] = O.chol_semidef_solve(f, n(c)[d - d0])
+        for r, d in rdof.items():
+            z[d] = O.chol_semidef_solve(lv2[r], n(c)[d])
         return t(z)
 
-    pieces = dict(residual=lambda x, y_ext: t(n(x) - A_loc @ n(y_ext)), level1=level1,
-                  restrict=lambda r: t(Phi.T @ n(r)), prolong=lambda z: t(Phi @ n(z)), level2=level2)
-    if pc.opts.use_2level:
+    pieces = dict(level1=level1, restrict=lambda r: t(Phi.T @ n(r)), prolong=lambda z: t(Phi @ n(z)),
+                  level2=level2)
+    if o.use_2level:
+        Ac, offs, lo_, hi_ = coarse(Phi.toarray(), {r: d.size for r, d in rdof.items()})
+        if not o.no_shift_A_cc:
+            Ac = Ac + O.NIL * np.eye(Ac.shape[0])
+        fac = O.chol_semidef(Ac)
+
         def coarse_rhs(c):
-            cg = np.zeros(nc)
-            cg[d0:d1] = n(c)
+            cg = np.zeros(Ac.shape[0])
+            cg[lo_:hi_] = n(c)
             return t(cg)
 
-        pieces.update(coarse_rhs=coarse_rhs,
-                      coarse_solve=lambda cg: t(O.chol_semidef_solve(pc.lv2c, n(cg))[d0:d1]))
+        pieces.update(coarse_rhs=coarse_rhs, coarse_solve=lambda cg: t(O.chol_semidef_solve(fac, n(cg))[lo_:hi_]))
     else:
-        off3 = np.concatenate([[0], np.cumsum([V.shape[1] for _, V in pc.V3])])
+        V3 = {}
+        for r, d in rdof.items():
+            bc = to_crop(lay.ranks[r])
+            cells = O.box_cells(crop["mesh"], bc) - off
+            PhiR = Phi[cells][:, d]
+            V3[r] = O.level3_basis(PhiR.T @ opc.neumann(bc) @ PhiR, o)[1]
+        Vloc = np.zeros((nd, sum(V.shape[1] for V in V3.values())))
+        c0 = 0
+        for r, d in rdof.items():
+            Vloc[d, c0:c0 + V3[r].shape[1]] = V3[r]
+            c0 += V3[r].shape[1]
+        Psi = np.asarray(Phi @ Vloc)
+        A3, off3, lo_, hi_ = coarse(Psi, {r: V.shape[1] for r, V in V3.items()})
+        if not o.no_shift_A_cc:
+            A3 = A3 + O.NIL * np.eye(A3.shape[0])  # :1361-1363
+        fac = O.chol_semidef(A3)
 
         def level3_rhs(c):
-            d3 = np.zeros(int(off3[-1]))
-            for vr in slab.vranks:
-                d, V = pc.V3[vr]
-                d3[off3[vr]:off3[vr + 1]] = V.T @ n(c)[d - d0]
+            d3 = np.zeros(A3.shape[0])
+            d3[lo_:hi_] = Vloc.T @ n(c)
             return t(d3)
 
-        def level3_back(w):
-            z = np.zeros(d1 - d0)
-            for vr in slab.vranks:
-                d, V = pc.V3[vr]
-                z[d - d0] = V @ n(w)[off3[vr]:off3[vr + 1]]
-            return t(z)
-
-        pieces.update(level3_rhs=level3_rhs, level3_back=level3_back,
-                      level3_solve=lambda d3: t(O.chol_semidef_solve(pc.lv3, n(d3))))
-    return pieces, lambda p: t(A_loc @ n(p))
+        pieces.update(level3_rhs=level3_rhs, level3_back=lambda w: t(Vloc @ n(w)[lo_:hi_]),
+                      level3_solve=lambda d3: t(O.chol_semidef_solve(fac, n(d3))))
+    A_loc = opc.A[rows].tocsr()  # slab rows, crop columns: [ghost below | slab | ghost above]
+    pieces["residual"] = lambda x, y_ext: t(n(x) - A_loc @ n(y_ext))
+    b = np.asarray(prob["source"])[slab.z0:slab.z1].ravel() + opc.bval.ravel()[rows]
+    return pieces, (lambda p_: t(A_loc @ n(p_))), b, exchanges
 
 
 def _worker(rank, world, port, name, out):
@@ -104,28 +179,27 @@ def _worker(rank, world, port, name, out):
     try:
         _, make, opts = CASES[name]
         prob = make()
-        o = O.Options(**opts)
-        op = O.Operator(prob)
-        pc = O.Preconditioner(op, o)
-        slab = shard.plan_slabs(prob["mesh"], o.vranks, world)[rank]
+        o = O.Options(**opts).normalized()
+        slabs = shard.plan_slabs(prob["mesh"], o.vranks, world)
+        slab = slabs[rank]
         halo = shard.Halo(slab)
-        pieces, stencil = _local_pieces(pc, op, slab)
-        cycle = shard.ShardedCycle(pc.schedule(), halo, **pieces)
+        pieces, stencil, b, setup_exchanges = _sharded_setup(prob, o, slab, slabs)
+        cycle = shard.ShardedCycle(O.cycle_schedule(o), halo, **pieces)
 
         def matvec(p):
             return stencil(halo.extend(p))
 
-        b = op.rhs()
+        n_global = int(np.prod(prob["mesh"]))
+        x, its, hist, reason = shard.pcg(torch.from_numpy(b), matvec, cycle.apply, n_global,
+                                         rtol=o.rtol, null_space=o.constant_null_space)
+        xg = torch.zeros(n_global, dtype=torch.float64)
         lo, hi = slab.first_cell, slab.first_cell + slab.ncell
-        x, its, hist, reason = shard.pcg(torch.from_numpy(b[lo:hi].copy()), matvec, cycle.apply, op.n,
-                                         rtol=pc.opts.rtol, null_space=o.constant_null_space)
-        xg = torch.zeros(op.n, dtype=torch.float64)
         xg[lo:hi] = x
         dist.all_reduce(xg)
         if rank == 0:
             np.save(out, xg.numpy())
             with open(out + ".txt", "w") as f:
-                f.write(f"{its} {reason} {halo.exchanges} {cycle.sums}\n")
+                f.write(f"{its} {reason} {halo.exchanges} {cycle.sums} {setup_exchanges}\n")
     finally:
         dist.destroy_process_group()
 
@@ -139,7 +213,7 @@ def test_sharded_solve_matches_single_process(name, tmp_path, monkeypatch):
         monkeypatch.setenv(v, "1")
     mp.spawn(_worker, args=(world, _free_port(), name, out), nprocs=world, join=True)
     x = np.load(out)
-    its, reason, exchanges, sums = open(out + ".txt").read().split()
+    its, reason, exchanges, sums, setup_exchanges = open(out + ".txt").read().split()
     prob = make()
     ref = O.solve(prob, O.Options(**opts))
     assert reason == ref["reason"] == "converged_rtol"
@@ -154,6 +228,8 @@ def test_sharded_solve_matches_single_process(name, tmp_path, monkeypatch):
     assert int(exchanges) == int(its) * len(sched)
     # one coarse right-hand side summed per level-3 (or 2-level) visit of each application
     assert int(sums) == int(its) * sum(1 for lvl in sched if lvl in (3, "2g"))
+    # the set-up exchanged the basis on the boundary planes once (Psi, or Phi for the 2-level branch)
+    assert int(setup_exchanges) == 1
 
 
 def test_slab_plan():
