@@ -132,9 +132,15 @@ int options_from_db(const OptionDB& db, Options* o, std::string* err) {
     *err = "Error in -pmf_eig_rel_floor (0 <= f < 1)";
     return 62;
   }
-  db.get_int("pmf_eig_guard", &o->eig_guard);
+  if (db.get_int("pmf_eig_guard", &o->eig_guard) && o->eig_guard < 0) {
+    *err = "Error in -pmf_eig_guard (must be >= 0)";
+    return 62;
+  }
   db.get_int("pmf_pcg_chunk", &o->pcg_chunk);
-  db.get_int("pmf_eig_ctas", &o->eig_ctas);
+  if (db.get_int("pmf_eig_ctas", &o->eig_ctas) && o->eig_ctas < 0) {
+    *err = "Error in -pmf_eig_ctas (must be >= 0; 0: one per SM)";
+    return 62;
+  }
   db.get_int("pmf_eig_batched", &o->eig_batched);
   db.get_int("pmf_eig_final", &o->eig_final);
   db.get_int("pmf_eig_init", &o->eig_init);

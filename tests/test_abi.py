@@ -65,11 +65,13 @@ def test_option_errors_come_before_the_device():
         return rc
 
     bad = ["-eg_op 7", "-pmf_precision half", "-ksp_constant_null_space maybe", "-pmf_eig_rel_floor 1.5",
-           "-pmf_eig_rel_floor -0.1", "-pmf_learned"]
+           "-pmf_eig_rel_floor -0.1", "-pmf_learned", "-pmf_eig_guard -1", "-pmf_eig_ctas -4",
+           "-pmf_lv1_kernel fast"]
     for opts in bad:
         assert create("-sd 2 " + opts) == 62, opts
     good = ["", "-ksp_constant_null_space", "-ksp_constant_null_space false", "-pmf_eig_rel_floor 1e-4",
-            "-pmf_eig_init 1 -pmf_precision mixed", "-use_2level -no_shift_A_cc"]
+            "-pmf_eig_init 1 -pmf_precision mixed", "-use_2level -no_shift_A_cc", "-pmf_lv1_kernel staged",
+            "-pmf_eig_guard 0"]
     for opts in good:
         assert create("-sd 2 " + opts) in (0, 76), opts
 
