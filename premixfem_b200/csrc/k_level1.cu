@@ -31,6 +31,10 @@
 // Requirements (checked by the host before this kernel is chosen): every
 // subdomain 16 cells wide in x with x0 a multiple of 4, M a multiple of 4
 // (16-byte aligned rows), ny*nz <= 256 lines.
+//
+// k_ic_apply_stg (below) is the same solve with steps 2 and 3 reorganised so
+// that every global load of a CTA is issued before any is used; the launch-
+// shape tuner chooses between the two and the natural-order kernel per visit.
 #include <stdint.h>
 
 #include "pmf_bulk.cuh"
