@@ -193,6 +193,8 @@ def exchange_planes(slab: Slab, top, bottom):
     """
 
     def swap(data, peer):
+        if data.dim() != 2:
+            raise ValueError("exchange_planes takes (plane cells, columns) tensors")
         data = data.contiguous()
         shape = torch.tensor(list(data.shape), dtype=torch.int64, device=data.device)
         peer_shape = torch.empty(2, dtype=torch.int64, device=data.device)
