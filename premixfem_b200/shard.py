@@ -238,7 +238,8 @@ def global_sum(*values, like=None):
     return out[0] if len(out) == 1 else out
 
 
-def pcg(b, matvec, apply_pc, n_global, rtol=1.0e-8, max_it=10000, abstol=1.0e-50, null_space=False):
+def pcg(b, matvec, apply_pc, n_global, rtol=1.0e-8, max_it=10000, abstol=1.0e-50, null_space=False,
+        fused=False, stats=None):
     """PETSc KSPSolve_CG (unpreconditioned norm, KSPConvergedDefault, zero
     initial guess) on this process's part of every vector.
 
@@ -247,26 +248,62 @@ def pcg(b, matvec, apply_pc, n_global, rtol=1.0e-8, max_it=10000, abstol=1.0e-50
     ``null_space`` the constant is removed from each preconditioned residual
     (MatNullSpaceRemove; ``n_global`` cells).  Returns (x, its, history,
     reason) with the reasons of oracle-style names.
+
+    PETSc's order takes three sums per iteration (p.w, ||r||^2 before the
+    preconditioner, z.r after it; four with the null space).  ``fused``
+    applies the preconditioner before the convergence test and sums
+    [||r||^2, z.r] (with the null space also sum z and sum r, from which
+    (z - mean z).r follows) in one all-reduce: two sums per iteration, the
+    same recurrence up to the rounding of that one product, and one more
+    preconditioner application at the iteration that converges.  ``stats``
+    (a dict) receives the counts of all-reduces and preconditioner
+    applications.
     """
+    if stats is None:
+        stats = {}
+    stats.update(allreduces=0, pc_applications=0)
+
+    def sums(*vals, like):
+        stats["allreduces"] += 1
+        return global_sum(*vals, like=like)
 
     def dot(a, c):
-        return global_sum(torch.dot(a, c).item(), like=a)
+        return sums(torch.dot(a, c).item(), like=a)
+
+    def pc(r):
+        stats["pc_applications"] += 1
+        return apply_pc(r)
 
     def precondition(r):
-        z = apply_pc(r)
+        z = pc(r)
         if null_space:
-            z = z - global_sum(z.sum().item(), like=z) / n_global
+            z = z - sums(z.sum().item(), like=z) / n_global
         return z
+
+    def precondition_fused(r):
+        """z = B r (mean removed with the null space), ||r|| and z.r from one sum."""
+        z = pc(r)
+        if null_space:
+            rr, zr, sz, sr = sums(torch.dot(r, r).item(), torch.dot(z, r).item(), z.sum().item(), r.sum().item(),
+                                  like=r)
+            m = sz / n_global
+            return z - m, math.sqrt(rr), zr - m * sr
+        rr, zr = sums(torch.dot(r, r).item(), torch.dot(z, r).item(), like=r)
+        return z, math.sqrt(rr), zr
 
     x = torch.zeros_like(b)
     r = b.clone()
-    dp = math.sqrt(dot(r, r))
+    if fused:
+        z, dp, beta = precondition_fused(r)
+    else:
+        dp = math.sqrt(dot(r, r))
     hist = [dp]
     ttol = max(rtol * dp, abstol)
     if dp <= ttol:
         return x, 0, hist, "converged_atol"
-    z = precondition(r)
-    beta = dot(z, r)
+    if not fused:
+        z = precondition(r)
+        beta = dot(z, r)
     p = None
     betaold = dpi = 0.0
     its = 0
@@ -284,12 +321,16 @@ def pcg(b, matvec, apply_pc, n_global, rtol=1.0e-8, max_it=10000, abstol=1.0e-50
         a = beta / dpi
         x += a * p
         r -= a * w
-        dp = math.sqrt(dot(r, r))
+        if fused:
+            z, dp, beta = precondition_fused(r)
+        else:
+            dp = math.sqrt(dot(r, r))
         hist.append(dp)
         if not math.isfinite(dp):
             return x, its, hist, "diverged_nanorinf"
         if dp <= ttol:
             return x, its, hist, "converged_rtol"
-        z = precondition(r)
-        beta = dot(z, r)
+        if not fused:
+            z = precondition(r)
+            beta = dot(z, r)
     return x, its, hist, "diverged_its"

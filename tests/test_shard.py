@@ -11,7 +11,9 @@ one all-reduce of that matrix and of the per-rank coarse counts.  These
 pieces stand in for the device kernels as shard.ShardedCycle's callables; the
 solve's exchanges are the module's too: halo planes before every stencil
 product, the level-3 right-hand side (and the 2-level coarse right-hand side)
-summed over the processes, and the CG dots.  The assembled solution and the
+summed over the processes, and the CG dots (in PETSc's order, and fused: p.w,
+then ||r||^2 and z.r in one sum; the counts of each are checked).  The
+assembled solution and the
 iteration count must match the single-process oracle (sums and products are
 only reordered: iterations +-1, solution 1e-10).
 """
@@ -173,7 +175,7 @@ def _sharded_setup(prob, o, slab, slabs):
     return pieces, (lambda p_: t(A_loc @ n(p_))), b, exchanges
 
 
-def _worker(rank, world, port, name, out):
+def _worker(rank, world, port, name, fused, out):
     torch.set_num_threads(1)  # several ranks share the host's cores
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
@@ -190,8 +192,9 @@ def _worker(rank, world, port, name, out):
             return stencil(halo.extend(p))
 
         n_global = int(np.prod(prob["mesh"]))
+        stats = {}
         x, its, hist, reason = shard.pcg(torch.from_numpy(b), matvec, cycle.apply, n_global,
-                                         rtol=o.rtol, null_space=o.constant_null_space)
+                                         rtol=o.rtol, null_space=o.constant_null_space, fused=fused, stats=stats)
         xg = torch.zeros(n_global, dtype=torch.float64)
         lo, hi = slab.first_cell, slab.first_cell + slab.ncell
         xg[lo:hi] = x
@@ -199,37 +202,47 @@ def _worker(rank, world, port, name, out):
         if rank == 0:
             np.save(out, xg.numpy())
             with open(out + ".txt", "w") as f:
-                f.write(f"{its} {reason} {halo.exchanges} {cycle.sums} {setup_exchanges}\n")
+                f.write(f"{its} {reason} {halo.exchanges} {cycle.sums} {setup_exchanges} {stats['allreduces']} "
+                        f"{stats['pc_applications']}\n")
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
-def test_sharded_solve_matches_single_process(name, tmp_path, monkeypatch):
+@pytest.mark.parametrize("name,fused", [(n, False) for n in sorted(CASES)]
+                         + [("grf16_w2", True), ("neumann_null_space_w2", True), ("two_level_w2", True)])
+def test_sharded_solve_matches_single_process(name, fused, tmp_path, monkeypatch):
     world, make, opts = CASES[name]
     out = str(tmp_path / "x.npy")
     # one BLAS / OpenMP thread per rank (read when the spawned ranks import numpy)
     for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         monkeypatch.setenv(v, "1")
-    mp.spawn(_worker, args=(world, _free_port(), name, out), nprocs=world, join=True)
+    mp.spawn(_worker, args=(world, _free_port(), name, fused, out), nprocs=world, join=True)
     x = np.load(out)
-    its, reason, exchanges, sums, setup_exchanges = open(out + ".txt").read().split()
+    its, reason, exchanges, sums, setup_exchanges, allreduces, napply = (
+        int(v) if v.isdigit() else v for v in open(out + ".txt").read().split())
     prob = make()
     ref = O.solve(prob, O.Options(**opts))
     assert reason == ref["reason"] == "converged_rtol"
-    assert abs(int(its) - ref["its"]) <= 1, (its, ref["its"])
+    assert abs(its - ref["its"]) <= 1, (its, ref["its"])
     a, b = ref["x"], x
     if not prob["dirichlet"]:
         a, b = a - a.mean(), b - b.mean()
     assert np.linalg.norm(b - a) <= 1e-10 * np.linalg.norm(a)
+    # preconditioner applications: PETSc's order one per iteration (the first
+    # before the loop, none after the converging residual); the fused form one more
+    assert napply == its + (1 if fused else 0)
+    # scalar all-reduces: p.w per iteration, then PETSc's order ||r||^2 and z.r
+    # separately (and sum z with the null space), the fused form all in one
+    null = 1 if opts.get("constant_null_space") else 0
+    assert allreduces == (2 * its + 1 if fused else 3 * its + 1 + null * its), allreduces
     # one halo exchange per A p of the CG step and per residual of the cycle
-    # after its first visit: its preconditioner applications and its A p
+    # after its first visit
     sched = ref["pc"].schedule()
-    assert int(exchanges) == int(its) * len(sched)
+    assert exchanges == its + napply * (len(sched) - 1)
     # one coarse right-hand side summed per level-3 (or 2-level) visit of each application
-    assert int(sums) == int(its) * sum(1 for lvl in sched if lvl in (3, "2g"))
+    assert sums == napply * sum(1 for lvl in sched if lvl in (3, "2g"))
     # the set-up exchanged the basis on the boundary planes once (Psi, or Phi for the 2-level branch)
-    assert int(setup_exchanges) == 1
+    assert setup_exchanges == 1
 
 
 def test_slab_plan():
