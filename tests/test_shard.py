@@ -13,9 +13,9 @@ solve's exchanges are the module's too: halo planes before every stencil
 product, the level-3 right-hand side (and the 2-level coarse right-hand side)
 summed over the processes, and the CG dots (in PETSc's order, and fused: p.w,
 then ||r||^2 and z.r in one sum; the counts of each are checked).  The
-assembled solution and the
-iteration count must match the single-process oracle (sums and products are
-only reordered: iterations +-1, solution 1e-10).
+assembled solution and the iteration count must match the single-process
+oracle (sums and products are only reordered: iterations +-1, solution
+1e-10).
 """
 import socket
 
