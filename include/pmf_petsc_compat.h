@@ -96,6 +96,20 @@ PetscErrorCode PetscError_pmf(int line, const char* func, const char* file, Pets
   } while (0)
 #define PetscMax(a, b) (((a) < (b)) ? (b) : (a))
 #define PetscMin(a, b) (((a) < (b)) ? (a) : (b))
+/* PETSc's integer power of an integer (petscmath.h), used by src/Expe_scal.c:28
+   and src/Expe_frac.c:26 for the permeability 10^cr: the base converts to
+   PetscInt, the result is exact while it fits in PetscInt.  A negative power
+   gives 0 (the integer part of 1 / base^|power| for |base| > 1). */
+static inline PetscInt PetscPowInt(PetscInt base, PetscInt power) {
+  PetscInt result = 1;
+  if (power < 0) return (base == 1 || base == -1) ? ((-power) % 2 ? base : 1) : 0;
+  while (power) {
+    if (power & 1) result *= base;
+    power >>= 1;
+    if (power) base *= base;
+  }
+  return result;
+}
 
 /* ---- initialisation, options, output, timing ---------------------------------------------- */
 PetscErrorCode PetscInitialize(int* argc, char*** argv, const char* file, const char* help);
