@@ -253,3 +253,10 @@ def test_slab_plan():
     assert slabs[0].ext_cells == (0, 10 * 120) and slabs[1].ext_cells == (8 * 120, 17 * 120)
     with pytest.raises(ValueError):
         shard.plan_slabs((12, 10, 17), (2, 1, 3), 2)
+
+
+def test_exchange_planes_takes_cell_by_column_tensors():
+    # the shape check comes before any communication
+    slab = shard.plan_slabs((4, 4, 8), (1, 1, 2), 2)[0]
+    with pytest.raises(ValueError):
+        shard.exchange_planes(slab, torch.zeros(16), torch.zeros(16))
